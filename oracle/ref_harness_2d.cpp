@@ -1,0 +1,512 @@
+// TEST INFRASTRUCTURE ONLY -- never linked into the product.
+//
+// C-ABI harness over the reference's own 2D AWCM Euler code (doseongju/C_pp-library),
+// compiled in place from the reference tree by oracle/Makefile (no reference source is
+// copied here).  The reference's step loop is main() of Wavelet/main_2d_euler(quad).cpp:56-350
+// (and the double-Mach variant Wavelet/main_2d_euler(dmach).cpp, which differs only in the
+// problem and in passing t to the boundary manager); ref2d_step() restates one pass of it as a
+// function with the same calls, order and arithmetic, OpenMP included.
+#include "OMP_MANAGER.h"
+#include "Problems/2D/PROBLEM_QUADRANTS.h"
+#include "Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h"
+#include "AWCM_2D.h"
+#include "WENO.h"
+#include "WENOZ.h"
+#include "EULER_EQUATION.h"
+
+#include <cstdint>
+#include <omp.h>
+#include <vector>
+
+namespace {
+
+enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2 };
+
+// One boundary manager per field, of the kind the problem uses.
+struct BC2D {
+    int kind;
+    BOUNDARY_MANAGER_QUAD* quad = nullptr;
+    BOUNDARY_MANAGER_DMACH* dmach = nullptr;
+    BOUNDARY_MANAGER_ISENVORTEX* periodic = nullptr;
+    BC2D(int k, FIELD_UNIFORM_2D<VECTOR_4D<double>>& Q) : kind(k)
+    {
+        if (k == BC_DMACH) dmach = new BOUNDARY_MANAGER_DMACH(Q);
+        else if (k == BC_PERIODIC) periodic = new BOUNDARY_MANAGER_ISENVORTEX(Q);
+        else quad = new BOUNDARY_MANAGER_QUAD(Q);
+    }
+    ~BC2D()
+    {
+        delete quad;
+        delete dmach;
+        delete periodic;
+    }
+    void apply(double t)
+    {
+        if (dmach) dmach->SetBoundaryCondition(t);
+        else if (periodic) periodic->SetBoundaryCondition();
+        else quad->SetBoundaryCondition();
+    }
+};
+
+struct Ref2D {
+    MRA_GRID_INT_2D mra;
+    AWCM_2D* awcm = nullptr;
+    GRID_UNIFORM_2D grid;
+    FIELD_UNIFORM_2D<VECTOR_4D<double>> Q, Q_0, Q_1, Q_2;
+    BC2D *bc = nullptr, *bc0 = nullptr, *bc1 = nullptr, *bc2 = nullptr;
+    double gamma = 1.4;
+    int nx = 0, ny = 0;
+    int bc_kind = BC_QUAD;
+    // When set, ref2d_step skips PrepareEuler and reuses the stored masks/levels, and the
+    // three LF speeds are taken from frozen_alpha instead of being recomputed.
+    int freeze_mask = 0;
+};
+
+FIELD_UNIFORM_2D<bool>& mask_ref(Ref2D* s, int id)
+{
+    switch (id) {
+        case 0: return s->awcm->mask0;
+        case 1: return s->awcm->mask1;
+        case 2: return s->awcm->mask2;
+        case 3: return s->awcm->mask3;
+        default: return s->awcm->mask_temp;
+    }
+}
+
+FIELD_UNIFORM_2D<int>& level_ref(Ref2D* s, int id)
+{
+    switch (id) {
+        case 0: return s->awcm->level0;
+        case 1: return s->awcm->level1;
+        case 2: return s->awcm->level2;
+        default: return s->awcm->level3;
+    }
+}
+
+// Per-row and per-column LF speeds over a mask (main_2d_euler(quad).cpp:86-104).
+void alpha2d(Ref2D* s, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qs, const FIELD_UNIFORM_2D<bool>& mask,
+             std::vector<double>& alpha_x, std::vector<double>& alpha_y)
+{
+    EULER_EQUATION_2D euler_eqn(s->gamma);
+    const GRID_UNIFORM_2D& grid = s->grid;
+    for (auto& a : alpha_x) a = 0;
+    for (auto& a : alpha_y) a = 0;
+#pragma omp parallel
+    {
+#pragma omp for
+        ITERATION_GRID_2D(grid, 0)
+        {
+            if (mask(i, j) == 0) continue;
+            alpha_x[j] = MAX(alpha_x[j], euler_eqn.Spectral_RadiusX(Qs(i, j)));
+        }
+#pragma omp for
+        ITERATION_GRID_2D_IJ(grid, 0)
+        {
+            if (mask(i, j) == 0) continue;
+            alpha_y[i] = MAX(alpha_y[i], euler_eqn.Spectral_RadiusY(Qs(i, j)));
+        }
+    }
+}
+
+// One RK3 stage body (main_2d_euler(quad).cpp:108-163, :188-243, :267-322).
+// out = Qin - dt/dx (dF + dG)                      (kind 1, 3)
+// out = 0.75 Qn + 0.25 (Qin - dt/dx (dF + dG))     (kind 2)
+void stage2d(Ref2D* s, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qin, FIELD_UNIFORM_2D<VECTOR_4D<double>>& out,
+             const FIELD_UNIFORM_2D<bool>& mask, const FIELD_UNIFORM_2D<int>& level,
+             const std::vector<double>& alpha_x, const std::vector<double>& alpha_y, double dt, int kind)
+{
+    const int max_lev = s->mra.num_levels - 1;
+    const GRID_UNIFORM_2D& grid = s->grid;
+    const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qn = s->Q;
+    AWCM_2D& awcm = *s->awcm;
+    EULER_EQUATION_2D euler_eqn(s->gamma);
+#pragma omp parallel
+    {
+        WENOZ_EULER_SOLVER_2D wenoz_solver;
+#pragma omp for
+        ITERATION_GRID_2D(grid, 0)
+        {
+            VECTOR_4D<double> dF, dG;
+            VECTOR_4D<double> F_ll, F_l, F_c, F_r, F_rr;
+            VECTOR_4D<double> G_bb, G_b, G_c, G_t, G_tt;
+            if (mask(i, j) == false) continue;
+            const int lev = level(i, j);
+            const int d = s->mra.grid[lev].dx;
+            const double dx = grid.dx * d;
+            if (lev == max_lev) {
+                VECTOR_4D<double> a, b;
+                wenoz_solver.ComputeFluxX(Qin(i - 3, j), Qin(i - 2, j), Qin(i - 1, j), Qin(i, j), Qin(i + 1, j),
+                                          Qin(i + 2, j), alpha_x[j], a);
+                wenoz_solver.ComputeFluxX(Qin(i - 2, j), Qin(i - 1, j), Qin(i, j), Qin(i + 1, j), Qin(i + 2, j),
+                                          Qin(i + 3, j), alpha_x[j], b);
+                dF = b - a;
+                wenoz_solver.ComputeFluxY(Qin(i, j - 3), Qin(i, j - 2), Qin(i, j - 1), Qin(i, j), Qin(i, j + 1),
+                                          Qin(i, j + 2), alpha_y[i], a);
+                wenoz_solver.ComputeFluxY(Qin(i, j - 2), Qin(i, j - 1), Qin(i, j), Qin(i, j + 1), Qin(i, j + 2),
+                                          Qin(i, j + 3), alpha_y[i], b);
+                dG = b - a;
+            } else {
+                // The reference evaluates F (G) at all five points; the ones its branch does not use
+                // (i-2d when i <= d, i+2d when i >= i_end-d) can lie outside the field, so they are skipped.
+                if (i > d) euler_eqn.ComputeFu(Qin(i - 2 * d, j), F_ll);
+                euler_eqn.ComputeFu(Qin(i - d, j), F_l), euler_eqn.ComputeFu(Qin(i, j), F_c);
+                euler_eqn.ComputeFu(Qin(i + d, j), F_r);
+                if (i <= d || i < grid.i_end - d) euler_eqn.ComputeFu(Qin(i + 2 * d, j), F_rr);
+                if (i <= d)
+                    awcm.DifferentiateAtLeftBoundary(F_l, F_c, F_r, F_rr, dF);
+                else if (i >= grid.i_end - d)
+                    awcm.DifferentiateAtRightBoundary(F_ll, F_l, F_c, F_r, dF);
+                else
+                    awcm.Differentiate(F_ll, F_l, F_c, F_r, F_rr, dF);
+
+                if (j > d) euler_eqn.ComputeGu(Qin(i, j - 2 * d), G_bb);
+                euler_eqn.ComputeGu(Qin(i, j - d), G_b), euler_eqn.ComputeGu(Qin(i, j), G_c);
+                euler_eqn.ComputeGu(Qin(i, j + d), G_t);
+                if (j <= d || j < grid.j_end - d) euler_eqn.ComputeGu(Qin(i, j + 2 * d), G_tt);
+                if (j <= d)
+                    awcm.DifferentiateAtLeftBoundary(G_b, G_c, G_t, G_tt, dG);
+                else if (j >= grid.j_end - d)
+                    awcm.DifferentiateAtRightBoundary(G_bb, G_b, G_c, G_t, dG);
+                else
+                    awcm.Differentiate(G_bb, G_b, G_c, G_t, G_tt, dG);
+            }
+            if (kind == 2)
+                out(i, j) = 0.75 * Qn(i, j) + 0.25 * (Qin(i, j) - dt / dx * (dF + dG));
+            else
+                out(i, j) = Qin(i, j) - dt / dx * (dF + dG);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// bc_kind: 0 transmissive (BOUNDARY_MANAGER_QUAD), 1 double Mach (BOUNDARY_MANAGER_DMACH),
+// 2 periodic (BOUNDARY_MANAGER_ISENVORTEX).
+void* ref2d_create(int num_levels, int nx_coarse, int ny_coarse, double x_min, double x_max, double y_min,
+                   double y_max, int bc_kind)
+{
+    Ref2D* s = new Ref2D();
+    s->mra.Initialize(num_levels, nx_coarse, ny_coarse);
+    s->awcm = new AWCM_2D(s->mra);
+    s->nx = s->mra.Nx;
+    s->ny = s->mra.Ny;
+    s->bc_kind = bc_kind;
+    s->grid.Initialize(0, 0, s->nx, s->ny, x_min, y_min, x_max, y_max);
+    s->Q.Initialize(s->grid, 3);
+    s->Q_0.Initialize(s->grid, 3);
+    s->Q_1.Initialize(s->grid, 3);
+    s->Q_2.Initialize(s->grid, 3);
+    s->bc = new BC2D(bc_kind, s->Q);
+    s->bc0 = new BC2D(bc_kind, s->Q_0);
+    s->bc1 = new BC2D(bc_kind, s->Q_1);
+    s->bc2 = new BC2D(bc_kind, s->Q_2);
+    return s;
+}
+
+void ref2d_destroy(void* h)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    delete s->bc;
+    delete s->bc0;
+    delete s->bc1;
+    delete s->bc2;
+    delete s->awcm;
+    delete s;
+}
+
+void ref2d_dims(void* h, int* nx, int* ny)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    *nx = s->nx;
+    *ny = s->ny;
+}
+
+// q: (Ny+6) rows of (Nx+6) points x 4 doubles, point (i,j) at ((j+3)*(Nx+6) + i+3)*4.
+void ref2d_set_q(void* h, const double* q)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const int w = s->nx + 6;
+    for (int j = -3; j < s->ny + 3; ++j)
+        for (int i = -3; i < s->nx + 3; ++i)
+            for (int p = 0; p < 4; ++p) s->Q(i, j)[p] = q[((size_t)(j + 3) * w + (i + 3)) * 4 + p];
+}
+
+void ref2d_get_q(void* h, double* q)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const int w = s->nx + 6;
+    for (int j = -3; j < s->ny + 3; ++j)
+        for (int i = -3; i < s->nx + 3; ++i)
+            for (int p = 0; p < 4; ++p) q[((size_t)(j + 3) * w + (i + 3)) * 4 + p] = s->Q(i, j)[p];
+}
+
+// Initial states built by the reference's problem classes, with the geometry of the harness grid.
+// kind 0: four-quadrant Riemann problem, QUADRANTS::Initialize states (PROBLEM_QUADRANTS.h:42-78)
+//         with the split at (a, b);
+// kind 1: double Mach reflection, DOUBLEMACH::Initialize (PROBLEM_DOUBLEMACH.h:34-62) with the
+//         pre-shock density a;
+// kind 2: isentropic vortex, ISENTROPIC_VORTEX_ADVECTION::Initialize (:38-64) centred at (a, b).
+void ref2d_init_problem(void* h, int kind, double a, double b)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const double gamma = s->gamma;
+    IDEAL_GAS_2D EOS(gamma);
+    const GRID_UNIFORM_2D& grid = s->grid;
+    FIELD_UNIFORM_2D<VECTOR_4D<double>>& Q = s->Q;
+    ITERATION_GRID_2D(grid, 3)
+    {
+        const double x = grid(i, j).x;
+        const double y = grid(i, j).y;
+        double rho, u, v, p;
+        if (kind == 0) {
+            if (x >= a && y >= b) { rho = 1.5; u = 0; v = 0; p = 1.5; }
+            else if (x < a && y >= b) { rho = 0.532258064516129; u = 1.206045378311055; v = 0; p = 0.3; }
+            else if (x < a && y < b) {
+                rho = 0.137992831541219; u = 1.206045378311055; v = 1.206045378311055; p = 0.029032258064516;
+            } else { rho = 0.532258064516129; u = 0; v = 1.206045378311055; p = 0.3; }
+            Q(i, j)[0] = rho;
+            Q(i, j)[1] = rho * u;
+            Q(i, j)[2] = rho * v;
+            Q(i, j)[3] = EOS.E(rho, u, v, p);
+        } else if (kind == 1) {
+            if (y > sqrt(3.0) * (x - 1.0 / 6.0)) { rho = 8; u = 8.25 * sqrt(3.0) * 0.5; v = -8.25 * 0.5; p = 116.5; }
+            else { rho = a; u = 0; v = 0; p = 1; }
+            Q(i, j)[0] = rho;
+            Q(i, j)[1] = rho * u;
+            Q(i, j)[2] = rho * v;
+            Q(i, j)[3] = EOS.E(rho, u, v, p);
+        } else {
+            const double rr = SQR(x - a) + SQR(y - b);
+            const double beta = 5;
+            double rhou, rhov;
+            rho = 1 - (gamma - 1) * SQR(beta) / (8 * gamma * PI * PI) * exp(1 - rr);
+            rho = pow(rho, 1.0 / (gamma - 1.0));
+            rhou = 0 - beta / (2 * PI) * exp((1 - rr) * 0.5) * (y - b);
+            rhou *= rho;
+            rhov = 1 + beta / (2 * PI) * exp((1 - rr) * 0.5) * (x - a);
+            rhov *= rho;
+            p = pow(rho, gamma);
+            Q(i, j)[0] = rho;
+            Q(i, j)[1] = rhou;
+            Q(i, j)[2] = rhov;
+            Q(i, j)[3] = EOS.E(rho, rhou / rho, rhov / rho, p);
+        }
+    }
+}
+
+// masks: 5 planes of (Ny+6) x (Nx+6) bytes: mask_temp, mask0..mask3 (ghosts included).
+void ref2d_get_masks(void* h, uint8_t* m)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const int w = s->nx + 6;
+    const size_t plane = (size_t)w * (s->ny + 6);
+    const int ids[5] = {4, 0, 1, 2, 3};
+    for (int r = 0; r < 5; ++r) {
+        FIELD_UNIFORM_2D<bool>& mk = mask_ref(s, ids[r]);
+        for (int j = -3; j < s->ny + 3; ++j)
+            for (int i = -3; i < s->nx + 3; ++i) m[r * plane + (size_t)(j + 3) * w + i + 3] = mk(i, j) ? 1 : 0;
+    }
+}
+
+void ref2d_set_masks(void* h, const uint8_t* m)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const int w = s->nx + 6;
+    const size_t plane = (size_t)w * (s->ny + 6);
+    const int ids[5] = {4, 0, 1, 2, 3};
+    for (int r = 0; r < 5; ++r) {
+        FIELD_UNIFORM_2D<bool>& mk = mask_ref(s, ids[r]);
+        for (int j = -3; j < s->ny + 3; ++j)
+            for (int i = -3; i < s->nx + 3; ++i) mk(i, j) = m[r * plane + (size_t)(j + 3) * w + i + 3] != 0;
+    }
+}
+
+// levels: 4 planes of Ny x Nx ints.
+void ref2d_get_levels(void* h, int* lv)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const size_t plane = (size_t)s->nx * s->ny;
+    for (int r = 0; r < 4; ++r) {
+        FIELD_UNIFORM_2D<int>& l = level_ref(s, r);
+        for (int j = 0; j < s->ny; ++j)
+            for (int i = 0; i < s->nx; ++i) lv[r * plane + (size_t)j * s->nx + i] = l(i, j);
+    }
+}
+
+void ref2d_set_levels(void* h, const int* lv)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const size_t plane = (size_t)s->nx * s->ny;
+    for (int r = 0; r < 4; ++r) {
+        FIELD_UNIFORM_2D<int>& l = level_ref(s, r);
+        for (int j = 0; j < s->ny; ++j)
+            for (int i = 0; i < s->nx; ++i) l(i, j) = lv[r * plane + (size_t)j * s->nx + i];
+    }
+}
+
+// AWCM_2D::PrepareEuler (Wavelet/AWCM_2D.h:114-147).
+void ref2d_prepare(void* h, double tol)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    s->awcm->PrepareEuler(s->Q, tol);
+}
+
+void ref2d_fwt(void* h, double tol)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    s->awcm->wavelet.ForwardWaveletTransformationEuler(s->Q, s->mra, s->awcm->mask0, tol);
+}
+
+void ref2d_iwt(void* h, int mask_id)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    s->awcm->wavelet.InverseWaveletTransformationEuler(s->Q, s->mra, mask_ref(s, mask_id));
+}
+
+void ref2d_interpolate(void* h, int from_id, int to_id)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    s->awcm->wavelet.InterpolateEuler(s->Q, s->mra, mask_ref(s, from_id), mask_ref(s, to_id));
+}
+
+// AWCM_MANAGER_2D passes on one of the facade's masks.
+// op 0 AddAdjacentZone, 1 CheckReconstruction, 2 AddPointForDifferentiation(level_id),
+// 3 ComputeLevel(level_id <- mask), 4 RemoveResidueEuler(Q, mask), 5 BandingMask.
+void ref2d_manager(void* h, int op, int mask_id, int level_id)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    FIELD_UNIFORM_2D<bool>& m = mask_ref(s, mask_id);
+    switch (op) {
+        case 0: AWCM_MANAGER_2D::AddAdjacentZone(m, s->mra); break;
+        case 1: AWCM_MANAGER_2D::CheckReconstruction(m, s->mra); break;
+        case 2: AWCM_MANAGER_2D::AddPointForDifferentiation(m, s->mra, level_ref(s, level_id)); break;
+        case 3: AWCM_MANAGER_2D::ComputeLevel(level_ref(s, level_id), m, s->mra); break;
+        case 4: AWCM_MANAGER_2D::RemoveResidueEuler(s->Q, m, s->mra); break;
+        case 5: {
+            BOUNDARY_MANAGER_SHOCK_VORTEX bm(s->Q);
+            bm.BandingMask(m);
+            break;
+        }
+        default: break;
+    }
+}
+
+void ref2d_apply_bc(void* h, double t)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    s->bc->apply(t);
+}
+
+// One pass of the driver loop (main_2d_euler(quad).cpp:58-334), output time t_next standing in
+// for arr_printing_times[cnt].  alpha_io: if freeze_mask is set, the six LF-speed arrays
+// (stage 1..3: alpha_x[Ny], alpha_y[Nx]) are read from it; otherwise, when non-null, the
+// computed ones are written to it.
+// out[0] = dt, out[1] = do_print, out[2..5] = |mask0..mask3| (interior), out[6] = max_velocity.
+void ref2d_step(void* h, double tol, double cfl, double t, double t_next, double dt_fixed, double* alpha_io,
+                double* out)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    AWCM_2D& awcm = *s->awcm;
+    FIELD_UNIFORM_2D<VECTOR_4D<double>>& Q = s->Q;
+    EULER_EQUATION_2D euler_eqn(s->gamma);
+    const GRID_UNIFORM_2D& grid = s->grid;
+    const double dx = grid.dx;
+    const int nth = omp_get_max_threads();
+    OMP_MANAGER omp_manager(nth);
+
+    if (!s->freeze_mask) awcm.PrepareEuler(Q, tol);
+
+    double max_velocity = 0;
+#pragma omp parallel
+    {
+        double max_velocity = 0;
+#pragma omp for
+        ITERATION_GRID_2D(grid, 0)
+        {
+            if (awcm.mask3(i, j) == false) continue;
+            max_velocity = MAX(max_velocity, euler_eqn.Spectral_RadiusX(Q(i, j)) + euler_eqn.Spectral_RadiusY(Q(i, j)));
+        }
+        omp_manager.Input(max_velocity);
+    }
+    max_velocity = omp_manager.Max_double();
+    double dt = cfl * dx / max_velocity;
+    if (dt_fixed > 0) dt = dt_fixed;
+    int do_print = 0;
+    if (t + dt > t_next) {
+        dt = t_next - t;
+        do_print = 1;
+    }
+
+    std::vector<double> ax(s->ny), ay(s->nx);
+    const int frozen = s->freeze_mask && alpha_io;
+    auto load_alpha = [&](int stage, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qs, const FIELD_UNIFORM_2D<bool>& m) {
+        double* base = alpha_io ? alpha_io + (size_t)stage * (s->nx + s->ny) : nullptr;
+        if (frozen) {
+            for (int j = 0; j < s->ny; ++j) ax[j] = base[j];
+            for (int i = 0; i < s->nx; ++i) ay[i] = base[s->ny + i];
+        } else {
+            alpha2d(s, Qs, m, ax, ay);
+            if (base) {
+                for (int j = 0; j < s->ny; ++j) base[j] = ax[j];
+                for (int i = 0; i < s->nx; ++i) base[s->ny + i] = ay[i];
+            }
+        }
+    };
+
+    s->bc->apply(t);
+    load_alpha(0, Q, awcm.mask3);
+    stage2d(s, Q, s->Q_2, awcm.mask2, awcm.level2, ax, ay, dt, 1);
+
+    s->bc2->apply(t);
+    load_alpha(1, s->Q_2, awcm.mask2);
+    stage2d(s, s->Q_2, s->Q_1, awcm.mask1, awcm.level1, ax, ay, dt, 2);
+
+    s->bc1->apply(t);
+    load_alpha(2, s->Q_1, awcm.mask1);
+    stage2d(s, s->Q_1, s->Q_0, awcm.mask0, awcm.level0, ax, ay, dt, 3);
+
+#pragma omp parallel for
+    ITERATION_GRID_2D(grid, 0)
+    {
+        if (awcm.mask0(i, j) == true) Q(i, j) = (Q(i, j) + 2.0 * s->Q_0(i, j)) / 3.0;
+    }
+    awcm.PostProcessEuler(Q);
+
+    long cnt[4] = {0, 0, 0, 0};
+    for (int j = 0; j < s->ny; ++j)
+        for (int i = 0; i < s->nx; ++i) {
+            cnt[0] += awcm.mask0(i, j);
+            cnt[1] += awcm.mask1(i, j);
+            cnt[2] += awcm.mask2(i, j);
+            cnt[3] += awcm.mask3(i, j);
+        }
+    out[0] = dt;
+    out[1] = do_print;
+    for (int k = 0; k < 4; ++k) out[2 + k] = (double)cnt[k];
+    out[6] = max_velocity;
+}
+
+void ref2d_set_freeze(void* h, int freeze) { static_cast<Ref2D*>(h)->freeze_mask = freeze; }
+
+// Steps until t >= t_end or max_steps; returns the step count, out[0] = t, out[1] = sum |mask0|.
+int ref2d_run(void* h, double tol, double cfl, double t_end, int max_steps, double* out)
+{
+    double t = 0, upd = 0, o[8];
+    int n = 0;
+    while (n < max_steps) {
+        ref2d_step(h, tol, cfl, t, t_end, 0.0, nullptr, o);
+        t += o[0];
+        upd += o[2];
+        ++n;
+        if (t >= t_end) break;
+    }
+    out[0] = t;
+    out[1] = upd;
+    return n;
+}
+
+int ref2d_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"
