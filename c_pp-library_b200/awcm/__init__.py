@@ -1,0 +1,14 @@
+"""awcm -- B200-native AWCM compressible-Euler path (host side).
+
+The compute runs in libawcm_b200.so (hand-written CUDA for sm_100a behind the C-ABI of
+include/awcm_b200.h); this package binds it with ctypes and mirrors the reference's call surface.
+"""
+from ._lib import AwcmError, LIB_PATH, exported_symbols, load
+from .solvers import (AAZ, APD, BAND, BC_DOUBLE_MACH, BC_PERIODIC, BC_TRANSMISSIVE, CL, CR, PROBLEM_DOUBLE_MACH,
+                      PROBLEM_QUADRANTS, PROBLEM_VORTEX, RR, WENO5, WENOZ, AWCM1D, AWCM1DBatch, AWCM2D)
+
+__all__ = [
+    "AwcmError", "LIB_PATH", "exported_symbols", "load", "AWCM1D", "AWCM1DBatch", "AWCM2D",
+    "AAZ", "CR", "APD", "CL", "RR", "BAND", "BC_TRANSMISSIVE", "BC_DOUBLE_MACH", "BC_PERIODIC",
+    "PROBLEM_QUADRANTS", "PROBLEM_DOUBLE_MACH", "PROBLEM_VORTEX", "WENOZ", "WENO5",
+]

@@ -1,0 +1,300 @@
+"""Host-side solver objects over the C-ABI.
+
+``AWCM2D`` is one 2D instance (AWCM_2D + its field, stage copies and boundary manager);
+``AWCM1DBatch`` is a batch of independent 1D instances advanced by one persistent launch per RK3
+step; ``AWCM1D`` is a batch of one.  Method names and argument meanings follow the checker in
+``oracle/`` so the parity tests read the same against both.
+
+Host layouts (reference layout, ghost ring of 3):
+  1D state (Nx+6, 3) float64; 2D state (Ny+6, Nx+6, 4) float64;
+  masks (5, ...) uint8 planes mask_temp, mask0..mask3; levels (4, ...) int32 planes.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import P_double, P_int, P_u8, c_void_p, call, ptr
+
+AAZ, CR, APD, CL, RR, BAND = 0, 1, 2, 3, 4, 5
+BC_TRANSMISSIVE, BC_DOUBLE_MACH, BC_PERIODIC = 0, 1, 2
+PROBLEM_QUADRANTS, PROBLEM_DOUBLE_MACH, PROBLEM_VORTEX = 0, 1, 2
+WENOZ, WENO5 = 0, 1
+
+
+class AWCM2D:
+    """One 2D AWCM compressible-Euler instance resident on the GPU."""
+
+    def __init__(self, num_levels: int, nx_coarse: int, ny_coarse: int, x_min: float, x_max: float,
+                 y_min: float, y_max: float, bc_kind: int = BC_TRANSMISSIVE):
+        h = c_void_p()
+        call("awcm2d_create", num_levels, nx_coarse, ny_coarse, x_min, x_max, y_min, y_max, bc_kind,
+             ctypes.byref(h))
+        self.h = h
+        nx, ny = ctypes.c_int(), ctypes.c_int()
+        call("awcm2d_dims", self.h, ctypes.byref(nx), ctypes.byref(ny))
+        self.nx, self.ny = nx.value, ny.value
+        self.num_levels = num_levels
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            call("awcm2d_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # state ------------------------------------------------------------------------------------
+    def set_q(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.ny + 6, self.nx + 6, 4)
+        call("awcm2d_set_q", self.h, ptr(q, ctypes.c_double))
+
+    def get_q(self):
+        q = np.empty((self.ny + 6, self.nx + 6, 4), np.float64)
+        call("awcm2d_get_q", self.h, ptr(q, ctypes.c_double))
+        return q
+
+    def get_masks(self):
+        m = np.empty((5, self.ny + 6, self.nx + 6), np.uint8)
+        call("awcm2d_get_masks", self.h, ptr(m, ctypes.c_uint8))
+        return m
+
+    def set_masks(self, m):
+        m = np.ascontiguousarray(m, dtype=np.uint8).reshape(5, self.ny + 6, self.nx + 6)
+        call("awcm2d_set_masks", self.h, ptr(m, ctypes.c_uint8))
+
+    def get_levels(self):
+        lv = np.empty((4, self.ny, self.nx), np.int32)
+        call("awcm2d_get_levels", self.h, ptr(lv, ctypes.c_int))
+        return lv
+
+    def set_levels(self, lv):
+        lv = np.ascontiguousarray(lv, dtype=np.int32).reshape(4, self.ny, self.nx)
+        call("awcm2d_set_levels", self.h, ptr(lv, ctypes.c_int))
+
+    def init_problem(self, kind, a, b):
+        call("awcm2d_init_problem", self.h, kind, a, b)
+
+    # passes -----------------------------------------------------------------------------------
+    def prepare(self, tol):
+        call("awcm2d_prepare", self.h, tol)
+
+    def fwt(self, tol):
+        call("awcm2d_fwt", self.h, tol)
+
+    def iwt(self, mask_id=3):
+        call("awcm2d_iwt", self.h, mask_id)
+
+    def interpolate(self, from_id=4, to_id=3):
+        call("awcm2d_interpolate", self.h, from_id, to_id)
+
+    def manager(self, op, mask_id, level_id=0):
+        call("awcm2d_manager", self.h, op, mask_id, level_id)
+
+    def apply_bc(self, t=0.0):
+        call("awcm2d_apply_bc", self.h, t)
+
+    # stepping ---------------------------------------------------------------------------------
+    def step(self, tol, cfl, t, t_next, dt_fixed=0.0):
+        out = np.zeros(8)
+        call("awcm2d_step", self.h, tol, cfl, t, t_next, dt_fixed, ptr(out, ctypes.c_double))
+        return out
+
+    def advance(self, tol, cfl, t_start, t_end, n_steps):
+        """n_steps graph replays without host round trips; returns (t, steps, sum|mask0|, stage points)."""
+        out = np.zeros(4)
+        call("awcm2d_advance", self.h, tol, cfl, t_start, t_end, n_steps, ptr(out, ctypes.c_double))
+        return out[0], int(out[1]), out[2], out[3]
+
+    def run(self, tol, cfl, t_end, max_steps=1 << 30, chunk=64):
+        t, steps, upd = 0.0, 0, 0.0
+        while steps < max_steps and t < t_end:
+            n = min(chunk, max_steps - steps)
+            t, k, u, _ = self.advance(tol, cfl, t, t_end, n)
+            steps += k
+            upd += u
+            if k < n:
+                break
+        return steps, t, upd
+
+    def launches_per_step(self):
+        n = ctypes.c_int()
+        call("awcm2d_launches_per_step", self.h, ctypes.byref(n))
+        return n.value
+
+    @property
+    def stream(self) -> int:
+        s = c_void_p()
+        call("awcm2d_stream", self.h, ctypes.byref(s))
+        return s.value or 0
+
+
+class AWCM1DBatch:
+    """Independent 1D AWCM instances advanced together (one persistent launch per RK3 step)."""
+
+    def __init__(self, num_levels, nx_coarse, x_min, x_max, gamma: float = 1.4, scheme: int = WENOZ):
+        num_levels = np.ascontiguousarray(num_levels, dtype=np.int32)
+        n = len(num_levels)
+        nxc = np.ascontiguousarray(np.broadcast_to(nx_coarse, (n,)), dtype=np.int32)
+        xmin = np.ascontiguousarray(np.broadcast_to(x_min, (n,)), dtype=np.float64)
+        xmax = np.ascontiguousarray(np.broadcast_to(x_max, (n,)), dtype=np.float64)
+        h = c_void_p()
+        call("awcm1d_batch_create", n, ptr(num_levels, ctypes.c_int), ptr(nxc, ctypes.c_int),
+             ptr(xmin, ctypes.c_double), ptr(xmax, ctypes.c_double), gamma, scheme, ctypes.byref(h))
+        self.h = h
+        self.n = n
+        self.nx = []
+        for k in range(n):
+            v = ctypes.c_int()
+            call("awcm1d_batch_nx", self.h, k, ctypes.byref(v))
+            self.nx.append(v.value)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            call("awcm1d_batch_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_q(self, k, q):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.nx[k] + 6, 3)
+        call("awcm1d_batch_set_q", self.h, k, ptr(q, ctypes.c_double))
+
+    def get_q(self, k):
+        q = np.empty((self.nx[k] + 6, 3), np.float64)
+        call("awcm1d_batch_get_q", self.h, k, ptr(q, ctypes.c_double))
+        return q
+
+    def get_masks(self, k):
+        m = np.empty((5, self.nx[k] + 6), np.uint8)
+        call("awcm1d_batch_get_masks", self.h, k, ptr(m, ctypes.c_uint8))
+        return m
+
+    def set_masks(self, k, m):
+        m = np.ascontiguousarray(m, dtype=np.uint8).reshape(5, self.nx[k] + 6)
+        call("awcm1d_batch_set_masks", self.h, k, ptr(m, ctypes.c_uint8))
+
+    def get_levels(self, k):
+        lv = np.empty((4, self.nx[k]), np.int32)
+        call("awcm1d_batch_get_levels", self.h, k, ptr(lv, ctypes.c_int))
+        return lv
+
+    def set_levels(self, k, lv):
+        lv = np.ascontiguousarray(lv, dtype=np.int32).reshape(4, self.nx[k])
+        call("awcm1d_batch_set_levels", self.h, k, ptr(lv, ctypes.c_int))
+
+    def init_riemann(self, k, x_interface, left, right):
+        l = np.ascontiguousarray(left, dtype=np.float64)
+        r = np.ascontiguousarray(right, dtype=np.float64)
+        call("awcm1d_batch_init_riemann", self.h, k, x_interface, ptr(l, ctypes.c_double), ptr(r, ctypes.c_double))
+
+    def set_run(self, tol, cfl, t, t_end, dt_fixed=0.0):
+        f = lambda v: np.ascontiguousarray(np.broadcast_to(v, (self.n,)), dtype=np.float64)
+        a, b, c, d = f(tol), f(cfl), f(t), f(t_end)
+        call("awcm1d_batch_set_run", self.h, ptr(a, ctypes.c_double), ptr(b, ctypes.c_double),
+             ptr(c, ctypes.c_double), ptr(d, ctypes.c_double), dt_fixed)
+
+    def steps(self, n_steps: int):
+        call("awcm1d_batch_steps", self.h, n_steps)
+
+    def sync(self):
+        call("awcm1d_batch_sync", self.h)
+
+    def status(self, k):
+        out = np.zeros(16)
+        call("awcm1d_batch_status", self.h, k, ptr(out, ctypes.c_double))
+        return out
+
+    def totals(self):
+        out = np.zeros(3)
+        call("awcm1d_batch_totals", self.h, ptr(out, ctypes.c_double))
+        return out
+
+    def pass_(self, k, op, mask_id, level_id=0):
+        call("awcm1d_batch_pass", self.h, k, op, mask_id, level_id)
+
+    def set_launch(self, threads: int, ctas_per_sm: int = 0):
+        call("awcm1d_batch_set_launch", self.h, threads, ctas_per_sm)
+
+    @property
+    def stream(self) -> int:
+        s = c_void_p()
+        call("awcm1d_batch_stream", self.h, ctypes.byref(s))
+        return s.value or 0
+
+
+class AWCM1D:
+    """A single 1D instance with the checker's call shape (a batch of one)."""
+
+    def __init__(self, num_levels: int, nx_coarse: int, x_min: float, x_max: float, gamma: float = 1.4,
+                 scheme: int = WENOZ):
+        self.b = AWCM1DBatch([num_levels], nx_coarse, x_min, x_max, gamma, scheme)
+        self.nx = self.b.nx[0]
+
+    def set_q(self, q):
+        self.b.set_q(0, q)
+
+    def get_q(self):
+        return self.b.get_q(0)
+
+    def get_masks(self):
+        return self.b.get_masks(0)
+
+    def set_masks(self, m):
+        self.b.set_masks(0, m)
+
+    def get_levels(self):
+        return self.b.get_levels(0)
+
+    def set_levels(self, lv):
+        self.b.set_levels(0, lv)
+
+    def init_riemann(self, x_interface, left, right):
+        self.b.init_riemann(0, x_interface, left, right)
+
+    def prepare(self, tol):
+        self.b.set_run(tol, 0.5, 0.0, 1.0)
+        self.b.pass_(0, 10, 0, 0)
+
+    def fwt(self, tol):
+        self.b.set_run(tol, 0.5, 0.0, 1.0)
+        self.b.pass_(0, 11, 0, 0)
+
+    def iwt(self, mask_id=3):
+        self.b.pass_(0, 12, mask_id, 0)
+
+    def manager(self, op, mask_id, level_id=0):
+        self.b.pass_(0, op, mask_id, level_id)
+
+    def step(self, tol, cfl, t, t_next):
+        """One driver-loop pass; returns the checker's out[10] (dt, do_print, |mask0..3|, alphas, speed)."""
+        self.b.set_run(tol, cfl, t, t_next)
+        self.b.steps(1)
+        s = self.b.status(0)
+        out = np.zeros(10)
+        out[0], out[1] = s[1], s[2]
+        out[2:6] = s[5:9]
+        out[6:9] = s[10:13]
+        out[9] = s[9]
+        return out
+
+    def run(self, tol, cfl, t_end, max_steps=1 << 30, chunk=256):
+        self.b.set_run(tol, cfl, 0.0, t_end)
+        steps = 0
+        while steps < max_steps:
+            n = min(chunk, max_steps - steps)
+            self.b.steps(n)
+            s = self.b.status(0)
+            steps = int(s[4])
+            if s[3]:
+                break
+        s = self.b.status(0)
+        return int(s[4]), s[0], s[13]

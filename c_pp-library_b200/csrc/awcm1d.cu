@@ -1,0 +1,1019 @@
+// 1D AWCM compressible-Euler path on one B200 (sm_100a), FP64: single instances and batches.
+//
+// A 1D instance is small (Nx = (nx_coarse-1) 2^(L-1) + 1 points, 1025 for the Sod case, up to
+// 8193 in the uneven batch), so one CTA advances one instance through a whole RK3 step --
+// PrepareEuler, CFL, three stages, residue removal -- separating the level-sequential phases with
+// block barriers instead of kernel launches.  A batch is one persistent launch: CTAs pull instance
+// ids from a queue (largest first), so hundreds of uneven instances share the GPU in one kernel;
+// a single instance is the same launch with one queue entry.  Each step is captured once into a
+// CUDA graph (queue reset + step kernel) and replayed.
+//
+// Per-instance layout in the pool (w = Nx + 6, ghost ring 3): doubles q[3][w] (conserved),
+// qc[3][w] (stage-start copy), qt[3][w] (stage input copy), fl[3][w] (face fluxes, face i+1/2 at
+// point i); bytes mask[w] (bits 0..3 mask0..3, 4 previous mask0, 5/6 work bits), level[4][w].
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "awcm_b200.h"
+#include "awcm_common.cuh"
+
+namespace awcm {
+namespace {
+
+struct Inst1 {
+    int nx, maxl, scheme, pad0;
+    double x_min, dx, gamma, tol, cfl, t, t_end, dt_fixed;
+    long long q_off;  // in doubles
+    long long m_off;  // in bytes
+    // results of the last step
+    double dt, mv, alpha[3];
+    int do_print, done, steps, err;
+    unsigned mask_cnt[4];
+    unsigned long long upd;
+};
+
+struct Pool {
+    double* q;
+    uint8_t* m;
+    Weights W;
+};
+
+__device__ __forceinline__ double block_max(double v, double* red)
+{
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double r = 0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int k = 0; k < nw; ++k) r = maxd(r, red[k]);
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ unsigned block_sum(unsigned v, unsigned* red)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    unsigned r = 0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int k = 0; k < nw; ++k) r += red[k];
+    __syncthreads();
+    return r;
+}
+
+// Block-wide stream compaction of the indices lo..hi whose predicate holds into `list` (order
+// preserved).  Returns the count.  Warp ballots plus a serial prefix over warps per round.
+template <class Pred>
+__device__ int block_compact(int lo, int hi, Pred pred, uint32_t* list, unsigned* red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    __shared__ int base_s;
+    if (threadIdx.x == 0) base_s = 0;
+    __syncthreads();
+    for (int start = lo; start <= hi; start += blockDim.x) {
+        const int i = start + threadIdx.x;
+        const bool p = i <= hi && pred(i);
+        const unsigned bal = __ballot_sync(0xffffffffu, p);
+        if (lane == 0) red[warp] = __popc(bal);
+        __syncthreads();
+        int off = base_s;
+        for (int k = 0; k < warp; ++k) off += red[k];
+        if (p) list[off + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)i;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tot = 0;
+            for (int k = 0; k < nw; ++k) tot += red[k];
+            base_s += tot;
+        }
+        __syncthreads();
+    }
+    const int n = base_s;
+    __syncthreads();
+    return n;
+}
+
+struct Ctx {
+    const Inst1& I;
+    double* q;   // q[p*w + i + 3]
+    double* qc;
+    double* qt;
+    double* fl;
+    uint8_t* m;  // m[i + 3]
+    int8_t* lv;  // lv[l*w + i + 3]
+    const Weights& W;
+    int w, nx, N1, maxl;
+    __device__ double& Q(int p, int i) const { return q[p * w + i + kGhost]; }
+    __device__ double& QT(int p, int i) const { return qt[p * w + i + kGhost]; }
+    __device__ double& QC(int p, int i) const { return qc[p * w + i + kGhost]; }
+    __device__ uint8_t& M(int i) const { return m[i + kGhost]; }
+    __device__ int8_t& L(int l, int i) const { return lv[l * w + i + kGhost]; }
+    __device__ bool bit(int i, int b) const { return (m[i + kGhost] >> b) & 1u; }
+    // Mask push; pushes off the ghosted line (only reachable from inconsistent user-set
+    // masks/levels, where the reference writes out of bounds) are dropped.
+    __device__ void set(int i, int b) const
+    {
+        if (i < -kGhost || i >= nx + kGhost) return;
+        m[i + kGhost] |= (uint8_t)(1u << b);
+    }
+    __device__ int D(int lev) const { return 1 << (maxl - lev); }
+    __device__ double w_(int cnt, int k) const { return W.w[cnt][k + 1]; }
+};
+
+// ------------------------------------------------------------------ PrepareEuler building blocks
+// ForwardWaveletTransformEuler (Wavelet/WAVELET_1D.h:282-335).
+__device__ void fwt1(const Ctx& c)
+{
+    for (int lev = c.maxl - 1; lev >= 0; --lev) {
+        const int D = c.D(lev), h = D >> 1, nd = c.N1 / D;
+        for (int a = threadIdx.x; a < nd; a += blockDim.x) {
+            const int i = h + a * D;
+            if (!c.bit(i, 0)) continue;
+            int s, k;
+            predict_stencil(i, D, c.N1, s, k);
+            double v = c.Q(0, i);
+            for (int cnt = 0; cnt < 4; ++cnt) v -= c.w_(cnt, k) * c.Q(0, s + cnt * D);
+            v *= 0.5;
+            c.Q(0, i) = v;
+            if (absd(v) < c.I.tol) c.M(i) &= (uint8_t)~1u;
+        }
+        __syncthreads();
+        for (int a = threadIdx.x; a < nd - 1; a += blockDim.x) {
+            const int i = D + a * D;
+            if (!c.bit(i, 0)) continue;
+            int s, k;
+            update_stencil(i, D, c.N1, s, k);
+            double v = c.Q(0, i);
+            for (int cnt = 0; cnt < 4; ++cnt) v += c.w_(cnt, k) * c.Q(0, s + cnt * D);
+            c.Q(0, i) = v;
+        }
+        __syncthreads();
+    }
+}
+
+// InverseWaveletTransformEuler (Wavelet/WAVELET_1D.h:337-391).
+__device__ void iwt1(const Ctx& c, int b)
+{
+    for (int lev = 0; lev < c.maxl; ++lev) {
+        const int D = c.D(lev), h = D >> 1, nd = c.N1 / D;
+        for (int a = threadIdx.x; a < nd - 1; a += blockDim.x) {
+            const int i = D + a * D;
+            if (!c.bit(i, b)) {
+                c.Q(0, i) = 0;
+                continue;
+            }
+            int s, k;
+            update_stencil(i, D, c.N1, s, k);
+            double v = c.Q(0, i);
+            for (int cnt = 0; cnt < 4; ++cnt) v -= c.w_(cnt, k) * c.Q(0, s + cnt * D);
+            c.Q(0, i) = v;
+        }
+        __syncthreads();
+        for (int a = threadIdx.x; a < nd; a += blockDim.x) {
+            const int i = h + a * D;
+            if (!c.bit(i, b)) {
+                c.Q(0, i) = 0;
+                continue;
+            }
+            int s, k;
+            predict_stencil(i, D, c.N1, s, k);
+            double v = c.Q(0, i);
+            v *= 2;
+            for (int cnt = 0; cnt < 4; ++cnt) v += c.w_(cnt, k) * c.Q(0, s + cnt * D);
+            c.Q(0, i) = v;
+        }
+        __syncthreads();
+    }
+}
+
+// AWCM_MANAGER_1D::CheckReconstruction (Wavelet/AWCM_MANAGER_1D.h:45-71), fine to coarse.
+__device__ void cr1(const Ctx& c, int b)
+{
+    for (int lev = c.maxl - 1; lev >= 0; --lev) {
+        const int D = c.D(lev), h = D >> 1, nd = c.N1 / D;
+        for (int a = threadIdx.x; a < nd; a += blockDim.x) {
+            const int i = h + a * D;
+            if (!c.bit(i, b)) continue;
+            int s, k;
+            predict_stencil(i, D, c.N1, s, k);
+            for (int cnt = 0; cnt < 4; ++cnt) c.set(s + cnt * D, b);
+        }
+        __syncthreads();
+    }
+}
+
+// AWCM_MANAGER_1D::AddAdjacentZone (Wavelet/AWCM_MANAGER_1D.h:14-43): detail points whose `src`
+// bit is set mark their finer neighbours in `b`.  i = odd * 2^t is a detail of level maxl-1-t.
+__device__ void aaz1(const Ctx& c, int b, int src)
+{
+    for (int i = 1 + threadIdx.x; i <= c.N1 - 1; i += blockDim.x) {
+        const int t = __ffs(i) - 1;
+        if (t >= c.maxl || !c.bit(i, src)) continue;
+        const int off = t == 0 ? 1 : (1 << (t - 1));
+        c.set(i - off, b);
+        c.set(i + off, b);
+    }
+    __syncthreads();
+}
+
+// AWCM_MANAGER_1D::AddPointForDifferentiation (Wavelet/AWCM_MANAGER_1D.h:73-107), reading the
+// copy bit and level set l.
+__device__ void apd1(const Ctx& c, int b, int l)
+{
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
+        if (!c.bit(i, kBitCopy)) continue;
+        const int lev = c.L(l, i);
+        const int D = c.D(lev);
+        const int is = i - 2 * D, ie = i + 2 * D;
+        if (lev == c.maxl) {
+            for (int cnt = -3; cnt < 4; ++cnt) c.set(i + cnt, b);
+        } else if (is <= 0) {
+            for (int cnt = 0; cnt < 6; ++cnt) c.set(cnt * D, b);
+        } else if (ie >= c.N1) {
+            for (int cnt = 0; cnt < 6; ++cnt) c.set(c.N1 - cnt * D, b);
+        } else {
+            for (int cnt = 0; cnt < 5; ++cnt) c.set(is + cnt * D, b);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool mask_or_ghost1(const Ctx& c, int i, int b)
+{
+    if (i < -kGhost || i >= c.nx + kGhost) return true;
+    return c.bit(i, b);
+}
+
+// AWCM_MANAGER_1D::ComputeLevel (Wavelet/AWCM_MANAGER_1D.h:109-133), with the optional copy
+// mask_{k+1} = mask_k of the own point.
+__device__ void cl1(const Ctx& c, int l, int b, int copy_to)
+{
+    for (int i = (int)threadIdx.x - kGhost; i <= c.N1 + kGhost; i += blockDim.x) {
+        const unsigned v = c.M(i);
+        const bool on = (v >> b) & 1u;
+        if (i < 0 || i > c.N1) {
+            // ghost byte: only the copy (the reference copies whole fields)
+        } else if (i >= 1 && i <= c.N1 - 1) {
+            if (!on) {
+                c.L(l, i) = 0;
+            } else {
+                int dx = 1;
+                for (int lev = c.maxl; lev >= 0; --lev) {
+                    if (mask_or_ghost1(c, i - dx, b) || mask_or_ghost1(c, i + dx, b)) {
+                        c.L(l, i) = (int8_t)lev;
+                        break;
+                    }
+                    dx *= 2;
+                }
+            }
+        } else {
+            c.L(l, i) = (int8_t)c.maxl;
+        }
+        if (copy_to >= 0) c.M(i) = (uint8_t)((v & ~(1u << copy_to)) | ((on ? 1u : 0u) << copy_to));
+    }
+    __syncthreads();
+}
+
+__device__ void copy_bit1(const Ctx& c, int from, int to, bool ghosts)
+{
+    const int lo = ghosts ? -kGhost : 0, hi = ghosts ? c.N1 + kGhost : c.N1;
+    for (int i = lo + (int)threadIdx.x; i <= hi; i += blockDim.x) {
+        const unsigned v = c.M(i);
+        c.M(i) = (uint8_t)((v & ~(1u << to)) | (((v >> from) & 1u) << to));
+    }
+    __syncthreads();
+}
+
+// WAVELET_1D::InterpolateEuler(q, mra, from, to) (Wavelet/WAVELET_1D.h:393-431).
+__device__ void interp1(const Ctx& c, int from, int to)
+{
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
+        const unsigned v = c.M(i);
+        const unsigned on = ((v >> to) & 1u) & ~((v >> from) & 1u);
+        c.M(i) = (uint8_t)((v & ~(1u << kBitInterp)) | (on << kBitInterp));
+    }
+    __syncthreads();
+    cr1(c, kBitInterp);
+    for (int lev = 0; lev < c.maxl; ++lev) {
+        const int D = c.D(lev), h = D >> 1, nd = c.N1 / D;
+        for (int a = threadIdx.x; a < nd; a += blockDim.x) {
+            const int i = h + a * D;
+            if (!c.bit(i, kBitInterp) || c.bit(i, from)) continue;
+            int s, k;
+            predict_stencil(i, D, c.N1, s, k);
+            for (int p = 1; p < 3; ++p) {
+                double v = 0;
+                for (int cnt = 0; cnt < 4; ++cnt) v += c.w_(cnt, k) * c.Q(p, s + cnt * D);
+                c.Q(p, i) = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// AWCM_1D::PrepareEuler (Wavelet/AWCM_1D.h:86-120).
+__device__ void prepare1(const Ctx& c)
+{
+    copy_bit1(c, 0, kBitTemp, true);
+    fwt1(c);
+    // BadingBoundary (AWCM_1D.h:73-80): three points at each end.
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
+        if (!(3 <= i && i <= c.N1 - 3)) c.set(i, 0);
+    __syncthreads();
+    copy_bit1(c, 0, kBitCopy, false);
+    aaz1(c, 0, kBitCopy);
+    cr1(c, 0);
+    for (int k = 1; k <= 3; ++k) {
+        cl1(c, k - 1, k - 1, k);      // level_{k-1} of mask_{k-1}; mask_k = mask_{k-1}
+        aaz1(c, k, k - 1);            // AddAdjacentZone(mask_k) reads its copy (== mask_{k-1})
+        copy_bit1(c, k, kBitCopy, false);
+        apd1(c, k, k - 1);            // AddPointForDifferentiation(mask_k, level_{k-1})
+        cr1(c, k);
+    }
+    cl1(c, 3, 3, -1);
+    iwt1(c, 3);
+    interp1(c, kBitTemp, 3);
+}
+
+// --------------------------------------------------------------------------------- RK3 stages
+__device__ void bc1(const Ctx& c, double* q)
+{
+    // BOUNDARY_MANAGER::SetBoundaryCondition (Problems/1D/PROBLEM_SHOCKTUBE.h:86-107).
+    if (threadIdx.x < 3 * kGhost) {
+        const int p = threadIdx.x / kGhost, g = threadIdx.x % kGhost + 1;
+        q[p * c.w + kGhost - g] = q[p * c.w + kGhost];
+        q[p * c.w + kGhost + c.N1 + g] = q[p * c.w + kGhost + c.N1];
+    }
+    __syncthreads();
+}
+
+__device__ double lf_speed1(const Ctx& c, int b, int l, double* red)
+{
+    // main_1d_euler.cpp:86-95: max |u|+c over the finest-level points of mask b.
+    double a = 0;
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
+        if (!c.bit(i, b) || c.L(l, i) != c.maxl) continue;
+        const double q0 = c.Q(0, i), q1 = c.Q(1, i), q2 = c.Q(2, i);
+        const double u = q1 / q0;
+        const double s = sound1(q0, q1, q2, c.I.gamma);
+        a = maxd(a, absd(u) + s);
+    }
+    return block_max(a, red);
+}
+
+__device__ void copy_q(const Ctx& c, double* dst)
+{
+    for (int t = threadIdx.x; t < 3 * c.w; t += blockDim.x) dst[t] = c.q[t];
+    __syncthreads();
+}
+
+// Coarse-level flux derivative (AWCM_1D::DifferentiateEuler*, Wavelet/AWCM_1D.h:142-189) with the
+// driver's branch selection (main_1d_euler.cpp:111-133); right-boundary forms mirror the left ones.
+__device__ void coarse_dF1(const Ctx& c, int i, int d, double* dF)
+{
+    const double g = 1.4;  // EULER_EQUATION_1D euler_eqn(1.4) in the reference helpers
+    auto F = [&](int ii, double* f) {
+        const double s[3] = {c.QT(0, ii), c.QT(1, ii), c.QT(2, ii)};
+        flux1(s, g, f);
+    };
+    const int iend = c.N1;
+    double a[3], b[3], e[3], f[3], h[3];
+    if (i - 2 * d > 0 && i + 2 * d < iend) {
+        F(i - 2 * d, a), F(i - d, b), F(i + d, e), F(i + 2 * d, f);
+        for (int p = 0; p < 3; ++p) dF[p] = kD1 * (e[p] - b[p]) + kD2 * (f[p] - a[p]);
+    } else if (i - 2 * d < 0) {
+        F(i - d, a), F(i, b), F(i + d, e), F(i + 2 * d, f);
+        for (int p = 0; p < 3; ++p) dF[p] = kD01 * a[p] + kD11 * b[p] + kD21 * e[p] + kD31 * f[p];
+    } else if (i == 2 * d) {
+        F(i - 2 * d, a), F(i - d, b), F(i, e), F(i + d, f), F(i + 2 * d, h);
+        for (int p = 0; p < 3; ++p) dF[p] = kD02 * a[p] + kD12 * b[p] + kD22 * e[p] + kD32 * f[p] + kD2 * h[p];
+    } else if (i > iend - 2 * d) {
+        F(i + d, a), F(i, b), F(i - d, e), F(i - 2 * d, f);
+        for (int p = 0; p < 3; ++p) dF[p] = kD01 * a[p] + kD11 * b[p] + kD21 * e[p] + kD31 * f[p];
+    } else {
+        F(i + 2 * d, a), F(i + d, b), F(i, e), F(i - d, f), F(i - 2 * d, h);
+        for (int p = 0; p < 3; ++p) dF[p] = kD02 * a[p] + kD12 * b[p] + kD22 * e[p] + kD32 * f[p] + kD2 * h[p];
+    }
+}
+
+// One stage over mask bit b / level set l (main_1d_euler.cpp:97-245).  Faces are computed once
+// (face i+1/2 is shared by points i and i+1; the reference evaluates it for both, identically).
+template <int SCHEME>
+__device__ void stage1(const Ctx& c, int b, int l, double alpha, double dt, int kind, uint32_t* list, unsigned* ured)
+{
+    copy_q(c, c.qt);
+    auto fin = [&](int i) { return i >= 0 && i <= c.N1 && c.bit(i, b) && c.L(l, i) == c.maxl; };
+    const int nf = block_compact(-1, c.N1, [&](int f) { return fin(f) || fin(f + 1); }, list, ured);
+    for (int e = threadIdx.x; e < nf; e += blockDim.x) {
+        const int f = (int)list[e];
+        double s[6][3];
+#pragma unroll
+        for (int p = 0; p < 6; ++p)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) s[p][k] = c.QT(k, f - 2 + p);
+        double o[3];
+        face_flux_1d<SCHEME>(s, alpha, c.I.gamma, o);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) c.fl[k * c.w + f + kGhost] = o[k];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
+        if (!c.bit(i, b)) continue;
+        const int lev = c.L(l, i);
+        if (lev < 0 || lev > c.maxl) continue;
+        const int d = c.D(lev);
+        if (lev != c.maxl && (i - 2 * d < -kGhost || i + 2 * d > c.N1 + kGhost)) continue;
+        double dF[3];
+        if (lev == c.maxl) {
+            for (int k = 0; k < 3; ++k) dF[k] = c.fl[k * c.w + i + kGhost] - c.fl[k * c.w + i - 1 + kGhost];
+        } else {
+            coarse_dF1(c, i, d, dF);
+        }
+        const double sc = dt / (c.I.dx * d);
+        for (int k = 0; k < 3; ++k) {
+            double& Qv = c.Q(k, i);
+            if (kind == 1) Qv = Qv - sc * dF[k];
+            else if (kind == 2) Qv = 0.75 * c.QC(k, i) + 0.25 * (Qv - sc * dF[k]);
+            else Qv = (c.QC(k, i) + 2.0 * (Qv - sc * dF[k])) / 3.0;
+        }
+    }
+    __syncthreads();
+}
+
+template <int SCHEME>
+__device__ void step_instance(Inst1& I, const Pool& P, uint32_t* list, double* dred, unsigned* ured)
+{
+    if (I.t >= I.t_end) {
+        if (threadIdx.x == 0) I.done = 1;
+        return;
+    }
+    const int w = I.nx + 2 * kGhost;
+    double* base = P.q + I.q_off;
+    uint8_t* mb = P.m + I.m_off;
+    const Ctx c{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + w), P.W, w, I.nx, I.nx - 1,
+                I.maxl};
+    prepare1(c);
+
+    // CFL (main_1d_euler.cpp:67-81)
+    double mv = 0;
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
+        if (!c.bit(i, 3)) continue;
+        const double q0 = c.Q(0, i), q1 = c.Q(1, i), q2 = c.Q(2, i);
+        const double s = sound1(q0, q1, q2, I.gamma);
+        const double u = q1 / q0;
+        mv = maxd(mv, absd(u) + s);
+    }
+    mv = block_max(mv, dred);
+    double dt = I.cfl * I.dx / mv;
+    if (I.dt_fixed > 0) dt = I.dt_fixed;
+    int do_print = 0;
+    if (I.t + dt > I.t_end) {
+        dt = I.t_end - I.t;
+        do_print = 1;
+    }
+    unsigned cnt[4];
+    for (int k = 0; k < 4; ++k) {
+        unsigned v = 0;
+        for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) v += c.bit(i, k);
+        cnt[k] = block_sum(v, ured);
+    }
+
+    bc1(c, c.q);
+    const double a1 = lf_speed1(c, 3, 3, dred);
+    copy_q(c, c.qc);
+    stage1<SCHEME>(c, 2, 2, a1, dt, 1, list, ured);
+    bc1(c, c.q);
+    const double a2 = lf_speed1(c, 2, 2, dred);
+    stage1<SCHEME>(c, 1, 1, a2, dt, 2, list, ured);
+    bc1(c, c.q);
+    const double a3 = lf_speed1(c, 1, 1, dred);
+    stage1<SCHEME>(c, 0, 0, a3, dt, 3, list, ured);
+    // RemoveResidue (AWCM_MANAGER_1D.h:135-157)
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
+        if (!c.bit(i, 0)) c.Q(0, i) = c.Q(1, i) = c.Q(2, i) = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        I.dt = dt;
+        I.mv = mv;
+        I.alpha[0] = a1;
+        I.alpha[1] = a2;
+        I.alpha[2] = a3;
+        I.do_print = do_print;
+        for (int k = 0; k < 4; ++k) I.mask_cnt[k] = cnt[k];
+        I.upd += cnt[0];
+        I.steps += 1;
+        I.t += dt;
+        I.done = I.t >= I.t_end;
+    }
+    __syncthreads();
+}
+
+// One RK3 step of every queued instance.  CTAs pull queue slots until the queue is exhausted.
+__global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, unsigned* queue, Pool P)
+{
+    extern __shared__ uint32_t list[];
+    __shared__ double dred[32];
+    __shared__ unsigned ured[32];
+    __shared__ int cur;
+    for (;;) {
+        if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int k = cur;
+        __syncthreads();
+        if (k >= n) break;
+        Inst1& I = insts[order[k]];
+        if (I.scheme == kWeno5) step_instance<kWeno5>(I, P, list, dred, ured);
+        else step_instance<kWenoZ>(I, P, list, dred, ured);
+        __syncthreads();
+    }
+}
+
+// Single passes for the C-ABI manager surface (one CTA per instance).
+__global__ void k_pass1d(Inst1* insts, int inst, Pool P, int op, int bit, int level_id)
+{
+    Inst1& I = insts[inst];
+    const int w = I.nx + 2 * kGhost;
+    double* base = P.q + I.q_off;
+    uint8_t* mb = P.m + I.m_off;
+    const Ctx c{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + w), P.W, w, I.nx, I.nx - 1,
+                I.maxl};
+    switch (op) {
+        case 0:  // AddAdjacentZone
+            copy_bit1(c, bit, kBitCopy, true);
+            aaz1(c, bit, kBitCopy);
+            break;
+        case 1: cr1(c, bit); break;
+        case 2:
+            copy_bit1(c, bit, kBitCopy, true);
+            apd1(c, bit, level_id);
+            break;
+        case 3: cl1(c, level_id, bit, -1); break;
+        case 4:
+            for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
+                if (!c.bit(i, bit)) c.Q(0, i) = c.Q(1, i) = c.Q(2, i) = 0;
+            break;
+        case 5:
+            for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
+                if (!(3 <= i && i <= c.N1 - 3)) c.set(i, bit);
+            break;
+        case 10: prepare1(c); break;
+        case 11: fwt1(c); break;
+        case 12: iwt1(c, bit); break;
+        default: break;
+    }
+}
+
+}  // namespace
+
+// ====================================================================================== Batch1D
+struct Batch1D {
+    std::vector<Inst1> host;
+    Inst1* d_inst = nullptr;
+    int* d_order = nullptr;
+    unsigned* d_queue = nullptr;
+    double* d_q = nullptr;
+    uint8_t* d_m = nullptr;
+    size_t q_doubles = 0, m_bytes = 0;
+    int max_w = 0;
+    Pool P{};
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int device = 0;
+    int block = 256;
+    int grid = 0;
+    int n = 0;
+
+    ~Batch1D()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (d_inst) cudaFree(d_inst);
+        if (d_order) cudaFree(d_order);
+        if (d_queue) cudaFree(d_queue);
+        if (d_q) cudaFree(d_q);
+        if (d_m) cudaFree(d_m);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    int create(int count, const int* num_levels, const int* nx_coarse, const double* x_min, const double* x_max,
+               double gamma, int scheme)
+    {
+        if (count <= 0 || !num_levels || !nx_coarse || !x_min || !x_max) return kErrArg;
+        if (scheme != kWenoZ && scheme != kWeno5) return kErrArg;
+        AWCM_CUDA_TRY(cudaGetDevice(&device));
+        n = count;
+        host.assign(n, Inst1{});
+        size_t qo = 0, mo = 0;
+        for (int k = 0; k < n; ++k) {
+            if (num_levels[k] < 2 || num_levels[k] > 20 || nx_coarse[k] < 5) return kErrArg;
+            Inst1& I = host[k];
+            I.nx = (nx_coarse[k] - 1) * (1 << (num_levels[k] - 1)) + 1;
+            I.maxl = num_levels[k] - 1;
+            I.scheme = scheme;
+            I.x_min = x_min[k];
+            I.dx = (x_max[k] - x_min[k]) / (I.nx - 1);
+            I.gamma = gamma;
+            I.t = 0;
+            I.t_end = 0;
+            const int w = I.nx + 2 * kGhost;
+            max_w = std::max(max_w, w);
+            I.q_off = (long long)qo;
+            I.m_off = (long long)mo;
+            qo += (size_t)12 * w;
+            qo = (qo + 31) & ~(size_t)31;
+            mo += (size_t)5 * w;
+            mo = (mo + 255) & ~(size_t)255;
+        }
+        q_doubles = qo;
+        m_bytes = mo;
+        AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        AWCM_CUDA_TRY(cudaMalloc(&d_inst, sizeof(Inst1) * n));
+        AWCM_CUDA_TRY(cudaMalloc(&d_order, sizeof(int) * n));
+        AWCM_CUDA_TRY(cudaMalloc(&d_queue, sizeof(unsigned)));
+        AWCM_CUDA_TRY(cudaMalloc(&d_q, sizeof(double) * q_doubles));
+        AWCM_CUDA_TRY(cudaMalloc(&d_m, m_bytes));
+        AWCM_CUDA_TRY(cudaMemsetAsync(d_q, 0, sizeof(double) * q_doubles, stream));
+        // AWCM_1D's constructor: mask0 true everywhere incl. ghosts, mask_temp and mask1..mask3
+        // false everywhere, levels 0 (Wavelet/AWCM_1D.h:23-34).  Ghost bytes also carry the work
+        // bits, which are never read there.
+        std::vector<uint8_t> hm(m_bytes, 0);
+        for (int k = 0; k < n; ++k) {
+            const int w = host[k].nx + 2 * kGhost;
+            uint8_t* mk = hm.data() + host[k].m_off;
+            for (int a = 0; a < w; ++a) {
+                const bool ghost = a < kGhost || a >= w - kGhost;
+                mk[a] = ghost ? 0xe1 : 0x01;
+            }
+        }
+        AWCM_CUDA_TRY(cudaMemcpy(d_m, hm.data(), m_bytes, cudaMemcpyHostToDevice));
+        // Largest instances first in the queue.
+        std::vector<int> order(n);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return host[a].nx > host[b].nx; });
+        AWCM_CUDA_TRY(cudaMemcpy(d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+        AWCM_CUDA_TRY(upload_inst());
+        P.q = d_q;
+        P.m = d_m;
+        P.W = make_weights();
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        set_launch(256, 0);
+        (void)sms;
+        return kOk;
+    }
+
+    cudaError_t upload_inst()
+    {
+        return cudaMemcpy(d_inst, host.data(), sizeof(Inst1) * n, cudaMemcpyHostToDevice);
+    }
+    cudaError_t download_inst()
+    {
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(host.data(), d_inst, sizeof(Inst1) * n, cudaMemcpyDeviceToHost);
+    }
+
+    size_t smem_bytes() const { return sizeof(uint32_t) * (size_t)(max_w + 32); }
+
+    // Launch shape: threads per CTA and CTAs per SM (0 = as many as fit).
+    int set_launch(int threads, int ctas_per_sm)
+    {
+        if (threads < 64 || threads > 1024 || threads % 32) return kErrArg;
+        block = threads;
+        int sms = 148, occ = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        cudaFuncSetAttribute(k_step1d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step1d, block, smem_bytes());
+        if (occ < 1) occ = 1;
+        if (ctas_per_sm > 0) occ = std::min(occ, ctas_per_sm);
+        grid = std::min(n, sms * occ);
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        return kOk;
+    }
+
+    void enq_step()
+    {
+        cudaMemsetAsync(d_queue, 0, sizeof(unsigned), stream);
+        k_step1d<<<grid, block, smem_bytes(), stream>>>(d_inst, n, d_order, d_queue, P);
+    }
+
+    int build_graph()
+    {
+        if (graph) return kOk;
+        cudaGraph_t gr;
+        AWCM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        enq_step();
+        cudaError_t e = cudaStreamEndCapture(stream, &gr);
+        if (e != cudaSuccess) {
+            set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+            return kErrCuda;
+        }
+        e = cudaGraphInstantiate(&graph, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) {
+            set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+            return kErrCuda;
+        }
+        return kOk;
+    }
+
+    int set_run(const double* tol, const double* cfl, const double* t, const double* t_end, double dt_fixed)
+    {
+        AWCM_CUDA_TRY(download_inst());
+        for (int k = 0; k < n; ++k) {
+            Inst1& I = host[k];
+            I.tol = tol[k];
+            I.cfl = cfl[k];
+            I.t = t[k];
+            I.t_end = t_end[k];
+            I.dt_fixed = dt_fixed;
+            I.done = I.t >= I.t_end;
+        }
+        AWCM_CUDA_TRY(upload_inst());
+        return kOk;
+    }
+
+    int steps(int n_steps)
+    {
+        int rc = build_graph();
+        if (rc) return rc;
+        for (int s = 0; s < n_steps; ++s) AWCM_CUDA_TRY(cudaGraphLaunch(graph, stream));
+        AWCM_CUDA_TRY(cudaGetLastError());
+        return kOk;
+    }
+
+    int pass(int inst, int op, int bit, int level_id)
+    {
+        if (inst < 0 || inst >= n) return kErrArg;
+        k_pass1d<<<1, 256, 0, stream>>>(d_inst, inst, P, op, bit, level_id);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int w_of(int k) const { return host[k].nx + 2 * kGhost; }
+
+    int set_q(int k, const double* aos)
+    {
+        const int w = w_of(k);
+        std::vector<double> soa(3 * (size_t)w);
+        for (int a = 0; a < w; ++a)
+            for (int p = 0; p < 3; ++p) soa[p * w + a] = aos[a * 3 + p];
+        AWCM_CUDA_TRY(cudaMemcpy(d_q + host[k].q_off, soa.data(), sizeof(double) * 3 * w, cudaMemcpyHostToDevice));
+        return kOk;
+    }
+
+    int get_q(int k, double* aos)
+    {
+        const int w = w_of(k);
+        std::vector<double> soa(3 * (size_t)w);
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        AWCM_CUDA_TRY(cudaMemcpy(soa.data(), d_q + host[k].q_off, sizeof(double) * 3 * w, cudaMemcpyDeviceToHost));
+        for (int a = 0; a < w; ++a)
+            for (int p = 0; p < 3; ++p) aos[a * 3 + p] = soa[p * w + a];
+        return kOk;
+    }
+
+    int get_masks(int k, uint8_t* planes)
+    {
+        const int w = w_of(k);
+        std::vector<uint8_t> mb(w);
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        AWCM_CUDA_TRY(cudaMemcpy(mb.data(), d_m + host[k].m_off, w, cudaMemcpyDeviceToHost));
+        const int bits[5] = {kBitTemp, 0, 1, 2, 3};
+        for (int r = 0; r < 5; ++r)
+            for (int a = 0; a < w; ++a) planes[r * w + a] = (mb[a] >> bits[r]) & 1u;
+        return kOk;
+    }
+
+    int set_masks(int k, const uint8_t* planes)
+    {
+        const int w = w_of(k);
+        std::vector<uint8_t> mb(w);
+        const int bits[5] = {kBitTemp, 0, 1, 2, 3};
+        for (int a = 0; a < w; ++a) {
+            const bool ghost = a < kGhost || a >= w - kGhost;
+            unsigned v = ghost ? 0xe0u : 0u;
+            for (int r = 0; r < 5; ++r) v |= (unsigned)(planes[r * w + a] != 0) << bits[r];
+            mb[a] = (uint8_t)v;
+        }
+        AWCM_CUDA_TRY(cudaMemcpy(d_m + host[k].m_off, mb.data(), w, cudaMemcpyHostToDevice));
+        return kOk;
+    }
+
+    int get_levels(int k, int* lv)
+    {
+        const int w = w_of(k), nx = host[k].nx;
+        std::vector<int8_t> l(4 * (size_t)w);
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        AWCM_CUDA_TRY(cudaMemcpy(l.data(), d_m + host[k].m_off + w, 4 * (size_t)w, cudaMemcpyDeviceToHost));
+        for (int r = 0; r < 4; ++r)
+            for (int i = 0; i < nx; ++i) lv[r * nx + i] = l[r * w + i + kGhost];
+        return kOk;
+    }
+
+    int set_levels(int k, const int* lv)
+    {
+        const int w = w_of(k), nx = host[k].nx;
+        std::vector<int8_t> l(4 * (size_t)w, 0);
+        for (int r = 0; r < 4; ++r)
+            for (int i = 0; i < nx; ++i) l[r * w + i + kGhost] = (int8_t)lv[r * nx + i];
+        AWCM_CUDA_TRY(cudaMemcpy(d_m + host[k].m_off + w, l.data(), 4 * (size_t)w, cudaMemcpyHostToDevice));
+        return kOk;
+    }
+
+    // Sod-type states on the cell-centred grid x_min + i dx (SHOCKTUBE::Initialize,
+    // Problems/1D/PROBLEM_SHOCKTUBE.h:14-54, with the interface and states as arguments).
+    int init_riemann(int k, double x_interface, const double* left, const double* right)
+    {
+        const Inst1& I = host[k];
+        const int w = w_of(k);
+        std::vector<double> aos(3 * (size_t)w);
+        for (int i = -kGhost; i < I.nx + kGhost; ++i) {
+            const double x = I.x_min + I.dx * i;
+            const double* s = x <= x_interface ? left : right;
+            const double rho = s[0], u = s[1], p = s[2];
+            double* o = &aos[3 * (size_t)(i + kGhost)];
+            o[0] = rho;
+            o[1] = rho * u;
+            o[2] = p / (I.gamma - 1) + 0.5 * rho * (u * u);
+        }
+        return set_q(k, aos.data());
+    }
+};
+
+}  // namespace awcm
+
+// ======================================================================================== C-ABI
+using awcm::Batch1D;
+
+struct awcm1d_batch_s {
+    Batch1D b;
+};
+
+extern "C" {
+
+int awcm1d_batch_create(int count, const int* num_levels, const int* nx_coarse, const double* x_min,
+                        const double* x_max, double gamma, int scheme, awcm1d_batch_t* out)
+{
+    if (!out) return awcm::kErrArg;
+    *out = nullptr;
+    awcm1d_batch_s* h = new (std::nothrow) awcm1d_batch_s();
+    if (!h) return awcm::kErrOom;
+    const int rc = h->b.create(count, num_levels, nx_coarse, x_min, x_max, gamma, scheme);
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return awcm::kOk;
+}
+
+int awcm1d_batch_destroy(awcm1d_batch_t h)
+{
+    delete h;
+    return awcm::kOk;
+}
+
+#define AWCM_B(h, k)                                                   \
+    if (!(h) || (k) < 0 || (k) >= (h)->b.n) return awcm::kErrArg;     \
+    cudaSetDevice((h)->b.device)
+
+int awcm1d_batch_count(awcm1d_batch_t h, int* n)
+{
+    if (!h || !n) return awcm::kErrArg;
+    *n = h->b.n;
+    return awcm::kOk;
+}
+int awcm1d_batch_nx(awcm1d_batch_t h, int k, int* nx)
+{
+    AWCM_B(h, k);
+    if (!nx) return awcm::kErrArg;
+    *nx = h->b.host[k].nx;
+    return awcm::kOk;
+}
+int awcm1d_batch_set_q(awcm1d_batch_t h, int k, const double* q)
+{
+    AWCM_B(h, k);
+    return q ? h->b.set_q(k, q) : awcm::kErrArg;
+}
+int awcm1d_batch_get_q(awcm1d_batch_t h, int k, double* q)
+{
+    AWCM_B(h, k);
+    return q ? h->b.get_q(k, q) : awcm::kErrArg;
+}
+int awcm1d_batch_get_masks(awcm1d_batch_t h, int k, uint8_t* m)
+{
+    AWCM_B(h, k);
+    return m ? h->b.get_masks(k, m) : awcm::kErrArg;
+}
+int awcm1d_batch_set_masks(awcm1d_batch_t h, int k, const uint8_t* m)
+{
+    AWCM_B(h, k);
+    return m ? h->b.set_masks(k, m) : awcm::kErrArg;
+}
+int awcm1d_batch_get_levels(awcm1d_batch_t h, int k, int* lv)
+{
+    AWCM_B(h, k);
+    return lv ? h->b.get_levels(k, lv) : awcm::kErrArg;
+}
+int awcm1d_batch_set_levels(awcm1d_batch_t h, int k, const int* lv)
+{
+    AWCM_B(h, k);
+    return lv ? h->b.set_levels(k, lv) : awcm::kErrArg;
+}
+int awcm1d_batch_init_riemann(awcm1d_batch_t h, int k, double x_interface, const double* left3,
+                              const double* right3)
+{
+    AWCM_B(h, k);
+    if (!left3 || !right3) return awcm::kErrArg;
+    return h->b.init_riemann(k, x_interface, left3, right3);
+}
+int awcm1d_batch_set_run(awcm1d_batch_t h, const double* tol, const double* cfl, const double* t,
+                         const double* t_end, double dt_fixed)
+{
+    if (!h || !tol || !cfl || !t || !t_end) return awcm::kErrArg;
+    cudaSetDevice(h->b.device);
+    return h->b.set_run(tol, cfl, t, t_end, dt_fixed);
+}
+int awcm1d_batch_steps(awcm1d_batch_t h, int n_steps)
+{
+    if (!h || n_steps < 0) return awcm::kErrArg;
+    cudaSetDevice(h->b.device);
+    return h->b.steps(n_steps);
+}
+int awcm1d_batch_sync(awcm1d_batch_t h)
+{
+    if (!h) return awcm::kErrArg;
+    AWCM_CUDA_TRY(cudaStreamSynchronize(h->b.stream));
+    return awcm::kOk;
+}
+// out[16]: t, dt, do_print, done, steps, |mask0..3|, max speed, alpha1..3, sum|mask0|, err, 0
+int awcm1d_batch_status(awcm1d_batch_t h, int k, double* out)
+{
+    AWCM_B(h, k);
+    if (!out) return awcm::kErrArg;
+    AWCM_CUDA_TRY(h->b.download_inst());
+    const auto& I = h->b.host[k];
+    out[0] = I.t;
+    out[1] = I.dt;
+    out[2] = I.do_print;
+    out[3] = I.done;
+    out[4] = I.steps;
+    for (int q = 0; q < 4; ++q) out[5 + q] = I.mask_cnt[q];
+    out[9] = I.mv;
+    out[10] = I.alpha[0];
+    out[11] = I.alpha[1];
+    out[12] = I.alpha[2];
+    out[13] = (double)I.upd;
+    out[14] = I.err;
+    out[15] = 0;
+    return awcm::kOk;
+}
+int awcm1d_batch_totals(awcm1d_batch_t h, double* out)
+{
+    if (!h || !out) return awcm::kErrArg;
+    cudaSetDevice(h->b.device);
+    AWCM_CUDA_TRY(h->b.download_inst());
+    double upd = 0, steps = 0, done = 0;
+    for (const auto& I : h->b.host) {
+        upd += (double)I.upd;
+        steps += I.steps;
+        done += I.done;
+    }
+    out[0] = upd;
+    out[1] = steps;
+    out[2] = done;
+    return awcm::kOk;
+}
+int awcm1d_batch_pass(awcm1d_batch_t h, int k, int op, int mask_id, int level_id)
+{
+    AWCM_B(h, k);
+    const int bit = mask_id >= 0 && mask_id <= 3 ? mask_id : awcm::kBitTemp;
+    if (level_id < 0 || level_id > 3) return awcm::kErrArg;
+    return h->b.pass(k, op, bit, level_id);
+}
+int awcm1d_batch_set_launch(awcm1d_batch_t h, int threads, int ctas_per_sm)
+{
+    if (!h) return awcm::kErrArg;
+    cudaSetDevice(h->b.device);
+    return h->b.set_launch(threads, ctas_per_sm);
+}
+int awcm1d_batch_stream(awcm1d_batch_t h, void** stream)
+{
+    if (!h || !stream) return awcm::kErrArg;
+    *stream = (void*)h->b.stream;
+    return awcm::kOk;
+}
+
+}  // extern "C"

@@ -1,0 +1,1733 @@
+// 2D AWCM compressible-Euler path on one B200 (sm_100a), FP64.
+//
+// Layout in HBM (one instance):
+//   conserved field Q and the RK stage fields Q2, Q1: four structure-of-arrays planes each
+//     (rho, rho u, rho v, E), row pitch `pitch` doubles, ghost ring of 3, point (i,j) at
+//     (j+3)*pitch + (i+3);
+//   face fluxes Fx (face i+1/2 stored at point i) and Fy (face j+1/2 at point j), four planes each;
+//   one mask byte per point: bits 0..3 = mask0..mask3, 4 = previous mask0, 5/6 = work bits;
+//   one int8 level plane per level set (level0..level3);
+//   per stage compacted worklists (row-ordered uint32 point indices) of finest-level points,
+//   coarse points, needed x faces and needed y faces, built by block ballot/prefix compaction.
+//
+// One RK3 step = PrepareEuler (level-by-level transform and mask kernels) + CFL/LF reductions +
+// three stages (boundary fill, face-flux kernels, point-update kernels) + residue removal.  All
+// scalars the step needs (t, dt, CFL speed, per-level dt/dx) stay on the device, so a step is a
+// fixed launch sequence captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "awcm_b200.h"
+#include "awcm_common.cuh"
+
+namespace awcm {
+namespace {
+
+constexpr int kMaxLevels = 24;
+constexpr int kStages = 3;
+
+struct Grid2 {
+    int nx, ny, maxl, pitch, rows, bc_kind;
+    double x_min, y_min, dx, dy, gamma;
+    Weights W;
+    __host__ __device__ __forceinline__ size_t at(int i, int j) const
+    {
+        return (size_t)(j + kGhost) * pitch + (size_t)(i + kGhost);
+    }
+    __host__ __device__ __forceinline__ double w(int cnt, int k) const { return W.w[cnt][k + 1]; }
+    __host__ __device__ __forceinline__ int D(int lev) const { return 1 << (maxl - lev); }
+};
+
+struct Field4 {
+    double* p[4];
+};
+
+// Device-resident step scalars.
+struct StepState {
+    double t, t_end, dt, cfl, dt_fixed, tol, mv;
+    double sc[kMaxLevels];        // dt / (dx * 2^(maxl-lev)) per level
+    int do_print, done, steps, full_zero;
+    unsigned cnt[4 * kStages];     // per stage: finest points, coarse points, x faces, y faces
+    unsigned mask_cnt[4];          // |mask0..mask3| over the grid points
+    unsigned long long upd;        // sum over steps of |mask0|
+    unsigned long long stage_pts;  // sum over steps of |mask2|+|mask1|+|mask0|
+};
+
+__device__ __forceinline__ int ctz_or(int v, int big) { return v == 0 ? big : __ffs(v) - 1; }
+
+// Sub-band geometry of level lev: which 0 = d1 (half x, coarse y), 1 = d2 (coarse x, half y),
+// 2 = d3 (half, half), 3 = c (coarse interior); extents of MRA_GRID_INT_2D::Initialize
+// (Wavelet/MRA_GRID_UNIFORM_2D.h:101-131).
+struct Band {
+    int i0, j0, cx, cy, D;
+};
+__host__ __device__ __forceinline__ Band band_of(const Grid2& g, int lev, int which)
+{
+    const int D = g.D(lev), h = D >> 1;
+    const int MX = (g.nx - 1) / D, MY = (g.ny - 1) / D;
+    Band b;
+    b.D = D;
+    switch (which) {
+        case 0: b.i0 = h, b.cx = MX, b.j0 = D, b.cy = MY - 1; break;
+        case 1: b.i0 = D, b.cx = MX - 1, b.j0 = h, b.cy = MY; break;
+        case 2: b.i0 = h, b.cx = MX, b.j0 = h, b.cy = MY; break;
+        default: b.i0 = D, b.cx = MX - 1, b.j0 = D, b.cy = MY - 1; break;
+    }
+    if (b.cx < 0) b.cx = 0;
+    if (b.cy < 0) b.cy = 0;
+    return b;
+}
+
+__device__ __forceinline__ bool band_point(const Band& b, long t, int& i, int& j)
+{
+    if (b.cx == 0 || t >= (long)b.cx * b.cy) return false;
+    i = b.i0 + (int)(t % b.cx) * b.D;
+    j = b.j0 + (int)(t / b.cx) * b.D;
+    return true;
+}
+
+__device__ __forceinline__ long gtid() { return (long)blockIdx.x * blockDim.x + threadIdx.x; }
+
+__device__ __forceinline__ void set_bit(uint8_t* m, size_t a, int bit) { m[a] |= (uint8_t)(1u << bit); }
+
+// Push of a mask bit at (i,j).  Under the reference's mask invariants every push lands on the
+// ghosted grid; pushes that would leave it (possible only for inconsistent user-set masks/levels,
+// where the reference itself writes out of bounds) are dropped.
+__device__ __forceinline__ void push_bit(const Grid2& g, uint8_t* m, int i, int j, int bit)
+{
+    if (i < -kGhost || i >= g.nx + kGhost || j < -kGhost || j >= g.ny + kGhost) return;
+    m[g.at(i, j)] |= (uint8_t)(1u << bit);
+}
+
+// ------------------------------------------------------------------------------------ transforms
+// Forward transform, one phase of one level (ForwardWaveletTransformationEuler, WAVELET_2D.h:478-624):
+// PH 0 = d3 predict + threshold, PH 1 = d1 and d2 predict + threshold, PH 2 = c update.
+template <int PH>
+__global__ void k_fwt(Grid2 g, double* __restrict__ q, uint8_t* __restrict__ m, int lev, const StepState* st)
+{
+    if (st->done) return;
+    const double tol = st->tol;
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    long t = gtid();
+    int i, j, which;
+    if (PH == 0) {
+        which = 2;
+    } else if (PH == 1) {
+        const Band b1 = band_of(g, lev, 0);
+        const long n1 = (long)b1.cx * b1.cy;
+        which = t < n1 ? 0 : 1;
+        if (which == 1) t -= n1;
+    } else {
+        which = 3;
+    }
+    const Band b = band_of(g, lev, which);
+    if (!band_point(b, t, i, j)) return;
+    const size_t a = g.at(i, j);
+    if (!(m[a] & 1u)) return;
+    const int D = b.D;
+    if (which == 2) {
+        int is, k1, js, k2;
+        predict_stencil(i, D, NX, is, k1);
+        predict_stencil(j, D, NY, js, k2);
+        double v = q[a];
+        for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+        v *= 0.25;
+        q[a] = v;
+        if (absd(v) < tol) m[a] &= (uint8_t)~1u;
+    } else if (which == 0 || which == 1) {
+        int s, k;
+        double v = q[a];
+        if (which == 0) {
+            predict_stencil(i, D, NX, s, k);
+            for (int c = 0; c < 4; ++c) v -= q[g.at(s + c * D, j)] * g.w(c, k);
+        } else {
+            predict_stencil(j, D, NY, s, k);
+            for (int c = 0; c < 4; ++c) v -= q[g.at(i, s + c * D)] * g.w(c, k);
+        }
+        v *= 0.5;
+        q[a] = v;
+        if (absd(v) < tol) m[a] &= (uint8_t)~1u;
+    } else {
+        int is, k1, js, k2;
+        update_stencil(i, D, NX, is, k1);
+        update_stencil(j, D, NY, js, k2);
+        double v = q[a];
+        for (int c = 0; c < 4; ++c) v += q[g.at(is + c * D, j)] * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v += q[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+        q[a] = v;
+    }
+}
+
+// Inverse transform, one phase (InverseWaveletTransformationEuler, WAVELET_2D.h:626-782):
+// PH 0 = c, PH 1 = d2 and d1, PH 2 = d3; points outside the mask get density 0.
+template <int PH>
+__global__ void k_iwt(Grid2 g, double* __restrict__ q, const uint8_t* __restrict__ m, int lev, int bit,
+                      const StepState* st)
+{
+    if (st && st->done) return;
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    long t = gtid();
+    int i, j, which;
+    if (PH == 0) {
+        which = 3;
+    } else if (PH == 1) {
+        const Band b1 = band_of(g, lev, 0);
+        const long n1 = (long)b1.cx * b1.cy;
+        which = t < n1 ? 0 : 1;
+        if (which == 1) t -= n1;
+    } else {
+        which = 2;
+    }
+    const Band b = band_of(g, lev, which);
+    if (!band_point(b, t, i, j)) return;
+    const size_t a = g.at(i, j);
+    if (!((m[a] >> bit) & 1u)) {
+        q[a] = 0;
+        return;
+    }
+    const int D = b.D;
+    if (which == 3) {
+        int is, k1, js, k2;
+        update_stencil(i, D, NX, is, k1);
+        update_stencil(j, D, NY, js, k2);
+        double v = q[a];
+        for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+        q[a] = v;
+    } else if (which == 1) {
+        int s, k;
+        predict_stencil(j, D, NY, s, k);
+        double v = q[a];
+        v *= 2.0;
+        for (int c = 0; c < 4; ++c) v += q[g.at(i, s + c * D)] * g.w(c, k);
+        q[a] = v;
+    } else if (which == 0) {
+        int s, k;
+        predict_stencil(i, D, NX, s, k);
+        double v = q[a];
+        v *= 2.0;
+        for (int c = 0; c < 4; ++c) v += q[g.at(s + c * D, j)] * g.w(c, k);
+        q[a] = v;
+    } else {
+        int is, k1, js, k2;
+        predict_stencil(i, D, NX, is, k1);
+        predict_stencil(j, D, NY, js, k2);
+        double v = q[a];
+        v *= 4.0;
+        for (int c = 0; c < 4; ++c) v += q[g.at(is + c * D, j)] * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v += q[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+        q[a] = v;
+    }
+}
+
+// CheckReconstruction, one phase of one level (AWCM_MANAGER_2D.h:63-158): PH 0 = d3 points mark
+// their 4 + 4 + 16 predict nodes, PH 1 = d1/d2 points mark their 4 nodes.  Plain byte
+// read-modify-writes are race-free here: a phase only ever sets the one bit `bit`.
+template <int PH>
+__global__ void k_cr(Grid2 g, uint8_t* __restrict__ m, int lev, int bit, const StepState* st)
+{
+    if (st && st->done) return;
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    long t = gtid();
+    int i, j, which;
+    if (PH == 0) {
+        which = 2;
+    } else {
+        const Band b1 = band_of(g, lev, 0);
+        const long n1 = (long)b1.cx * b1.cy;
+        which = t < n1 ? 0 : 1;
+        if (which == 1) t -= n1;
+    }
+    const Band b = band_of(g, lev, which);
+    if (!band_point(b, t, i, j)) return;
+    if (!((m[g.at(i, j)] >> bit) & 1u)) return;
+    const int D = b.D;
+    int is, js, k;
+    if (which == 2) {
+        predict_stencil(i, D, NX, is, k);
+        predict_stencil(j, D, NY, js, k);
+        for (int c = 0; c < 4; ++c) set_bit(m, g.at(is + c * D, j), bit);
+        for (int c = 0; c < 4; ++c) set_bit(m, g.at(i, js + c * D), bit);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) set_bit(m, g.at(is + c1 * D, js + c2 * D), bit);
+    } else if (which == 0) {
+        predict_stencil(i, D, NX, is, k);
+        for (int c = 0; c < 4; ++c) set_bit(m, g.at(is + c * D, j), bit);
+    } else {
+        predict_stencil(j, D, NY, js, k);
+        for (int c = 0; c < 4; ++c) set_bit(m, g.at(i, js + c * D), bit);
+    }
+}
+
+// InterpolateEuler, one phase of one level (WAVELET_2D.h:784-907): PH 0 = d1 and d2, PH 1 = d3;
+// components 1..3 at points of the work mask that were not active before (`from_bit`).
+template <int PH>
+__global__ void k_interp(Grid2 g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit,
+                         const StepState* st)
+{
+    if (st && st->done) return;
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    long t = gtid();
+    int i, j, which;
+    if (PH == 0) {
+        const Band b1 = band_of(g, lev, 0);
+        const long n1 = (long)b1.cx * b1.cy;
+        which = t < n1 ? 0 : 1;
+        if (which == 1) t -= n1;
+    } else {
+        which = 2;
+    }
+    const Band b = band_of(g, lev, which);
+    if (!band_point(b, t, i, j)) return;
+    const size_t a = g.at(i, j);
+    const unsigned mb = m[a];
+    if (!((mb >> kBitInterp) & 1u) || ((mb >> from_bit) & 1u)) return;
+    const int D = b.D;
+    if (which == 0) {
+        int s, k;
+        predict_stencil(i, D, NX, s, k);
+        for (int p = 1; p < 4; ++p) {
+            const double* qp = q.p[p];
+            double v = 0.0;
+            for (int c = 0; c < 4; ++c) v += qp[g.at(s + c * D, j)] * g.w(c, k);
+            q.p[p][a] = v;
+        }
+    } else if (which == 1) {
+        int s, k;
+        predict_stencil(j, D, NY, s, k);
+        for (int p = 1; p < 4; ++p) {
+            const double* qp = q.p[p];
+            double v = 0.0;
+            for (int c = 0; c < 4; ++c) v += qp[g.at(i, s + c * D)] * g.w(c, k);
+            q.p[p][a] = v;
+        }
+    } else {
+        int is, k1, js, k2;
+        predict_stencil(i, D, NX, is, k1);
+        predict_stencil(j, D, NY, js, k2);
+        for (int p = 1; p < 4; ++p) {
+            const double* qp = q.p[p];
+            double v = 0.0;
+            for (int c = 0; c < 4; ++c) v += qp[g.at(is + c * D, j)] * g.w(c, k1);
+            for (int c = 0; c < 4; ++c) v += qp[g.at(i, js + c * D)] * g.w(c, k2);
+            for (int c2 = 0; c2 < 4; ++c2)
+                for (int c1 = 0; c1 < 4; ++c1) v -= qp[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+            q.p[p][a] = v;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------- dense mask passes
+__device__ __forceinline__ bool grid_point(const Grid2& g, long t, int& i, int& j)
+{
+    if (t >= (long)g.nx * g.ny) return false;
+    i = (int)(t % g.nx);
+    j = (int)(t / g.nx);
+    return true;
+}
+
+__global__ void k_copy_bit_all(uint8_t* m, size_t n, int from, int to, const StepState* st)
+{
+    if (st && st->done) return;
+    const size_t a = (size_t)gtid();
+    if (a >= n) return;
+    const unsigned v = m[a];
+    m[a] = (uint8_t)((v & ~(1u << to)) | (((v >> from) & 1u) << to));
+}
+
+// BandingMask (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:205-213) on `bit`, then copies the
+// result into the work bit read by the following add-adjacent-zone pass.
+__global__ void k_band_copy(Grid2 g, uint8_t* m, int bit, int copy_to, const StepState* st)
+{
+    if (st && st->done) return;
+    int i, j;
+    if (!grid_point(g, gtid(), i, j)) return;
+    const size_t a = g.at(i, j);
+    unsigned v = m[a];
+    if (!(2 <= i && i <= g.nx - 3 && j >= 2 && j <= g.ny - 3)) v |= 1u << bit;
+    if (copy_to >= 0) v = (v & ~(1u << copy_to)) | (((v >> bit) & 1u) << copy_to);
+    m[a] = (uint8_t)v;
+}
+
+// AddAdjacentZone (AWCM_MANAGER_2D.h:14-61): every detail point whose copy bit is set marks its
+// finer neighbours in `bit`.  A point (i,j) = (odd*2^a, odd*2^b) is a detail of level
+// maxl-1-min(a,b): d1 if a < b, d2 if a > b, d3 if a == b (boundary rows/columns excluded as in
+// the sub-grids).
+__global__ void k_aaz(Grid2 g, uint8_t* m, int bit, int src, const StepState* st)
+{
+    if (st && st->done) return;
+    int i, j;
+    if (!grid_point(g, gtid(), i, j)) return;
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    const int ti = ctz_or(i, 64), tj = ctz_or(j, 64);
+    const int mn = ti < tj ? ti : tj;
+    if (mn >= g.maxl) return;
+    if (ti < tj && (j == 0 || j == NY)) return;
+    if (tj < ti && (i == 0 || i == NX)) return;
+    if (!((m[g.at(i, j)] >> src) & 1u)) return;
+    const int lev = g.maxl - 1 - mn;
+    if (lev == g.maxl - 1) {
+        push_bit(g, m, i - 1, j, bit);
+        push_bit(g, m, i + 1, j, bit);
+        push_bit(g, m, i, j - 1, bit);
+        push_bit(g, m, i, j + 1, bit);
+    } else {
+        const int D = g.D(lev), h = D / 2, q4 = D / 4;
+        push_bit(g, m, i - q4, j, bit);
+        push_bit(g, m, i + q4, j, bit);
+        push_bit(g, m, i, j - q4, bit);
+        push_bit(g, m, i, j + q4, bit);
+        push_bit(g, m, i - h, j, bit);
+        push_bit(g, m, i + h, j, bit);
+        push_bit(g, m, i, j - h, bit);
+        push_bit(g, m, i, j + h, bit);
+    }
+}
+
+__device__ __forceinline__ bool mask_or_ghost(const Grid2& g, const uint8_t* m, int i, int j, int bit)
+{
+    // Beyond the ghost ring a mask reads as set, like the ghosts themselves.
+    if (i < -kGhost || i >= g.nx + kGhost || j < -kGhost || j >= g.ny + kGhost) return true;
+    return (m[g.at(i, j)] >> bit) & 1u;
+}
+
+// ComputeLevel (AWCM_MANAGER_2D.h:215-241) of mask `bit` into `lvl`; a level is left unchanged when
+// no neighbour is found.  When copy_to >= 0 the pass also performs `mask_{k+1} = mask_k` on every
+// byte of the plane, ghost ring included (the reference copies whole fields).  One thread per
+// plane byte; the level search runs for grid points only.
+__global__ void k_cl(Grid2 g, uint8_t* m, int8_t* lvl, int bit, int copy_to, size_t plane, const StepState* st)
+{
+    if (st && st->done) return;
+    const size_t a = (size_t)gtid();
+    if (a >= plane) return;
+    const int i = (int)(a % (size_t)g.pitch) - kGhost, j = (int)(a / (size_t)g.pitch) - kGhost;
+    const unsigned v = m[a];
+    const bool on = (v >> bit) & 1u;
+    if (i >= 0 && i < g.nx && j >= 0 && j < g.ny) {
+        if (!on) {
+            lvl[a] = 0;
+        } else {
+            int dx = 1;
+            for (int lev = g.maxl; lev >= 0; --lev) {
+                if (mask_or_ghost(g, m, i - dx, j, bit) || mask_or_ghost(g, m, i + dx, j, bit) ||
+                    mask_or_ghost(g, m, i, j - dx, bit) || mask_or_ghost(g, m, i, j + dx, bit)) {
+                    lvl[a] = (int8_t)lev;
+                    break;
+                }
+                dx *= 2;
+            }
+        }
+    }
+    if (copy_to >= 0) m[a] = (uint8_t)((v & ~(1u << copy_to)) | ((on ? 1u : 0u) << copy_to));
+}
+
+// AddPointForDifferentiation (AWCM_MANAGER_2D.h:160-213): points of mask `src` mark their flux
+// stencil in `bit` (finest level: the +-3 cross; coarser: +-2 spacings, shifted at the edges).
+__global__ void k_apd(Grid2 g, uint8_t* m, const int8_t* lvl, int bit, int src, const StepState* st)
+{
+    if (st && st->done) return;
+    int i, j;
+    if (!grid_point(g, gtid(), i, j)) return;
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    if (i < 1 || i > NX - 1 || j < 1 || j > NY - 1) return;
+    const size_t a = g.at(i, j);
+    if (!((m[a] >> src) & 1u)) return;
+    const int lev = lvl[a];
+    if (lev == g.maxl) {
+        for (int c = -3; c <= 3; ++c) {
+            push_bit(g, m, i + c, j, bit);
+            push_bit(g, m, i, j + c, bit);
+        }
+        return;
+    }
+    const int D = g.D(lev);
+    int lo = -2, hi = 2;
+    if (i - 2 * D < 0) lo = -1;
+    else if (i + 2 * D > NX) hi = 1;
+    for (int c = lo; c <= hi; ++c) push_bit(g, m, i + D * c, j, bit);
+    lo = -2, hi = 2;
+    if (j - 2 * D < 0) lo = -1;
+    else if (j + 2 * D > NY) hi = 1;
+    for (int c = lo; c <= hi; ++c) push_bit(g, m, i, j + D * c, bit);
+}
+
+// Work mask of InterpolateEuler: `to` minus `from` over the grid points (ghost bits stay set).
+__global__ void k_interp_init(Grid2 g, uint8_t* m, int from, int to, const StepState* st)
+{
+    if (st && st->done) return;
+    int i, j;
+    if (!grid_point(g, gtid(), i, j)) return;
+    const size_t a = g.at(i, j);
+    const unsigned v = m[a];
+    const unsigned on = ((v >> to) & 1u) & ~((v >> from) & 1u);
+    m[a] = (uint8_t)((v & ~(1u << kBitInterp)) | (on << kBitInterp));
+}
+
+// RemoveResidueEuler (AWCM_MANAGER_2D.h:267-280): zero interior points outside `bit`.  In the
+// step only points that can hold non-zero values (in mask3 or in the previous mask0) are written.
+__global__ void k_remove_residue(Grid2 g, Field4 q, const uint8_t* m, int bit, int sparse, const StepState* st)
+{
+    if (st && st->done) return;
+    int i, j;
+    if (!grid_point(g, gtid(), i, j)) return;
+    if (i < 1 || i > g.nx - 2 || j < 1 || j > g.ny - 2) return;
+    const size_t a = g.at(i, j);
+    const unsigned v = m[a];
+    if ((v >> bit) & 1u) return;
+    const bool full = !sparse || (st && st->full_zero);
+    if (!full && !(v & ((1u << 3) | (1u << kBitTemp)))) return;
+    q.p[0][a] = 0.0;
+    q.p[1][a] = 0.0;
+    q.p[2][a] = 0.0;
+    q.p[3][a] = 0.0;
+}
+
+// ------------------------------------------------------------------------------------ boundaries
+__device__ __forceinline__ double euler_E(double g, double rho, double u, double v, double p)
+{
+    return p / (g - 1) + 0.5 * rho * (u * u + v * v);
+}
+
+// Ghost fill of the edge strips (corners are never read by the axis-aligned stencils):
+// transmissive BOUNDARY_MANAGER_QUAD (Problems/2D/PROBLEM_QUADRANTS.h:123-203), double Mach
+// BOUNDARY_MANAGER_DMACH(t) (Problems/2D/PROBLEM_DOUBLEMACH.h:106-245) and periodic
+// BOUNDARY_MANAGER_ISENVORTEX (Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h:107-171).
+__global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host)
+{
+    if (st && st->done) return;
+    const double t = st ? st->t : t_host;
+    const long tid = gtid();
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    const long nside = (long)kGhost * g.ny, nbt = (long)kGhost * g.nx;
+    int i, j, si, sj;  // ghost point and source point
+    const double g14 = 1.4;
+    if (tid < 2 * nside) {
+        const bool right = tid >= nside;
+        const long r = right ? tid - nside : tid;
+        j = (int)(r / kGhost);
+        const int c = (int)(r % kGhost);
+        if (!right) {
+            i = -1 - c;
+            si = g.bc_kind == AWCM_BC_PERIODIC ? NX - c : 0;
+        } else {
+            i = NX + 1 + c;
+            si = g.bc_kind == AWCM_BC_PERIODIC ? c : NX;
+        }
+        sj = j;
+        const size_t a = g.at(i, j);
+        if (!right && g.bc_kind == AWCM_BC_DOUBLE_MACH) {
+            const double rho = 8, u = 8.25 * sqrt(3.0) * 0.5, v = -8.25 * 0.5, p = 116.5;
+            f.p[0][a] = rho;
+            f.p[1][a] = rho * u;
+            f.p[2][a] = rho * v;
+            f.p[3][a] = euler_E(g.gamma, rho, u, v, p);
+            return;
+        }
+        const size_t s = g.at(si, sj);
+        for (int k = 0; k < 4; ++k) f.p[k][a] = f.p[k][s];
+        return;
+    }
+    const long r0 = tid - 2 * nside;
+    if (r0 >= 2 * nbt) return;
+    const bool top = r0 >= nbt;
+    const long r = top ? r0 - nbt : r0;
+    i = (int)(r / kGhost);
+    const int c = (int)(r % kGhost);
+    if (!top) {
+        j = -1 - c;
+        sj = g.bc_kind == AWCM_BC_PERIODIC ? NY - c : 0;
+    } else {
+        j = NY + 1 + c;
+        sj = g.bc_kind == AWCM_BC_PERIODIC ? c : NY;
+    }
+    const size_t a = g.at(i, j);
+    if (g.bc_kind == AWCM_BC_DOUBLE_MACH) {
+        const double sqrt3 = sqrt(3.0);
+        const double x = g.x_min + i * g.dx;
+        const double post[4] = {8, 8 * 8.25 * sqrt3 * 0.5, -8 * 8.25 * 0.5,
+                                euler_E(g14, 8, 8.25 * sqrt3 * 0.5, -8.25 * 0.5, 116.5)};
+        if (!top) {
+            if (x > 1.0 / 6.0) {
+                const size_t s = g.at(i, 0);
+                f.p[0][a] = f.p[0][s];
+                f.p[1][a] = f.p[1][s];
+                f.p[2][a] = -f.p[2][s];
+                f.p[3][a] = f.p[3][s];
+            } else {
+                for (int k = 0; k < 4; ++k) f.p[k][a] = post[k];
+            }
+        } else {
+            const double pre[4] = {1.4, 1.4 * 0, 1.4 * 0, euler_E(g14, 1.4, 0, 0, 1)};
+            const bool behind = x < 1.0 / 6.0 + (1 + 20 * t) / sqrt3;
+            for (int k = 0; k < 4; ++k) f.p[k][a] = behind ? post[k] : pre[k];
+        }
+        return;
+    }
+    const size_t s = g.at(i, sj);
+    for (int k = 0; k < 4; ++k) f.p[k][a] = f.p[k][s];
+}
+
+// ------------------------------------------------------------------------- CFL and LF reductions
+// Per-row alpha_x[j] = max |u|+c and per-column alpha_y[i] = max |v|+c over the points of mask
+// `bit` (main_2d_euler(quad).cpp:86-104); with mv != null also the CFL speed
+// max (|u|+c)+(|v|+c) (:61-76).  Tiles of 32 columns x 32 rows; maxima are order-independent.
+__global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t* __restrict__ m, int bit,
+                                               double* ax, double* ay, double* mv, const StepState* st)
+{
+    if (st && st->done) return;
+    __shared__ double col[8][32];
+    __shared__ double cfl[8];
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    double cmax = 0, vmax = 0;
+    for (int r = 0; r < 4; ++r) {
+        const int j = blockIdx.y * 32 + threadIdx.y * 4 + r;
+        double sx = 0;
+        if (i < g.nx && j < g.ny) {
+            const size_t a = g.at(i, j);
+            if ((m[a] >> bit) & 1u) {
+                const double q[4] = {f.p[0][a], f.p[1][a], f.p[2][a], f.p[3][a]};
+                const double c = sound2(q, g.gamma);
+                sx = absd(q[1] / q[0]) + c;
+                const double sy = absd(q[2] / q[0]) + c;
+                cmax = maxd(cmax, sy);
+                vmax = maxd(vmax, sx + sy);
+            }
+        }
+        const double rowmax = warp_max(sx);
+        if (threadIdx.x == 0 && j < g.ny && rowmax > 0) atomic_max_nonneg(&ax[j], rowmax);
+    }
+    col[threadIdx.y][threadIdx.x] = cmax;
+    vmax = warp_max(vmax);
+    if (threadIdx.x == 0) cfl[threadIdx.y] = vmax;
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        double c = col[0][threadIdx.x];
+        for (int y = 1; y < 8; ++y) c = maxd(c, col[y][threadIdx.x]);
+        if (i < g.nx && c > 0) atomic_max_nonneg(&ay[i], c);
+        if (mv && threadIdx.x == 0) {
+            double v = cfl[0];
+            for (int y = 1; y < 8; ++y) v = maxd(v, cfl[y]);
+            if (v > 0) atomic_max_nonneg(mv, v);
+        }
+    }
+}
+
+// dt = cfl dx / max speed, clipped to the output time (main_2d_euler(quad).cpp:76-83), and the
+// per-level stage factor dt / (dx 2^(maxl-lev)) of the RK updates.
+__global__ void k_dt(Grid2 g, StepState* st)
+{
+    if (st->done) return;
+    double dt = st->cfl * g.dx / st->mv;
+    if (st->dt_fixed > 0) dt = st->dt_fixed;
+    st->do_print = 0;
+    if (st->t + dt > st->t_end) {
+        dt = st->t_end - st->t;
+        st->do_print = 1;
+    }
+    st->dt = dt;
+    for (int lev = 0; lev <= g.maxl; ++lev) {
+        const double dxl = g.dx * g.D(lev);
+        st->sc[lev] = dt / dxl;
+    }
+}
+
+__global__ void k_begin(StepState* st)
+{
+    st->done = st->t >= st->t_end ? 1 : 0;
+    if (st->done) return;
+    st->mv = 0;
+    for (int k = 0; k < 4 * kStages; ++k) st->cnt[k] = 0;
+    for (int k = 0; k < 4; ++k) st->mask_cnt[k] = 0;
+}
+
+__global__ void k_finish(StepState* st)
+{
+    if (st->done) return;
+    st->t += st->dt;
+    st->steps += 1;
+    st->upd += st->mask_cnt[0];
+    st->stage_pts += (unsigned long long)st->mask_cnt[2] + st->mask_cnt[1] + st->mask_cnt[0];
+    st->full_zero = 0;
+}
+
+// ------------------------------------------------------------------------------------ worklists
+// Builds, for the three stages (mask2/level2, mask1/level1, mask0/level0), row-ordered lists of
+// finest-level points, coarse points, x faces (i+1/2, j) and y faces (i, j+1/2) whose flux a
+// finest-level point needs.  A CTA covers 256 consecutive columns of kListRows rows of the grid
+// extended by one row/column on the low side (faces -1/2); compaction is a warp ballot, a
+// per-block prefix over warps and one atomicAdd per list per block.
+constexpr int kListRows = 8;
+constexpr int kNumLists = 4 * kStages;
+
+struct ListArgs {
+    uint32_t* list[kNumLists];
+};
+
+__device__ __forceinline__ bool fin_at(const Grid2& g, const uint8_t* m, const int8_t* lvl, int i, int j, int bit)
+{
+    if (i < 0 || i >= g.nx || j < 0 || j >= g.ny) return false;
+    const size_t a = g.at(i, j);
+    return ((m[a] >> bit) & 1u) && lvl[a] == g.maxl;
+}
+
+__global__ void __launch_bounds__(256) k_lists(Grid2 g, const uint8_t* __restrict__ m, const int8_t* __restrict__ l2,
+                                               const int8_t* __restrict__ l1, const int8_t* __restrict__ l0,
+                                               ListArgs la, StepState* st)
+{
+    if (st->done) return;
+    __shared__ unsigned wcnt[8][kNumLists];
+    __shared__ unsigned woff[8][kNumLists];
+    __shared__ unsigned mcnt[4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = (int)blockIdx.x * 256 + threadIdx.x - 1;  // -1 .. nx-1 (+ padding)
+    const int8_t* lvls[3] = {l2, l1, l0};
+    const int bits[3] = {2, 1, 0};
+    if (threadIdx.x < kNumLists)
+        for (int w = 0; w < 8; ++w) wcnt[w][threadIdx.x] = 0;
+    if (threadIdx.x < 4) mcnt[threadIdx.x] = 0;
+    __syncthreads();
+
+    auto preds = [&](int j, bool* p, unsigned& mbits) {
+        mbits = 0;
+        const bool inside = i >= 0 && i < g.nx && j >= 0 && j < g.ny;
+        if (inside) mbits = m[g.at(i, j)] & 15u;
+#pragma unroll
+        for (int s = 0; s < kStages; ++s) {
+            const int bit = bits[s];
+            const int8_t* lvl = lvls[s];
+            bool act = false, fin = false;
+            if (inside) {
+                act = (mbits >> bit) & 1u;
+                fin = act && lvl[g.at(i, j)] == g.maxl;
+            }
+            p[4 * s + 0] = fin;
+            p[4 * s + 1] = act && !fin;
+            p[4 * s + 2] = j >= 0 && j < g.ny && i <= g.nx - 1 && (fin || fin_at(g, m, lvl, i + 1, j, bit));
+            p[4 * s + 3] = i >= 0 && i < g.nx && j <= g.ny - 1 && (fin || fin_at(g, m, lvl, i, j + 1, bit));
+        }
+    };
+
+    const int j0 = (int)blockIdx.y * kListRows - 1;
+    unsigned mloc[4] = {0, 0, 0, 0};
+    for (int r = 0; r < kListRows; ++r) {
+        const int j = j0 + r;
+        bool p[kNumLists];
+        unsigned mb;
+        preds(j, p, mb);
+        if (j >= 0 && i >= 0)
+            for (int k = 0; k < 4; ++k) mloc[k] += (mb >> k) & 1u;
+#pragma unroll
+        for (int L = 0; L < kNumLists; ++L) {
+            const unsigned bal = __ballot_sync(0xffffffffu, p[L]);
+            if (lane == 0) wcnt[warp][L] += __popc(bal);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        unsigned v = mloc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(&mcnt[k], v);
+    }
+    __syncthreads();
+    if (threadIdx.x < kNumLists) {
+        const int L = threadIdx.x;
+        unsigned tot = 0;
+        for (int w = 0; w < 8; ++w) {
+            woff[w][L] = tot;
+            tot += wcnt[w][L];
+        }
+        const unsigned base = tot ? atomicAdd(&st->cnt[L], tot) : 0;
+        for (int w = 0; w < 8; ++w) woff[w][L] += base;
+    }
+    if (threadIdx.x < 4 && mcnt[threadIdx.x]) atomicAdd(&st->mask_cnt[threadIdx.x], mcnt[threadIdx.x]);
+    __syncthreads();
+    unsigned run[kNumLists];
+#pragma unroll
+    for (int L = 0; L < kNumLists; ++L) run[L] = woff[warp][L];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int r = 0; r < kListRows; ++r) {
+        const int j = j0 + r;
+        bool p[kNumLists];
+        unsigned mb;
+        preds(j, p, mb);
+        const uint32_t idx = (uint32_t)((size_t)(j + kGhost) * g.pitch + (size_t)(i + kGhost));
+#pragma unroll
+        for (int L = 0; L < kNumLists; ++L) {
+            const unsigned bal = __ballot_sync(0xffffffffu, p[L]);
+            if (p[L]) la.list[L][run[L] + __popc(bal & lt)] = idx;
+            run[L] += __popc(bal);
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------- stage kernels
+// Face flux from the compacted face list: x faces (DIR 0) read cells i-2..i+3 of row j, y faces
+// (DIR 1) cells j-2..j+3 of column i (WENOZ_EULER_SOLVER_2D::ComputeFluxX/Y, WENOZ.h:236-320).
+template <int DIR>
+__global__ void __launch_bounds__(128) k_face(Grid2 g, Field4 f, Field4 out, const uint32_t* __restrict__ list,
+                                              const unsigned* __restrict__ count, const double* __restrict__ alpha,
+                                              const StepState* st)
+{
+    if (st->done) return;
+    const unsigned n = *count;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long e = gtid(); e < n; e += stride) {
+        const uint32_t idx = list[e];
+        const int ii = (int)(idx % (uint32_t)g.pitch) - kGhost;
+        const int jj = (int)(idx / (uint32_t)g.pitch) - kGhost;
+        const long step = DIR == 0 ? 1 : g.pitch;
+        double s[6][4];
+#pragma unroll
+        for (int p = 0; p < 6; ++p) {
+            const long a = (long)idx + (p - 2) * step;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) s[p][k] = f.p[k][a];
+        }
+        const double al = DIR == 0 ? alpha[jj] : alpha[ii];
+        double o[4];
+        face_flux_2d<DIR>(s, al, g.gamma, o);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) out.p[k][idx] = o[k];
+    }
+}
+
+// RK combinations of the three stages (main_2d_euler(quad).cpp:162, 242, 321 and 325-332):
+// KIND 1: out = in - sc (dF+dG); KIND 2: out = 0.75 qn + 0.25 (in - sc (dF+dG));
+// KIND 3: qn = (qn + 2 (in - sc (dF+dG))) / 3.
+template <int KIND>
+__device__ __forceinline__ void rk_store(Field4 in, Field4 out, Field4 qn, size_t a, const double* dF,
+                                         const double* dG, double sc)
+{
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double r = in.p[k][a] - sc * (dF[k] + dG[k]);
+        if (KIND == 1) out.p[k][a] = r;
+        else if (KIND == 2) out.p[k][a] = 0.75 * qn.p[k][a] + 0.25 * r;
+        else qn.p[k][a] = (qn.p[k][a] + 2.0 * r) / 3.0;
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(256) k_update_fin(Grid2 g, Field4 in, Field4 out, Field4 qn, Field4 fx, Field4 fy,
+                                                    const uint32_t* __restrict__ list,
+                                                    const unsigned* __restrict__ count, const StepState* st)
+{
+    if (st->done) return;
+    const unsigned n = *count;
+    const double sc = st->sc[g.maxl];
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long e = gtid(); e < n; e += stride) {
+        const size_t a = list[e];
+        double dF[4], dG[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            dF[k] = fx.p[k][a] - fx.p[k][a - 1];
+            dG[k] = fy.p[k][a] - fy.p[k][a - g.pitch];
+        }
+        rk_store<KIND>(in, out, qn, a, dF, dG, sc);
+    }
+}
+
+// Coarse-level points: 4th-order central differences of F and G at spacing d = 2^(maxl-lev), with
+// the reference's one-sided forms next to the boundary (AWCM_2D::Differentiate*, Wavelet/AWCM_2D.h:154-187,
+// branch selection main_2d_euler(quad).cpp:132-160).
+template <int KIND>
+__global__ void __launch_bounds__(256) k_update_crs(Grid2 g, Field4 in, Field4 out, Field4 qn,
+                                                    const int8_t* __restrict__ lvl,
+                                                    const uint32_t* __restrict__ list,
+                                                    const unsigned* __restrict__ count, const StepState* st)
+{
+    if (st->done) return;
+    const unsigned n = *count;
+    const long stride = (long)gridDim.x * blockDim.x;
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    for (long e = gtid(); e < n; e += stride) {
+        const size_t a = list[e];
+        const int i = (int)(a % (size_t)g.pitch) - kGhost;
+        const int j = (int)(a / (size_t)g.pitch) - kGhost;
+        const int lev = lvl[a];
+        if (lev < 0 || lev > g.maxl) continue;
+        const int d = g.D(lev);
+        // Coarse stencils stay on the ghosted grid whenever the levels come from ComputeLevel on
+        // a reconstruction-closed mask; any other point is skipped rather than read out of bounds.
+        const int lo_x = i <= d ? i - d : i - 2 * d, hi_x = i >= NX - d && !(i <= d) ? i + d : i + 2 * d;
+        const int lo_y = j <= d ? j - d : j - 2 * d, hi_y = j >= NY - d && !(j <= d) ? j + d : j + 2 * d;
+        if (lo_x < -kGhost || hi_x > NX + kGhost || lo_y < -kGhost || hi_y > NY + kGhost) continue;
+        double dF[4], dG[4];
+        {
+            double fl[4], fr[4], fo[4], q[4];
+            auto load = [&](long off, double* o) {
+                for (int k = 0; k < 4; ++k) q[k] = in.p[k][(long)a + off];
+                flux2<0>(q, g.gamma, o);
+            };
+            load(-d, fl);
+            load(d, fr);
+            if (i <= d) {
+                load(2 * d, fo);
+                for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fo[k] - fl[k]);
+            } else if (i >= NX - d) {
+                load(-2 * d, fo);
+                for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fr[k] - fo[k]);
+            } else {
+                double fll[4];
+                load(-2 * d, fll);
+                load(2 * d, fo);
+                for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fo[k] - fll[k]);
+            }
+        }
+        {
+            const long P = g.pitch;
+            double gb[4], gt[4], go[4], q[4];
+            auto load = [&](long off, double* o) {
+                for (int k = 0; k < 4; ++k) q[k] = in.p[k][(long)a + off * P];
+                flux2<1>(q, g.gamma, o);
+            };
+            load(-d, gb);
+            load(d, gt);
+            if (j <= d) {
+                load(2 * d, go);
+                for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (go[k] - gb[k]);
+            } else if (j >= NY - d) {
+                load(-2 * d, go);
+                for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (gt[k] - go[k]);
+            } else {
+                double gbb[4];
+                load(-2 * d, gbb);
+                load(2 * d, go);
+                for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (go[k] - gbb[k]);
+            }
+        }
+        rk_store<KIND>(in, out, qn, a, dF, dG, st->sc[lev]);
+    }
+}
+
+// ------------------------------------------------------------------------- layout conversions
+__global__ void k_aos_to_soa(Grid2 g, const double* __restrict__ aos, Field4 f)
+{
+    const long t = gtid();
+    const int w = g.nx + 2 * kGhost;
+    if (t >= (long)w * (g.ny + 2 * kGhost)) return;
+    const int ii = (int)(t % w), jj = (int)(t / w);
+    const size_t a = (size_t)jj * g.pitch + ii;
+    for (int k = 0; k < 4; ++k) f.p[k][a] = aos[t * 4 + k];
+}
+
+__global__ void k_soa_to_aos(Grid2 g, Field4 f, double* __restrict__ aos)
+{
+    const long t = gtid();
+    const int w = g.nx + 2 * kGhost;
+    if (t >= (long)w * (g.ny + 2 * kGhost)) return;
+    const int ii = (int)(t % w), jj = (int)(t / w);
+    const size_t a = (size_t)jj * g.pitch + ii;
+    for (int k = 0; k < 4; ++k) aos[t * 4 + k] = f.p[k][a];
+}
+
+// masks: 5 planes (mask_temp, mask0..mask3) of (ny+6) x (nx+6) bytes <-> bit byte per point.
+__global__ void k_pack_masks(Grid2 g, const uint8_t* __restrict__ planes, uint8_t* m)
+{
+    const long t = gtid();
+    const int w = g.nx + 2 * kGhost;
+    const long n = (long)w * (g.ny + 2 * kGhost);
+    if (t >= n) return;
+    const int ii = (int)(t % w), jj = (int)(t / w);
+    const int bits[5] = {kBitTemp, 0, 1, 2, 3};
+    unsigned v = (1u << kBitInterp) | (1u << kBitCopy) | (1u << 7);
+    for (int r = 0; r < 5; ++r) v |= (unsigned)(planes[r * n + t] != 0) << bits[r];
+    const bool ghost = ii < kGhost || ii >= g.nx + kGhost || jj < kGhost || jj >= g.ny + kGhost;
+    if (!ghost) v &= ~((1u << kBitInterp) | (1u << kBitCopy) | (1u << 7));
+    m[(size_t)jj * g.pitch + ii] = (uint8_t)v;
+}
+
+__global__ void k_unpack_masks(Grid2 g, const uint8_t* m, uint8_t* __restrict__ planes)
+{
+    const long t = gtid();
+    const int w = g.nx + 2 * kGhost;
+    const long n = (long)w * (g.ny + 2 * kGhost);
+    if (t >= n) return;
+    const int ii = (int)(t % w), jj = (int)(t / w);
+    const int bits[5] = {kBitTemp, 0, 1, 2, 3};
+    const unsigned v = m[(size_t)jj * g.pitch + ii];
+    for (int r = 0; r < 5; ++r) planes[r * n + t] = (v >> bits[r]) & 1u;
+}
+
+__global__ void k_levels_in(Grid2 g, const int* __restrict__ lv, int8_t* l0, int8_t* l1, int8_t* l2, int8_t* l3)
+{
+    const long t = gtid();
+    const long n = (long)g.nx * g.ny;
+    if (t >= n) return;
+    const size_t a = g.at((int)(t % g.nx), (int)(t / g.nx));
+    l0[a] = (int8_t)lv[t];
+    l1[a] = (int8_t)lv[n + t];
+    l2[a] = (int8_t)lv[2 * n + t];
+    l3[a] = (int8_t)lv[3 * n + t];
+}
+
+__global__ void k_levels_out(Grid2 g, const int8_t* l0, const int8_t* l1, const int8_t* l2, const int8_t* l3,
+                             int* __restrict__ lv)
+{
+    const long t = gtid();
+    const long n = (long)g.nx * g.ny;
+    if (t >= n) return;
+    const size_t a = g.at((int)(t % g.nx), (int)(t / g.nx));
+    lv[t] = l0[a];
+    lv[n + t] = l1[a];
+    lv[2 * n + t] = l2[a];
+    lv[3 * n + t] = l3[a];
+}
+
+__global__ void k_fill_u8(uint8_t* p, size_t n, uint8_t v)
+{
+    const size_t a = (size_t)gtid();
+    if (a < n) p[a] = v;
+}
+
+__global__ void k_fill_i8(int8_t* p, size_t n, int8_t v)
+{
+    const size_t a = (size_t)gtid();
+    if (a < n) p[a] = v;
+}
+
+// EULER_EQUATION_2D batch entry points.
+__global__ void k_euler_flux(const double* q, double* f, int n, int dir, double gamma)
+{
+    const long t = gtid();
+    if (t >= n) return;
+    double s[4] = {q[4 * t], q[4 * t + 1], q[4 * t + 2], q[4 * t + 3]}, o[4];
+    if (dir == 0) flux2<0>(s, gamma, o);
+    else flux2<1>(s, gamma, o);
+    for (int k = 0; k < 4; ++k) f[4 * t + k] = o[k];
+}
+
+__global__ void k_euler_sr(const double* q, double* out, int n, int dir, double gamma)
+{
+    const long t = gtid();
+    if (t >= n) return;
+    const double s[4] = {q[4 * t], q[4 * t + 1], q[4 * t + 2], q[4 * t + 3]};
+    const double c = sound2(s, gamma);
+    out[t] = absd((dir == 0 ? s[1] : s[2]) / s[0]) + c;
+}
+
+inline unsigned blocks_for(long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace
+
+// ===================================================================================== Solver2D
+struct Solver2D {
+    Grid2 g{};
+    size_t plane = 0;
+    Field4 q{}, q2{}, q1{}, fx{}, fy{};
+    uint8_t* m = nullptr;
+    int8_t* lvl[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* ax[kStages] = {};
+    double* ay[kStages] = {};
+    StepState* st = nullptr;
+    uint32_t* lists[kNumLists] = {};
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int launches = 0;
+    int device = 0;
+    int list_rows_blocks = 0;
+    int face_blocks = 0;
+
+    ~Solver2D() { release(); }
+
+    void release()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        auto fr = [](void* p) {
+            if (p) cudaFree(p);
+        };
+        for (int k = 0; k < 4; ++k) {
+            fr(q.p[k]);
+            fr(q2.p[k]);
+            fr(q1.p[k]);
+            fr(fx.p[k]);
+            fr(fy.p[k]);
+            fr(lvl[k]);
+        }
+        fr(m);
+        for (int s = 0; s < kStages; ++s) {
+            fr(ax[s]);
+            fr(ay[s]);
+        }
+        fr(st);
+        for (auto& l : lists) fr(l);
+        fr(staging);
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+
+    int create(int num_levels, int nxc, int nyc, double x_min, double x_max, double y_min, double y_max, int bc)
+    {
+        if (num_levels < 2 || num_levels > kMaxLevels - 1 || nxc < 5 || nyc < 5) return kErrArg;
+        if (bc < 0 || bc > 2) return kErrArg;
+        const long nx = (long)(nxc - 1) * (1L << (num_levels - 1)) + 1;
+        const long ny = (long)(nyc - 1) * (1L << (num_levels - 1)) + 1;
+        const long pitch = ((nx + 2 * kGhost + 31) / 32) * 32;
+        if ((pitch * (ny + 2 * kGhost)) >= (1L << 32)) return kErrArg;
+        AWCM_CUDA_TRY(cudaGetDevice(&device));
+        g.nx = (int)nx;
+        g.ny = (int)ny;
+        g.maxl = num_levels - 1;
+        g.pitch = (int)pitch;
+        g.rows = (int)(ny + 2 * kGhost);
+        g.bc_kind = bc;
+        g.x_min = x_min;
+        g.y_min = y_min;
+        g.dx = (x_max - x_min) / (nx - 1);
+        g.dy = (y_max - y_min) / (ny - 1);
+        g.gamma = 1.4;
+        g.W = make_weights();
+        plane = (size_t)g.pitch * g.rows;
+        AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        for (int k = 0; k < 4; ++k) {
+            AWCM_CUDA_TRY(cudaMalloc(&q.p[k], plane * sizeof(double)));
+            AWCM_CUDA_TRY(cudaMalloc(&q2.p[k], plane * sizeof(double)));
+            AWCM_CUDA_TRY(cudaMalloc(&q1.p[k], plane * sizeof(double)));
+            AWCM_CUDA_TRY(cudaMalloc(&fx.p[k], plane * sizeof(double)));
+            AWCM_CUDA_TRY(cudaMalloc(&fy.p[k], plane * sizeof(double)));
+            AWCM_CUDA_TRY(cudaMalloc(&lvl[k], plane));
+            AWCM_CUDA_TRY(cudaMemsetAsync(q.p[k], 0, plane * sizeof(double), stream));
+            AWCM_CUDA_TRY(cudaMemsetAsync(q2.p[k], 0, plane * sizeof(double), stream));
+            AWCM_CUDA_TRY(cudaMemsetAsync(q1.p[k], 0, plane * sizeof(double), stream));
+            AWCM_CUDA_TRY(cudaMemsetAsync(fx.p[k], 0, plane * sizeof(double), stream));
+            AWCM_CUDA_TRY(cudaMemsetAsync(fy.p[k], 0, plane * sizeof(double), stream));
+        }
+        AWCM_CUDA_TRY(cudaMalloc(&m, plane));
+        for (int s = 0; s < kStages; ++s) {
+            AWCM_CUDA_TRY(cudaMalloc(&ax[s], sizeof(double) * g.ny));
+            AWCM_CUDA_TRY(cudaMalloc(&ay[s], sizeof(double) * g.nx));
+        }
+        AWCM_CUDA_TRY(cudaMalloc(&st, sizeof(StepState)));
+        AWCM_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(StepState), stream));
+        const size_t cap = (size_t)(g.nx + 2) * (g.ny + 2);
+        for (auto& l : lists) AWCM_CUDA_TRY(cudaMalloc(&l, cap * sizeof(uint32_t)));
+        // AWCM_2D's constructor: every mask byte all ones on the ghosts, mask0 true inside, all
+        // levels at the finest level (Wavelet/AWCM_2D.h:26-41).
+        k_fill_u8<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, 0xff);
+        for (int k = 0; k < 4; ++k) k_fill_i8<<<blocks_for((long)plane, 256), 256, 0, stream>>>(lvl[k], plane, (int8_t)g.maxl);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        {
+            // AWCM_2D's constructor (Wavelet/AWCM_2D.h:26-37): mask0 true on every point, ghosts
+            // included; mask_temp and mask1..mask3 false everywhere.
+            const size_t n = (size_t)(g.nx + 6) * (g.ny + 6);
+            std::vector<uint8_t> planes(5 * n, 0);
+            for (size_t t = 0; t < n; ++t) planes[n + t] = 1;
+            int rc = set_masks(planes.data());
+            if (rc) return rc;
+        }
+        int dev_sms = 148;
+        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
+        face_blocks = dev_sms * 8;
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int ensure_staging(size_t bytes)
+    {
+        if (bytes <= staging_bytes) return kOk;
+        if (staging) cudaFree(staging);
+        staging = nullptr;
+        staging_bytes = 0;
+        AWCM_CUDA_TRY(cudaMalloc(&staging, bytes));
+        staging_bytes = bytes;
+        return kOk;
+    }
+
+    size_t ghosted_points() const { return (size_t)(g.nx + 6) * (g.ny + 6); }
+
+    int set_q(const double* host)
+    {
+        const size_t n = ghosted_points();
+        int rc = ensure_staging(n * 4 * sizeof(double));
+        if (rc) return rc;
+        AWCM_CUDA_TRY(cudaMemcpyAsync(staging, host, n * 4 * sizeof(double), cudaMemcpyHostToDevice, stream));
+        k_aos_to_soa<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, (const double*)staging, q);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        mark_full_zero();
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int get_q(double* host)
+    {
+        const size_t n = ghosted_points();
+        int rc = ensure_staging(n * 4 * sizeof(double));
+        if (rc) return rc;
+        k_soa_to_aos<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, q, (double*)staging);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaMemcpyAsync(host, staging, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int set_masks(const uint8_t* host)
+    {
+        const size_t n = ghosted_points();
+        int rc = ensure_staging(5 * n);
+        if (rc) return rc;
+        AWCM_CUDA_TRY(cudaMemcpyAsync(staging, host, 5 * n, cudaMemcpyHostToDevice, stream));
+        k_pack_masks<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, (const uint8_t*)staging, m);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        mark_full_zero();
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int get_masks(uint8_t* host)
+    {
+        const size_t n = ghosted_points();
+        int rc = ensure_staging(5 * n);
+        if (rc) return rc;
+        k_unpack_masks<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, m, (uint8_t*)staging);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaMemcpyAsync(host, staging, 5 * n, cudaMemcpyDeviceToHost, stream));
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int set_levels(const int* host)
+    {
+        const size_t n = (size_t)g.nx * g.ny;
+        int rc = ensure_staging(4 * n * sizeof(int));
+        if (rc) return rc;
+        AWCM_CUDA_TRY(cudaMemcpyAsync(staging, host, 4 * n * sizeof(int), cudaMemcpyHostToDevice, stream));
+        k_levels_in<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, (const int*)staging, lvl[0], lvl[1], lvl[2], lvl[3]);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int get_levels(int* host)
+    {
+        const size_t n = (size_t)g.nx * g.ny;
+        int rc = ensure_staging(4 * n * sizeof(int));
+        if (rc) return rc;
+        k_levels_out<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, lvl[0], lvl[1], lvl[2], lvl[3], (int*)staging);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaMemcpyAsync(host, staging, 4 * n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    void mark_full_zero()
+    {
+        // After an external write the sparse residue removal's invariant (values only inside
+        // mask3 or the previous mask0) is not known to hold: the next step zeroes densely.
+        const int one = 1;
+        cudaMemcpyAsync(&st->full_zero, &one, sizeof(int), cudaMemcpyHostToDevice, stream);
+    }
+
+    // ---------------------------------------------------------------- enqueue helpers
+    long grid_points() const { return (long)g.nx * g.ny; }
+
+    void enq_cr(int bit, const StepState* s)
+    {
+        for (int lev = g.maxl - 1; lev >= 0; --lev) {
+            const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1);
+            k_cr<0><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, m, lev, bit, s);
+            k_cr<1><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, m, lev, bit, s);
+            launches += 2;
+        }
+    }
+
+    void enq_fwt(const StepState* s)
+    {
+        for (int lev = g.maxl - 1; lev >= 0; --lev) {
+            const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1), bc = band_of(g, lev, 3);
+            k_fwt<0><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, s);
+            k_fwt<1><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, s);
+            k_fwt<2><<<blocks_for((long)bc.cx * bc.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, s);
+            launches += 3;
+        }
+    }
+
+    void enq_iwt(int bit, const StepState* s)
+    {
+        for (int lev = 0; lev < g.maxl; ++lev) {
+            const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1), bc = band_of(g, lev, 3);
+            k_iwt<0><<<blocks_for((long)bc.cx * bc.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            k_iwt<1><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            k_iwt<2><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            launches += 3;
+        }
+    }
+
+    void enq_interp(int from, int to, const StepState* s)
+    {
+        k_interp_init<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, m, from, to, s);
+        launches += 1;
+        enq_cr(kBitInterp, s);
+        for (int lev = 0; lev < g.maxl; ++lev) {
+            const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1);
+            k_interp<0><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+            k_interp<1><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+            launches += 2;
+        }
+    }
+
+    void enq_aaz(int bit, const StepState* s)
+    {
+        k_copy_bit_all<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, bit, kBitCopy, s);
+        k_aaz<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, m, bit, kBitCopy, s);
+        launches += 2;
+    }
+
+    // AWCM_2D::PrepareEuler (Wavelet/AWCM_2D.h:114-147).
+    void enq_prepare(const StepState* s)
+    {
+        const long np = grid_points();
+        k_copy_bit_all<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, 0, kBitTemp, s);
+        launches += 1;
+        enq_fwt(s);
+        k_band_copy<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
+        k_aaz<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
+        launches += 2;
+        enq_cr(0, s);
+        for (int k = 1; k <= 3; ++k) {
+            k_cl<<<blocks_for((long)plane, 256), 256, 0, stream>>>(g, m, lvl[k - 1], k - 1, k, plane, s);
+            k_apd<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, lvl[k - 1], k, k - 1, s);
+            launches += 2;
+            enq_cr(k, s);
+        }
+        enq_iwt(3, s);
+        enq_interp(kBitTemp, 3, s);
+    }
+
+    void enq_bc(Field4 f, const StepState* s)
+    {
+        const long n = 2L * kGhost * g.ny + 2L * kGhost * g.nx;
+        k_bc<<<blocks_for(n, 256), 256, 0, stream>>>(g, f, s, 0.0);
+        launches += 1;
+    }
+
+    void enq_alpha(Field4 f, int bit, int stage, bool with_cfl)
+    {
+        cudaMemsetAsync(ax[stage], 0, sizeof(double) * g.ny, stream);
+        cudaMemsetAsync(ay[stage], 0, sizeof(double) * g.nx, stream);
+        dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32), block(32, 8);
+        k_alpha<<<grid, block, 0, stream>>>(g, f, m, bit, ax[stage], ay[stage], with_cfl ? &st->mv : nullptr, st);
+        launches += 1;
+    }
+
+    void enq_faces_update(int stage, Field4 in, Field4 out)
+    {
+        uint32_t* const* L = lists + 4 * stage;
+        const unsigned* C = st->cnt + 4 * stage;
+        k_face<0><<<face_blocks, 128, 0, stream>>>(g, in, fx, L[2], C + 2, ax[stage], st);
+        k_face<1><<<face_blocks, 128, 0, stream>>>(g, in, fy, L[3], C + 3, ay[stage], st);
+        launches += 2;
+        const int ub = face_blocks / 2;
+        if (stage == 0) {
+            k_update_fin<1><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            k_update_crs<1><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[2], L[1], C + 1, st);
+        } else if (stage == 1) {
+            k_update_fin<2><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            k_update_crs<2><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[1], L[1], C + 1, st);
+        } else {
+            k_update_fin<3><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            k_update_crs<3><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[0], L[1], C + 1, st);
+        }
+        launches += 2;
+    }
+
+    // One pass of the driver loop (main_2d_euler(quad).cpp:58-334).
+    void enq_step()
+    {
+        launches = 0;
+        k_begin<<<1, 1, 0, stream>>>(st);
+        launches += 1;
+        enq_prepare(st);
+        enq_bc(q, st);
+        enq_alpha(q, 3, 0, true);
+        k_dt<<<1, 1, 0, stream>>>(g, st);
+        launches += 1;
+        {
+            ListArgs la;
+            for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
+            dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
+            k_lists<<<grid, 256, 0, stream>>>(g, m, lvl[2], lvl[1], lvl[0], la, st);
+            launches += 1;
+        }
+        enq_faces_update(0, q, q2);
+        enq_bc(q2, st);
+        enq_alpha(q2, 2, 1, false);
+        enq_faces_update(1, q2, q1);
+        enq_bc(q1, st);
+        enq_alpha(q1, 1, 2, false);
+        enq_faces_update(2, q1, q1);
+        k_remove_residue<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, q, m, 0, 1, st);
+        k_finish<<<1, 1, 0, stream>>>(st);
+        launches += 2;
+    }
+
+    int build_graph()
+    {
+        if (graph) return kOk;
+        cudaGraph_t gr;
+        AWCM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        enq_step();
+        cudaError_t e = cudaStreamEndCapture(stream, &gr);
+        if (e != cudaSuccess) {
+            set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+            return kErrCuda;
+        }
+        e = cudaGraphInstantiate(&graph, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) {
+            set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+            return kErrCuda;
+        }
+        return kOk;
+    }
+
+    int write_params(double tol, double cfl, double t, double t_end, double dt_fixed)
+    {
+        StepState h;
+        AWCM_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof(StepState), cudaMemcpyDeviceToHost, stream));
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        h.tol = tol;
+        h.cfl = cfl;
+        h.t = t;
+        h.t_end = t_end;
+        h.dt_fixed = dt_fixed;
+        h.done = 0;
+        AWCM_CUDA_TRY(cudaMemcpyAsync(st, &h, sizeof(StepState), cudaMemcpyHostToDevice, stream));
+        return kOk;
+    }
+
+    int read_state(StepState* h)
+    {
+        AWCM_CUDA_TRY(cudaMemcpyAsync(h, st, sizeof(StepState), cudaMemcpyDeviceToHost, stream));
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int step(double tol, double cfl, double t, double t_next, double dt_fixed, double* out)
+    {
+        int rc = build_graph();
+        if (rc) return rc;
+        rc = write_params(tol, cfl, t, t_next, dt_fixed);
+        if (rc) return rc;
+        AWCM_CUDA_TRY(cudaGraphLaunch(graph, stream));
+        StepState h;
+        rc = read_state(&h);
+        if (rc) return rc;
+        if (out) {
+            out[0] = h.dt;
+            out[1] = h.do_print;
+            for (int k = 0; k < 4; ++k) out[2 + k] = h.mask_cnt[k];
+            out[6] = h.mv;
+            out[7] = 0;
+        }
+        return kOk;
+    }
+
+    int advance(double tol, double cfl, double t_start, double t_end, int n_steps, double* out)
+    {
+        int rc = build_graph();
+        if (rc) return rc;
+        rc = write_params(tol, cfl, t_start, t_end, 0.0);
+        if (rc) return rc;
+        StepState h0;
+        rc = read_state(&h0);
+        if (rc) return rc;
+        for (int s = 0; s < n_steps; ++s) AWCM_CUDA_TRY(cudaGraphLaunch(graph, stream));
+        StepState h;
+        rc = read_state(&h);
+        if (rc) return rc;
+        if (out) {
+            out[0] = h.t;
+            out[1] = h.steps - h0.steps;
+            out[2] = (double)(h.upd - h0.upd);
+            out[3] = (double)(h.stage_pts - h0.stage_pts);
+        }
+        return kOk;
+    }
+
+    int prepare(double tol)
+    {
+        int rc = write_params(tol, 0, 0, 1, 0);
+        if (rc) return rc;
+        k_begin<<<1, 1, 0, stream>>>(st);
+        enq_prepare(st);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int fwt(double tol)
+    {
+        int rc = write_params(tol, 0, 0, 1, 0);
+        if (rc) return rc;
+        k_begin<<<1, 1, 0, stream>>>(st);
+        enq_fwt(st);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    static int bit_of(int mask_id) { return mask_id >= 0 && mask_id <= 3 ? mask_id : kBitTemp; }
+
+    int iwt(int mask_id)
+    {
+        enq_iwt(bit_of(mask_id), nullptr);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int interpolate(int from_id, int to_id)
+    {
+        enq_interp(bit_of(from_id), bit_of(to_id), nullptr);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int manager(int op, int mask_id, int level_id)
+    {
+        const int b = bit_of(mask_id);
+        const long np = grid_points();
+        if (level_id < 0 || level_id > 3) return kErrArg;
+        switch (op) {
+            case 0: enq_aaz(b, nullptr); break;
+            case 1: enq_cr(b, nullptr); break;
+            case 2:
+                k_copy_bit_all<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, b, kBitCopy, nullptr);
+                k_apd<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, lvl[level_id], b, kBitCopy, nullptr);
+                break;
+            case 3: k_cl<<<blocks_for((long)plane, 256), 256, 0, stream>>>(g, m, lvl[level_id], b, -1, plane, nullptr); break;
+            case 4: k_remove_residue<<<blocks_for(np, 256), 256, 0, stream>>>(g, q, m, b, 0, nullptr); break;
+            case 5: k_band_copy<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, b, -1, nullptr); break;
+            default: return kErrArg;
+        }
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int apply_bc(double t)
+    {
+        const long n = 2L * kGhost * g.ny + 2L * kGhost * g.nx;
+        k_bc<<<blocks_for(n, 256), 256, 0, stream>>>(g, q, nullptr, t);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    int init_problem(int kind, double a, double b)
+    {
+        // Problem initial states (Problems/2D/PROBLEM_QUADRANTS.h:34-80, PROBLEM_DOUBLEMACH.h:34-62,
+        // PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h:38-64), evaluated on the host with the grid's node
+        // coordinates x_min + i dx, ghosts included.
+        const int w = g.nx + 6;
+        std::vector<double> h((size_t)w * (g.ny + 6) * 4);
+        const double gam = g.gamma;
+        const double PI = 4. * std::atan(1.);
+        auto E = [&](double rho, double u, double v, double p) { return p / (gam - 1) + 0.5 * rho * (u * u + v * v); };
+        for (int j = -3; j < g.ny + 3; ++j)
+            for (int i = -3; i < g.nx + 3; ++i) {
+                const double x = g.x_min + i * g.dx, y = g.y_min + j * g.dy;
+                double rho, u, v, p, Q[4];
+                if (kind == AWCM_PROBLEM_QUADRANTS) {
+                    if (x >= a && y >= b) rho = 1.5, u = 0, v = 0, p = 1.5;
+                    else if (x < a && y >= b) rho = 0.532258064516129, u = 1.206045378311055, v = 0, p = 0.3;
+                    else if (x < a && y < b)
+                        rho = 0.137992831541219, u = 1.206045378311055, v = 1.206045378311055, p = 0.029032258064516;
+                    else rho = 0.532258064516129, u = 0, v = 1.206045378311055, p = 0.3;
+                    Q[0] = rho, Q[1] = rho * u, Q[2] = rho * v, Q[3] = E(rho, u, v, p);
+                } else if (kind == AWCM_PROBLEM_DOUBLE_MACH) {
+                    if (y > std::sqrt(3.0) * (x - 1.0 / 6.0)) rho = 8, u = 8.25 * std::sqrt(3.0) * 0.5, v = -8.25 * 0.5, p = 116.5;
+                    else rho = a, u = 0, v = 0, p = 1;
+                    Q[0] = rho, Q[1] = rho * u, Q[2] = rho * v, Q[3] = E(rho, u, v, p);
+                } else if (kind == AWCM_PROBLEM_VORTEX) {
+                    const double rr = (x - a) * (x - a) + (y - b) * (y - b);
+                    const double beta = 5;
+                    rho = 1 - (gam - 1) * (beta * beta) / (8 * gam * PI * PI) * std::exp(1 - rr);
+                    rho = std::pow(rho, 1.0 / (gam - 1.0));
+                    double rhou = 0 - beta / (2 * PI) * std::exp((1 - rr) * 0.5) * (y - b);
+                    rhou *= rho;
+                    double rhov = 1 + beta / (2 * PI) * std::exp((1 - rr) * 0.5) * (x - a);
+                    rhov *= rho;
+                    p = std::pow(rho, gam);
+                    Q[0] = rho, Q[1] = rhou, Q[2] = rhov, Q[3] = E(rho, rhou / rho, rhov / rho, p);
+                } else {
+                    return kErrArg;
+                }
+                for (int k = 0; k < 4; ++k) h[((size_t)(j + 3) * w + (i + 3)) * 4 + k] = Q[k];
+            }
+        return set_q(h.data());
+    }
+};
+
+}  // namespace awcm
+
+// ======================================================================================== C-ABI
+using awcm::Solver2D;
+
+struct awcm2d_s {
+    Solver2D s;
+};
+
+extern "C" {
+
+int awcm2d_create(int num_levels, int nx_coarse, int ny_coarse, double x_min, double x_max, double y_min,
+                  double y_max, int bc_kind, awcm2d_t* out)
+{
+    if (!out) return awcm::kErrArg;
+    *out = nullptr;
+    awcm2d_s* h = new (std::nothrow) awcm2d_s();
+    if (!h) return awcm::kErrOom;
+    const int rc = h->s.create(num_levels, nx_coarse, ny_coarse, x_min, x_max, y_min, y_max, bc_kind);
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return awcm::kOk;
+}
+
+int awcm2d_destroy(awcm2d_t h)
+{
+    delete h;
+    return awcm::kOk;
+}
+
+#define AWCM_H(h)                         \
+    if (!(h)) return awcm::kErrArg;       \
+    cudaSetDevice((h)->s.device)
+
+int awcm2d_dims(awcm2d_t h, int* nx, int* ny)
+{
+    if (!h || !nx || !ny) return awcm::kErrArg;
+    *nx = h->s.g.nx;
+    *ny = h->s.g.ny;
+    return awcm::kOk;
+}
+
+int awcm2d_set_q(awcm2d_t h, const double* q)
+{
+    AWCM_H(h);
+    return q ? h->s.set_q(q) : awcm::kErrArg;
+}
+int awcm2d_get_q(awcm2d_t h, double* q)
+{
+    AWCM_H(h);
+    return q ? h->s.get_q(q) : awcm::kErrArg;
+}
+int awcm2d_get_masks(awcm2d_t h, uint8_t* m)
+{
+    AWCM_H(h);
+    return m ? h->s.get_masks(m) : awcm::kErrArg;
+}
+int awcm2d_set_masks(awcm2d_t h, const uint8_t* m)
+{
+    AWCM_H(h);
+    return m ? h->s.set_masks(m) : awcm::kErrArg;
+}
+int awcm2d_get_levels(awcm2d_t h, int* lv)
+{
+    AWCM_H(h);
+    return lv ? h->s.get_levels(lv) : awcm::kErrArg;
+}
+int awcm2d_set_levels(awcm2d_t h, const int* lv)
+{
+    AWCM_H(h);
+    return lv ? h->s.set_levels(lv) : awcm::kErrArg;
+}
+int awcm2d_init_problem(awcm2d_t h, int kind, double a, double b)
+{
+    AWCM_H(h);
+    return h->s.init_problem(kind, a, b);
+}
+int awcm2d_prepare(awcm2d_t h, double tol)
+{
+    AWCM_H(h);
+    return h->s.prepare(tol);
+}
+int awcm2d_fwt(awcm2d_t h, double tol)
+{
+    AWCM_H(h);
+    return h->s.fwt(tol);
+}
+int awcm2d_iwt(awcm2d_t h, int mask_id)
+{
+    AWCM_H(h);
+    return h->s.iwt(mask_id);
+}
+int awcm2d_interpolate(awcm2d_t h, int from_id, int to_id)
+{
+    AWCM_H(h);
+    return h->s.interpolate(from_id, to_id);
+}
+int awcm2d_manager(awcm2d_t h, int op, int mask_id, int level_id)
+{
+    AWCM_H(h);
+    return h->s.manager(op, mask_id, level_id);
+}
+int awcm2d_apply_bc(awcm2d_t h, double t)
+{
+    AWCM_H(h);
+    return h->s.apply_bc(t);
+}
+int awcm2d_step(awcm2d_t h, double tol, double cfl, double t, double t_next, double dt_fixed, double* out)
+{
+    AWCM_H(h);
+    return h->s.step(tol, cfl, t, t_next, dt_fixed, out);
+}
+int awcm2d_advance(awcm2d_t h, double tol, double cfl, double t_start, double t_end, int n_steps, double* out)
+{
+    AWCM_H(h);
+    if (n_steps < 0) return awcm::kErrArg;
+    return h->s.advance(tol, cfl, t_start, t_end, n_steps, out);
+}
+int awcm2d_launches_per_step(awcm2d_t h, int* n)
+{
+    AWCM_H(h);
+    if (!n) return awcm::kErrArg;
+    int rc = h->s.build_graph();
+    *n = h->s.launches;
+    return rc;
+}
+int awcm2d_stream(awcm2d_t h, void** stream)
+{
+    if (!h || !stream) return awcm::kErrArg;
+    *stream = (void*)h->s.stream;
+    return awcm::kOk;
+}
+
+int euler2d_flux(const double* q_dev, double* f_dev, int n, int dir, double gamma, void* stream)
+{
+    if (n < 0 || (n && (!q_dev || !f_dev)) || (dir != 0 && dir != 1)) return awcm::kErrArg;
+    if (!n) return awcm::kOk;
+    awcm::k_euler_flux<<<awcm::blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(q_dev, f_dev, n, dir, gamma);
+    AWCM_CUDA_TRY(cudaGetLastError());
+    return awcm::kOk;
+}
+
+int euler2d_spectral_radius(const double* q_dev, double* s_dev, int n, int dir, double gamma, void* stream)
+{
+    if (n < 0 || (n && (!q_dev || !s_dev)) || (dir != 0 && dir != 1)) return awcm::kErrArg;
+    if (!n) return awcm::kOk;
+    awcm::k_euler_sr<<<awcm::blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(q_dev, s_dev, n, dir, gamma);
+    AWCM_CUDA_TRY(cudaGetLastError());
+    return awcm::kOk;
+}
+
+}  // extern "C"

@@ -1,0 +1,166 @@
+/*
+ * awcm_b200.h -- C-ABI of the B200-native AWCM compressible-Euler path.
+ *
+ * This is the drop-in boundary for the adaptive wavelet collocation (AWCM) Euler hot path of
+ * doseongju/C_pp-library.  The reference exposes that path as header-only C++ classes with no ABI:
+ * AWCM_1D/AWCM_2D (Wavelet/AWCM_1D.h, Wavelet/AWCM_2D.h), the static passes of AWCM_MANAGER_1D/2D
+ * (Wavelet/AWCM_MANAGER_1D.h, Wavelet/AWCM_MANAGER_2D.h), EULER_EQUATION_1D/2D (EULER_EQUATION.h)
+ * and the BOUNDARY_MANAGER* classes of Problems/, driven by an RK3 loop written inline in main()
+ * (Wavelet/main_1d_euler.cpp:61-260, Wavelet/main_2d_euler(quad).cpp:56-350).  Each entry point
+ * below names the reference interface it replaces.  The C++ mirror classes that keep the
+ * reference's names are in awcm_b200.hpp.
+ *
+ * Conventions
+ *   - Every function returns an int status: 0 ok, AWCM_ERR_* otherwise; awcm_last_error() gives text.
+ *   - State lives on the GPU (one device, the current one at create time).  Host arrays use the
+ *     reference's own memory layout so a caller can hand over its FIELD_UNIFORM_* storage:
+ *       1D conserved state : (Nx+6) x 3 doubles, point i (ghosts -3..Nx+2) at [(i+3)*3 + p]
+ *       2D conserved state : (Ny+6) x (Nx+6) x 4 doubles, point (i,j) at [((j+3)*(Nx+6) + i+3)*4 + p]
+ *       masks              : 5 planes of one byte per ghosted point: mask_temp, mask0..mask3
+ *       levels             : 4 planes of one int per interior point: level0..level3
+ *   - Mask ids: 0..3 = mask0..mask3, 4 = mask_temp.  Level ids 0..3.
+ *   - Arithmetic is IEEE double with the reference's operation order; results are bit-identical
+ *     to the reference's CPU code for identical inputs.
+ */
+#ifndef AWCM_B200_H
+#define AWCM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AWCM_OK 0
+#define AWCM_ERR_ARG 1
+#define AWCM_ERR_OOM 2
+#define AWCM_ERR_CUDA 3
+#define AWCM_ERR_TIMEOUT 4
+#define AWCM_ERR_NONFINITE 5
+#define AWCM_ERR_STATE 6
+
+/* Manager pass op codes (AWCM_MANAGER_1D/2D static methods). */
+#define AWCM_OP_ADD_ADJACENT_ZONE 0            /* AddAdjacentZone(mask)                  */
+#define AWCM_OP_CHECK_RECONSTRUCTION 1         /* CheckReconstruction(mask)              */
+#define AWCM_OP_ADD_POINT_FOR_DIFFERENTIATION 2 /* AddPointForDifferentiation(mask, level) */
+#define AWCM_OP_COMPUTE_LEVEL 3                /* ComputeLevel(level, mask)              */
+#define AWCM_OP_REMOVE_RESIDUE 4               /* RemoveResidue(Euler)(q, mask)          */
+#define AWCM_OP_BANDING 5                      /* BadingBoundary / BandingMask(mask)     */
+
+/* Boundary kinds (BOUNDARY_MANAGER classes of Problems/). */
+#define AWCM_BC_TRANSMISSIVE 0 /* BOUNDARY_MANAGER (1D), BOUNDARY_MANAGER_QUAD (2D)   */
+#define AWCM_BC_DOUBLE_MACH 1  /* BOUNDARY_MANAGER_DMACH::SetBoundaryCondition(t)      */
+#define AWCM_BC_PERIODIC 2     /* BOUNDARY_MANAGER_ISENVORTEX                          */
+
+/* 2D problem initial states (Problems/2D/*::Initialize). */
+#define AWCM_PROBLEM_QUADRANTS 0   /* a, b = split point                      */
+#define AWCM_PROBLEM_DOUBLE_MACH 1 /* a = pre-shock density                   */
+#define AWCM_PROBLEM_VORTEX 2      /* a, b = vortex centre                    */
+
+/* Last error message of the calling thread ("" if none). */
+const char* awcm_last_error(void);
+/* Library version string. */
+const char* awcm_version(void);
+
+/* ------------------------------------------------------------------------------------------- 2D
+ * One 2D AWCM Euler instance: the MRA_GRID_INT_2D dyadic node grid
+ * (Wavelet/MRA_GRID_UNIFORM_2D.h:87-134, Nx = (nx_coarse-1)*2^(num_levels-1)+1), the AWCM_2D
+ * masks/levels (Wavelet/AWCM_2D.h:24-48) and the conserved field with its three RK stage copies. */
+typedef struct awcm2d_s* awcm2d_t;
+
+/* AWCM_2D::AWCM_2D + FIELD_UNIFORM_2D::Initialize(grid, 3) + the boundary manager of bc_kind. */
+int awcm2d_create(int num_levels, int nx_coarse, int ny_coarse, double x_min, double x_max, double y_min,
+                  double y_max, int bc_kind, awcm2d_t* out);
+int awcm2d_destroy(awcm2d_t h);
+int awcm2d_dims(awcm2d_t h, int* nx, int* ny);
+/* Conserved state in the reference layout (host memory), ghosts included. */
+int awcm2d_set_q(awcm2d_t h, const double* q);
+int awcm2d_get_q(awcm2d_t h, double* q);
+int awcm2d_get_masks(awcm2d_t h, uint8_t* masks);
+int awcm2d_set_masks(awcm2d_t h, const uint8_t* masks);
+int awcm2d_get_levels(awcm2d_t h, int* levels);
+int awcm2d_set_levels(awcm2d_t h, const int* levels);
+/* QUADRANTS / DOUBLEMACH / ISENTROPIC_VORTEX_ADVECTION::Initialize (Problems/2D/). */
+int awcm2d_init_problem(awcm2d_t h, int kind, double a, double b);
+
+/* AWCM_2D::PrepareEuler(Q, tol) (Wavelet/AWCM_2D.h:114-147). */
+int awcm2d_prepare(awcm2d_t h, double tol);
+/* WAVELET_2D::ForwardWaveletTransformationEuler(Q, mra, mask0, tol) (Wavelet/WAVELET_2D.h:478-624). */
+int awcm2d_fwt(awcm2d_t h, double tol);
+/* WAVELET_2D::InverseWaveletTransformationEuler(Q, mra, mask) (Wavelet/WAVELET_2D.h:626-782). */
+int awcm2d_iwt(awcm2d_t h, int mask_id);
+/* WAVELET_2D::InterpolateEuler(Q, mra, mask_from, mask_to) (Wavelet/WAVELET_2D.h:784-907). */
+int awcm2d_interpolate(awcm2d_t h, int from_id, int to_id);
+/* AWCM_MANAGER_2D passes (Wavelet/AWCM_MANAGER_2D.h:14-280) and the banding of AWCM_2D.h:122-124. */
+int awcm2d_manager(awcm2d_t h, int op, int mask_id, int level_id);
+/* BOUNDARY_MANAGER_{QUAD,DMACH,ISENVORTEX}::SetBoundaryCondition([t]) on the conserved field. */
+int awcm2d_apply_bc(awcm2d_t h, double t);
+
+/* One pass of the reference driver loop (Wavelet/main_2d_euler(quad).cpp:58-334): PrepareEuler,
+ * CFL dt (clipped to t_next), three SSP-RK3 stages with WENO-Z/Roe fluxes on the finest level and
+ * 4th-order central differences on coarser levels, PostProcessEuler.  dt_fixed > 0 replaces the
+ * CFL step.  out[8]: dt, do_print, |mask0..mask3|, max wave speed, (unused).  Synchronous. */
+int awcm2d_step(awcm2d_t h, double tol, double cfl, double t, double t_next, double dt_fixed, double* out);
+/* Advances n_steps steps from the device-held time without host round trips (one CUDA graph per
+ * step), stopping early once t >= t_end.  out[4]: final t, steps taken, sum |mask0| over the steps,
+ * sum of stage points (|mask2|+|mask1|+|mask0|). */
+int awcm2d_advance(awcm2d_t h, double tol, double cfl, double t_start, double t_end, int n_steps, double* out);
+/* Kernel launches enqueued by one step (for instrumentation). */
+int awcm2d_launches_per_step(awcm2d_t h, int* n);
+/* CUDA stream the instance runs on (cudaStream_t), for event timing by the caller. */
+int awcm2d_stream(awcm2d_t h, void** stream);
+
+/* ------------------------------------------------------------------------------------------- 1D
+ * A batch of independent 1D AWCM Euler instances (AWCM_1D, Wavelet/AWCM_1D.h, on
+ * MRA_GRID_INT_1D, Wavelet/MRA_GRID_UNIFORM_1D.h:70-98), each with its own finest level, CFL step
+ * and end time.  One RK3 step of all instances is ONE persistent kernel launch (one CTA advances
+ * one instance through PrepareEuler, the three stages and PostProcessEuler); a batch of one is the
+ * plain single-instance form of Wavelet/main_1d_euler.cpp:61-260.  Instances are indexed 0..count-1.
+ * scheme 0 = WENO-Z face fluxes (WENOZ_EULER_SOLVER_1D::ComputeFlux, WENOZ.h:160-205),
+ * scheme 1 = the shipped driver's WENO5 ComputedF (WENO.h:176-184). */
+typedef struct awcm1d_batch_s* awcm1d_batch_t;
+
+/* x_min/x_max: first and last node of each instance's cell-centred grid (GRID_UNIFORM_1D). */
+int awcm1d_batch_create(int count, const int* num_levels, const int* nx_coarse, const double* x_min,
+                        const double* x_max, double gamma, int scheme, awcm1d_batch_t* out);
+int awcm1d_batch_destroy(awcm1d_batch_t h);
+int awcm1d_batch_count(awcm1d_batch_t h, int* n);
+int awcm1d_batch_nx(awcm1d_batch_t h, int k, int* nx);
+int awcm1d_batch_set_q(awcm1d_batch_t h, int k, const double* q);
+int awcm1d_batch_get_q(awcm1d_batch_t h, int k, double* q);
+int awcm1d_batch_get_masks(awcm1d_batch_t h, int k, uint8_t* masks);
+int awcm1d_batch_set_masks(awcm1d_batch_t h, int k, const uint8_t* masks);
+int awcm1d_batch_get_levels(awcm1d_batch_t h, int k, int* levels);
+int awcm1d_batch_set_levels(awcm1d_batch_t h, int k, const int* levels);
+/* SHOCKTUBE::Initialize (Problems/1D/PROBLEM_SHOCKTUBE.h:14-54) with interface and (rho,u,p) states. */
+int awcm1d_batch_init_riemann(awcm1d_batch_t h, int k, double x_interface, const double* left3,
+                              const double* right3);
+/* Per-instance tolerance, CFL number, current time and end (output) time; dt_fixed > 0 overrides CFL. */
+int awcm1d_batch_set_run(awcm1d_batch_t h, const double* tol, const double* cfl, const double* t,
+                         const double* t_end, double dt_fixed);
+/* Enqueues n_steps RK3 steps of every unfinished instance (one CUDA graph replay per step). */
+int awcm1d_batch_steps(awcm1d_batch_t h, int n_steps);
+int awcm1d_batch_sync(awcm1d_batch_t h);
+/* out[16]: t, dt, do_print, done, steps, |mask0..mask3|, max speed, alpha of stages 1..3,
+ * sum over steps of |mask0|, error code, 0. */
+int awcm1d_batch_status(awcm1d_batch_t h, int k, double* out);
+/* out[3]: sum over instances and steps of |mask0|, total steps, finished instances. */
+int awcm1d_batch_totals(awcm1d_batch_t h, double* out);
+/* AWCM_MANAGER_1D pass (AWCM_OP_*) on instance k; also 10 = PrepareEuler (AWCM_1D.h:86-120),
+ * 11 = ForwardWaveletTransformEuler (WAVELET_1D.h:282-335), 12 = InverseWaveletTransformEuler(mask). */
+int awcm1d_batch_pass(awcm1d_batch_t h, int k, int op, int mask_id, int level_id);
+/* Launch shape of the step kernel: threads per CTA and CTAs per SM (0 = occupancy limit). */
+int awcm1d_batch_set_launch(awcm1d_batch_t h, int threads, int ctas_per_sm);
+int awcm1d_batch_stream(awcm1d_batch_t h, void** stream);
+
+/* EULER_EQUATION_2D on a batch of n conserved states in device memory (n x 4 doubles):
+ * ComputeFu/ComputeGu (EULER_EQUATION.h:74-99) and Spectral_RadiusX/Y (:118-142). */
+int euler2d_flux(const double* q_dev, double* f_dev, int n, int dir, double gamma, void* stream);
+int euler2d_spectral_radius(const double* q_dev, double* s_dev, int n, int dir, double gamma, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AWCM_B200_H */

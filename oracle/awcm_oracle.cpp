@@ -159,7 +159,11 @@ struct O1D {
     std::vector<int> lv[4];  // levels, interior points
     int D(int lev) const { return 1 << (maxl - lev); }
     bool get(int i, int b) const { return (m[i + G] >> b) & 1; }
-    void set(int i, int b) { m[i + G] |= (uint8_t)(1u << b); }
+    void set(int i, int b)
+    {
+        if (i < -G || i >= nx + G) return;  // off the ghosted line: dropped (reference UB)
+        m[i + G] |= (uint8_t)(1u << b);
+    }
     void clr(int i, int b) { m[i + G] &= (uint8_t)~(1u << b); }
     double& Q(int p, int i) { return q[p][i + G]; }
 };
@@ -612,7 +616,11 @@ struct O2D {
     int D(int lev) const { return 1 << (maxl - lev); }
     size_t at(int i, int j) const { return (size_t)(j + G) * w + (i + G); }
     bool get(int i, int j, int b) const { return (m[at(i, j)] >> b) & 1; }
-    void set(int i, int j, int b) { m[at(i, j)] |= (uint8_t)(1u << b); }
+    void set(int i, int j, int b)
+    {
+        if (i < -G || i >= nx + G || j < -G || j >= ny + G) return;  // dropped (reference UB)
+        m[at(i, j)] |= (uint8_t)(1u << b);
+    }
     void clr(int i, int j, int b) { m[at(i, j)] &= (uint8_t)~(1u << b); }
     int& LV(int l, int i, int j) { return lv[l][(size_t)j * nx + i]; }
 };
