@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 AWCM compressible-Euler path.
+
+Headline workload: the 2D four-quadrant Riemann problem on [0,1]^2 split at (0.5, 0.5), 2049^2
+finest nodes (nx_coarse 33, 7 levels: Jmin 5 .. Jmax 11), threshold 1e-3, CFL 0.4, WENO-Z + Roe,
+SSP-RK3, transmissive boundaries, FP64.  One step = one full AWCM RK3 step (PrepareEuler, CFL,
+three stages, PostProcessEuler).  Metric: active-point RK3 updates per second, i.e. the sum over
+the timed steps of |mask0| divided by the device time of those steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 (launched by torch.distributed.run) runs N independent replicas, one per GPU: the path has
+no data-parallel split of one instance, and batched instances need no exchange.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "c_pp-library_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+WORKLOAD = {
+    "workload": "2D four-quadrant Riemann problem, 2049x2049 finest (Jmin 5, Jmax 11), eps 1e-3, "
+                "CFL 0.4, WENO-Z+Roe, SSP-RK3, transmissive, t_end 0.3",
+    "num_levels": 7, "nx_coarse": 33, "ny_coarse": 33, "domain": [0.0, 1.0, 0.0, 1.0],
+    "split": [0.5, 0.5], "tol": 1e-3, "cfl": 0.4, "t_end": 0.3,
+}
+METRIC = "active-pt RK3 updates/s"
+UNIT = "updates/s"
+# Algorithmic FP64 operations of one 2D WENO-Z/Roe face flux in the reference
+# (WENOZ_EULER_SOLVER_2D::ComputeFluxX, WENOZ.h:236-277): 589 add, 643 mul, 113 div, 9 sqrt.
+FLOPS_PER_FACE = 1354
+L2_BYTES = 126 * 2 ** 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ------------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ------------------------------------------------------------------------------------- CPU arms
+def reference_solver():
+    """The reference's own 2D code (oracle/_ref), all host threads, on the benchmark workload."""
+    import oracle
+
+    w = WORKLOAD
+    if not oracle.reference_available():
+        return None, "reference build (oracle/_ref) not present"
+    s = oracle.Oracle2D(w["num_levels"], w["nx_coarse"], w["ny_coarse"], *w["domain"], bc_kind=0, kind="reference")
+    s.init_problem(0, *w["split"])
+    return s, None
+
+
+def time_reference(steps_max: int, seconds: float, warmup: int = 0):
+    """Steps of the reference solver from the initial state; returns (updates/s, steps, wall, threads)."""
+    s, why = reference_solver()
+    if s is None:
+        return None, why
+    w = WORKLOAD
+    t = 0.0
+    for _ in range(warmup):
+        t += s.step(w["tol"], w["cfl"], t, w["t_end"])[0]
+    upd, n = 0.0, 0
+    t0 = time.perf_counter()
+    while n < steps_max:
+        o = s.step(w["tol"], w["cfl"], t, w["t_end"])
+        t += o[0]
+        upd += o[2]
+        n += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    wall = time.perf_counter() - t0
+    return {"value": upd / wall, "steps": n, "wall_s": wall, "cores": s.threads, "warmup": warmup}, None
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    k = max(1, min(args.steps, 20))
+    w = max(0, min(args.warmup, 2))
+    r, why = time_reference(k, 1e9, warmup=w)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+        "steps": r["steps"], "warmup": w, "ms_per_step": 1e3 * r["wall_s"] / r["steps"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (deterministic initial state)",
+        "config": {k2: v for k2, v in WORKLOAD.items()},
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                         "sample": f"steps {w + 1}..{w + r['steps']} of the workload from its initial state "
+                                   f"(reference code compiled from the reference tree, OpenMP {r['cores']} threads)"},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------------------------- GPU arm
+def run_b200(args):
+    rank, world, local = dist_env()
+    import numpy as np
+    import torch
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    import awcm
+
+    w = WORKLOAD
+    s = awcm.AWCM2D(w["num_levels"], w["nx_coarse"], w["ny_coarse"], *w["domain"], bc_kind=0)
+    s.init_problem(0, *w["split"])
+    stream = torch.cuda.ExternalStream(s.stream)
+    tol, cfl, t_end = w["tol"], w["cfl"], w["t_end"]
+    launches = s.launches_per_step()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        tt = torch.tensor([v], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        return float(tt.item())
+
+    def sum_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        tt = torch.tensor([v], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.SUM)
+        return float(tt.item())
+
+    warmup = max(3, args.warmup)
+    t, n, _, _ = s.advance(tol, cfl, 0.0, t_end, warmup)
+    t_after_warmup = t
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        e0.record(stream)
+        t, n_steps, upd, stage_pts = s.advance(tol, cfl, t, t_end, args.steps)
+        e1.record(stream)
+        barrier()
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms)
+    upd_all = sum_over_ranks(upd)
+    value = upd_all / (ms_max / 1e3)
+    clocks = clk.summary()
+
+    # Roofline of the dominant kernel (the WENO-Z/Roe face flux): profiled steps with CUDA events
+    # around the face kernels on the solver's stream, same kernels as the graph.
+    prof = []
+    for _ in range(3):
+        prof.append(s.profile_step(tol, cfl, t, t_end))
+        t += prof[-1]["dt"]
+    face_ms = sum(sum(p["face_ms"]) for p in prof)
+    faces = sum(sum(p["faces"]) for p in prof)
+    step_ms = sum(p["total_ms"] for p in prof)
+    achieved = faces * FLOPS_PER_FACE / (face_ms * 1e-3) / 1e12
+    peak = awcm.measure_fp64_peak()
+    phase = {k: (sum(p[k] for p in prof) / len(prof) if not isinstance(prof[0][k], list)
+                 else [sum(p[k][i] for p in prof) / len(prof) for i in range(3)])
+             for k in ("prepare_ms", "setup_ms", "face_ms", "update_ms", "between_ms", "post_ms", "total_ms")}
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "face_flux_traffic.json")
+    if os.path.exists(tr_path):
+        try:
+            per_face = json.load(open(tr_path))["dram_bytes_per_face"]
+            traffic = per_face * faces / (len(prof) * 6)
+        except Exception:
+            traffic = None
+
+    # End to end through the public C-ABI with host buffers: every step uploads the conserved
+    # field in the reference's host layout from pinned memory, advances one step and reads it back.
+    e2e = None
+    if not args.no_e2e:
+        shape = (s.ny + 6, s.nx + 6, 4)
+        host_in = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+        host_out = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+        host_in.numpy()[...] = s.get_q()
+        n_e2e = max(3, min(args.steps, 10))
+        barrier()
+        t0 = time.perf_counter()
+        upd_e = 0.0
+        for _ in range(n_e2e):
+            awcm._lib.call("awcm2d_set_q", s.h, awcm._lib.ptr(host_in.numpy(), ctypes.c_double))
+            t, k, u, _ = s.advance(tol, cfl, t, t_end, 1)
+            upd_e += u
+            awcm._lib.call("awcm2d_get_q", s.h, awcm._lib.ptr(host_out.numpy(), ctypes.c_double))
+            host_in, host_out = host_out, host_in
+        barrier()
+        wall = max_over_ranks(time.perf_counter() - t0)
+        nbytes = int(np.prod(shape)) * 8
+        e2e = {"value": sum_over_ranks(upd_e) / wall, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": n_e2e,
+               "note": "per step: H2D of the dense conserved field (reference layout, pinned), one RK3 step, D2H"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r, why = time_reference(200, args.cpu_seconds, warmup=0)
+        if r is not None:
+            cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                   "sample": f"first {r['steps']} RK3 steps of the same 2049^2 workload from its initial state "
+                             f"({r['wall_s']:.1f} s, reference code compiled from the reference tree, OpenMP)"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
+
+    pitch = (s.nx + 6 + 31) // 32 * 32
+    state_bytes = 5 * 4 * 8 * pitch * (s.ny + 6)  # Q, Q2, Q1, Fx, Fy planes
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": n_steps, "warmup": warmup,
+        "ms_per_step": ms_max / max(1, n_steps), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (deterministic four-quadrant initial state, no dataset)",
+        "config": dict(WORKLOAD, parallelism=f"replicas{world}" if world > 1 else "single GPU",
+                       l2="no flush: device state %.0f MB > 126 MB L2" % (state_bytes / 1e6),
+                       steps_from=f"after {warmup} warm-up steps from t=0 (t={t_after_warmup:.3e})"),
+        "roofline": {"bound": "fp64", "kernel": "k_face (WENO-Z/Roe face flux)", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_note": "of measured: dense DFMA probe on this GPU (2 flops per FMA)",
+                     "flops_per_face": FLOPS_PER_FACE, "faces_per_step": faces / len(prof),
+                     "face_ms_per_step": face_ms / len(prof)},
+        "phase_ms_per_step": phase,
+        "active_points_per_step": upd_all / max(1, n_steps) / world,
+        "stage_points_per_step": stage_pts / max(1, n_steps),
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "gpu_launches": launches * n_steps,
+        "launches_per_step": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -42,6 +42,10 @@ _SIGS = {
     "awcm2d_advance": [c_void_p, c_double, c_double, c_double, c_double, c_int, P_double],
     "awcm2d_launches_per_step": [c_void_p, P_int],
     "awcm2d_stream": [c_void_p, ctypes.POINTER(c_void_p)],
+    "awcm2d_set_prepare_mode": [c_void_p, c_int],
+    "awcm2d_profile_step": [c_void_p, c_double, c_double, c_double, c_double, P_double],
+    "awcm_measure_fp64_peak": [c_int, c_int, P_double],
+    "awcm2d_profile_kernels": [c_void_p, c_double, c_double, c_double, c_double, c_int, ctypes.c_char_p, P_double, P_int],
     "awcm1d_batch_create": [c_int, P_int, P_int, P_double, P_double, c_double, c_int, ctypes.POINTER(c_void_p)],
     "awcm1d_batch_destroy": [c_void_p],
     "awcm1d_batch_count": [c_void_p, P_int],

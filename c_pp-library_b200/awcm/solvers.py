@@ -23,6 +23,13 @@ PROBLEM_QUADRANTS, PROBLEM_DOUBLE_MACH, PROBLEM_VORTEX = 0, 1, 2
 WENOZ, WENO5 = 0, 1
 
 
+def measure_fp64_peak(iters: int = 20000, repeats: int = 5) -> float:
+    """Dense FP64 FMA throughput of the current device, TFLOP/s."""
+    v = ctypes.c_double()
+    call("awcm_measure_fp64_peak", iters, repeats, ctypes.byref(v))
+    return v.value
+
+
 class AWCM2D:
     """One 2D AWCM compressible-Euler instance resident on the GPU."""
 
@@ -120,6 +127,29 @@ class AWCM2D:
             if k < n:
                 break
         return steps, t, upd
+
+    def profile_step(self, tol, cfl, t, t_end):
+        """One eagerly launched step with phase events; returns a dict of device times and counts."""
+        out = np.zeros(19)
+        call("awcm2d_profile_step", self.h, tol, cfl, t, t_end, ptr(out, ctypes.c_double))
+        return {
+            "prepare_ms": out[0], "setup_ms": out[1], "face_ms": out[2:5].tolist(),
+            "update_ms": out[5:8].tolist(), "between_ms": out[8], "post_ms": out[9], "total_ms": out[10],
+            "faces": out[11:14].tolist(), "stage_points": out[14:17].tolist(), "mask0": out[17], "dt": out[18],
+        }
+
+    def profile_kernels(self, tol, cfl, t, t_end, cap=512):
+        """One step with an event after every kernel; returns [(kernel, ms)] in launch order."""
+        names = ctypes.create_string_buffer(32 * cap)
+        ms = np.zeros(cap)
+        n = ctypes.c_int()
+        call("awcm2d_profile_kernels", self.h, tol, cfl, t, t_end, cap, names, ptr(ms, ctypes.c_double), ctypes.byref(n))
+        raw = names.raw
+        return [(raw[32 * k:32 * k + 32].split(b"\0")[0].decode(), float(ms[k])) for k in range(n.value)]
+
+    def set_prepare_mode(self, mode: int):
+        """0: persistent cooperative prepare kernel (default); 1: one launch per pass."""
+        call("awcm2d_set_prepare_mode", self.h, mode)
 
     def launches_per_step(self):
         n = ctypes.c_int()

@@ -121,10 +121,12 @@ struct Ctx {
     __device__ bool bit(int i, int b) const { return (m[i + kGhost] >> b) & 1u; }
     // Mask push; pushes off the ghosted line (only reachable from inconsistent user-set
     // masks/levels, where the reference writes out of bounds) are dropped.
+    // atomicOr on the containing 32-bit word: no dependent round trip per push.
     __device__ void set(int i, int b) const
     {
         if (i < -kGhost || i >= nx + kGhost) return;
-        m[i + kGhost] |= (uint8_t)(1u << b);
+        const uintptr_t a = reinterpret_cast<uintptr_t>(m + i + kGhost);
+        atomicOr(reinterpret_cast<unsigned*>(a & ~(uintptr_t)3), 1u << (8 * (unsigned)(a & 3) + b));
     }
     __device__ int D(int lev) const { return 1 << (maxl - lev); }
     __device__ double w_(int cnt, int k) const { return W.w[cnt][k + 1]; }

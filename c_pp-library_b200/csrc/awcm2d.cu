@@ -14,8 +14,10 @@
 // three stages (boundary fill, face-flux kernels, point-update kernels) + residue removal.  All
 // scalars the step needs (t, dt, CFL speed, per-level dt/dx) stay on the device, so a step is a
 // fixed launch sequence captured once into a CUDA graph and replayed.
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -54,6 +56,9 @@ struct StepState {
     unsigned mask_cnt[4];          // |mask0..mask3| over the grid points
     unsigned long long upd;        // sum over steps of |mask0|
     unsigned long long stage_pts;  // sum over steps of |mask2|+|mask1|+|mask0|
+    unsigned bar[2];               // grid barrier of the persistent prepare: arrivals, generation
+    int bar_err;                   // set when a barrier wait ran out (or another CTA failed)
+    int error;                     // first error of the run (reported by the host API)
 };
 
 __device__ __forceinline__ int ctz_or(int v, int big) { return v == 0 ? big : __ffs(v) - 1; }
@@ -81,318 +86,355 @@ __host__ __device__ __forceinline__ Band band_of(const Grid2& g, int lev, int wh
     return b;
 }
 
-__device__ __forceinline__ bool band_point(const Band& b, long t, int& i, int& j)
-{
-    if (b.cx == 0 || t >= (long)b.cx * b.cy) return false;
-    i = b.i0 + (int)(t % b.cx) * b.D;
-    j = b.j0 + (int)(t / b.cx) * b.D;
-    return true;
-}
-
-__device__ __forceinline__ long gtid() { return (long)blockIdx.x * blockDim.x + threadIdx.x; }
-
-__device__ __forceinline__ void set_bit(uint8_t* m, size_t a, int bit) { m[a] |= (uint8_t)(1u << bit); }
+// Global thread index (all grids here are far below 2^32 threads; 32-bit index arithmetic avoids
+// the emulated 64-bit division).
+__device__ __forceinline__ unsigned gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 
 // Push of a mask bit at (i,j).  Under the reference's mask invariants every push lands on the
 // ghosted grid; pushes that would leave it (possible only for inconsistent user-set masks/levels,
 // where the reference itself writes out of bounds) are dropped.
+// The push is an atomicOr on the 32-bit word holding the byte: fire-and-forget (no dependent
+// round trip per push, unlike a byte read-modify-write) and race-free next to other pushes.
 __device__ __forceinline__ void push_bit(const Grid2& g, uint8_t* m, int i, int j, int bit)
 {
     if (i < -kGhost || i >= g.nx + kGhost || j < -kGhost || j >= g.ny + kGhost) return;
-    m[g.at(i, j)] |= (uint8_t)(1u << bit);
+    const size_t a = g.at(i, j);
+    atomicOr(reinterpret_cast<unsigned*>(m + (a & ~(size_t)3)), 1u << (8 * (unsigned)(a & 3) + bit));
 }
 
-// ------------------------------------------------------------------------------------ transforms
-// Forward transform, one phase of one level (ForwardWaveletTransformationEuler, WAVELET_2D.h:478-624):
-// PH 0 = d3 predict + threshold, PH 1 = d1 and d2 predict + threshold, PH 2 = c update.
-template <int PH>
-__global__ void k_fwt(Grid2 g, double* __restrict__ q, uint8_t* __restrict__ m, int lev, const StepState* st)
+// Point t of the concatenation of the listed sub-bands of level lev (see band_of).
+template <int NB>
+__device__ __forceinline__ bool union_point(const Grid2& g, int lev, const int (&which)[NB], unsigned t, int& i,
+                                            int& j, int& w)
 {
-    if (st->done) return;
-    const double tol = st->tol;
-    const int NX = g.nx - 1, NY = g.ny - 1;
-    long t = gtid();
-    int i, j, which;
-    if (PH == 0) {
-        which = 2;
-    } else if (PH == 1) {
-        const Band b1 = band_of(g, lev, 0);
-        const long n1 = (long)b1.cx * b1.cy;
-        which = t < n1 ? 0 : 1;
-        if (which == 1) t -= n1;
-    } else {
-        which = 3;
-    }
-    const Band b = band_of(g, lev, which);
-    if (!band_point(b, t, i, j)) return;
-    const size_t a = g.at(i, j);
-    if (!(m[a] & 1u)) return;
-    const int D = b.D;
-    if (which == 2) {
-        int is, k1, js, k2;
-        predict_stencil(i, D, NX, is, k1);
-        predict_stencil(j, D, NY, js, k2);
-        double v = q[a];
-        for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
-        for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
-        for (int c2 = 0; c2 < 4; ++c2)
-            for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-        v *= 0.25;
-        q[a] = v;
-        if (absd(v) < tol) m[a] &= (uint8_t)~1u;
-    } else if (which == 0 || which == 1) {
-        int s, k;
-        double v = q[a];
-        if (which == 0) {
-            predict_stencil(i, D, NX, s, k);
-            for (int c = 0; c < 4; ++c) v -= q[g.at(s + c * D, j)] * g.w(c, k);
-        } else {
-            predict_stencil(j, D, NY, s, k);
-            for (int c = 0; c < 4; ++c) v -= q[g.at(i, s + c * D)] * g.w(c, k);
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        const Band b = band_of(g, lev, which[k]);
+        const unsigned n = (unsigned)b.cx * (unsigned)b.cy;
+        if (t < n) {
+            i = b.i0 + (int)(t % (unsigned)b.cx) * b.D;
+            j = b.j0 + (int)(t / (unsigned)b.cx) * b.D;
+            w = which[k];
+            return true;
         }
-        v *= 0.5;
-        q[a] = v;
-        if (absd(v) < tol) m[a] &= (uint8_t)~1u;
-    } else {
+        t -= n;
+    }
+    return false;
+}
+
+// ------------------------------------------------------------------------------- phase bodies
+// Every PrepareEuler pass is a device function over a virtual thread range (t0, stride), so the
+// same body runs as a standalone kernel (one thread per point) or inside the persistent prepare
+// kernel (grid-stride over the phase's points between grid barriers).
+struct Span {
+    unsigned t0, stride;
+};
+__device__ __forceinline__ Span grid_span() { return Span{gtid(), gridDim.x * blockDim.x}; }
+
+__device__ __forceinline__ unsigned band_n(const Grid2& g, int lev, int which)
+{
+    const Band b = band_of(g, lev, which);
+    return (unsigned)b.cx * (unsigned)b.cy;
+}
+
+// Forward transform of one level (ForwardWaveletTransformationEuler, WAVELET_2D.h:478-624) in two
+// phases.  The reference orders d3 -> d1 -> d2 -> c because d3 must see untransformed d1/d2
+// values; phase A computes all three detail sub-bands at once with the d1/d2 results staged in
+// the scratch plane `tb`, and phase B applies the c update (reading d1/d2 from `tb`) and moves the
+// staged details into q.  Same operations on the same operands: identical results.
+__device__ void ph_fwt_a(const Grid2& g, double* __restrict__ q, double* __restrict__ tb, uint8_t* __restrict__ m,
+                         int lev, double tol, Span sp)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    const int which[3] = {2, 0, 1};
+    const unsigned n = band_n(g, lev, 0) + band_n(g, lev, 1) + band_n(g, lev, 2);
+    const int D = g.D(lev);
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j, w;
+        union_point(g, lev, which, t, i, j, w);
+        const size_t a = g.at(i, j);
+        const bool on = m[a] & 1u;
+        if (w == 2) {
+            if (!on) continue;
+            int is, k1, js, k2;
+            predict_stencil(i, D, NX, is, k1);
+            predict_stencil(j, D, NY, js, k2);
+            double v = q[a];
+            for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
+            for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
+            for (int c2 = 0; c2 < 4; ++c2)
+                for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+            v *= 0.25;
+            q[a] = v;
+            if (absd(v) < tol) m[a] &= (uint8_t)~1u;
+            continue;
+        }
+        double v = q[a];
+        if (on) {
+            int s0, k;
+            if (w == 0) {
+                predict_stencil(i, D, NX, s0, k);
+                for (int c = 0; c < 4; ++c) v -= q[g.at(s0 + c * D, j)] * g.w(c, k);
+            } else {
+                predict_stencil(j, D, NY, s0, k);
+                for (int c = 0; c < 4; ++c) v -= q[g.at(i, s0 + c * D)] * g.w(c, k);
+            }
+            v *= 0.5;
+            if (absd(v) < tol) m[a] &= (uint8_t)~1u;
+        }
+        tb[a] = v;
+    }
+}
+
+__device__ void ph_fwt_b(const Grid2& g, double* __restrict__ q, const double* __restrict__ tb,
+                         const uint8_t* __restrict__ m, int lev, Span sp)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    const int which[3] = {3, 0, 1};
+    const unsigned n = band_n(g, lev, 3) + band_n(g, lev, 0) + band_n(g, lev, 1);
+    const int D = g.D(lev);
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j, w;
+        union_point(g, lev, which, t, i, j, w);
+        const size_t a = g.at(i, j);
+        if (w != 3) {
+            q[a] = tb[a];
+            continue;
+        }
+        if (!(m[a] & 1u)) continue;
         int is, k1, js, k2;
         update_stencil(i, D, NX, is, k1);
         update_stencil(j, D, NY, js, k2);
         double v = q[a];
-        for (int c = 0; c < 4; ++c) v += q[g.at(is + c * D, j)] * g.w(c, k1);
-        for (int c = 0; c < 4; ++c) v += q[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c = 0; c < 4; ++c) v += tb[g.at(is + c * D, j)] * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v += tb[g.at(i, js + c * D)] * g.w(c, k2);
         for (int c2 = 0; c2 < 4; ++c2)
             for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
         q[a] = v;
     }
 }
 
-// Inverse transform, one phase (InverseWaveletTransformationEuler, WAVELET_2D.h:626-782):
+// Inverse transform, one phase of one level (InverseWaveletTransformationEuler, WAVELET_2D.h:626-782):
 // PH 0 = c, PH 1 = d2 and d1, PH 2 = d3; points outside the mask get density 0.
 template <int PH>
-__global__ void k_iwt(Grid2 g, double* __restrict__ q, const uint8_t* __restrict__ m, int lev, int bit,
-                      const StepState* st)
+__device__ void ph_iwt(const Grid2& g, double* __restrict__ q, const uint8_t* __restrict__ m, int lev, int bit, Span sp)
 {
-    if (st && st->done) return;
     const int NX = g.nx - 1, NY = g.ny - 1;
-    long t = gtid();
-    int i, j, which;
-    if (PH == 0) {
-        which = 3;
-    } else if (PH == 1) {
-        const Band b1 = band_of(g, lev, 0);
-        const long n1 = (long)b1.cx * b1.cy;
-        which = t < n1 ? 0 : 1;
-        if (which == 1) t -= n1;
-    } else {
-        which = 2;
-    }
-    const Band b = band_of(g, lev, which);
-    if (!band_point(b, t, i, j)) return;
-    const size_t a = g.at(i, j);
-    if (!((m[a] >> bit) & 1u)) {
-        q[a] = 0;
-        return;
-    }
-    const int D = b.D;
-    if (which == 3) {
-        int is, k1, js, k2;
-        update_stencil(i, D, NX, is, k1);
-        update_stencil(j, D, NY, js, k2);
-        double v = q[a];
-        for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
-        for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
-        for (int c2 = 0; c2 < 4; ++c2)
-            for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-        q[a] = v;
-    } else if (which == 1) {
-        int s, k;
-        predict_stencil(j, D, NY, s, k);
-        double v = q[a];
-        v *= 2.0;
-        for (int c = 0; c < 4; ++c) v += q[g.at(i, s + c * D)] * g.w(c, k);
-        q[a] = v;
-    } else if (which == 0) {
-        int s, k;
-        predict_stencil(i, D, NX, s, k);
-        double v = q[a];
-        v *= 2.0;
-        for (int c = 0; c < 4; ++c) v += q[g.at(s + c * D, j)] * g.w(c, k);
-        q[a] = v;
-    } else {
-        int is, k1, js, k2;
-        predict_stencil(i, D, NX, is, k1);
-        predict_stencil(j, D, NY, js, k2);
-        double v = q[a];
-        v *= 4.0;
-        for (int c = 0; c < 4; ++c) v += q[g.at(is + c * D, j)] * g.w(c, k1);
-        for (int c = 0; c < 4; ++c) v += q[g.at(i, js + c * D)] * g.w(c, k2);
-        for (int c2 = 0; c2 < 4; ++c2)
-            for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-        q[a] = v;
+    const int D = g.D(lev);
+    unsigned n;
+    if (PH == 0) n = band_n(g, lev, 3);
+    else if (PH == 1) n = band_n(g, lev, 0) + band_n(g, lev, 1);
+    else n = band_n(g, lev, 2);
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j, w;
+        if (PH == 0) {
+            const int wh[1] = {3};
+            union_point(g, lev, wh, t, i, j, w);
+        } else if (PH == 1) {
+            const int wh[2] = {0, 1};
+            union_point(g, lev, wh, t, i, j, w);
+        } else {
+            const int wh[1] = {2};
+            union_point(g, lev, wh, t, i, j, w);
+        }
+        const size_t a = g.at(i, j);
+        if (!((m[a] >> bit) & 1u)) {
+            q[a] = 0;
+            continue;
+        }
+        if (w == 3) {
+            int is, k1, js, k2;
+            update_stencil(i, D, NX, is, k1);
+            update_stencil(j, D, NY, js, k2);
+            double v = q[a];
+            for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
+            for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
+            for (int c2 = 0; c2 < 4; ++c2)
+                for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+            q[a] = v;
+        } else if (w == 1) {
+            int s0, k;
+            predict_stencil(j, D, NY, s0, k);
+            double v = q[a];
+            v *= 2.0;
+            for (int c = 0; c < 4; ++c) v += q[g.at(i, s0 + c * D)] * g.w(c, k);
+            q[a] = v;
+        } else if (w == 0) {
+            int s0, k;
+            predict_stencil(i, D, NX, s0, k);
+            double v = q[a];
+            v *= 2.0;
+            for (int c = 0; c < 4; ++c) v += q[g.at(s0 + c * D, j)] * g.w(c, k);
+            q[a] = v;
+        } else {
+            int is, k1, js, k2;
+            predict_stencil(i, D, NX, is, k1);
+            predict_stencil(j, D, NY, js, k2);
+            double v = q[a];
+            v *= 4.0;
+            for (int c = 0; c < 4; ++c) v += q[g.at(is + c * D, j)] * g.w(c, k1);
+            for (int c = 0; c < 4; ++c) v += q[g.at(i, js + c * D)] * g.w(c, k2);
+            for (int c2 = 0; c2 < 4; ++c2)
+                for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+            q[a] = v;
+        }
     }
 }
 
-// CheckReconstruction, one phase of one level (AWCM_MANAGER_2D.h:63-158): PH 0 = d3 points mark
-// their 4 + 4 + 16 predict nodes, PH 1 = d1/d2 points mark their 4 nodes.  Plain byte
-// read-modify-writes are race-free here: a phase only ever sets the one bit `bit`.
-template <int PH>
-__global__ void k_cr(Grid2 g, uint8_t* __restrict__ m, int lev, int bit, const StepState* st)
+// CheckReconstruction of one level (AWCM_MANAGER_2D.h:63-158) in one phase.  The reference runs
+// d3 -> d1 -> d2 so that d1/d2 points switched on by a d3 point also mark their stencils; those
+// stencils ((is..is+3D, n) for a d1 point (i, n), (m, js..js+3D) for a d2 point (m, j)) lie inside
+// the d3 point's own 4x4 block of marks, so all three sub-bands can run concurrently.
+__device__ void ph_cr(const Grid2& g, uint8_t* __restrict__ m, int lev, int bit, Span sp)
 {
-    if (st && st->done) return;
     const int NX = g.nx - 1, NY = g.ny - 1;
-    long t = gtid();
-    int i, j, which;
-    if (PH == 0) {
-        which = 2;
-    } else {
-        const Band b1 = band_of(g, lev, 0);
-        const long n1 = (long)b1.cx * b1.cy;
-        which = t < n1 ? 0 : 1;
-        if (which == 1) t -= n1;
-    }
-    const Band b = band_of(g, lev, which);
-    if (!band_point(b, t, i, j)) return;
-    if (!((m[g.at(i, j)] >> bit) & 1u)) return;
-    const int D = b.D;
-    int is, js, k;
-    if (which == 2) {
-        predict_stencil(i, D, NX, is, k);
-        predict_stencil(j, D, NY, js, k);
-        for (int c = 0; c < 4; ++c) set_bit(m, g.at(is + c * D, j), bit);
-        for (int c = 0; c < 4; ++c) set_bit(m, g.at(i, js + c * D), bit);
-        for (int c2 = 0; c2 < 4; ++c2)
-            for (int c1 = 0; c1 < 4; ++c1) set_bit(m, g.at(is + c1 * D, js + c2 * D), bit);
-    } else if (which == 0) {
-        predict_stencil(i, D, NX, is, k);
-        for (int c = 0; c < 4; ++c) set_bit(m, g.at(is + c * D, j), bit);
-    } else {
-        predict_stencil(j, D, NY, js, k);
-        for (int c = 0; c < 4; ++c) set_bit(m, g.at(i, js + c * D), bit);
+    const int which[3] = {2, 0, 1};
+    const unsigned n = band_n(g, lev, 0) + band_n(g, lev, 1) + band_n(g, lev, 2);
+    const int D = g.D(lev);
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j, w;
+        union_point(g, lev, which, t, i, j, w);
+        if (!((m[g.at(i, j)] >> bit) & 1u)) continue;
+        int is, js, k;
+        if (w == 2) {
+            predict_stencil(i, D, NX, is, k);
+            predict_stencil(j, D, NY, js, k);
+            for (int c = 0; c < 4; ++c) push_bit(g, m, is + c * D, j, bit);
+            for (int c = 0; c < 4; ++c) push_bit(g, m, i, js + c * D, bit);
+            for (int c2 = 0; c2 < 4; ++c2)
+                for (int c1 = 0; c1 < 4; ++c1) push_bit(g, m, is + c1 * D, js + c2 * D, bit);
+        } else if (w == 0) {
+            predict_stencil(i, D, NX, is, k);
+            for (int c = 0; c < 4; ++c) push_bit(g, m, is + c * D, j, bit);
+        } else {
+            predict_stencil(j, D, NY, js, k);
+            for (int c = 0; c < 4; ++c) push_bit(g, m, i, js + c * D, bit);
+        }
     }
 }
 
 // InterpolateEuler, one phase of one level (WAVELET_2D.h:784-907): PH 0 = d1 and d2, PH 1 = d3;
 // components 1..3 at points of the work mask that were not active before (`from_bit`).
 template <int PH>
-__global__ void k_interp(Grid2 g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit,
-                         const StepState* st)
+__device__ void ph_interp(const Grid2& g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit, Span sp)
 {
-    if (st && st->done) return;
     const int NX = g.nx - 1, NY = g.ny - 1;
-    long t = gtid();
-    int i, j, which;
-    if (PH == 0) {
-        const Band b1 = band_of(g, lev, 0);
-        const long n1 = (long)b1.cx * b1.cy;
-        which = t < n1 ? 0 : 1;
-        if (which == 1) t -= n1;
-    } else {
-        which = 2;
-    }
-    const Band b = band_of(g, lev, which);
-    if (!band_point(b, t, i, j)) return;
-    const size_t a = g.at(i, j);
-    const unsigned mb = m[a];
-    if (!((mb >> kBitInterp) & 1u) || ((mb >> from_bit) & 1u)) return;
-    const int D = b.D;
-    if (which == 0) {
-        int s, k;
-        predict_stencil(i, D, NX, s, k);
-        for (int p = 1; p < 4; ++p) {
-            const double* qp = q.p[p];
-            double v = 0.0;
-            for (int c = 0; c < 4; ++c) v += qp[g.at(s + c * D, j)] * g.w(c, k);
-            q.p[p][a] = v;
+    const int D = g.D(lev);
+    const unsigned n = PH == 0 ? band_n(g, lev, 0) + band_n(g, lev, 1) : band_n(g, lev, 2);
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j, w;
+        if (PH == 0) {
+            const int wh[2] = {0, 1};
+            union_point(g, lev, wh, t, i, j, w);
+        } else {
+            const int wh[1] = {2};
+            union_point(g, lev, wh, t, i, j, w);
         }
-    } else if (which == 1) {
-        int s, k;
-        predict_stencil(j, D, NY, s, k);
-        for (int p = 1; p < 4; ++p) {
-            const double* qp = q.p[p];
-            double v = 0.0;
-            for (int c = 0; c < 4; ++c) v += qp[g.at(i, s + c * D)] * g.w(c, k);
-            q.p[p][a] = v;
-        }
-    } else {
-        int is, k1, js, k2;
-        predict_stencil(i, D, NX, is, k1);
-        predict_stencil(j, D, NY, js, k2);
-        for (int p = 1; p < 4; ++p) {
-            const double* qp = q.p[p];
-            double v = 0.0;
-            for (int c = 0; c < 4; ++c) v += qp[g.at(is + c * D, j)] * g.w(c, k1);
-            for (int c = 0; c < 4; ++c) v += qp[g.at(i, js + c * D)] * g.w(c, k2);
-            for (int c2 = 0; c2 < 4; ++c2)
-                for (int c1 = 0; c1 < 4; ++c1) v -= qp[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-            q.p[p][a] = v;
+        const size_t a = g.at(i, j);
+        const unsigned mb = m[a];
+        if (!((mb >> kBitInterp) & 1u) || ((mb >> from_bit) & 1u)) continue;
+        if (w == 0) {
+            int s0, k;
+            predict_stencil(i, D, NX, s0, k);
+            for (int p = 1; p < 4; ++p) {
+                const double* qp = q.p[p];
+                double v = 0.0;
+                for (int c = 0; c < 4; ++c) v += qp[g.at(s0 + c * D, j)] * g.w(c, k);
+                q.p[p][a] = v;
+            }
+        } else if (w == 1) {
+            int s0, k;
+            predict_stencil(j, D, NY, s0, k);
+            for (int p = 1; p < 4; ++p) {
+                const double* qp = q.p[p];
+                double v = 0.0;
+                for (int c = 0; c < 4; ++c) v += qp[g.at(i, s0 + c * D)] * g.w(c, k);
+                q.p[p][a] = v;
+            }
+        } else {
+            int is, k1, js, k2;
+            predict_stencil(i, D, NX, is, k1);
+            predict_stencil(j, D, NY, js, k2);
+            for (int p = 1; p < 4; ++p) {
+                const double* qp = q.p[p];
+                double v = 0.0;
+                for (int c = 0; c < 4; ++c) v += qp[g.at(is + c * D, j)] * g.w(c, k1);
+                for (int c = 0; c < 4; ++c) v += qp[g.at(i, js + c * D)] * g.w(c, k2);
+                for (int c2 = 0; c2 < 4; ++c2)
+                    for (int c1 = 0; c1 < 4; ++c1) v -= qp[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+                q.p[p][a] = v;
+            }
         }
     }
 }
 
 // ------------------------------------------------------------------------------- dense mask passes
-__device__ __forceinline__ bool grid_point(const Grid2& g, long t, int& i, int& j)
+__device__ __forceinline__ bool grid_point(const Grid2& g, unsigned t, int& i, int& j)
 {
-    if (t >= (long)g.nx * g.ny) return false;
-    i = (int)(t % g.nx);
-    j = (int)(t / g.nx);
+    if (t >= (unsigned)g.nx * (unsigned)g.ny) return false;
+    i = (int)(t % (unsigned)g.nx);
+    j = (int)(t / (unsigned)g.nx);
     return true;
 }
 
-__global__ void k_copy_bit_all(uint8_t* m, size_t n, int from, int to, const StepState* st)
+__device__ void ph_copy_bit_all(uint8_t* m, size_t n, int from, int to, Span sp)
 {
-    if (st && st->done) return;
-    const size_t a = (size_t)gtid();
-    if (a >= n) return;
-    const unsigned v = m[a];
-    m[a] = (uint8_t)((v & ~(1u << to)) | (((v >> from) & 1u) << to));
+    for (unsigned a = sp.t0; a < n; a += sp.stride) {
+        const unsigned v = m[a];
+        m[a] = (uint8_t)((v & ~(1u << to)) | (((v >> from) & 1u) << to));
+    }
 }
 
 // BandingMask (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:205-213) on `bit`, then copies the
 // result into the work bit read by the following add-adjacent-zone pass.
-__global__ void k_band_copy(Grid2 g, uint8_t* m, int bit, int copy_to, const StepState* st)
+__device__ void ph_band_copy(const Grid2& g, uint8_t* m, int bit, int copy_to, Span sp)
 {
-    if (st && st->done) return;
-    int i, j;
-    if (!grid_point(g, gtid(), i, j)) return;
-    const size_t a = g.at(i, j);
-    unsigned v = m[a];
-    if (!(2 <= i && i <= g.nx - 3 && j >= 2 && j <= g.ny - 3)) v |= 1u << bit;
-    if (copy_to >= 0) v = (v & ~(1u << copy_to)) | (((v >> bit) & 1u) << copy_to);
-    m[a] = (uint8_t)v;
+    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j;
+        grid_point(g, t, i, j);
+        const size_t a = g.at(i, j);
+        unsigned v = m[a];
+        if (!(2 <= i && i <= g.nx - 3 && j >= 2 && j <= g.ny - 3)) v |= 1u << bit;
+        if (copy_to >= 0) v = (v & ~(1u << copy_to)) | (((v >> bit) & 1u) << copy_to);
+        m[a] = (uint8_t)v;
+    }
 }
 
 // AddAdjacentZone (AWCM_MANAGER_2D.h:14-61): every detail point whose copy bit is set marks its
 // finer neighbours in `bit`.  A point (i,j) = (odd*2^a, odd*2^b) is a detail of level
 // maxl-1-min(a,b): d1 if a < b, d2 if a > b, d3 if a == b (boundary rows/columns excluded as in
 // the sub-grids).
-__global__ void k_aaz(Grid2 g, uint8_t* m, int bit, int src, const StepState* st)
+__device__ void ph_aaz(const Grid2& g, uint8_t* m, int bit, int src, Span sp)
 {
-    if (st && st->done) return;
-    int i, j;
-    if (!grid_point(g, gtid(), i, j)) return;
     const int NX = g.nx - 1, NY = g.ny - 1;
-    const int ti = ctz_or(i, 64), tj = ctz_or(j, 64);
-    const int mn = ti < tj ? ti : tj;
-    if (mn >= g.maxl) return;
-    if (ti < tj && (j == 0 || j == NY)) return;
-    if (tj < ti && (i == 0 || i == NX)) return;
-    if (!((m[g.at(i, j)] >> src) & 1u)) return;
-    const int lev = g.maxl - 1 - mn;
-    if (lev == g.maxl - 1) {
-        push_bit(g, m, i - 1, j, bit);
-        push_bit(g, m, i + 1, j, bit);
-        push_bit(g, m, i, j - 1, bit);
-        push_bit(g, m, i, j + 1, bit);
-    } else {
-        const int D = g.D(lev), h = D / 2, q4 = D / 4;
-        push_bit(g, m, i - q4, j, bit);
-        push_bit(g, m, i + q4, j, bit);
-        push_bit(g, m, i, j - q4, bit);
-        push_bit(g, m, i, j + q4, bit);
-        push_bit(g, m, i - h, j, bit);
-        push_bit(g, m, i + h, j, bit);
-        push_bit(g, m, i, j - h, bit);
-        push_bit(g, m, i, j + h, bit);
+    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j;
+        grid_point(g, t, i, j);
+        const int ti = ctz_or(i, 64), tj = ctz_or(j, 64);
+        const int mn = ti < tj ? ti : tj;
+        if (mn >= g.maxl) continue;
+        if (ti < tj && (j == 0 || j == NY)) continue;
+        if (tj < ti && (i == 0 || i == NX)) continue;
+        if (!((m[g.at(i, j)] >> src) & 1u)) continue;
+        const int lev = g.maxl - 1 - mn;
+        if (lev == g.maxl - 1) {
+            push_bit(g, m, i - 1, j, bit);
+            push_bit(g, m, i + 1, j, bit);
+            push_bit(g, m, i, j - 1, bit);
+            push_bit(g, m, i, j + 1, bit);
+        } else {
+            const int D = g.D(lev), h = D / 2, q4 = D / 4;
+            push_bit(g, m, i - q4, j, bit);
+            push_bit(g, m, i + q4, j, bit);
+            push_bit(g, m, i, j - q4, bit);
+            push_bit(g, m, i, j + q4, bit);
+            push_bit(g, m, i - h, j, bit);
+            push_bit(g, m, i + h, j, bit);
+            push_bit(g, m, i, j - h, bit);
+            push_bit(g, m, i, j + h, bit);
+        }
     }
 }
 
@@ -405,93 +447,283 @@ __device__ __forceinline__ bool mask_or_ghost(const Grid2& g, const uint8_t* m, 
 
 // ComputeLevel (AWCM_MANAGER_2D.h:215-241) of mask `bit` into `lvl`; a level is left unchanged when
 // no neighbour is found.  When copy_to >= 0 the pass also performs `mask_{k+1} = mask_k` on every
-// byte of the plane, ghost ring included (the reference copies whole fields).  One thread per
-// plane byte; the level search runs for grid points only.
-__global__ void k_cl(Grid2 g, uint8_t* m, int8_t* lvl, int bit, int copy_to, size_t plane, const StepState* st)
+// byte of the plane, ghost ring included (the reference copies whole fields).  The level search
+// runs for grid points only.
+__device__ void ph_cl(const Grid2& g, uint8_t* m, int8_t* lvl, int bit, int copy_to, size_t plane, Span sp)
 {
-    if (st && st->done) return;
-    const size_t a = (size_t)gtid();
-    if (a >= plane) return;
-    const int i = (int)(a % (size_t)g.pitch) - kGhost, j = (int)(a / (size_t)g.pitch) - kGhost;
-    const unsigned v = m[a];
-    const bool on = (v >> bit) & 1u;
-    if (i >= 0 && i < g.nx && j >= 0 && j < g.ny) {
-        if (!on) {
-            lvl[a] = 0;
-        } else {
-            int dx = 1;
-            for (int lev = g.maxl; lev >= 0; --lev) {
-                if (mask_or_ghost(g, m, i - dx, j, bit) || mask_or_ghost(g, m, i + dx, j, bit) ||
-                    mask_or_ghost(g, m, i, j - dx, bit) || mask_or_ghost(g, m, i, j + dx, bit)) {
-                    lvl[a] = (int8_t)lev;
-                    break;
+    for (unsigned a = sp.t0; a < plane; a += sp.stride) {
+        const int i = (int)(a % (unsigned)g.pitch) - kGhost, j = (int)(a / (unsigned)g.pitch) - kGhost;
+        const unsigned v = m[a];
+        const bool on = (v >> bit) & 1u;
+        if (i >= 0 && i < g.nx && j >= 0 && j < g.ny) {
+            if (!on) {
+                lvl[a] = 0;
+            } else {
+                int dx = 1;
+                for (int lev = g.maxl; lev >= 0; --lev) {
+                    if (mask_or_ghost(g, m, i - dx, j, bit) || mask_or_ghost(g, m, i + dx, j, bit) ||
+                        mask_or_ghost(g, m, i, j - dx, bit) || mask_or_ghost(g, m, i, j + dx, bit)) {
+                        lvl[a] = (int8_t)lev;
+                        break;
+                    }
+                    dx *= 2;
                 }
-                dx *= 2;
             }
         }
+        if (copy_to >= 0) m[a] = (uint8_t)((v & ~(1u << copy_to)) | ((on ? 1u : 0u) << copy_to));
     }
-    if (copy_to >= 0) m[a] = (uint8_t)((v & ~(1u << copy_to)) | ((on ? 1u : 0u) << copy_to));
 }
 
 // AddPointForDifferentiation (AWCM_MANAGER_2D.h:160-213): points of mask `src` mark their flux
 // stencil in `bit` (finest level: the +-3 cross; coarser: +-2 spacings, shifted at the edges).
-__global__ void k_apd(Grid2 g, uint8_t* m, const int8_t* lvl, int bit, int src, const StepState* st)
+__device__ void ph_apd(const Grid2& g, uint8_t* m, const int8_t* lvl, int bit, int src, Span sp)
 {
-    if (st && st->done) return;
-    int i, j;
-    if (!grid_point(g, gtid(), i, j)) return;
     const int NX = g.nx - 1, NY = g.ny - 1;
-    if (i < 1 || i > NX - 1 || j < 1 || j > NY - 1) return;
-    const size_t a = g.at(i, j);
-    if (!((m[a] >> src) & 1u)) return;
-    const int lev = lvl[a];
-    if (lev == g.maxl) {
-        for (int c = -3; c <= 3; ++c) {
-            push_bit(g, m, i + c, j, bit);
-            push_bit(g, m, i, j + c, bit);
+    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j;
+        grid_point(g, t, i, j);
+        if (i < 1 || i > NX - 1 || j < 1 || j > NY - 1) continue;
+        const size_t a = g.at(i, j);
+        if (!((m[a] >> src) & 1u)) continue;
+        const int lev = lvl[a];
+        if (lev == g.maxl) {
+            for (int c = -3; c <= 3; ++c) {
+                push_bit(g, m, i + c, j, bit);
+                push_bit(g, m, i, j + c, bit);
+            }
+            continue;
         }
-        return;
+        const int D = g.D(lev);
+        int lo = -2, hi = 2;
+        if (i - 2 * D < 0) lo = -1;
+        else if (i + 2 * D > NX) hi = 1;
+        for (int c = lo; c <= hi; ++c) push_bit(g, m, i + D * c, j, bit);
+        lo = -2, hi = 2;
+        if (j - 2 * D < 0) lo = -1;
+        else if (j + 2 * D > NY) hi = 1;
+        for (int c = lo; c <= hi; ++c) push_bit(g, m, i, j + D * c, bit);
     }
-    const int D = g.D(lev);
-    int lo = -2, hi = 2;
-    if (i - 2 * D < 0) lo = -1;
-    else if (i + 2 * D > NX) hi = 1;
-    for (int c = lo; c <= hi; ++c) push_bit(g, m, i + D * c, j, bit);
-    lo = -2, hi = 2;
-    if (j - 2 * D < 0) lo = -1;
-    else if (j + 2 * D > NY) hi = 1;
-    for (int c = lo; c <= hi; ++c) push_bit(g, m, i, j + D * c, bit);
 }
 
-// Work mask of InterpolateEuler: `to` minus `from` over the grid points (ghost bits stay set).
-__global__ void k_interp_init(Grid2 g, uint8_t* m, int from, int to, const StepState* st)
+// Work mask of InterpolateEuler: `to` minus `from` over the grid points (ghost bits untouched).
+__device__ void ph_interp_init(const Grid2& g, uint8_t* m, int from, int to, Span sp)
 {
-    if (st && st->done) return;
-    int i, j;
-    if (!grid_point(g, gtid(), i, j)) return;
-    const size_t a = g.at(i, j);
-    const unsigned v = m[a];
-    const unsigned on = ((v >> to) & 1u) & ~((v >> from) & 1u);
-    m[a] = (uint8_t)((v & ~(1u << kBitInterp)) | (on << kBitInterp));
+    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j;
+        grid_point(g, t, i, j);
+        const size_t a = g.at(i, j);
+        const unsigned v = m[a];
+        const unsigned on = ((v >> to) & 1u) & ~((v >> from) & 1u);
+        m[a] = (uint8_t)((v & ~(1u << kBitInterp)) | (on << kBitInterp));
+    }
 }
 
 // RemoveResidueEuler (AWCM_MANAGER_2D.h:267-280): zero interior points outside `bit`.  In the
 // step only points that can hold non-zero values (in mask3 or in the previous mask0) are written.
+__device__ void ph_remove_residue(const Grid2& g, Field4 q, const uint8_t* m, int bit, bool full, Span sp)
+{
+    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int i, j;
+        grid_point(g, t, i, j);
+        if (i < 1 || i > g.nx - 2 || j < 1 || j > g.ny - 2) continue;
+        const size_t a = g.at(i, j);
+        const unsigned v = m[a];
+        if ((v >> bit) & 1u) continue;
+        if (!full && !(v & ((1u << 3) | (1u << kBitTemp)))) continue;
+        q.p[0][a] = 0.0;
+        q.p[1][a] = 0.0;
+        q.p[2][a] = 0.0;
+        q.p[3][a] = 0.0;
+    }
+}
+
+// ------------------------------------------------------------------------ standalone kernels
+#define AWCM_SKIP_IF_DONE(st) \
+    if ((st) && (st)->done) return
+
+__global__ void k_fwt_a(Grid2 g, double* q, double* tb, uint8_t* m, int lev, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_fwt_a(g, q, tb, m, lev, st->tol, grid_span());
+}
+__global__ void k_fwt_b(Grid2 g, double* q, const double* tb, const uint8_t* m, int lev, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_fwt_b(g, q, tb, m, lev, grid_span());
+}
+template <int PH>
+__global__ void k_iwt(Grid2 g, double* q, const uint8_t* m, int lev, int bit, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_iwt<PH>(g, q, m, lev, bit, grid_span());
+}
+__global__ void k_cr(Grid2 g, uint8_t* m, int lev, int bit, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_cr(g, m, lev, bit, grid_span());
+}
+template <int PH>
+__global__ void k_interp(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_interp<PH>(g, q, m, lev, from_bit, grid_span());
+}
+__global__ void k_copy_bit_all(uint8_t* m, size_t n, int from, int to, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_copy_bit_all(m, n, from, to, grid_span());
+}
+__global__ void k_band_copy(Grid2 g, uint8_t* m, int bit, int copy_to, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_band_copy(g, m, bit, copy_to, grid_span());
+}
+__global__ void k_aaz(Grid2 g, uint8_t* m, int bit, int src, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_aaz(g, m, bit, src, grid_span());
+}
+__global__ void k_cl(Grid2 g, uint8_t* m, int8_t* lvl, int bit, int copy_to, size_t plane, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_cl(g, m, lvl, bit, copy_to, plane, grid_span());
+}
+__global__ void k_apd(Grid2 g, uint8_t* m, const int8_t* lvl, int bit, int src, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_apd(g, m, lvl, bit, src, grid_span());
+}
+__global__ void k_interp_init(Grid2 g, uint8_t* m, int from, int to, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_interp_init(g, m, from, to, grid_span());
+}
 __global__ void k_remove_residue(Grid2 g, Field4 q, const uint8_t* m, int bit, int sparse, const StepState* st)
 {
-    if (st && st->done) return;
-    int i, j;
-    if (!grid_point(g, gtid(), i, j)) return;
-    if (i < 1 || i > g.nx - 2 || j < 1 || j > g.ny - 2) return;
-    const size_t a = g.at(i, j);
-    const unsigned v = m[a];
-    if ((v >> bit) & 1u) return;
+    AWCM_SKIP_IF_DONE(st);
     const bool full = !sparse || (st && st->full_zero);
-    if (!full && !(v & ((1u << 3) | (1u << kBitTemp)))) return;
-    q.p[0][a] = 0.0;
-    q.p[1][a] = 0.0;
-    q.p[2][a] = 0.0;
-    q.p[3][a] = 0.0;
+    ph_remove_residue(g, q, m, bit, full, grid_span());
+}
+
+// ------------------------------------------------------------------- persistent PrepareEuler
+// Grid-wide barrier for the persistent prepare kernel (all CTAs co-resident: cooperative launch).
+// Arrive = device-scope acq_rel increment of `count`; the last CTA resets `count` and bumps the
+// generation; the others spin on the generation with a bounded number of polls.  A spin that
+// runs out, or an error already raised by another CTA, sets `err` and every CTA leaves at its
+// next barrier: the step then reports a timeout instead of hanging.
+constexpr unsigned kSpinLimit = 1u << 22;  // polls of >= 64 ns: well over a second
+
+struct GridSync {
+    unsigned* count;
+    unsigned* gen;
+    int* err;
+    unsigned nb;
+    __device__ bool sync() const
+    {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            volatile int* ve = err;
+            if (*ve == 0) {
+                cuda::atomic_ref<unsigned, cuda::thread_scope_device> G(*gen), C(*count);
+                const unsigned my = G.load(cuda::memory_order_acquire);
+                __threadfence();
+                if (C.fetch_add(1u, cuda::memory_order_acq_rel) == nb - 1) {
+                    C.store(0u, cuda::memory_order_relaxed);
+                    G.fetch_add(1u, cuda::memory_order_release);
+                } else {
+                    unsigned spins = 0;
+                    while (G.load(cuda::memory_order_acquire) == my) {
+                        if (++spins > kSpinLimit || *ve) {
+                            atomicCAS(err, 0, (int)kErrTimeout);
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+                __threadfence();
+            }
+        }
+        __syncthreads();
+        return *(volatile int*)err == 0;
+    }
+};
+
+struct PrepArgs {
+    Grid2 g;
+    Field4 q;
+    double* tb;
+    uint8_t* m;
+    int8_t* lvl[4];
+    const StepState* st;
+    unsigned* sync;  // [0] arrival count, [1] generation
+    int* err;
+    size_t plane;
+};
+
+
+constexpr int kPrepThreads = 1024;
+
+// AWCM_2D::PrepareEuler (Wavelet/AWCM_2D.h:114-147) as one persistent kernel: the reference's
+// level-sequential passes run back to back, separated by grid barriers instead of launches.
+__global__ void __launch_bounds__(kPrepThreads, 1) k_prepare(PrepArgs A)
+{
+    if (A.st->done) return;
+    const Grid2& g = A.g;
+    const Span sp = grid_span();
+    const GridSync gs{A.sync, A.sync + 1, A.err, gridDim.x};
+    const double tol = A.st->tol;
+#define SYNC_OR_LEAVE \
+    if (!gs.sync()) return
+    ph_copy_bit_all(A.m, A.plane, 0, kBitTemp, sp);
+    SYNC_OR_LEAVE;
+    for (int lev = g.maxl - 1; lev >= 0; --lev) {
+        ph_fwt_a(g, A.q.p[0], A.tb, A.m, lev, tol, sp);
+        SYNC_OR_LEAVE;
+        ph_fwt_b(g, A.q.p[0], A.tb, A.m, lev, sp);
+        SYNC_OR_LEAVE;
+    }
+    ph_band_copy(g, A.m, 0, kBitCopy, sp);
+    SYNC_OR_LEAVE;
+    ph_aaz(g, A.m, 0, kBitCopy, sp);
+    SYNC_OR_LEAVE;
+    for (int lev = g.maxl - 1; lev >= 0; --lev) {
+        ph_cr(g, A.m, lev, 0, sp);
+        SYNC_OR_LEAVE;
+    }
+    for (int k = 1; k <= 3; ++k) {
+        ph_cl(g, A.m, A.lvl[k - 1], k - 1, k, A.plane, sp);
+        SYNC_OR_LEAVE;
+        ph_apd(g, A.m, A.lvl[k - 1], k, k - 1, sp);
+        SYNC_OR_LEAVE;
+        for (int lev = g.maxl - 1; lev >= 0; --lev) {
+            ph_cr(g, A.m, lev, k, sp);
+            SYNC_OR_LEAVE;
+        }
+    }
+    for (int lev = 0; lev < g.maxl; ++lev) {
+        ph_iwt<0>(g, A.q.p[0], A.m, lev, 3, sp);
+        SYNC_OR_LEAVE;
+        ph_iwt<1>(g, A.q.p[0], A.m, lev, 3, sp);
+        SYNC_OR_LEAVE;
+        ph_iwt<2>(g, A.q.p[0], A.m, lev, 3, sp);
+        SYNC_OR_LEAVE;
+    }
+    ph_interp_init(g, A.m, kBitTemp, 3, sp);
+    SYNC_OR_LEAVE;
+    for (int lev = g.maxl - 1; lev >= 0; --lev) {
+        ph_cr(g, A.m, lev, kBitInterp, sp);
+        SYNC_OR_LEAVE;
+    }
+    for (int lev = 0; lev < g.maxl; ++lev) {
+        ph_interp<0>(g, A.q, A.m, lev, kBitTemp, sp);
+        SYNC_OR_LEAVE;
+        ph_interp<1>(g, A.q, A.m, lev, kBitTemp, sp);
+        if (lev + 1 < g.maxl) SYNC_OR_LEAVE;
+    }
+#undef SYNC_OR_LEAVE
 }
 
 // ------------------------------------------------------------------------------------ boundaries
@@ -645,8 +877,10 @@ __global__ void k_dt(Grid2 g, StepState* st)
 
 __global__ void k_begin(StepState* st)
 {
-    st->done = st->t >= st->t_end ? 1 : 0;
+    st->done = (st->t >= st->t_end || st->error) ? 1 : 0;
     if (st->done) return;
+    st->bar[0] = 0;
+    st->bar_err = 0;
     st->mv = 0;
     for (int k = 0; k < 4 * kStages; ++k) st->cnt[k] = 0;
     for (int k = 0; k < 4; ++k) st->mask_cnt[k] = 0;
@@ -655,6 +889,11 @@ __global__ void k_begin(StepState* st)
 __global__ void k_finish(StepState* st)
 {
     if (st->done) return;
+    if (st->bar_err) {
+        st->error = st->bar_err;
+        st->done = 1;
+        return;
+    }
     st->t += st->dt;
     st->steps += 1;
     st->upd += st->mask_cnt[0];
@@ -855,8 +1094,8 @@ __global__ void __launch_bounds__(256) k_update_crs(Grid2 g, Field4 in, Field4 o
     const int NX = g.nx - 1, NY = g.ny - 1;
     for (long e = gtid(); e < n; e += stride) {
         const size_t a = list[e];
-        const int i = (int)(a % (size_t)g.pitch) - kGhost;
-        const int j = (int)(a / (size_t)g.pitch) - kGhost;
+        const int i = (int)((unsigned)a % (unsigned)g.pitch) - kGhost;
+        const int j = (int)((unsigned)a / (unsigned)g.pitch) - kGhost;
         const int lev = lvl[a];
         if (lev < 0 || lev > g.maxl) continue;
         const int d = g.D(lev);
@@ -1042,6 +1281,23 @@ struct Solver2D {
     int device = 0;
     int list_rows_blocks = 0;
     int face_blocks = 0;
+    // Phase marks of a profiled step (null while capturing the graph).
+    cudaEvent_t* prof_ev = nullptr;
+    int prof_n = 0;
+    void mark()
+    {
+        if (prof_ev) cudaEventRecord(prof_ev[prof_n++], stream);
+    }
+    // Per-launch marks of a finely profiled step: an event after every kernel.
+    std::vector<std::pair<const char*, cudaEvent_t>>* fine = nullptr;
+    void after(const char* name)
+    {
+        if (!fine) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, stream);
+        fine->emplace_back(name, e);
+    }
 
     ~Solver2D() { release(); }
 
@@ -1134,6 +1390,13 @@ struct Solver2D {
         int dev_sms = 148;
         cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
         face_blocks = dev_sms * 8;
+        {
+            int per_sm = 0;
+            AWCM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_prepare, kPrepThreads, 0));
+            int coop = 0;
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+            prep_blocks = (coop && per_sm > 0) ? dev_sms : 0;  // one CTA per SM; 0 = per-phase launches
+        }
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
     }
@@ -1236,24 +1499,33 @@ struct Solver2D {
     // ---------------------------------------------------------------- enqueue helpers
     long grid_points() const { return (long)g.nx * g.ny; }
 
+    long band_count(int lev, int which) const
+    {
+        const Band b = band_of(g, lev, which);
+        return (long)b.cx * b.cy;
+    }
+    long details(int lev) const { return band_count(lev, 0) + band_count(lev, 1) + band_count(lev, 2); }
+
     void enq_cr(int bit, const StepState* s)
     {
         for (int lev = g.maxl - 1; lev >= 0; --lev) {
-            const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1);
-            k_cr<0><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, m, lev, bit, s);
-            k_cr<1><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, m, lev, bit, s);
-            launches += 2;
+            k_cr<<<blocks_for(details(lev), 256), 256, 0, stream>>>(g, m, lev, bit, s);
+            after("k_cr");
+            launches += 1;
         }
     }
 
+    // The forward transform's scratch plane is the first x-face flux plane (faces are not live
+    // during PrepareEuler).
     void enq_fwt(const StepState* s)
     {
         for (int lev = g.maxl - 1; lev >= 0; --lev) {
-            const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1), bc = band_of(g, lev, 3);
-            k_fwt<0><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, s);
-            k_fwt<1><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, s);
-            k_fwt<2><<<blocks_for((long)bc.cx * bc.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, s);
-            launches += 3;
+            k_fwt_a<<<blocks_for(details(lev), 256), 256, 0, stream>>>(g, q.p[0], fx.p[0], m, lev, s);
+            after("k_fwt_a");
+            const long nb = band_count(lev, 3) + band_count(lev, 0) + band_count(lev, 1);
+            k_fwt_b<<<blocks_for(nb, 256), 256, 0, stream>>>(g, q.p[0], fx.p[0], m, lev, s);
+            after("k_fwt_b");
+            launches += 2;
         }
     }
 
@@ -1262,8 +1534,11 @@ struct Solver2D {
         for (int lev = 0; lev < g.maxl; ++lev) {
             const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1), bc = band_of(g, lev, 3);
             k_iwt<0><<<blocks_for((long)bc.cx * bc.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            after("k_iwt<0>");
             k_iwt<1><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            after("k_iwt<1>");
             k_iwt<2><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            after("k_iwt<2>");
             launches += 3;
         }
     }
@@ -1271,12 +1546,14 @@ struct Solver2D {
     void enq_interp(int from, int to, const StepState* s)
     {
         k_interp_init<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, m, from, to, s);
+        after("k_interp_init");
         launches += 1;
         enq_cr(kBitInterp, s);
         for (int lev = 0; lev < g.maxl; ++lev) {
-            const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1);
-            k_interp<0><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, q, m, lev, from, s);
-            k_interp<1><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+            k_interp<0><<<blocks_for(band_count(lev, 0) + band_count(lev, 1), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+            after("k_interp<0>");
+            k_interp<1><<<blocks_for(band_count(lev, 2), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+            after("k_interp<1>");
             launches += 2;
         }
     }
@@ -1284,24 +1561,61 @@ struct Solver2D {
     void enq_aaz(int bit, const StepState* s)
     {
         k_copy_bit_all<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, bit, kBitCopy, s);
+        after("k_copy_bit_all");
         k_aaz<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, m, bit, kBitCopy, s);
+        after("k_aaz");
         launches += 2;
     }
 
-    // AWCM_2D::PrepareEuler (Wavelet/AWCM_2D.h:114-147).
+    // AWCM_2D::PrepareEuler (Wavelet/AWCM_2D.h:114-147): one launch per phase (prep_mode 1, the
+    // default: the phases are latency-bound and run at full occupancy as separate kernels), or
+    // (prep_mode 0) the persistent cooperative kernel with grid barriers.
+    int prep_mode = 1;
+    int prep_blocks = 0;
+
     void enq_prepare(const StepState* s)
     {
+        if (prep_mode == 0 && s == st && prep_blocks > 0) {
+            PrepArgs A;
+            A.g = g;
+            A.q = q;
+            A.tb = fx.p[0];
+            A.m = m;
+            for (int k = 0; k < 4; ++k) A.lvl[k] = lvl[k];
+            A.st = st;
+            A.sync = st->bar;
+            A.err = &st->bar_err;
+            A.plane = plane;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(prep_blocks);
+            cfg.blockDim = dim3(kPrepThreads);
+            cfg.stream = stream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            cudaLaunchKernelEx(&cfg, k_prepare, A);
+            after("k_prepare");
+            launches += 1;
+            return;
+        }
         const long np = grid_points();
         k_copy_bit_all<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, 0, kBitTemp, s);
+        after("k_copy_bit_all");
         launches += 1;
         enq_fwt(s);
         k_band_copy<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
+        after("k_band_copy");
         k_aaz<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
+        after("k_aaz");
         launches += 2;
         enq_cr(0, s);
         for (int k = 1; k <= 3; ++k) {
             k_cl<<<blocks_for((long)plane, 256), 256, 0, stream>>>(g, m, lvl[k - 1], k - 1, k, plane, s);
+            after("k_cl");
             k_apd<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, lvl[k - 1], k, k - 1, s);
+            after("k_apd");
             launches += 2;
             enq_cr(k, s);
         }
@@ -1313,6 +1627,7 @@ struct Solver2D {
     {
         const long n = 2L * kGhost * g.ny + 2L * kGhost * g.nx;
         k_bc<<<blocks_for(n, 256), 256, 0, stream>>>(g, f, s, 0.0);
+        after("k_bc");
         launches += 1;
     }
 
@@ -1322,6 +1637,7 @@ struct Solver2D {
         cudaMemsetAsync(ay[stage], 0, sizeof(double) * g.nx, stream);
         dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32), block(32, 8);
         k_alpha<<<grid, block, 0, stream>>>(g, f, m, bit, ax[stage], ay[stage], with_cfl ? &st->mv : nullptr, st);
+        after("k_alpha");
         launches += 1;
     }
 
@@ -1329,39 +1645,55 @@ struct Solver2D {
     {
         uint32_t* const* L = lists + 4 * stage;
         const unsigned* C = st->cnt + 4 * stage;
+        mark();
         k_face<0><<<face_blocks, 128, 0, stream>>>(g, in, fx, L[2], C + 2, ax[stage], st);
+        after("k_face<0>");
         k_face<1><<<face_blocks, 128, 0, stream>>>(g, in, fy, L[3], C + 3, ay[stage], st);
+        after("k_face<1>");
         launches += 2;
+        mark();
         const int ub = face_blocks / 2;
         if (stage == 0) {
             k_update_fin<1><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            after("k_update_fin<1>");
             k_update_crs<1><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[2], L[1], C + 1, st);
+            after("k_update_crs<1>");
         } else if (stage == 1) {
             k_update_fin<2><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            after("k_update_fin<2>");
             k_update_crs<2><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[1], L[1], C + 1, st);
+            after("k_update_crs<2>");
         } else {
             k_update_fin<3><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            after("k_update_fin<3>");
             k_update_crs<3><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[0], L[1], C + 1, st);
+            after("k_update_crs<3>");
         }
         launches += 2;
+        mark();
     }
 
     // One pass of the driver loop (main_2d_euler(quad).cpp:58-334).
     void enq_step()
     {
         launches = 0;
+        mark();
         k_begin<<<1, 1, 0, stream>>>(st);
+        after("k_begin");
         launches += 1;
         enq_prepare(st);
+        mark();
         enq_bc(q, st);
         enq_alpha(q, 3, 0, true);
         k_dt<<<1, 1, 0, stream>>>(g, st);
+        after("k_dt");
         launches += 1;
         {
             ListArgs la;
             for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
             dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
             k_lists<<<grid, 256, 0, stream>>>(g, m, lvl[2], lvl[1], lvl[0], la, st);
+            after("k_lists");
             launches += 1;
         }
         enq_faces_update(0, q, q2);
@@ -1372,8 +1704,11 @@ struct Solver2D {
         enq_alpha(q1, 1, 2, false);
         enq_faces_update(2, q1, q1);
         k_remove_residue<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, q, m, 0, 1, st);
+        after("k_remove_residue");
         k_finish<<<1, 1, 0, stream>>>(st);
+        after("k_finish");
         launches += 2;
+        mark();
     }
 
     int build_graph()
@@ -1407,6 +1742,9 @@ struct Solver2D {
         h.t_end = t_end;
         h.dt_fixed = dt_fixed;
         h.done = 0;
+        h.error = 0;
+        h.bar_err = 0;
+        h.bar[0] = 0;
         AWCM_CUDA_TRY(cudaMemcpyAsync(st, &h, sizeof(StepState), cudaMemcpyHostToDevice, stream));
         return kOk;
     }
@@ -1428,6 +1766,10 @@ struct Solver2D {
         StepState h;
         rc = read_state(&h);
         if (rc) return rc;
+        if (h.error) {
+            set_last_error("grid barrier wait ran out in the prepare kernel", __FILE__, __LINE__);
+            return h.error;
+        }
         if (out) {
             out[0] = h.dt;
             out[1] = h.do_print;
@@ -1451,12 +1793,89 @@ struct Solver2D {
         StepState h;
         rc = read_state(&h);
         if (rc) return rc;
+        if (h.error) {
+            set_last_error("grid barrier wait ran out in the prepare kernel", __FILE__, __LINE__);
+            return h.error;
+        }
         if (out) {
             out[0] = h.t;
             out[1] = h.steps - h0.steps;
             out[2] = (double)(h.upd - h0.upd);
             out[3] = (double)(h.stage_pts - h0.stage_pts);
         }
+        return kOk;
+    }
+
+    // One step with the same kernels launched eagerly and CUDA events at the phase boundaries.
+    // out[0] prepare ms, [1] CFL/LF speeds/dt/worklists ms, [2..4] face kernels ms per stage,
+    // [5..7] point-update kernels ms per stage, [8] boundary fills + LF speeds of stages 2-3 ms,
+    // [9] residue removal ms, [10] total ms, [11..13] faces per stage, [14..16] stage points,
+    // [17] |mask0|, [18] dt.
+    int profile_step(double tol, double cfl, double t, double t_end, double* out)
+    {
+        int rc = write_params(tol, cfl, t, t_end, 0.0);
+        if (rc) return rc;
+        cudaEvent_t ev[16];
+        for (auto& e : ev) AWCM_CUDA_TRY(cudaEventCreate(&e));
+        prof_ev = ev;
+        prof_n = 0;
+        enq_step();
+        prof_ev = nullptr;
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        // marks: 0 start, 1 after prepare, then per stage (faces begin, faces end, updates end), last = end
+        float ms[16] = {};
+        for (int k = 1; k < prof_n; ++k) cudaEventElapsedTime(&ms[k], ev[k - 1], ev[k]);
+        out[0] = ms[1];
+        out[1] = ms[2];  // mark 2 = faces begin of stage 0
+        double between = 0;
+        for (int s2 = 0; s2 < kStages; ++s2) {
+            out[2 + s2] = ms[3 + 3 * s2];
+            out[5 + s2] = ms[4 + 3 * s2];
+            if (s2 > 0) between += ms[2 + 3 * s2];
+        }
+        out[8] = between;
+        out[9] = ms[prof_n - 1];
+        float tot = 0;
+        cudaEventElapsedTime(&tot, ev[0], ev[prof_n - 1]);
+        out[10] = tot;
+        StepState h;
+        rc = read_state(&h);
+        for (auto& e : ev) cudaEventDestroy(e);
+        if (rc) return rc;
+        for (int s2 = 0; s2 < kStages; ++s2) {
+            out[11 + s2] = (double)h.cnt[4 * s2 + 2] + h.cnt[4 * s2 + 3];
+            out[14 + s2] = (double)h.cnt[4 * s2 + 0] + h.cnt[4 * s2 + 1];
+        }
+        out[17] = h.mask_cnt[0];
+        out[18] = h.dt;
+        return kOk;
+    }
+
+    // One step with an event after every kernel: per-launch device times (ms) in launch order.
+    int profile_fine(double tol, double cfl, double t, double t_end, std::vector<std::pair<const char*, float>>& out)
+    {
+        int rc = write_params(tol, cfl, t, t_end, 0.0);
+        if (rc) return rc;
+        std::vector<std::pair<const char*, cudaEvent_t>> evs;
+        cudaEvent_t e0;
+        cudaEventCreate(&e0);
+        cudaEventRecord(e0, stream);
+        fine = &evs;
+        enq_step();
+        fine = nullptr;
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        cudaEvent_t prev = e0;
+        out.clear();
+        for (auto& pe : evs) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, prev, pe.second);
+            out.emplace_back(pe.first, ms);
+            prev = pe.second;
+        }
+        for (auto& pe : evs) cudaEventDestroy(pe.second);
+        cudaEventDestroy(e0);
         return kOk;
     }
 
@@ -1704,6 +2123,37 @@ int awcm2d_launches_per_step(awcm2d_t h, int* n)
     int rc = h->s.build_graph();
     *n = h->s.launches;
     return rc;
+}
+int awcm2d_profile_step(awcm2d_t h, double tol, double cfl, double t, double t_end, double* out)
+{
+    AWCM_H(h);
+    if (!out) return awcm::kErrArg;
+    return h->s.profile_step(tol, cfl, t, t_end, out);
+}
+int awcm2d_profile_kernels(awcm2d_t h, double tol, double cfl, double t, double t_end, int cap, char* names,
+                           double* ms, int* n)
+{
+    AWCM_H(h);
+    if (!names || !ms || !n || cap <= 0) return awcm::kErrArg;
+    std::vector<std::pair<const char*, float>> v;
+    const int rc = h->s.profile_fine(tol, cfl, t, t_end, v);
+    if (rc) return rc;
+    *n = (int)std::min<size_t>(v.size(), (size_t)cap);
+    for (int k = 0; k < *n; ++k) {
+        std::strncpy(names + 32 * k, v[k].first, 31);
+        names[32 * k + 31] = 0;
+        ms[k] = v[k].second;
+    }
+    return awcm::kOk;
+}
+int awcm2d_set_prepare_mode(awcm2d_t h, int mode)
+{
+    AWCM_H(h);
+    if (mode != 0 && mode != 1) return awcm::kErrArg;
+    h->s.prep_mode = mode;
+    if (h->s.graph) cudaGraphExecDestroy(h->s.graph);
+    h->s.graph = nullptr;
+    return awcm::kOk;
 }
 int awcm2d_stream(awcm2d_t h, void** stream)
 {

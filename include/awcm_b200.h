@@ -62,6 +62,9 @@ extern "C" {
 const char* awcm_last_error(void);
 /* Library version string. */
 const char* awcm_version(void);
+/* Dense FP64 FMA throughput of the current device in TFLOP/s (2 flops per DFMA), best of
+ * `repeats` launches of `iters` FMA rounds: the denominator of the FP64 roofline. */
+int awcm_measure_fp64_peak(int iters, int repeats, double* tflops);
 
 /* ------------------------------------------------------------------------------------------- 2D
  * One 2D AWCM Euler instance: the MRA_GRID_INT_2D dyadic node grid
@@ -106,8 +109,20 @@ int awcm2d_step(awcm2d_t h, double tol, double cfl, double t, double t_next, dou
  * step), stopping early once t >= t_end.  out[4]: final t, steps taken, sum |mask0| over the steps,
  * sum of stage points (|mask2|+|mask1|+|mask0|). */
 int awcm2d_advance(awcm2d_t h, double tol, double cfl, double t_start, double t_end, int n_steps, double* out);
+/* One step with the step's kernels launched eagerly and CUDA events at the phase boundaries.
+ * out[19]: ms of prepare, CFL+LF speeds+dt+worklists, face kernels (stages 1..3), point-update
+ * kernels (stages 1..3), boundary fills + LF speeds of stages 2-3, residue removal, total; faces
+ * per stage (3), stage points (3), |mask0|, dt. */
+int awcm2d_profile_step(awcm2d_t h, double tol, double cfl, double t, double t_end, double* out);
+/* One step with a CUDA event after every kernel: names (32 bytes each) and device ms of up to
+ * cap launches in launch order; *n = launches recorded.  Instrumentation only. */
+int awcm2d_profile_kernels(awcm2d_t h, double tol, double cfl, double t, double t_end, int cap, char* names,
+                           double* ms, int* n);
 /* Kernel launches enqueued by one step (for instrumentation). */
 int awcm2d_launches_per_step(awcm2d_t h, int* n);
+/* PrepareEuler execution: 1 = one kernel launch per pass (default), 0 = one persistent
+ * cooperative kernel with bounded-spin grid barriers.  Both give identical results. */
+int awcm2d_set_prepare_mode(awcm2d_t h, int mode);
 /* CUDA stream the instance runs on (cudaStream_t), for event timing by the caller. */
 int awcm2d_stream(awcm2d_t h, void** stream);
 
