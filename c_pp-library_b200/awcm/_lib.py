@@ -65,6 +65,8 @@ _SIGS = {
     "awcm1d_batch_pass": [c_void_p, c_int, c_int, c_int, c_int],
     "awcm1d_batch_set_launch": [c_void_p, c_int, c_int],
     "awcm1d_batch_stream": [c_void_p, ctypes.POINTER(c_void_p)],
+    "awcm1d_step_noalloc": [c_int, c_int, c_double, c_double, c_double, c_int, c_double, c_double, c_double, c_double,
+                            c_void_p, c_void_p, c_void_p, c_void_p],
     "euler2d_flux": [c_void_p, c_void_p, c_int, c_int, c_double, c_void_p],
     "euler2d_spectral_radius": [c_void_p, c_void_p, c_int, c_int, c_double, c_void_p],
     "awcm_last_error": [],

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -452,18 +453,10 @@ __device__ void stage1(const Ctx& c, int b, int l, double alpha, double dt, int 
     __syncthreads();
 }
 
+// One RK3 step of one instance on the context's buffers (q, stage copies, faces, mask bytes, levels).
 template <int SCHEME>
-__device__ void step_instance(Inst1& I, const Pool& P, uint32_t* list, double* dred, unsigned* ured)
+__device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, unsigned* ured)
 {
-    if (I.t >= I.t_end) {
-        if (threadIdx.x == 0) I.done = 1;
-        return;
-    }
-    const int w = I.nx + 2 * kGhost;
-    double* base = P.q + I.q_off;
-    uint8_t* mb = P.m + I.m_off;
-    const Ctx c{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + w), P.W, w, I.nx, I.nx - 1,
-                I.maxl};
     prepare1(c);
 
     // CFL (main_1d_euler.cpp:67-81)
@@ -518,6 +511,21 @@ __device__ void step_instance(Inst1& I, const Pool& P, uint32_t* list, double* d
         I.done = I.t >= I.t_end;
     }
     __syncthreads();
+}
+
+template <int SCHEME>
+__device__ void step_instance(Inst1& I, const Pool& P, uint32_t* list, double* dred, unsigned* ured)
+{
+    if (I.t >= I.t_end) {
+        if (threadIdx.x == 0) I.done = 1;
+        return;
+    }
+    const int w = I.nx + 2 * kGhost;
+    double* base = P.q + I.q_off;
+    uint8_t* mb = P.m + I.m_off;
+    const Ctx c{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + w), P.W, w, I.nx, I.nx - 1,
+                I.maxl};
+    step_ctx<SCHEME>(I, c, list, dred, ured);
 }
 
 // One RK3 step of every queued instance.  CTAs pull queue slots until the queue is exhausted.
@@ -854,6 +862,86 @@ struct Batch1D {
     }
 };
 
+// =========================================================================== allocation-free step
+// One RK3 step of a single 1D instance whose conserved field and mask/level state live in device
+// buffers the caller owns, with every other buffer the step needs -- the stage-start and stage-input
+// copies of the field, the face fluxes and the instance descriptor -- placed in the file-scope
+// array below instead of memory allocated per instance.  It is sized for instances of up to
+// kNoAllocMaxNx points (Jmax 13 with 17 coarse points): 9 x 8199 doubles plus a 256-byte
+// descriptor, about 577 KiB, which every GPU that loads this library holds until the process exits.
+constexpr int kNoAllocMaxNx = 8193;
+constexpr int kNoAllocMaxW = kNoAllocMaxNx + 2 * kGhost;
+constexpr int kNoAllocHeader = 32;  // doubles reserved for the descriptor (Inst1 fits in 256 bytes)
+constexpr size_t kNoAllocDoubles = kNoAllocHeader + (size_t)9 * kNoAllocMaxW;
+static_assert(sizeof(Inst1) <= kNoAllocHeader * sizeof(double), "descriptor does not fit the reserved header");
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+namespace {
+
+// scratch: the device address of g_noalloc_scratch (resolved on the host once per device).
+__global__ void k_step1d_noalloc(Inst1 param, double* q, uint8_t* state, double* scratch, double* out, Weights W)
+{
+    extern __shared__ uint32_t list[];
+    __shared__ double dred[32];
+    __shared__ unsigned ured[32];
+    Inst1& I = *reinterpret_cast<Inst1*>(scratch);
+    if (threadIdx.x == 0) I = param;  // the descriptor is rewritten by every call
+    __syncthreads();
+    const int w = param.nx + 2 * kGhost;
+    double* qc = scratch + kNoAllocHeader;
+    double* qt = qc + 3 * w;
+    double* fl = qt + 3 * w;
+    if (I.t < I.t_end) {
+        const Ctx c{I, q, qc, qt, fl, state, (int8_t*)(state + w), W, w, I.nx, I.nx - 1, I.maxl};
+        if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
+        else step_ctx<kWenoZ>(I, c, list, dred, ured);
+    } else if (threadIdx.x == 0) {
+        I.done = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        out[0] = I.t;
+        out[1] = I.dt;
+        out[2] = I.do_print;
+        out[3] = I.done;
+        out[4] = I.steps;
+        for (int k = 0; k < 4; ++k) out[5 + k] = I.mask_cnt[k];
+        out[9] = I.mv;
+        out[10] = I.alpha[0];
+        out[11] = I.alpha[1];
+        out[12] = I.alpha[2];
+        out[13] = (double)I.upd;
+        out[14] = I.err;
+        out[15] = 0;
+    }
+}
+
+// Device address of the scratch array, resolved once per device (host code must not use the
+// symbol itself: on the host it is only a stand-in for the device copy).
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+int noalloc_scratch(int dev, double** ptr)
+{
+    if (dev < 0 || dev >= kMaxDevices) return kErrArg;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+            return kErrCuda;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *ptr = static_cast<double*>(g_noalloc_addr[dev]);
+    return kOk;
+}
+
+}  // namespace
+
 }  // namespace awcm
 
 // ======================================================================================== C-ABI
@@ -1016,6 +1104,51 @@ int awcm1d_batch_stream(awcm1d_batch_t h, void** stream)
     if (!h || !stream) return awcm::kErrArg;
     *stream = (void*)h->b.stream;
     return awcm::kOk;
+}
+
+int awcm1d_step_noalloc(int num_levels, int nx_coarse, double x_min, double x_max, double gamma, int scheme,
+                        double tol, double cfl, double t, double t_end, double* q_dev, uint8_t* state_dev,
+                        double* out_dev, void* stream)
+{
+    using namespace awcm;
+    if (num_levels < 2 || num_levels > 20 || nx_coarse < 5 || !q_dev || !state_dev || !out_dev) {
+        set_last_error("awcm1d_step_noalloc: bad argument", __FILE__, __LINE__);
+        return kErrArg;
+    }
+    if (scheme != kWenoZ && scheme != kWeno5) {
+        set_last_error("awcm1d_step_noalloc: scheme must be 0 (WENO-Z) or 1 (WENO5)", __FILE__, __LINE__);
+        return kErrArg;
+    }
+    const long long nx = (long long)(nx_coarse - 1) * (1LL << (num_levels - 1)) + 1;
+    if (nx > kNoAllocMaxNx) {
+        char msg[160];
+        std::snprintf(msg, sizeof(msg),
+                      "awcm1d_step_noalloc: Nx = %lld exceeds the static scratch limit of %d points", nx,
+                      kNoAllocMaxNx);
+        set_last_error(msg, __FILE__, __LINE__);
+        return kErrArg;
+    }
+    int dev = 0;
+    AWCM_CUDA_TRY(cudaGetDevice(&dev));
+    double* scratch = nullptr;
+    const int rc = noalloc_scratch(dev, &scratch);
+    if (rc) return rc;
+    Inst1 I{};
+    I.nx = (int)nx;
+    I.maxl = num_levels - 1;
+    I.scheme = scheme;
+    I.x_min = x_min;
+    I.dx = (x_max - x_min) / (double)(nx - 1);
+    I.gamma = gamma;
+    I.tol = tol;
+    I.cfl = cfl;
+    I.t = t;
+    I.t_end = t_end;
+    const int w = (int)nx + 2 * kGhost;
+    const size_t smem = sizeof(uint32_t) * (size_t)(w + 32);
+    k_step1d_noalloc<<<1, 256, smem, (cudaStream_t)stream>>>(I, q_dev, state_dev, scratch, out_dev, make_weights());
+    AWCM_CUDA_TRY(cudaGetLastError());
+    return kOk;
 }
 
 }  // extern "C"

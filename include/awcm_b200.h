@@ -169,6 +169,32 @@ int awcm1d_batch_pass(awcm1d_batch_t h, int k, int op, int mask_id, int level_id
 int awcm1d_batch_set_launch(awcm1d_batch_t h, int threads, int ctas_per_sm);
 int awcm1d_batch_stream(awcm1d_batch_t h, void** stream);
 
+/* Allocation-free RK3 step of ONE 1D instance.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: a host framework whose GPU memory belongs to
+ * its own caching allocator (a cudaMalloc/cudaFree behind its back fragments that pool, and both
+ * calls can synchronize the device and stall its pipeline), or an embedded or real-time loop that
+ * gets a fixed memory budget at start-up and may not allocate afterwards.  Such a caller passes its
+ * own device buffers for the instance's state and results; everything else the step needs comes
+ * from a static scratch array inside this library, so the call performs no cudaMalloc, cudaFree or
+ * other allocation.
+ *
+ *   q_dev     (in/out) conserved field, 3 component planes of Nx+6 doubles (ghost ring of 3):
+ *             q_dev[p*(Nx+6) + i+3];
+ *   state_dev (in/out) Nx+6 mask bytes (bits 0..3 = mask0..mask3, bit 4 = previous mask0;
+ *             before the first step: 0x01 inside, 0xe1 on the ghost ring) followed by 4 planes of
+ *             Nx+6 int8 levels (level0..level3; start at 0);
+ *   out_dev   (out) 16 doubles in the layout of awcm1d_batch_status.
+ * Nx = (nx_coarse-1)*2^(num_levels-1)+1 must not exceed 8193; larger instances are rejected with
+ * AWCM_ERR_ARG.  The work is enqueued on `stream` (0 = default stream) and the call returns
+ * without waiting.  The first call on a device resolves the scratch array's device address (a
+ * cudaGetSymbolAddress, no allocation); make that first call before any stream capture.  All
+ * calls on a device share the one scratch array, which keeps the last call's contents: calls that
+ * overlap on the GPU (other streams, other host threads) race, so serialize them. */
+int awcm1d_step_noalloc(int num_levels, int nx_coarse, double x_min, double x_max, double gamma, int scheme,
+                        double tol, double cfl, double t, double t_end, double* q_dev, uint8_t* state_dev,
+                        double* out_dev, void* stream);
+
 /* EULER_EQUATION_2D on a batch of n conserved states in device memory (n x 4 doubles):
  * ComputeFu/ComputeGu (EULER_EQUATION.h:74-99) and Spectral_RadiusX/Y (:118-142). */
 int euler2d_flux(const double* q_dev, double* f_dev, int n, int dir, double gamma, void* stream);
