@@ -208,19 +208,7 @@ def run_b200(args):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        tt = torch.tensor([v], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        return float(tt.item())
-
-    def sum_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        tt = torch.tensor([v], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.SUM)
-        return float(tt.item())
+    from awcm.dist import reduce_run
 
     warmup = max(3, args.warmup)
     t, n, _, _ = s.advance(tol, cfl, 0.0, t_end, warmup)
@@ -234,8 +222,7 @@ def run_b200(args):
         e1.record(stream)
         barrier()
     ms = e0.elapsed_time(e1)
-    ms_max = max_over_ranks(ms)
-    upd_all = sum_over_ranks(upd)
+    ms_max, upd_all = reduce_run(ms, upd, device="cuda")
     value = upd_all / (ms_max / 1e3)
     clocks = clk.summary()
 
@@ -281,9 +268,9 @@ def run_b200(args):
             awcm._lib.call("awcm2d_get_q", s.h, awcm._lib.ptr(host_out.numpy(), ctypes.c_double))
             host_in, host_out = host_out, host_in
         barrier()
-        wall = max_over_ranks(time.perf_counter() - t0)
+        wall, upd_e_all = reduce_run(time.perf_counter() - t0, upd_e, device="cuda")
         nbytes = int(np.prod(shape)) * 8
-        e2e = {"value": sum_over_ranks(upd_e) / wall, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+        e2e = {"value": upd_e_all / wall, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": n_e2e,
                "note": "per step: H2D of the dense conserved field (reference layout, pinned), one RK3 step, D2H"}
 

@@ -1,0 +1,90 @@
+"""The CPU restatement against the reference itself (compiled from the reference tree), on cases
+beyond the committed fixtures.  Skipped where the reference build is absent."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import Oracle1D, Oracle2D
+
+pytestmark = pytest.mark.skipif(not oracle.reference_available(), reason="reference build (oracle/_ref) absent")
+
+
+def corner_free(q):
+    keep = np.ones(q.shape[:2], bool)
+    keep[:3, :3] = keep[:3, -3:] = keep[-3:, :3] = keep[-3:, -3:] = False
+    return q[keep]
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_1d_sod_long(scheme):
+    n = 1025
+    a = Oracle1D(7, 17, 0.5 / n, 1 - 0.5 / n, scheme=scheme, kind="port")
+    b = Oracle1D(7, 17, 0.5 / n, 1 - 0.5 / n, scheme=scheme, kind="reference")
+    for o in (a, b):
+        o.init_riemann(0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+    t = 0.0
+    for k in range(300):
+        oa, ob = a.step(1e-4, 0.5, t, 0.2), b.step(1e-4, 0.5, t, 0.2)
+        assert np.array_equal(oa, ob), k
+        t += oa[0]
+    assert np.array_equal(a.get_q(), b.get_q())
+    assert np.array_equal(a.get_masks(), b.get_masks())
+    assert np.array_equal(a.get_levels(), b.get_levels())
+
+
+def test_1d_shipped_driver_geometry():
+    """The shipped driver's own grid: 16 coarse points, 11 levels, [0,10], tol 1e-6 (first steps)."""
+    nx = 15 * 2 ** 10 + 1
+    dxf = 10.0 / nx
+    a = Oracle1D(11, 16, 0.5 * dxf, 10 - 0.5 * dxf, scheme=1, kind="port")
+    b = Oracle1D(11, 16, 0.5 * dxf, 10 - 0.5 * dxf, scheme=1, kind="reference")
+    for o in (a, b):
+        o.init_riemann(5.0, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+    t = 0.0
+    for k in range(20):
+        oa, ob = a.step(1e-6, 0.5, t, 2.0), b.step(1e-6, 0.5, t, 2.0)
+        assert np.array_equal(oa, ob), k
+        t += oa[0]
+    assert np.array_equal(a.get_q(), b.get_q())
+
+
+@pytest.mark.parametrize("case", [
+    (6, 17, 17, (0.0, 1.0, 0.0, 1.0), 0, 0, 0.5, 0.5, 1e-3, 0.4, 2),   # 513^2 quadrants
+    (5, 17, 5, (0.0, 4.0, 0.0, 1.0), 1, 1, 1.5, 0.0, 1e-3, 0.5, 3),   # double Mach, reference IC density 1.5
+    (5, 9, 9, (0.0, 10.0, -5.0, 5.0), 2, 2, 5.0, 0.0, 1e-3, 0.4, 3),  # vortex at the reference's centre
+])
+def test_2d_cases(case):
+    nl, nxc, nyc, dom, bc, prob, a_, b_, tol, cfl, steps = case
+    a = Oracle2D(nl, nxc, nyc, *dom, bc_kind=bc, kind="port")
+    b = Oracle2D(nl, nxc, nyc, *dom, bc_kind=bc, kind="reference")
+    for o in (a, b):
+        o.init_problem(prob, a_, b_)
+    assert np.array_equal(a.get_q(), b.get_q())
+    t = 0.0
+    for k in range(steps):
+        oa, ob = a.step(tol, cfl, t, 10.0), b.step(tol, cfl, t, 10.0)
+        assert np.array_equal(oa, ob), k
+        t += oa[0]
+        assert np.array_equal(corner_free(a.get_q()), corner_free(b.get_q()))
+        assert np.array_equal(a.get_masks(), b.get_masks())
+        assert np.array_equal(a.get_levels()[:3], b.get_levels()[:3])
+
+
+def test_2d_passes_individually():
+    a = Oracle2D(5, 9, 9, 0.0, 1.0, 0.0, 1.0, kind="port")
+    b = Oracle2D(5, 9, 9, 0.0, 1.0, 0.0, 1.0, kind="reference")
+    for o in (a, b):
+        o.init_problem(0, 0.5, 0.5)
+        o.fwt(1e-3)
+    assert np.array_equal(a.get_q(), b.get_q()) and np.array_equal(a.get_masks(), b.get_masks())
+    for op, mask_id, level_id in [(oracle.BAND, 0, 0), (oracle.AAZ, 0, 0), (oracle.CR, 0, 0), (oracle.CL, 0, 0),
+                                  (oracle.APD, 0, 0), (oracle.CR, 0, 0), (oracle.RR, 0, 0)]:
+        a.manager(op, mask_id, level_id)
+        b.manager(op, mask_id, level_id)
+        assert np.array_equal(a.get_masks(), b.get_masks()), op
+        assert np.array_equal(a.get_levels()[0], b.get_levels()[0]), op
+        assert np.array_equal(a.get_q(), b.get_q()), op
+    for o in (a, b):
+        o.iwt(0)
+        o.interpolate(4, 0)
+    assert np.array_equal(a.get_q(), b.get_q())
