@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
+    ap.add_argument("--capture", type=int, default=-1,
+                    help="profiling mode: K graph-replayed steps, then one eagerly launched step; prints its phases")
     return ap.parse_args()
 
 
@@ -313,8 +315,23 @@ def run_b200(args):
         torch.distributed.destroy_process_group()
 
 
+def run_capture(k: int):
+    """Small, self-ending run for ncu: the benchmark instance, k graph-replayed steps and one
+    profiled step (its face kernels are launches 6k+1 .. 6k+6 of k_face)."""
+    import awcm
+
+    w = WORKLOAD
+    s = awcm.AWCM2D(w["num_levels"], w["nx_coarse"], w["ny_coarse"], *w["domain"], bc_kind=0)
+    s.init_problem(0, *w["split"])
+    t, _, _, _ = s.advance(w["tol"], w["cfl"], 0.0, w["t_end"], k)
+    print(json.dumps(s.profile_step(w["tol"], w["cfl"], t, w["t_end"])))
+
+
 def main():
     args = parse()
+    if args.capture >= 0:
+        run_capture(args.capture)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:

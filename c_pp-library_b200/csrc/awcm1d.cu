@@ -698,6 +698,11 @@ struct Batch1D {
     int set_launch(int threads, int ctas_per_sm)
     {
         if (threads < 64 || threads > 1024 || threads % 32) return kErrArg;
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, k_step1d) == cudaSuccess && threads > fa.maxThreadsPerBlock) {
+            set_last_error("launch shape exceeds the step kernel's register budget", __FILE__, __LINE__);
+            return kErrArg;
+        }
         block = threads;
         int sms = 148, occ = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
