@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched shock-tube comparison")
     ap.add_argument("--capture", type=int, default=-1,
                     help="profiling mode: K graph-replayed steps, then one eagerly launched step; prints its phases")
     return ap.parse_args()
@@ -182,6 +183,90 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------------- batched shock tubes
+BATCHED = {
+    "workload": "512 seeded 1D shock tubes, Jmin 4, Jmax uniform in {8..13} (257..8193 points), eps 1e-4, "
+                "CFL 0.5, WENO-Z+Roe, t_end 0.15; rho/p log-uniform [0.1,10], u uniform [-1,1], interface U[0.3,0.7]",
+    "instances": 512, "tol": 1e-4, "cfl": 0.5, "t_end": 0.15,
+}
+
+
+def run_batched(rank: int, world: int):
+    """Batched form (one persistent launch, one CUDA graph per RK3 step, autotuned launch shape)
+    against the plain form (one instance per launch) on the same seeded tubes.  Instances are
+    sharded over ranks; timing is max over ranks."""
+    import torch
+
+    import awcm
+    from awcm import autotune, workloads
+    from awcm.dist import reduce_run, shard_instances
+
+    b_cfg = BATCHED
+    tubes_all = workloads.shock_tubes(b_cfg["instances"])
+    mine = shard_instances([t["nx"] for t in tubes_all], rank, world)
+    tubes = [tubes_all[k] for k in mine]
+    tol, cfl, t_end = b_cfg["tol"], b_cfg["cfl"], b_cfg["t_end"]
+    best, rates = autotune.tune(lambda: workloads.make_batch(awcm, tubes), t_end, tol, cfl)
+    b = workloads.make_batch(awcm, tubes)
+    b.set_launch(*best)
+    b.set_run(tol, cfl, 0.0, t_end)
+    b.steps(3)
+    b.sync()
+    u0 = b.totals()[0]
+    st = torch.cuda.ExternalStream(b.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 3
+    torch.cuda.synchronize()
+    e0.record(st)
+    steady = None
+    while True:
+        b.steps(250)
+        launches += 250
+        tot = b.totals()
+        if steady is None:
+            e1.record(st)
+            torch.cuda.synchronize()
+            steady = ((tot[0] - u0) / (e0.elapsed_time(e1) / 1e3))
+        if tot[2] == b.n or launches > 200000:
+            break
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms, upd = reduce_run(e0.elapsed_time(e1), tot[0] - u0, device="cuda")
+    value = upd / (ms / 1e3)
+    # plain form: instances one per launch (a sample across the size mix), same kernel and graph
+    sample = [tubes[k] for k in range(0, len(tubes), max(1, len(tubes) // 6))][:6]
+    p_ms, p_upd = 0.0, 0.0
+    for t in sample:
+        p = workloads.make_batch(awcm, [t])
+        p.set_launch(256, 0)
+        p.set_run(tol, cfl, 0.0, t_end)
+        p.steps(3)
+        p.sync()
+        pu0 = p.totals()[0]
+        pst = torch.cuda.ExternalStream(p.stream)
+        torch.cuda.synchronize()
+        e0.record(pst)
+        t0 = time.perf_counter()
+        while p.totals()[2] < 1 and time.perf_counter() - t0 < 4.0:
+            p.steps(100)
+        e1.record(pst)
+        torch.cuda.synchronize()
+        p_ms += e0.elapsed_time(e1)
+        p_upd += p.totals()[0] - pu0
+        p.close()
+    p_ms, p_upd = reduce_run(p_ms, p_upd, device="cuda")
+    plain = p_upd / (p_ms / 1e3)
+    return {
+        "workload": b_cfg["workload"], "metric": METRIC, "value": value, "unit": UNIT,
+        "steady_value": steady, "launches": launches, "instances": len(tubes_all), "ms": ms,
+        "launch_shape": {"threads": best[0], "ctas_per_sm": best[1]},
+        "autotune": {f"{k[0]}x{k[1]}": v for k, v in rates.items()},
+        "plain": {"value": plain, "unit": UNIT, "sample": f"{len(sample)} instances across the size mix, "
+                  "each alone in its own launch per step, up to 4 s each"},
+        "batched_over_plain": value / plain,
+    }
+
+
 # ------------------------------------------------------------------------------------- GPU arm
 def run_b200(args):
     rank, world, local = dist_env()
@@ -286,6 +371,8 @@ def run_b200(args):
         else:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
 
+    batched = None if args.no_batched else run_batched(rank, world)
+
     pitch = (s.nx + 6 + 31) // 32 * 32
     state_bytes = 5 * 4 * 8 * pitch * (s.ny + 6)  # Q, Q2, Q1, Fx, Fy planes
     line = {
@@ -306,6 +393,7 @@ def run_b200(args):
         "clocks": clocks,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "batched_1d": batched,
         "gpu_launches": launches * n_steps,
         "launches_per_step": launches,
     }

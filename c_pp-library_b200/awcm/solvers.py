@@ -162,6 +162,46 @@ class AWCM2D:
         call("awcm2d_stream", self.h, ctypes.byref(s))
         return s.value or 0
 
+    # frozen-mask run and adjoint --------------------------------------------------------------
+    @property
+    def tape_stride(self) -> int:
+        """Doubles of LF-speed tape per step: 3 stages x (alpha_x[Ny], alpha_y[Nx])."""
+        return 3 * (self.nx + self.ny)
+
+    def frozen_run(self, t0, dt, n_steps, replay=False):
+        """n_steps frozen-mask steps (no PrepareEuler / residue removal, fixed dt); LF speeds
+        recorded on the tape, or replayed from it.  Returns (t, device ms, sum |mask0|)."""
+        out = np.zeros(3)
+        call("awcm2d_frozen_run", self.h, t0, dt, n_steps, 2 if replay else 1, ptr(out, ctypes.c_double))
+        return out[0], out[1], out[2]
+
+    def set_wenoz_eps(self, eps: float):
+        """WENO-Z epsilon of the face reconstructions (WENOZ5::eps; 1e-40 as in the reference,
+        1e-6 in the differentiable mode of the gradient checks)."""
+        call("awcm2d_set_wenoz_eps", self.h, float(eps))
+
+    def adjoint(self, t0, dt, n_steps, target, checkpoint_every=0, replay=False, with_grad=True):
+        """Loss 1/2 |rho(t0 + n dt) - target|^2 of the frozen run from the current state and its
+        gradient w.r.t. the state at t0 ((Ny+6, Nx+6, 4), zero on ghosts).  Returns
+        (loss, grad or None, info dict)."""
+        tgt = np.ascontiguousarray(target, dtype=np.float64).reshape(self.ny, self.nx)
+        grad = np.empty((self.ny + 6, self.nx + 6, 4), np.float64) if with_grad else None
+        out = np.zeros(5)
+        call("awcm2d_adjoint", self.h, t0, dt, n_steps, checkpoint_every, 2 if replay else 1,
+             ptr(tgt, ctypes.c_double), ptr(grad, ctypes.c_double) if with_grad else None,
+             ptr(out, ctypes.c_double))
+        info = {"forward_ms": out[1], "reverse_ms": out[2], "checkpoint_every": int(out[3]), "device_bytes": out[4]}
+        return out[0], grad, info
+
+    def get_alpha_tape(self, n_steps):
+        t = np.empty((n_steps, self.tape_stride), np.float64)
+        call("awcm2d_get_alpha_tape", self.h, n_steps, ptr(t, ctypes.c_double))
+        return t
+
+    def set_alpha_tape(self, tape):
+        t = np.ascontiguousarray(tape, dtype=np.float64).reshape(-1, self.tape_stride)
+        call("awcm2d_set_alpha_tape", self.h, t.shape[0], ptr(t, ctypes.c_double))
+
 
 class AWCM1DBatch:
     """Independent 1D AWCM instances advanced together (one persistent launch per RK3 step)."""

@@ -4,7 +4,9 @@
 
 Flags: -gencode arch=compute_100a,code=sm_100a, -O3, -lineinfo, --fmad=false (the reference's
 IEEE double arithmetic has no fused multiply-add; keeping products and sums separately rounded is
-what makes results bit-identical to it).
+what makes results bit-identical to it).  The adjoint kernels (awcm2d_adjoint.cu) are a derivative
+checked against finite differences rather than a bit-exact restatement, and build with
+--fmad=true.
 """
 from __future__ import annotations
 
@@ -17,8 +19,10 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libawcm_b200.so")
-SOURCES = ["awcm_common.cu", "awcm2d.cu", "awcm1d.cu"]
-HEADERS = ["awcm_common.cuh", "awcm_numerics.cuh"]
+SOURCES = ["awcm_common.cu", "awcm2d.cu", "awcm1d.cu", "awcm2d_adjoint.cu"]
+HEADERS = ["awcm_common.cuh", "awcm_numerics.cuh", "awcm2d_types.cuh"]
+# per-file overrides of the contraction flags
+FMA_SOURCES = {"awcm2d_adjoint.cu"}
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -48,7 +52,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [_nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+        flags = NVCC_FLAGS
+        if src in FMA_SOURCES:
+            flags = [f.replace("--fmad=false", "--fmad=true").replace("-ffp-contract=off", "-ffp-contract=fast")
+                     for f in NVCC_FLAGS]
+        cmd = [_nvcc(), *flags, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -24,28 +24,10 @@
 
 #include "awcm_b200.h"
 #include "awcm_common.cuh"
+#include "awcm2d_types.cuh"
 
 namespace awcm {
 namespace {
-
-constexpr int kMaxLevels = 24;
-constexpr int kStages = 3;
-
-struct Grid2 {
-    int nx, ny, maxl, pitch, rows, bc_kind;
-    double x_min, y_min, dx, dy, gamma;
-    Weights W;
-    __host__ __device__ __forceinline__ size_t at(int i, int j) const
-    {
-        return (size_t)(j + kGhost) * pitch + (size_t)(i + kGhost);
-    }
-    __host__ __device__ __forceinline__ double w(int cnt, int k) const { return W.w[cnt][k + 1]; }
-    __host__ __device__ __forceinline__ int D(int lev) const { return 1 << (maxl - lev); }
-};
-
-struct Field4 {
-    double* p[4];
-};
 
 // Device-resident step scalars.
 struct StepState {
@@ -1036,7 +1018,7 @@ __global__ void __launch_bounds__(128) k_face(Grid2 g, Field4 f, Field4 out, con
         }
         const double al = DIR == 0 ? alpha[jj] : alpha[ii];
         double o[4];
-        face_flux_2d<DIR>(s, al, g.gamma, o);
+        face_flux_2d<DIR>(s, al, g.gamma, o, g.wz_eps);
 #pragma unroll
         for (int k = 0; k < 4; ++k) out.p[k][idx] = o[k];
     }
@@ -1324,6 +1306,10 @@ struct Solver2D {
         fr(st);
         for (auto& l : lists) fr(l);
         fr(staging);
+        free_adj();
+        fr(tape);
+        tape = nullptr;
+        tape_steps = 0;
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
     }
@@ -1348,6 +1334,7 @@ struct Solver2D {
         g.dx = (x_max - x_min) / (nx - 1);
         g.dy = (y_max - y_min) / (ny - 1);
         g.gamma = 1.4;
+        g.wz_eps = 1e-40;
         g.W = make_weights();
         plane = (size_t)g.pitch * g.rows;
         AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -1950,6 +1937,289 @@ struct Solver2D {
         return kOk;
     }
 
+    // ---------------------------------------------------------- frozen-mask run and its adjoint
+    // Frozen-mask step (the gradient configuration): the driver loop of main_2d_euler(quad).cpp
+    // without PrepareEuler and without residue removal, at a fixed dt, on the masks and levels of
+    // the last PrepareEuler.  The per-stage LF speeds are computed (and written to `tout` when
+    // given) or, with `tin`, replayed; tape layout per step: stage 0..2 x (alpha_x[Ny], alpha_y[Nx]).
+    // With `save`, the three stage inputs after their boundary fill (Q, Q2, Q1) are copied out.
+    size_t tape_stride() const { return (size_t)kStages * (g.nx + g.ny); }
+
+    void copy_field(Field4 dst, Field4 src)
+    {
+        for (int k = 0; k < 4; ++k)
+            cudaMemcpyAsync(dst.p[k], src.p[k], plane * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+    }
+
+    void enq_alpha_frozen(Field4 f, int bit, int stage, const double* tin, double* tout)
+    {
+        const size_t o = (size_t)stage * (g.nx + g.ny);
+        if (tin) {
+            cudaMemcpyAsync(ax[stage], tin + o, sizeof(double) * g.ny, cudaMemcpyDeviceToDevice, stream);
+            cudaMemcpyAsync(ay[stage], tin + o + g.ny, sizeof(double) * g.nx, cudaMemcpyDeviceToDevice, stream);
+            return;
+        }
+        enq_alpha(f, bit, stage, false);
+        if (tout) {
+            cudaMemcpyAsync(tout + o, ax[stage], sizeof(double) * g.ny, cudaMemcpyDeviceToDevice, stream);
+            cudaMemcpyAsync(tout + o + g.ny, ay[stage], sizeof(double) * g.nx, cudaMemcpyDeviceToDevice, stream);
+        }
+    }
+
+    void enq_frozen_step(const double* tin, double* tout, const Field4* save)
+    {
+        k_begin<<<1, 1, 0, stream>>>(st);
+        enq_bc(q, st);
+        if (save) copy_field(save[0], q);
+        enq_alpha_frozen(q, 3, 0, tin, tout);
+        k_dt<<<1, 1, 0, stream>>>(g, st);
+        {
+            ListArgs la;
+            for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
+            dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
+            k_lists<<<grid, 256, 0, stream>>>(g, m, lvl[2], lvl[1], lvl[0], la, st);
+        }
+        enq_faces_update(0, q, q2);
+        enq_bc(q2, st);
+        if (save) copy_field(save[1], q2);
+        enq_alpha_frozen(q2, 2, 1, tin, tout);
+        enq_faces_update(1, q2, q1);
+        enq_bc(q1, st);
+        if (save) copy_field(save[2], q1);
+        enq_alpha_frozen(q1, 1, 2, tin, tout);
+        enq_faces_update(2, q1, q1);
+        k_finish<<<1, 1, 0, stream>>>(st);
+    }
+
+    // Device buffers of the frozen run and the adjoint, grown on demand and kept.
+    double* tape = nullptr;
+    size_t tape_steps = 0;
+    std::vector<void*> adj_mem;
+    size_t adj_key[3] = {0, 0, 0};
+    Field4 lam{}, lam1{}, lam2{}, nu{}, qkeep{};
+    std::vector<Field4> ckpt, seg;
+    double* target = nullptr;
+    double* rowsum = nullptr;
+    double* loss_dev = nullptr;
+
+    int alloc_plane(double** p)
+    {
+        AWCM_CUDA_TRY(cudaMalloc(p, plane * sizeof(double)));
+        adj_mem.push_back(*p);
+        return kOk;
+    }
+    int alloc_field(Field4& f)
+    {
+        for (int k = 0; k < 4; ++k) {
+            const int rc = alloc_plane(&f.p[k]);
+            if (rc) return rc;
+        }
+        return kOk;
+    }
+    void free_adj()
+    {
+        for (void* p : adj_mem) cudaFree(p);
+        adj_mem.clear();
+        ckpt.clear();
+        seg.clear();
+        adj_key[0] = adj_key[1] = adj_key[2] = 0;
+    }
+    int ensure_tape(size_t steps)
+    {
+        if (steps <= tape_steps) return kOk;
+        if (tape) cudaFree(tape);
+        tape = nullptr;
+        tape_steps = 0;
+        AWCM_CUDA_TRY(cudaMalloc(&tape, std::max<size_t>(steps, 1) * tape_stride() * sizeof(double)));
+        tape_steps = steps;
+        return kOk;
+    }
+    int ensure_adj(size_t n_ckpt, size_t seg_len)
+    {
+        if (adj_key[0] && n_ckpt <= adj_key[1] && seg_len <= adj_key[2]) return kOk;
+        free_adj();
+        int rc;
+        for (Field4* f : {&lam, &lam1, &lam2, &nu, &qkeep})
+            if ((rc = alloc_field(*f))) return rc;
+        ckpt.resize(n_ckpt);
+        for (auto& f : ckpt)
+            if ((rc = alloc_field(f))) return rc;
+        seg.resize(3 * seg_len);
+        for (auto& f : seg)
+            if ((rc = alloc_field(f))) return rc;
+        AWCM_CUDA_TRY(cudaMalloc(&target, sizeof(double) * g.nx * g.ny));
+        adj_mem.push_back(target);
+        AWCM_CUDA_TRY(cudaMalloc(&rowsum, sizeof(double) * g.ny));
+        adj_mem.push_back(rowsum);
+        AWCM_CUDA_TRY(cudaMalloc(&loss_dev, sizeof(double)));
+        adj_mem.push_back(loss_dev);
+        adj_key[0] = 1;
+        adj_key[1] = n_ckpt;
+        adj_key[2] = seg_len;
+        return kOk;
+    }
+
+    // n frozen steps from t0 at fixed dt.  mode 1: LF speeds computed and recorded into the
+    // solver's tape; mode 2: replayed from the tape of the last recording run.
+    // out[0] = t, out[1] = device ms, out[2] = sum |mask0| over the steps.
+    int frozen_run(double t0, double dt, int n, int mode, double* out)
+    {
+        if (n < 0 || !(dt > 0) || (mode != 1 && mode != 2)) return kErrArg;
+        if (mode == 2 && (size_t)n > tape_steps) {
+            set_last_error("frozen replay longer than the recorded LF-speed tape", __FILE__, __LINE__);
+            return kErrState;
+        }
+        if (mode == 1) {
+            const int rc = ensure_tape((size_t)n);
+            if (rc) return rc;
+        }
+        int rc = write_params(0.0, 1.0, t0, 1e300, dt);
+        if (rc) return rc;
+        StepState h0;
+        if ((rc = read_state(&h0))) return rc;
+        cudaEvent_t e0, e1;
+        AWCM_CUDA_TRY(cudaEventCreate(&e0));
+        AWCM_CUDA_TRY(cudaEventCreate(&e1));
+        cudaEventRecord(e0, stream);
+        for (int s = 0; s < n; ++s) {
+            double* row = tape + (size_t)s * tape_stride();
+            enq_frozen_step(mode == 2 ? row : nullptr, mode == 1 ? row : nullptr, nullptr);
+        }
+        cudaEventRecord(e1, stream);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        StepState h;
+        if ((rc = read_state(&h))) return rc;
+        if (out) {
+            out[0] = h.t;
+            out[1] = ms;
+            out[2] = (double)(h.upd - h0.upd);
+        }
+        return kOk;
+    }
+
+    // Reverse sweep of one frozen step: stage inputs sv[0..2] = Q, Q2, Q1 (boundary-filled), LF
+    // speeds of the step `ts`; lam holds the adjoint of the step's output on entry and of its
+    // input on exit.
+    void enq_adjoint_step(const Field4* sv, const double* ts)
+    {
+        const double* sc = st->sc;
+        Field4 lam_out[3] = {lam, lam2, lam1};  // adjoint receiving the VJP of stage fs
+        for (int fs = kStages - 1; fs >= 0; --fs) {
+            const int bit = 2 - fs;
+            const int8_t* lv = lvl[bit];
+            if (fs == 2) adj_launch_rk(3, g, plane, m, lv, sc, lam, lam, lam1, nu, stream);
+            else if (fs == 1) adj_launch_rk(2, g, plane, m, lv, sc, lam1, lam, lam2, nu, stream);
+            else adj_launch_rk(1, g, plane, m, lv, sc, lam2, lam, lam2, nu, stream);
+            AdjStage A;
+            A.g = g;
+            A.qin = sv[fs];
+            A.lam = lam_out[fs];
+            A.nu = nu;
+            A.m = m;
+            A.lvl = lv;
+            A.bit = bit;
+            A.xf = lists[4 * fs + 2];
+            A.nxf = st->cnt + 4 * fs + 2;
+            A.yf = lists[4 * fs + 3];
+            A.nyf = st->cnt + 4 * fs + 3;
+            A.crs = lists[4 * fs + 1];
+            A.ncrs = st->cnt + 4 * fs + 1;
+            A.ax = ts + (size_t)fs * (g.nx + g.ny);
+            A.ay = A.ax + g.ny;
+            adj_launch_stage(A, face_blocks, stream);
+            adj_launch_fold(g, lam_out[fs], stream);
+        }
+    }
+
+    // Loss L = 1/2 sum over grid points of (rho(t0 + n dt) - target)^2 of the frozen run from the
+    // current state, and dL/dQ(t0) by the discrete adjoint.  The forward run records the LF speeds
+    // (mode 1) or replays the tape (mode 2); the reverse sweep recomputes the stage inputs segment
+    // by segment from checkpoints of Q taken every `every` steps (every >= n: one segment, all
+    // stage inputs kept from the forward run, no recomputation).  The state is left at the end of
+    // the forward run.  out[0] = loss, [1] forward ms, [2] reverse ms (recomputation included),
+    // [3] checkpoint interval, [4] device bytes of checkpoints + stage inputs + adjoint fields.
+    int adjoint(double t0, double dt, int n, int every, int mode, const double* target_host, double* grad_host,
+                double* out)
+    {
+        if (n <= 0 || !(dt > 0) || !target_host || (mode != 1 && mode != 2)) return kErrArg;
+        if (every <= 0) every = std::max(1, (int)std::ceil(std::sqrt((double)n)));
+        every = std::min(every, n);
+        const int n_seg = (n + every - 1) / every;
+        const bool keep_all = n_seg == 1;
+        int rc = ensure_adj(keep_all ? 0 : (size_t)n_seg, (size_t)every);
+        if (rc) return rc;
+        if (mode == 1 && (rc = ensure_tape((size_t)n))) return rc;
+        if (mode == 2 && (size_t)n > tape_steps) {
+            set_last_error("adjoint replay longer than the recorded LF-speed tape", __FILE__, __LINE__);
+            return kErrState;
+        }
+        AWCM_CUDA_TRY(cudaMemcpyAsync(target, target_host, sizeof(double) * g.nx * g.ny, cudaMemcpyHostToDevice, stream));
+        if ((rc = write_params(0.0, 1.0, t0, 1e300, dt))) return rc;
+        cudaEvent_t ev[3];
+        for (auto& e : ev) AWCM_CUDA_TRY(cudaEventCreate(&e));
+        // forward: checkpoints (or every stage input) and the LF-speed tape
+        cudaEventRecord(ev[0], stream);
+        for (int s = 0; s < n; ++s) {
+            if (!keep_all && s % every == 0) copy_field(ckpt[s / every], q);
+            double* row = tape + (size_t)s * tape_stride();
+            enq_frozen_step(mode == 2 ? row : nullptr, mode == 1 ? row : nullptr, keep_all ? &seg[3 * s] : nullptr);
+        }
+        adj_launch_seed(g, q, target, lam, rowsum, loss_dev, stream);
+        cudaEventRecord(ev[1], stream);
+        // reverse
+        if (!keep_all) copy_field(qkeep, q);
+        for (int k = n_seg - 1; k >= 0; --k) {
+            const int s0 = k * every, s1 = std::min(n, s0 + every);
+            if (!keep_all) {
+                copy_field(q, ckpt[k]);
+                // the segment's start time, for the time-dependent boundary fill
+                const double tk = t0 + s0 * dt;
+                cudaMemcpyAsync(&st->t, &tk, sizeof(double), cudaMemcpyHostToDevice, stream);
+                for (int s = s0; s < s1; ++s)
+                    enq_frozen_step(tape + (size_t)s * tape_stride(), nullptr, &seg[3 * (s - s0)]);
+            }
+            for (int s = s1 - 1; s >= s0; --s)
+                enq_adjoint_step(&seg[3 * (s - s0)], tape + (size_t)s * tape_stride());
+        }
+        cudaEventRecord(ev[2], stream);
+        if (!keep_all) copy_field(q, qkeep);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        float f_ms = 0, r_ms = 0;
+        cudaEventElapsedTime(&f_ms, ev[0], ev[1]);
+        cudaEventElapsedTime(&r_ms, ev[1], ev[2]);
+        for (auto& e : ev) cudaEventDestroy(e);
+        // the state's clock at the end of the forward run
+        {
+            const double tn = t0 + n * dt;
+            AWCM_CUDA_TRY(cudaMemcpyAsync(&st->t, &tn, sizeof(double), cudaMemcpyHostToDevice, stream));
+        }
+        double loss = 0;
+        AWCM_CUDA_TRY(cudaMemcpyAsync(&loss, loss_dev, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        if (grad_host) {
+            const size_t np = ghosted_points();
+            if ((rc = ensure_staging(np * 4 * sizeof(double)))) return rc;
+            k_soa_to_aos<<<blocks_for((long)np, 256), 256, 0, stream>>>(g, lam, (double*)staging);
+            AWCM_CUDA_TRY(cudaGetLastError());
+            AWCM_CUDA_TRY(cudaMemcpyAsync(grad_host, staging, np * 4 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        }
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        if (out) {
+            out[0] = loss;
+            out[1] = f_ms;
+            out[2] = r_ms;
+            out[3] = every;
+            out[4] = (double)((keep_all ? 0 : n_seg) + 3 * every + 5) * 4 * plane * sizeof(double) +
+                     (double)n * tape_stride() * sizeof(double);
+        }
+        return kOk;
+    }
+
     int init_problem(int kind, double a, double b)
     {
         // Problem initial states (Problems/2D/PROBLEM_QUADRANTS.h:34-80, PROBLEM_DOUBLEMACH.h:34-62,
@@ -2153,6 +2423,44 @@ int awcm2d_set_prepare_mode(awcm2d_t h, int mode)
     h->s.prep_mode = mode;
     if (h->s.graph) cudaGraphExecDestroy(h->s.graph);
     h->s.graph = nullptr;
+    return awcm::kOk;
+}
+int awcm2d_frozen_run(awcm2d_t h, double t0, double dt, int n_steps, int mode, double* out)
+{
+    AWCM_H(h);
+    return h->s.frozen_run(t0, dt, n_steps, mode, out);
+}
+int awcm2d_adjoint(awcm2d_t h, double t0, double dt, int n_steps, int checkpoint_every, int mode,
+                   const double* target, double* grad, double* out)
+{
+    AWCM_H(h);
+    return h->s.adjoint(t0, dt, n_steps, checkpoint_every, mode, target, grad, out);
+}
+int awcm2d_set_wenoz_eps(awcm2d_t h, double eps)
+{
+    AWCM_H(h);
+    if (!(eps > 0) || !std::isfinite(eps)) return awcm::kErrArg;
+    h->s.g.wz_eps = eps;
+    if (h->s.graph) cudaGraphExecDestroy(h->s.graph);
+    h->s.graph = nullptr;
+    return awcm::kOk;
+}
+int awcm2d_get_alpha_tape(awcm2d_t h, int n_steps, double* tape)
+{
+    AWCM_H(h);
+    if (!tape || n_steps < 0 || (size_t)n_steps > h->s.tape_steps) return awcm::kErrArg;
+    AWCM_CUDA_TRY(cudaMemcpy(tape, h->s.tape, (size_t)n_steps * h->s.tape_stride() * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+    return awcm::kOk;
+}
+int awcm2d_set_alpha_tape(awcm2d_t h, int n_steps, const double* tape)
+{
+    AWCM_H(h);
+    if (!tape || n_steps < 0) return awcm::kErrArg;
+    const int rc = h->s.ensure_tape((size_t)n_steps);
+    if (rc) return rc;
+    AWCM_CUDA_TRY(cudaMemcpy(h->s.tape, tape, (size_t)n_steps * h->s.tape_stride() * sizeof(double),
+                             cudaMemcpyHostToDevice));
     return awcm::kOk;
 }
 int awcm2d_stream(awcm2d_t h, void** stream)

@@ -126,6 +126,39 @@ int awcm2d_set_prepare_mode(awcm2d_t h, int mode);
 /* CUDA stream the instance runs on (cudaStream_t), for event timing by the caller. */
 int awcm2d_stream(awcm2d_t h, void** stream);
 
+/* ---------------------------------------------------------------- 2D frozen-mask run and adjoint
+ * No counterpart in the reference (it has no derivative code).  The frozen-mask step is the
+ * driver loop of Wavelet/main_2d_euler(quad).cpp:58-334 with PrepareEuler and PostProcessEuler
+ * left out: the masks and levels of the last awcm2d_prepare stay fixed, dt is fixed, and the
+ * per-stage Lax-Friedrichs speeds (alpha_x per row, alpha_y per column; :86-104, :170-185,
+ * :250-265) are either computed and recorded on the instance's LF-speed tape (mode 1) or replayed
+ * from it (mode 2).  Tape layout per step: stage 1..3 x (alpha_x[Ny], alpha_y[Nx]) doubles, the
+ * layout of the CPU checkers' frozen mode.
+ *
+ * awcm2d_frozen_run: n_steps frozen steps from t0.  out[3]: final t, device ms, sum |mask0|. */
+int awcm2d_frozen_run(awcm2d_t h, double t0, double dt, int n_steps, int mode, double* out);
+/* Loss L = 1/2 sum over the Nx x Ny grid points of (rho(t0 + n dt) - target)^2 after n frozen
+ * steps from the current state, and the discrete adjoint dL/dQ(t0) with the LF speeds held at
+ * their recorded values (the exact gradient of the mode-2 map).  target: Ny x Nx doubles (row j,
+ * column i), host.  grad: host, the awcm2d_get_q layout ((Ny+6) x (Nx+6) x 4, zero on the ghost
+ * ring), or NULL.  checkpoint_every: the reverse sweep restores Q from checkpoints taken every
+ * that many steps and recomputes each segment's stage inputs (<= 0: ceil(sqrt(n)); >= n: all
+ * stage inputs kept from the forward run, nothing recomputed).  mode 1 records the LF speeds in
+ * the forward run, 2 replays the tape.  The state is left at t0 + n dt.
+ * out[5]: loss, forward ms, reverse ms (recomputation included), checkpoint interval, device
+ * bytes held by checkpoints, stage inputs, adjoint fields and the tape. */
+int awcm2d_adjoint(awcm2d_t h, double t0, double dt, int n_steps, int checkpoint_every, int mode,
+                   const double* target, double* grad, double* out);
+/* WENO-Z epsilon of the 2D face reconstructions: the public member WENOZ5::eps (WENOZ.h:13-18),
+ * 1e-40 by default as in the reference.  With 1e-40 the Z weights tau/(b + eps) jump between
+ * regimes wherever the smoothness indicators b are near zero (uniform far fields, exponential
+ * tails), so the map is not differentiable at the scale of a finite-difference check; the
+ * gradient checks run the forward and the adjoint with eps = 1e-6 (the differentiable mode). */
+int awcm2d_set_wenoz_eps(awcm2d_t h, double eps);
+/* Copy the first n_steps steps of the LF-speed tape out of / into the instance. */
+int awcm2d_get_alpha_tape(awcm2d_t h, int n_steps, double* tape);
+int awcm2d_set_alpha_tape(awcm2d_t h, int n_steps, const double* tape);
+
 /* ------------------------------------------------------------------------------------------- 1D
  * A batch of independent 1D AWCM Euler instances (AWCM_1D, Wavelet/AWCM_1D.h, on
  * MRA_GRID_INT_1D, Wavelet/MRA_GRID_UNIFORM_1D.h:70-98), each with its own finest level, CFL step

@@ -184,6 +184,7 @@ class Oracle2D:
         self._apply_bc = b("apply_bc", None, [_vp, _c_double])
         self._step = b("step", None, [_vp] + [_c_double] * 5 + [_dp, _dp])
         self._set_freeze = b("set_freeze", None, [_vp, _c_int])
+        self._set_wenoz_eps = b("set_wenoz_eps", None, [_vp, _c_double])
         self._run = b("run", _c_int, [_vp, _c_double, _c_double, _c_double, _c_int, _dp])
         self._threads = b("threads", _c_int, [])
         self.h = self._create(num_levels, nx_coarse, ny_coarse, x_min, x_max, y_min, y_max, bc_kind)
@@ -248,8 +249,15 @@ class Oracle2D:
     def apply_bc(self, t=0.0):
         self._apply_bc(self.h, t)
 
-    def set_freeze(self, freeze: bool):
-        self._set_freeze(self.h, int(freeze))
+    def set_freeze(self, mode: int):
+        """0 normal; 1 frozen mask (no PrepareEuler, no residue removal), LF speeds computed and
+        recorded into the alpha buffer given to step(); 2 frozen mask with the LF speeds replayed."""
+        self._set_freeze(self.h, int(mode))
+
+    def set_wenoz_eps(self, eps: float):
+        """WENO-Z epsilon of the face reconstructions (WENOZ5::eps; the reference's default is
+        1e-40, the differentiable mode of the gradient checks uses 1e-6)."""
+        self._set_wenoz_eps(self.h, float(eps))
 
     def step(self, tol, cfl, t, t_next, dt_fixed=0.0, alpha=None):
         out = np.zeros(8)

@@ -54,7 +54,7 @@ inline double maxd(double a, double b) { return a > b ? a : b; }
 // Reconstruction.  WENOZ5::ReconstructLeft (WENOZ.h:75-104): Z weights with tau = |b0 - b2| and
 // exponent 1, eps 1e-40.  WENO5::ReconstructLeft (WENO.h:71-99): classic weights, eps 1e-6.
 // ReconstructRight(a,b,c,d,e) is ReconstructLeft(e,d,c,b,a) in both (WENOZ.h:106-108, WENO.h:101-104).
-inline double recon_left(double ll, double l, double c, double r, double rr, int scheme)
+inline double recon_left(double ll, double l, double c, double r, double rr, int scheme, double wz_eps = 1e-40)
 {
     const double b0 = C13_12 * sqr(c - 2 * r + rr) + 0.25 * sqr(3 * c - 4 * r + rr);
     const double b1 = C13_12 * sqr(l - 2 * c + r) + 0.25 * sqr(l - r);
@@ -66,7 +66,7 @@ inline double recon_left(double ll, double l, double c, double r, double rr, int
         a1 = 0.6 / sqr(eps + b1);
         a2 = 0.3 / sqr(eps + b2);
     } else {
-        const double eps = 1e-40;
+        const double eps = wz_eps;
         const double tau = absd(b0 - b2);
         a0 = 0.1 * (1 + tau / (b0 + eps));
         a1 = 0.6 * (1 + tau / (b1 + eps));
@@ -542,7 +542,7 @@ inline void invy(double u, double v, double H, double c, const double* b, double
 }
 
 // WENOZ_EULER_SOLVER_2D::ComputeFluxX / ComputeFluxY (WENOZ.h:236-320); s[0..5] = cells -3..+2.
-V4 face_flux_2d(const double* const* s, double alpha, double g, int dir)
+V4 face_flux_2d(const double* const* s, double alpha, double g, int dir, double wz_eps)
 {
     double f[6][4], RQ[6][4], RF[6][4], fp[6][4], fm[6][4];
     for (int p = 0; p < 6; ++p) {
@@ -591,8 +591,8 @@ V4 face_flux_2d(const double* const* s, double alpha, double g, int dir)
         }
     double S[4];
     for (int k = 0; k < 4; ++k) {
-        const double lr = recon_left(fp[4][k], fp[3][k], fp[2][k], fp[1][k], fp[0][k], 0);
-        const double rl = recon_left(fm[1][k], fm[2][k], fm[3][k], fm[4][k], fm[5][k], 0);
+        const double lr = recon_left(fp[4][k], fp[3][k], fp[2][k], fp[1][k], fp[0][k], 0, wz_eps);
+        const double rl = recon_left(fm[1][k], fm[2][k], fm[3][k], fm[4][k], fm[5][k], 0, wz_eps);
         S[k] = lr + rl;
     }
     V4 out;
@@ -610,6 +610,7 @@ struct O2D {
     double gamma = 1.4, x_min = 0, y_min = 0, dx = 0, dy = 0;
     int bc_kind = BC_QUAD;
     int freeze = 0;
+    double wz_eps = 1e-40;  // WENOZ5::eps (WENOZ.h:13-18), a public member of the reference solver
     std::vector<double> q[4], q2[4], q1[4], q0[4];
     std::vector<uint8_t> m;
     std::vector<int> lv[4];
@@ -1103,10 +1104,10 @@ void stage2d(O2D& s, std::vector<double>* in, std::vector<double>* out, int b, i
                     px[o] = bx[o];
                     py[o] = by[o];
                 }
-                V4 a = face_flux_2d(px, ax[j], g, 0), bb = face_flux_2d(px + 1, ax[j], g, 0);
+                V4 a = face_flux_2d(px, ax[j], g, 0, s.wz_eps), bb = face_flux_2d(px + 1, ax[j], g, 0, s.wz_eps);
                 for (int p = 0; p < 4; ++p) dF[p] = bb.v[p] - a.v[p];
-                a = face_flux_2d(py, ay[i], g, 1);
-                bb = face_flux_2d(py + 1, ay[i], g, 1);
+                a = face_flux_2d(py, ay[i], g, 1, s.wz_eps);
+                bb = face_flux_2d(py + 1, ay[i], g, 1, s.wz_eps);
                 for (int p = 0; p < 4; ++p) dG[p] = bb.v[p] - a.v[p];
             } else {
                 double b5[5][4];
@@ -1170,7 +1171,9 @@ void step2d(O2D& s, double tol, double cfl, double t, double t_next, double dt_f
     if (t + dt > t_next) { dt = t_next - t; do_print = 1; }
 
     std::vector<double> ax, ay;
-    const bool frozen = s.freeze && alpha_io;
+    // freeze 2: replay the recorded LF speeds from alpha_io; 1 (or normal mode): compute them and
+    // record them into alpha_io when it is given.
+    const bool frozen = s.freeze == 2 && alpha_io;
     auto load_alpha = [&](int stage, std::vector<double>* f, int b) {
         double* base = alpha_io ? alpha_io + (size_t)stage * (s.nx + s.ny) : nullptr;
         if (frozen) {
@@ -1200,7 +1203,9 @@ void step2d(O2D& s, double tol, double cfl, double t, double t_next, double dt_f
             const size_t a = s.at(i, j);
             for (int p = 0; p < 4; ++p) s.q[p][a] = (s.q[p][a] + 2.0 * s.q0[p][a]) / 3.0;
         }
-    remove_residue_2d(s, 0);
+    // Frozen-mask mode (the gradient configuration) keeps the points outside mask0: without the
+    // per-step PrepareEuler nothing would refill the stencil points of mask3 \ mask0.
+    if (!s.freeze) remove_residue_2d(s, 0);
     long cnt[4] = {0, 0, 0, 0};
     for (int j = 0; j < s.ny; ++j)
         for (int i = 0; i < s.nx; ++i)
@@ -1500,6 +1505,7 @@ void or2d_step(void* h, double tol, double cfl, double t, double t_next, double 
 }
 
 void or2d_set_freeze(void* h, int freeze) { static_cast<O2D*>(h)->freeze = freeze; }
+void or2d_set_wenoz_eps(void* h, double eps) { static_cast<O2D*>(h)->wz_eps = eps; }
 
 int or2d_run(void* h, double tol, double cfl, double t_end, int max_steps, double* out)
 {

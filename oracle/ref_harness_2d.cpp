@@ -57,9 +57,12 @@ struct Ref2D {
     double gamma = 1.4;
     int nx = 0, ny = 0;
     int bc_kind = BC_QUAD;
-    // When set, ref2d_step skips PrepareEuler and reuses the stored masks/levels, and the
-    // three LF speeds are taken from frozen_alpha instead of being recomputed.
+    // When set, ref2d_step skips PrepareEuler and PostProcessEuler (masks/levels stay as stored)
+    // and, given an alpha buffer, takes the three LF speeds from it instead of recomputing them.
     int freeze_mask = 0;
+    // Value given to the public member WENOZ5::eps (WENOZ.h:13-18) of every WENOZ_EULER_SOLVER_2D
+    // the stages construct; the solver's own default is 1e-40.
+    double wenoz_eps = 1e-40;
 };
 
 FIELD_UNIFORM_2D<bool>& mask_ref(Ref2D* s, int id)
@@ -123,6 +126,7 @@ void stage2d(Ref2D* s, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qin, FIELD_UNI
 #pragma omp parallel
     {
         WENOZ_EULER_SOLVER_2D wenoz_solver;
+        wenoz_solver.wenoz.eps = s->wenoz_eps;
 #pragma omp for
         ITERATION_GRID_2D(grid, 0)
         {
@@ -440,7 +444,9 @@ void ref2d_step(void* h, double tol, double cfl, double t, double t_next, double
     }
 
     std::vector<double> ax(s->ny), ay(s->nx);
-    const int frozen = s->freeze_mask && alpha_io;
+    // freeze_mask 2: replay the recorded LF speeds from alpha_io; 1 (or normal mode): compute them
+    // and record them into alpha_io when it is given.
+    const int frozen = s->freeze_mask == 2 && alpha_io;
     auto load_alpha = [&](int stage, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qs, const FIELD_UNIFORM_2D<bool>& m) {
         double* base = alpha_io ? alpha_io + (size_t)stage * (s->nx + s->ny) : nullptr;
         if (frozen) {
@@ -472,7 +478,9 @@ void ref2d_step(void* h, double tol, double cfl, double t, double t_next, double
     {
         if (awcm.mask0(i, j) == true) Q(i, j) = (Q(i, j) + 2.0 * s->Q_0(i, j)) / 3.0;
     }
-    awcm.PostProcessEuler(Q);
+    // Frozen-mask mode (gradient configuration): no PrepareEuler and no residue removal, so the
+    // stencil points outside mask0 keep their values; fixed dt and recorded LF speeds.
+    if (!s->freeze_mask) awcm.PostProcessEuler(Q);
 
     long cnt[4] = {0, 0, 0, 0};
     for (int j = 0; j < s->ny; ++j)
@@ -489,6 +497,7 @@ void ref2d_step(void* h, double tol, double cfl, double t, double t_next, double
 }
 
 void ref2d_set_freeze(void* h, int freeze) { static_cast<Ref2D*>(h)->freeze_mask = freeze; }
+void ref2d_set_wenoz_eps(void* h, double eps) { static_cast<Ref2D*>(h)->wenoz_eps = eps; }
 
 // Steps until t >= t_end or max_steps; returns the step count, out[0] = t, out[1] = sum |mask0|.
 int ref2d_run(void* h, double tol, double cfl, double t_end, int max_steps, double* out)

@@ -6,7 +6,7 @@ oracle/Makefile behind oracle/ref_harness_{1d,2d}.cpp, run on small seeded/deter
 Only this script touches the reference build; the tests replay the fixtures against the CPU
 restatement (everywhere) and the CUDA path (on a GPU).
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [1d] [2d] [adjoint]
 """
 from __future__ import annotations
 
@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "c_pp-library_b200"))
 
 import oracle  # noqa: E402
 
@@ -84,10 +85,67 @@ def gen_2d():
     return out
 
 
+# Gradient workload on a small grid: vortex + seeded density bumps on periodic [0,10]^2, frozen
+# masks from one PrepareEuler, WENO-Z eps 1e-6 (the differentiable mode), fixed dt.
+ADJ_CASE = dict(num_levels=4, nx_coarse=9, tol=1e-3, eps=1e-6, steps=10, n_dirs=16, dir_seed=7, h=1e-6)
+
+
+def frozen_replay(kind, q, masks, levels, tape, dt, eps, nl, nxc):
+    r = oracle.Oracle2D(nl, nxc, nxc, 0.0, 10.0, 0.0, 10.0, bc_kind=2, kind=kind)
+    r.set_q(q)
+    r.set_masks(masks)
+    r.set_levels(levels)
+    r.set_wenoz_eps(eps)
+    r.set_freeze(2)
+    t = 0.0
+    tp = np.array(tape, copy=True)
+    for s in range(tp.shape[0]):
+        r.step(0.0, 1.0, t, 1e300, dt, tp[s])
+        t += dt
+    return r.get_q()
+
+
+def gen_adjoint():
+    from awcm import gradient as G
+    c = ADJ_CASE
+    nl, nxc = c["num_levels"], c["nx_coarse"]
+    r = oracle.Oracle2D(nl, nxc, nxc, 0.0, 10.0, 0.0, 10.0, bc_kind=2, kind="reference")
+    q0 = G.vortex_bumps(r)
+    target = G.target_density(r)
+    dt = G.stable_dt(q0, 10.0 / (r.nx - 1))
+    r.set_q(q0)
+    r.prepare(c["tol"])
+    qp, masks, levels = r.get_q(), r.get_masks(), r.get_levels()
+    # recording run (LF speeds computed), then central differences with the speeds replayed
+    r.set_wenoz_eps(c["eps"])
+    r.set_freeze(1)
+    tape = np.zeros((c["steps"], 3 * (r.nx + r.ny)))
+    t = 0.0
+    for s in range(c["steps"]):
+        r.step(0.0, 1.0, t, 1e300, dt, tape[s])
+        t += dt
+    q_end = r.get_q()
+    dirs = G.unit_directions(qp.shape, c["n_dirs"], c["dir_seed"])
+    fd = []
+    for d in dirs:
+        a = frozen_replay("reference", qp + c["h"] * d, masks, levels, tape, dt, c["eps"], nl, nxc)
+        b = frozen_replay("reference", qp - c["h"] * d, masks, levels, tape, dt, c["eps"], nl, nxc)
+        fd.append(G.loss_difference(a, b, target) / (2 * c["h"]))
+    return {"adjoint_vortex65": dict(q=qp, masks=masks, levels=levels, tape=tape, target=target, q_end=q_end,
+                                     fd=np.array(fd), dt=dt,
+                                     params=np.array([nl, nxc, c["tol"], c["eps"], c["steps"], c["n_dirs"],
+                                                      c["dir_seed"], c["h"]]))}
+
+
 def main():
     if not oracle.reference_available():
         oracle.build(with_reference=True)
-    for name, rec in {**gen_1d(), **gen_2d()}.items():
+    groups = {"1d": gen_1d, "2d": gen_2d, "adjoint": gen_adjoint}
+    chosen = sys.argv[1:] or list(groups)
+    recs = {}
+    for g in chosen:
+        recs.update(groups[g]())
+    for name, rec in recs.items():
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **rec)
         print(path, os.path.getsize(path))

@@ -1,0 +1,219 @@
+"""Frozen-mask run and discrete adjoint of the 2D path on the GPU.
+
+* The frozen-mask forward (no PrepareEuler / residue removal, fixed dt, LF speeds recorded or
+  replayed) is bit-identical to the CPU restatement and to the reference's own code, and its
+  central differences equal the reference's (tests/golden/adjoint_vortex65.npz) bit for bit.
+* The adjoint's directional derivatives agree with FP64 central finite differences (h = 1e-6,
+  16 seeded unit directions) to 1e-6 relative, in the differentiable mode (WENO-Z eps = 1e-6),
+  on the small fixture grid and on the 513^2 / 200-step gradient workload.
+* Checkpoint intervals (every step, sqrt(N), keep-all) give the same gradient.
+* The torch.autograd.Function harness passes torch.autograd.gradcheck (fast mode).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import Oracle2D
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FD_REL_TOL = 1e-6
+EPS_DIFF = 1e-6  # WENO-Z epsilon of the differentiable mode
+
+
+def fixture():
+    return dict(np.load(os.path.join(GOLDEN, "adjoint_vortex65.npz")))
+
+
+def small_solver(awcm, g):
+    nl, nxc = int(g["params"][0]), int(g["params"][1])
+    s = awcm.AWCM2D(nl, nxc, nxc, 0.0, 10.0, 0.0, 10.0, bc_kind=awcm.BC_PERIODIC)
+    return s
+
+
+def prepared_small(awcm):
+    """GPU instance of the fixture case after one PrepareEuler on the seeded initial state."""
+    from awcm import gradient as G
+
+    g = fixture()
+    s = small_solver(awcm, g)
+    q0 = G.vortex_bumps(s)
+    s.set_q(q0)
+    s.prepare(float(g["params"][2]))
+    return s, g
+
+
+def replay_q(s, q, dt, n):
+    s.set_q(q)
+    s.frozen_run(0.0, dt, n, replay=True)
+    return s.get_q()
+
+
+def test_prepared_state_matches_fixture(awcm_lib):
+    s, g = prepared_small(awcm_lib)
+    assert np.array_equal(s.get_q(), g["q"])
+    assert np.array_equal(s.get_masks(), g["masks"])
+    assert np.array_equal(s.get_levels(), g["levels"])
+
+
+@pytest.mark.parametrize("eps", [1e-40, EPS_DIFF])
+def test_frozen_run_bitexact_vs_checkers(awcm_lib, eps):
+    """Recording run: end state and LF-speed tape equal the restatement's (and the reference's,
+    when its build is present) bit for bit."""
+    s, g = prepared_small(awcm_lib)
+    s.set_wenoz_eps(eps)
+    nl, nxc, steps = int(g["params"][0]), int(g["params"][1]), int(g["params"][4])
+    dt = float(g["dt"])
+    qp = s.get_q()
+    s.frozen_run(0.0, dt, steps)
+    q_gpu, tape_gpu = s.get_q(), s.get_alpha_tape(steps)
+    kinds = ["port"] + (["reference"] if oracle.reference_available() else [])
+    for kind in kinds:
+        o = Oracle2D(nl, nxc, nxc, 0.0, 10.0, 0.0, 10.0, bc_kind=2, kind=kind)
+        o.set_q(qp)
+        o.set_masks(g["masks"])
+        o.set_levels(g["levels"])
+        o.set_wenoz_eps(eps)
+        o.set_freeze(1)
+        tape = np.zeros_like(tape_gpu)
+        t = 0.0
+        for k in range(steps):
+            o.step(0.0, 1.0, t, 1e300, dt, tape[k])
+            t += dt
+        assert np.array_equal(tape, tape_gpu), kind
+        qo = o.get_q()
+        inner = (slice(3, -3), slice(3, -3))
+        assert np.array_equal(q_gpu[inner], qo[inner]), kind
+    if eps == EPS_DIFF:
+        assert np.array_equal(tape_gpu, g["tape"])
+        assert np.array_equal(q_gpu[3:-3, 3:-3], g["q_end"][3:-3, 3:-3])
+
+
+def test_gpu_finite_differences_equal_reference(awcm_lib):
+    """Central differences of the GPU frozen replay equal the reference's bit for bit."""
+    from awcm import gradient as G
+
+    s, g = prepared_small(awcm_lib)
+    s.set_wenoz_eps(EPS_DIFF)
+    _, _, _, _, steps, n_dirs, seed, h = g["params"]
+    steps, n_dirs, seed = int(steps), int(n_dirs), int(seed)
+    s.set_alpha_tape(g["tape"])
+    dirs = G.unit_directions(g["q"].shape, n_dirs, seed)
+    for k in range(n_dirs):
+        a = replay_q(s, g["q"] + h * dirs[k], float(g["dt"]), steps)
+        b = replay_q(s, g["q"] - h * dirs[k], float(g["dt"]), steps)
+        assert G.loss_difference(a, b, g["target"]) / (2 * h) == g["fd"][k], k
+
+
+def directional_errors(grad, dirs, fd):
+    ad = np.array([float(np.sum(grad * d)) for d in dirs])
+    return ad, np.abs(ad - fd) / np.abs(fd)
+
+
+def test_adjoint_vs_reference_directional_gradient(awcm_lib):
+    """Adjoint directional derivatives against the reference solver's central differences."""
+    from awcm import gradient as G
+
+    s, g = prepared_small(awcm_lib)
+    s.set_wenoz_eps(EPS_DIFF)
+    _, _, _, _, steps, n_dirs, seed, h = g["params"]
+    s.set_alpha_tape(g["tape"])
+    loss, grad, info = s.adjoint(0.0, float(g["dt"]), int(steps), g["target"], replay=True)
+    dirs = G.unit_directions(g["q"].shape, int(n_dirs), int(seed))
+    ad, rel = directional_errors(grad, dirs, g["fd"])
+    assert rel.max() <= FD_REL_TOL, (rel, ad, g["fd"])
+    # loss of the replayed run, same value as the recording run's
+    qe = g["q_end"][3:-3, 3:-3, 0] - g["target"]
+    assert loss == pytest.approx(0.5 * float(np.sum(qe * qe)), rel=1e-13)
+    assert np.all(grad[:3] == 0) and np.all(grad[-3:] == 0) and np.all(grad[:, :3] == 0) and np.all(grad[:, -3:] == 0)
+
+
+def test_checkpoint_intervals_agree(awcm_lib):
+    s, g = prepared_small(awcm_lib)
+    s.set_wenoz_eps(EPS_DIFF)
+    steps, dt = int(g["params"][4]), float(g["dt"])
+    s.set_alpha_tape(g["tape"])
+    grads = []
+    for every in (1, 3, 0, steps):
+        s.set_q(g["q"])
+        loss, grad, info = s.adjoint(0.0, dt, steps, g["target"], checkpoint_every=every, replay=True)
+        grads.append((loss, grad, info))
+        # the state is left at the end of the forward run
+        assert np.array_equal(s.get_q()[3:-3, 3:-3], g["q_end"][3:-3, 3:-3])
+    ref_loss, ref_grad, _ = grads[-1]
+    scale = np.abs(ref_grad).max()
+    for loss, grad, info in grads[:-1]:
+        assert loss == ref_loss
+        assert np.abs(grad - ref_grad).max() <= 1e-12 * scale, info
+    assert grads[2][2]["checkpoint_every"] == int(np.ceil(np.sqrt(steps)))
+
+
+def test_adjoint_recording_equals_replay(awcm_lib):
+    """mode 1 (record during the adjoint's forward) and mode 2 (replay) give the same result."""
+    s, g = prepared_small(awcm_lib)
+    s.set_wenoz_eps(EPS_DIFF)
+    steps, dt = int(g["params"][4]), float(g["dt"])
+    s.set_q(g["q"])
+    l1, g1, _ = s.adjoint(0.0, dt, steps, g["target"])
+    assert np.array_equal(s.get_alpha_tape(steps), g["tape"])
+    s.set_q(g["q"])
+    l2, g2, _ = s.adjoint(0.0, dt, steps, g["target"], replay=True)
+    assert l1 == l2
+    assert np.abs(g1 - g2).max() <= 1e-12 * np.abs(g2).max()
+
+
+def test_gradient_workload_full_size(awcm_lib):
+    """513^2 periodic vortex + bumps, 200 frozen steps, sqrt(N) checkpoints: 16 seeded unit
+    directions against central differences of the GPU frozen replay (h = 1e-6)."""
+    from awcm import gradient as G
+
+    s = awcm_lib.AWCM2D(6, 17, 17, 0.0, 10.0, 0.0, 10.0, bc_kind=awcm_lib.BC_PERIODIC)
+    assert (s.nx, s.ny) == (513, 513)
+    q0 = G.vortex_bumps(s)
+    target = G.target_density(s)
+    dt = G.stable_dt(q0, 10.0 / 512)
+    s.set_q(q0)
+    s.prepare(1e-3)
+    s.set_wenoz_eps(EPS_DIFF)
+    qp = s.get_q()
+    n = 200
+    loss, grad, info = s.adjoint(0.0, dt, n, target)
+    assert info["checkpoint_every"] == 15
+    assert np.isfinite(loss) and np.isfinite(grad).all()
+    h = 1e-6
+    dirs = G.unit_directions(qp.shape, 16, 11)
+    fd = []
+    for d in dirs:
+        a = replay_q(s, qp + h * d, dt, n)
+        b = replay_q(s, qp - h * d, dt, n)
+        fd.append(G.loss_difference(a, b, target) / (2 * h))
+    ad, rel = directional_errors(grad, dirs, np.array(fd))
+    print("full-size adjoint: loss %.6e fwd %.1f ms rev %.1f ms max rel %.2e" %
+          (loss, info["forward_ms"], info["reverse_ms"], rel.max()))
+    assert rel.max() <= FD_REL_TOL, (rel, ad, fd)
+
+
+def test_torch_autograd_harness(awcm_lib):
+    import torch
+
+    from awcm import gradient as G
+
+    s = awcm_lib.AWCM2D(3, 9, 9, 0.0, 10.0, 0.0, 10.0, bc_kind=awcm_lib.BC_PERIODIC)
+    q0 = G.vortex_bumps(s)
+    target = G.target_density(s)
+    dt = G.stable_dt(q0, 10.0 / (s.nx - 1))
+    s.set_q(q0)
+    s.prepare(1e-3)
+    s.set_wenoz_eps(EPS_DIFF)
+    qp = s.get_q()
+    s.frozen_run(0.0, dt, 4)  # records the LF-speed tape the harness replays
+    F = G.frozen_loss_function()
+    x = torch.from_numpy(qp).requires_grad_(True)
+    loss = F.apply(x, s, target, 0.0, dt, 4, 0)
+    loss.backward()
+    assert x.grad is not None and torch.isfinite(x.grad).all()
+    assert torch.autograd.gradcheck(lambda y: F.apply(y, s, target, 0.0, dt, 4, 0), (x,), eps=1e-6, atol=1e-8,
+                                    rtol=1e-5, fast_mode=True)

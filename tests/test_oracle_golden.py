@@ -82,3 +82,49 @@ def test_2d_steps(name):
     assert np.array_equal(q[keep], g["q"][keep])
     assert np.array_equal(o.get_masks(), g["masks"])
     assert np.array_equal(o.get_levels()[:3], g["levels"])
+
+
+def test_frozen_gradient_fixture():
+    """Frozen-mask mode with the LF speeds replayed and WENO-Z eps 1e-6: the restatement gives the
+    reference's end state and its central differences of the loss on all 16 directions, bit for bit."""
+    from awcm import gradient as G
+
+    g = load("adjoint_vortex65")
+    nl, nxc, tol, eps, steps, n_dirs, seed, h = g["params"]
+    nl, nxc, steps, n_dirs, seed = int(nl), int(nxc), int(steps), int(n_dirs), int(seed)
+    dt = float(g["dt"])
+
+    def replay(q):
+        o = Oracle2D(nl, nxc, nxc, 0.0, 10.0, 0.0, 10.0, bc_kind=2, kind="port")
+        o.set_q(q)
+        o.set_masks(g["masks"])
+        o.set_levels(g["levels"])
+        o.set_wenoz_eps(eps)
+        o.set_freeze(2)
+        t, tape = 0.0, np.array(g["tape"], copy=True)
+        for s in range(steps):
+            o.step(0.0, 1.0, t, 1e300, dt, tape[s])
+            t += dt
+        return o.get_q()
+
+    assert np.array_equal(replay(g["q"]), g["q_end"])
+    dirs = G.unit_directions(g["q"].shape, n_dirs, seed)
+    for k in (0, 5, 11):
+        a, b = replay(g["q"] + h * dirs[k]), replay(g["q"] - h * dirs[k])
+        assert G.loss_difference(a, b, g["target"]) / (2 * h) == g["fd"][k]
+
+
+def test_frozen_gradient_workload_builder():
+    """The workload builder reproduces the fixture's target and prepared state from the seeds."""
+    from awcm import gradient as G
+
+    g = load("adjoint_vortex65")
+    nl, nxc, tol = int(g["params"][0]), int(g["params"][1]), float(g["params"][2])
+    o = Oracle2D(nl, nxc, nxc, 0.0, 10.0, 0.0, 10.0, bc_kind=2, kind="port")
+    q0 = G.vortex_bumps(o)
+    assert np.array_equal(G.target_density(o), g["target"])
+    assert G.stable_dt(q0, 10.0 / (o.nx - 1)) == float(g["dt"])
+    o.set_q(q0)
+    o.prepare(tol)
+    assert np.array_equal(o.get_q(), g["q"])
+    assert np.array_equal(o.get_masks(), g["masks"])
