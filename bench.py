@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched shock-tube comparison")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
     ap.add_argument("--capture", type=int, default=-1,
                     help="profiling mode: K graph-replayed steps, then one eagerly launched step; prints its phases")
     return ap.parse_args()
@@ -267,6 +268,78 @@ def run_batched(rank: int, world: int):
     }
 
 
+GRADIENT = {
+    "workload": "frozen-mask discrete adjoint: isentropic vortex (strength 5, radius 1) + 16 seeded density "
+                "bumps on periodic [0,10]^2, 513x513 finest (17 coarse, 6 levels), eps 1e-3, 200 RK3 steps "
+                "at dt = 0.4 dx / max(|u|+c+|v|+c), loss 1/2 |rho - target|^2 over mask0, sqrt(N) checkpoints, "
+                "differentiable mode (WENO-Z eps 1e-6, smoothed |b0-b2| with delta 1e-6)",
+    "num_levels": 6, "nx_coarse": 17, "tol": 1e-3, "steps": 200, "wenoz_eps": 1e-6, "tau_delta": 1e-6,
+}
+
+
+def run_adjoint(rank: int, world: int):
+    """Reverse sweep (checkpoint recomputation included) against the frozen-mask forward run of
+    the gradient workload; each rank runs one replica, times are max over ranks."""
+    import awcm
+    from awcm import gradient as G
+    from awcm.dist import reduce_run
+
+    c = GRADIENT
+    s = awcm.AWCM2D(c["num_levels"], c["nx_coarse"], c["nx_coarse"], 0.0, 10.0, 0.0, 10.0,
+                    bc_kind=awcm.BC_PERIODIC)
+    q0 = G.vortex_bumps(s)
+    target = G.target_density(s)
+    dt = G.stable_dt(q0, 10.0 / (s.nx - 1))
+    s.set_q(q0)
+    s.prepare(c["tol"])
+    s.set_wenoz(c["wenoz_eps"], c["tau_delta"])
+    qp = s.get_q()
+    n = c["steps"]
+    s.adjoint(0.0, dt, n, target)  # warm-up; records the LF-speed tape
+    fwd, rev, fwd_only, keep = [], [], [], []
+    for _ in range(3):
+        s.set_q(qp)
+        loss, _, info = s.adjoint(0.0, dt, n, target, replay=True, with_grad=False)
+        fwd.append(info["forward_ms"])
+        rev.append(info["reverse_ms"])
+        s.set_q(qp)
+        fwd_only.append(s.frozen_run(0.0, dt, n, replay=True)[1])
+    s.set_q(qp)
+    _, _, kinfo = s.adjoint(0.0, dt, n, target, checkpoint_every=n, replay=True, with_grad=False)
+    # gradient check: 16 seeded unit directions, central differences of the frozen replay
+    s.set_q(qp)
+    _, grad, _ = s.adjoint(0.0, dt, n, target, replay=True)
+    act = G.active_points(s.get_masks())
+    h = 1e-5
+    rel = []
+    for d in G.unit_directions(qp.shape, 16, 11):
+        fd = []
+        for sign in (1.0, -1.0):
+            s.set_q(qp + sign * h * d)
+            s.frozen_run(0.0, dt, n, replay=True)
+            fd.append(s.get_q())
+        fdv = G.loss_difference(fd[0], fd[1], target, act) / (2 * h)
+        rel.append(abs(float((grad * d).sum()) - fdv) / abs(fdv))
+    f_ms, _ = reduce_run(statistics.median(fwd), 0.0, device="cuda")
+    r_ms, _ = reduce_run(statistics.median(rev), 0.0, device="cuda")
+    fo_ms, _ = reduce_run(statistics.median(fwd_only), 0.0, device="cuda")
+    k_ms, _ = reduce_run(kinfo["reverse_ms"], 0.0, device="cuda")
+    m = s.get_masks()
+    return {
+        "workload": c["workload"], "steps": n, "dt": dt, "loss": loss,
+        "checkpoint_every": info["checkpoint_every"], "device_bytes": info["device_bytes"],
+        "forward_ms": fo_ms, "adjoint_forward_ms": f_ms, "reverse_ms": r_ms,
+        "adjoint_over_forward": r_ms / fo_ms,
+        "keep_all_reverse_ms": k_ms, "keep_all_over_forward": k_ms / fo_ms,
+        "keep_all_device_bytes": kinfo["device_bytes"],
+        "mask0_points": int(m[1, 3:-3, 3:-3].sum()), "mask3_points": int(m[4, 3:-3, 3:-3].sum()),
+        "fd_check": {"directions": 16, "h": h, "max_rel": max(rel), "median_rel": statistics.median(rel)},
+        "note": "forward = 200 frozen-mask steps replaying the LF speeds; reverse = the adjoint sweep "
+                "including the recomputation of each checkpoint segment's stage inputs (device time, "
+                "median of 3)",
+    }
+
+
 # ------------------------------------------------------------------------------------- GPU arm
 def run_b200(args):
     rank, world, local = dist_env()
@@ -372,6 +445,7 @@ def run_b200(args):
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
 
     batched = None if args.no_batched else run_batched(rank, world)
+    gradient = None if args.no_adjoint else run_adjoint(rank, world)
 
     pitch = (s.nx + 6 + 31) // 32 * 32
     state_bytes = 5 * 4 * 8 * pitch * (s.ny + 6)  # Q, Q2, Q1, Fx, Fy planes
@@ -394,6 +468,7 @@ def run_b200(args):
         "e2e": e2e,
         "cpu_baseline": cpu,
         "batched_1d": batched,
+        "adjoint": gradient,
         "gpu_launches": launches * n_steps,
         "launches_per_step": launches,
     }

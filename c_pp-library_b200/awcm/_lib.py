@@ -48,7 +48,7 @@ _SIGS = {
     "awcm2d_profile_kernels": [c_void_p, c_double, c_double, c_double, c_double, c_int, ctypes.c_char_p, P_double, P_int],
     "awcm2d_frozen_run": [c_void_p, c_double, c_double, c_int, c_int, P_double],
     "awcm2d_adjoint": [c_void_p, c_double, c_double, c_int, c_int, c_int, P_double, P_double, P_double],
-    "awcm2d_set_wenoz_eps": [c_void_p, c_double],
+    "awcm2d_set_wenoz": [c_void_p, c_double, c_double],
     "awcm2d_get_alpha_tape": [c_void_p, c_int, P_double],
     "awcm2d_set_alpha_tape": [c_void_p, c_int, P_double],
     "awcm1d_batch_create": [c_int, P_int, P_int, P_double, P_double, c_double, c_int, ctypes.POINTER(c_void_p)],

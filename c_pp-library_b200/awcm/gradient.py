@@ -7,7 +7,9 @@ Workload (isentropic vortex with seeded density bumps on the periodic square [0,
   * plus 16 Gaussian density bumps rho += a exp(-|x - c|^2 / w^2) with a ~ U[0, 0.05],
     w ~ U[0.3, 1], c ~ U[0,10]^2 (distances taken periodically), velocity and pressure kept;
   * target = the density of the same construction from a second seed;
-  * loss = 1/2 sum over grid points (rho(t_end) - target)^2 after n frozen-mask RK3 steps.
+  * loss = 1/2 sum over the active points (mask0 of the frozen masks) of (rho(t_end) - target)^2
+    after n frozen-mask RK3 steps; points outside the masks hold no solution value (PrepareEuler
+    leaves them at zero).
 
 ``FrozenLoss`` wraps ``AWCM2D.adjoint`` as a torch.autograd.Function: its forward runs the frozen
 run with the LF speeds replayed from the solver's tape and returns the loss, its backward hands
@@ -97,11 +99,21 @@ def unit_directions(shape, count: int, seed: int) -> np.ndarray:
     return out
 
 
-def loss_difference(q_plus: np.ndarray, q_minus: np.ndarray, target: np.ndarray) -> float:
-    """L(q+) - L(q-) of L = 1/2 |rho - target|^2, summed as 1/2 (a+ - a-)(a+ + a-) per point to keep
-    the cancellation out of the difference."""
-    ap = q_plus[3:-3, 3:-3, 0] - target
-    am = q_minus[3:-3, 3:-3, 0] - target
+def active_points(masks: np.ndarray) -> np.ndarray:
+    """Ny x Nx bool of mask0 from the (5, Ny+6, Nx+6) mask planes (mask_temp, mask0..mask3)."""
+    return masks[1, 3:-3, 3:-3].astype(bool)
+
+
+def loss(q: np.ndarray, target: np.ndarray, active: np.ndarray) -> float:
+    a = (q[3:-3, 3:-3, 0] - target)[active]
+    return float(0.5 * np.sum(a * a))
+
+
+def loss_difference(q_plus: np.ndarray, q_minus: np.ndarray, target: np.ndarray, active: np.ndarray) -> float:
+    """L(q+) - L(q-) of L = 1/2 sum over the active points of (rho - target)^2, summed as
+    1/2 (a+ - a-)(a+ + a-) per point to keep the cancellation out of the difference."""
+    ap = (q_plus[3:-3, 3:-3, 0] - target)[active]
+    am = (q_minus[3:-3, 3:-3, 0] - target)[active]
     return float(0.5 * np.sum((ap - am) * (ap + am)))
 
 

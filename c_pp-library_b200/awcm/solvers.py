@@ -175,10 +175,11 @@ class AWCM2D:
         call("awcm2d_frozen_run", self.h, t0, dt, n_steps, 2 if replay else 1, ptr(out, ctypes.c_double))
         return out[0], out[1], out[2]
 
-    def set_wenoz_eps(self, eps: float):
-        """WENO-Z epsilon of the face reconstructions (WENOZ5::eps; 1e-40 as in the reference,
-        1e-6 in the differentiable mode of the gradient checks)."""
-        call("awcm2d_set_wenoz_eps", self.h, float(eps))
+    def set_wenoz(self, eps: float, tau_delta: float = 0.0):
+        """WENO-Z epsilon of the face reconstructions (WENOZ5::eps; 1e-40 as in the reference) and
+        the smoothing tau = sqrt((b0-b2)^2 + tau_delta^2) (0: |b0 - b2| as in the reference).
+        The gradient checks run the differentiable mode eps = tau_delta = 1e-6."""
+        call("awcm2d_set_wenoz", self.h, float(eps), float(tau_delta))
 
     def adjoint(self, t0, dt, n_steps, target, checkpoint_every=0, replay=False, with_grad=True):
         """Loss 1/2 |rho(t0 + n dt) - target|^2 of the frozen run from the current state and its

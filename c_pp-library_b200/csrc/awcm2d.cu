@@ -1018,7 +1018,7 @@ __global__ void __launch_bounds__(128) k_face(Grid2 g, Field4 f, Field4 out, con
         }
         const double al = DIR == 0 ? alpha[jj] : alpha[ii];
         double o[4];
-        face_flux_2d<DIR>(s, al, g.gamma, o, g.wz_eps);
+        face_flux_2d<DIR>(s, al, g.gamma, o, g.wz_eps, g.wz_delta);
 #pragma unroll
         for (int k = 0; k < 4; ++k) out.p[k][idx] = o[k];
     }
@@ -1335,6 +1335,7 @@ struct Solver2D {
         g.dy = (y_max - y_min) / (ny - 1);
         g.gamma = 1.4;
         g.wz_eps = 1e-40;
+        g.wz_delta = 0.0;
         g.W = make_weights();
         plane = (size_t)g.pitch * g.rows;
         AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -2136,8 +2137,8 @@ struct Solver2D {
         }
     }
 
-    // Loss L = 1/2 sum over grid points of (rho(t0 + n dt) - target)^2 of the frozen run from the
-    // current state, and dL/dQ(t0) by the discrete adjoint.  The forward run records the LF speeds
+    // Loss L = 1/2 sum over the mask0 points of (rho(t0 + n dt) - target)^2 of the frozen run from
+    // the current state, and dL/dQ(t0) by the discrete adjoint.  The forward run records the LF speeds
     // (mode 1) or replays the tape (mode 2); the reverse sweep recomputes the stage inputs segment
     // by segment from checkpoints of Q taken every `every` steps (every >= n: one segment, all
     // stage inputs kept from the forward run, no recomputation).  The state is left at the end of
@@ -2169,7 +2170,7 @@ struct Solver2D {
             double* row = tape + (size_t)s * tape_stride();
             enq_frozen_step(mode == 2 ? row : nullptr, mode == 1 ? row : nullptr, keep_all ? &seg[3 * s] : nullptr);
         }
-        adj_launch_seed(g, q, target, lam, rowsum, loss_dev, stream);
+        adj_launch_seed(g, q, m, target, lam, rowsum, loss_dev, stream);
         cudaEventRecord(ev[1], stream);
         // reverse
         if (!keep_all) copy_field(qkeep, q);
@@ -2436,11 +2437,12 @@ int awcm2d_adjoint(awcm2d_t h, double t0, double dt, int n_steps, int checkpoint
     AWCM_H(h);
     return h->s.adjoint(t0, dt, n_steps, checkpoint_every, mode, target, grad, out);
 }
-int awcm2d_set_wenoz_eps(awcm2d_t h, double eps)
+int awcm2d_set_wenoz(awcm2d_t h, double eps, double tau_delta)
 {
     AWCM_H(h);
-    if (!(eps > 0) || !std::isfinite(eps)) return awcm::kErrArg;
+    if (!(eps > 0) || !std::isfinite(eps) || !(tau_delta >= 0) || !std::isfinite(tau_delta)) return awcm::kErrArg;
     h->s.g.wz_eps = eps;
+    h->s.g.wz_delta = tau_delta;
     if (h->s.graph) cudaGraphExecDestroy(h->s.graph);
     h->s.graph = nullptr;
     return awcm::kOk;

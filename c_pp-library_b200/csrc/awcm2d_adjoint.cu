@@ -37,10 +37,10 @@ __device__ __forceinline__ void atomic_add(double* p, double v)
 
 // ---------------------------------------------------------------------------- WENO-Z reverse
 // Reverse of recon_left<kWenoZ> (WENOZ5::ReconstructLeft, WENOZ.h:75-104): adds d(out)/d(input)
-// times ob to g[0..4] for the inputs (ll, l, c, r, rr); |b0 - b2| is differentiated as
-// sign(b0 - b2).
+// times ob to g[0..4] for the inputs (ll, l, c, r, rr).  tau = |b0 - b2| is differentiated as
+// sign(b0 - b2); with delta > 0, tau = sqrt((b0 - b2)^2 + delta^2) and dtau = (b0 - b2) / tau.
 __device__ __forceinline__ void recon_left_vjp(double ll, double l, double c, double r, double rr, double ob,
-                                               double eps, double* g)
+                                               double eps, double delta, double* g)
 {
     const double A0 = c - 2 * r + rr, B0 = 3 * c - 4 * r + rr;
     const double A1 = l - 2 * c + r, B1 = l - r;
@@ -49,8 +49,14 @@ __device__ __forceinline__ void recon_left_vjp(double ll, double l, double c, do
     const double b1 = kC13_12 * A1 * A1 + 0.25 * B1 * B1;
     const double b2 = kC13_12 * A2 * A2 + 0.25 * B2 * B2;
     const double dl = b0 - b2;
-    const double tau = fabs(dl);
-    const double sg = dl > 0 ? 1.0 : (dl < 0 ? -1.0 : 0.0);
+    double tau, sg;
+    if (delta > 0) {
+        tau = sqrt(dl * dl + delta * delta);
+        sg = dl / tau;
+    } else {
+        tau = fabs(dl);
+        sg = dl > 0 ? 1.0 : (dl < 0 ? -1.0 : 0.0);
+    }
     const double ie0 = 1.0 / (b0 + eps), ie1 = 1.0 / (b1 + eps), ie2 = 1.0 / (b2 + eps);
     const double a0 = 0.1 * (1 + tau * ie0), a1 = 0.6 * (1 + tau * ie1), a2 = 0.3 * (1 + tau * ie2);
     const double iS = 1.0 / (a0 + a1 + a2);
@@ -186,7 +192,7 @@ __device__ __forceinline__ void inv2_vjp(const RoeAdj& R, const double* b, const
 // Forward values are recomputed here; alpha (the frozen LF speed) has no adjoint.
 template <int DIR>
 __device__ void face_flux_2d_vjp(const double (&s)[6][4], double alpha, double g, const double* ob, double eps,
-                                 double (&gs)[6][4])
+                                 double delta, double (&gs)[6][4])
 {
     // ---- forward: Roe average of the face states s[2], s[3] (ROESOLVER.h:49-70)
     const double* L = s[2];
@@ -224,8 +230,8 @@ __device__ void face_flux_2d_vjp(const double (&s)[6][4], double alpha, double g
             fp[p] = 0.5 * (RF[p][k] + alpha * RQ[p][k]);
             fm[p] = 0.5 * (RF[p][k] - alpha * RQ[p][k]);
         }
-        S[k] = recon_left<kWenoZ>(fp[4], fp[3], fp[2], fp[1], fp[0], eps) +
-               recon_left<kWenoZ>(fm[1], fm[2], fm[3], fm[4], fm[5], eps);
+        S[k] = recon_left<kWenoZ>(fp[4], fp[3], fp[2], fp[1], fp[0], eps, delta) +
+               recon_left<kWenoZ>(fm[1], fm[2], fm[3], fm[4], fm[5], eps, delta);
     }
     const double u = R.u, v = R.v, H = R.H, c = R.c;
     double Sb[4];
@@ -260,8 +266,8 @@ __device__ void face_flux_2d_vjp(const double (&s)[6][4], double alpha, double g
         }
         // left_r = ReconstructLeft(fp4, fp3, fp2, fp1, fp0); right_l = ReconstructLeft(fm1..fm5)
         double gl[5] = {0, 0, 0, 0, 0}, gr[5] = {0, 0, 0, 0, 0};
-        recon_left_vjp(fp[4], fp[3], fp[2], fp[1], fp[0], Sb[k], eps, gl);
-        recon_left_vjp(fm[1], fm[2], fm[3], fm[4], fm[5], Sb[k], eps, gr);
+        recon_left_vjp(fp[4], fp[3], fp[2], fp[1], fp[0], Sb[k], eps, delta, gl);
+        recon_left_vjp(fm[1], fm[2], fm[3], fm[4], fm[5], Sb[k], eps, delta, gr);
         fpb[4] += gl[0], fpb[3] += gl[1], fpb[2] += gl[2], fpb[1] += gl[3], fpb[0] += gl[4];
         fmb[1] += gr[0], fmb[2] += gr[1], fmb[3] += gr[2], fmb[4] += gr[3], fmb[5] += gr[4];
 #pragma unroll
@@ -358,7 +364,7 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjStage A, const uint32_t* __
             }
         }
         const double al = DIR == 0 ? alpha[jj] : alpha[ii];
-        face_flux_2d_vjp<DIR>(s, al, g.gamma, w, g.wz_eps, gs);
+        face_flux_2d_vjp<DIR>(s, al, g.gamma, w, g.wz_eps, g.wz_delta, gs);
 #pragma unroll
         for (int p = 0; p < 6; ++p) {
             const long a = (long)idx + (p - 2) * step;
@@ -501,16 +507,18 @@ __global__ void k_adj_fold(Grid2 g, Field4 lam)
     }
 }
 
-// Loss and seed: rowsum[j] = sum_i (rho - target)^2 / 2 in order of i; lam = rho - target on grid
-// points (component 0), 0 elsewhere.
-__global__ void k_adj_seed(Grid2 g, Field4 q, const double* __restrict__ target, Field4 lam, double* rowsum)
+// Loss and seed over the active points (mask0; the other points carry no solution value):
+// rowsum[j] = sum_i (rho - target)^2 / 2 in order of i; lam = rho - target on mask0 points
+// (component 0), 0 elsewhere.
+__global__ void k_adj_seed(Grid2 g, Field4 q, const uint8_t* __restrict__ m, const double* __restrict__ target,
+                           Field4 lam, double* rowsum)
 {
     const int j = (int)gtid();
     if (j >= g.ny) return;
     double acc = 0;
     for (int i = 0; i < g.nx; ++i) {
         const size_t a = g.at(i, j);
-        const double d = q.p[0][a] - target[(size_t)j * g.nx + i];
+        const double d = (m[a] & 1u) ? q.p[0][a] - target[(size_t)j * g.nx + i] : 0.0;
         acc += 0.5 * d * d;
         lam.p[0][a] = d;
         lam.p[1][a] = lam.p[2][a] = lam.p[3][a] = 0;
@@ -547,10 +555,10 @@ void adj_launch_fold(const Grid2& g, Field4 lam, cudaStream_t s)
     k_adj_fold<<<(n + 127) / 128, 128, 0, s>>>(g, lam);
 }
 
-void adj_launch_seed(const Grid2& g, Field4 q, const double* target, Field4 lam, double* rowsum, double* loss,
-                     cudaStream_t s)
+void adj_launch_seed(const Grid2& g, Field4 q, const uint8_t* m, const double* target, Field4 lam, double* rowsum,
+                     double* loss, cudaStream_t s)
 {
-    k_adj_seed<<<(g.ny + 127) / 128, 128, 0, s>>>(g, q, target, lam, rowsum);
+    k_adj_seed<<<(g.ny + 127) / 128, 128, 0, s>>>(g, q, m, target, lam, rowsum);
     k_sum_rows<<<1, 32, 0, s>>>(rowsum, g.ny, loss);
 }
 

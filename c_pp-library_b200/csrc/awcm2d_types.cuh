@@ -12,7 +12,8 @@ constexpr int kStages = 3;
 struct Grid2 {
     int nx, ny, maxl, pitch, rows, bc_kind;
     double x_min, y_min, dx, dy, gamma;
-    double wz_eps;  // WENO-Z epsilon of the face reconstructions (1e-40 as in the reference)
+    double wz_eps;    // WENO-Z epsilon of the face reconstructions (1e-40 as in the reference)
+    double wz_delta;  // > 0: tau = sqrt((b0-b2)^2 + wz_delta^2) instead of |b0 - b2| (0 as in the reference)
     Weights W;
     __host__ __device__ __forceinline__ size_t at(int i, int j) const
     {
@@ -51,9 +52,9 @@ void adj_launch_stage(const AdjStage& a, int face_blocks, cudaStream_t s);
 void adj_launch_rk(int stage, const Grid2& g, size_t plane, const uint8_t* m, const int8_t* lvl, const double* sc,
                    Field4 lam_next, Field4 lam_n, Field4 lam_in, Field4 nu, cudaStream_t s);
 void adj_launch_fold(const Grid2& g, Field4 lam, cudaStream_t s);
-// Loss 1/2 sum over grid points of (rho - target)^2 (rows summed in order, then rows in order)
-// and its gradient seed; target: Ny x Nx doubles on the device; rowsum: Ny doubles scratch.
-void adj_launch_seed(const Grid2& g, Field4 q, const double* target, Field4 lam, double* rowsum, double* loss,
-                     cudaStream_t s);
+// Loss 1/2 sum over the mask0 points of (rho - target)^2 (rows summed in order, then rows in
+// order) and its gradient seed; target: Ny x Nx doubles on the device; rowsum: Ny doubles scratch.
+void adj_launch_seed(const Grid2& g, Field4 q, const uint8_t* m, const double* target, Field4 lam, double* rowsum,
+                     double* loss, cudaStream_t s);
 
 }  // namespace awcm

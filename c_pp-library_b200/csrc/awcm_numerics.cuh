@@ -38,9 +38,11 @@ __device__ __forceinline__ double maxd(double a, double b) { return a > b ? a : 
 // WENOZ5::ReconstructLeft (WENOZ.h:75-104): tau = |b0 - b2|, alpha_k = d_k (1 + tau/(b_k + eps)),
 // eps = 1e-40.  WENO5::ReconstructLeft (WENO.h:71-99): alpha_k = d_k / (eps + b_k)^2, eps = 1e-6.
 // wz_eps: WENOZ5::eps (WENOZ.h:13-18), a public member of the reference solver, 1e-40 by default.
+// wz_delta > 0 replaces tau = |b0 - b2| by sqrt((b0 - b2)^2 + wz_delta^2) (the differentiable
+// mode of the gradient checks; the reference has only |.|).
 template <int SCHEME>
 __device__ __forceinline__ double recon_left(double ll, double l, double c, double r, double rr,
-                                             double wz_eps = 1e-40)
+                                             double wz_eps = 1e-40, double wz_delta = 0.0)
 {
     const double b0 = kC13_12 * sqr(c - 2 * r + rr) + 0.25 * sqr(3 * c - 4 * r + rr);
     const double b1 = kC13_12 * sqr(l - 2 * c + r) + 0.25 * sqr(l - r);
@@ -53,7 +55,7 @@ __device__ __forceinline__ double recon_left(double ll, double l, double c, doub
         a2 = 0.3 / sqr(eps + b2);
     } else {
         const double eps = wz_eps;
-        const double tau = absd(b0 - b2);
+        const double tau = wz_delta > 0 ? sqrt(sqr(b0 - b2) + sqr(wz_delta)) : absd(b0 - b2);
         a0 = 0.1 * (1 + tau / (b0 + eps));
         a1 = 0.6 * (1 + tau / (b1 + eps));
         a2 = 0.3 * (1 + tau / (b2 + eps));
@@ -220,7 +222,7 @@ __device__ __forceinline__ Roe2 roe2(const double* l, const double* r, double g)
 // s[p] = cells -3..+2 across the face along DIR.
 template <int DIR>
 __device__ __forceinline__ void face_flux_2d(const double (&s)[6][4], double alpha, double g, double* out,
-                                             double wz_eps = 1e-40)
+                                             double wz_eps = 1e-40, double wz_delta = 0.0)
 {
     const Roe2 R = roe2(s[2], s[3], g);
     double fp[6][4], fm[6][4];
@@ -239,8 +241,8 @@ __device__ __forceinline__ void face_flux_2d(const double (&s)[6][4], double alp
     double S[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const double lr = recon_left<kWenoZ>(fp[4][k], fp[3][k], fp[2][k], fp[1][k], fp[0][k], wz_eps);
-        const double rl = recon_left<kWenoZ>(fm[1][k], fm[2][k], fm[3][k], fm[4][k], fm[5][k], wz_eps);
+        const double lr = recon_left<kWenoZ>(fp[4][k], fp[3][k], fp[2][k], fp[1][k], fp[0][k], wz_eps, wz_delta);
+        const double rl = recon_left<kWenoZ>(fm[1][k], fm[2][k], fm[3][k], fm[4][k], fm[5][k], wz_eps, wz_delta);
         S[k] = lr + rl;
     }
     const double u = R.u, v = R.v, H = R.H, c = R.c;

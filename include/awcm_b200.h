@@ -137,8 +137,8 @@ int awcm2d_stream(awcm2d_t h, void** stream);
  *
  * awcm2d_frozen_run: n_steps frozen steps from t0.  out[3]: final t, device ms, sum |mask0|. */
 int awcm2d_frozen_run(awcm2d_t h, double t0, double dt, int n_steps, int mode, double* out);
-/* Loss L = 1/2 sum over the Nx x Ny grid points of (rho(t0 + n dt) - target)^2 after n frozen
- * steps from the current state, and the discrete adjoint dL/dQ(t0) with the LF speeds held at
+/* Loss L = 1/2 sum over the points of mask0 (the active points; the others hold no solution
+ * value) of (rho(t0 + n dt) - target)^2 after n frozen steps from the current state, and the discrete adjoint dL/dQ(t0) with the LF speeds held at
  * their recorded values (the exact gradient of the mode-2 map).  target: Ny x Nx doubles (row j,
  * column i), host.  grad: host, the awcm2d_get_q layout ((Ny+6) x (Nx+6) x 4, zero on the ghost
  * ring), or NULL.  checkpoint_every: the reverse sweep restores Q from checkpoints taken every
@@ -149,12 +149,15 @@ int awcm2d_frozen_run(awcm2d_t h, double t0, double dt, int n_steps, int mode, d
  * bytes held by checkpoints, stage inputs, adjoint fields and the tape. */
 int awcm2d_adjoint(awcm2d_t h, double t0, double dt, int n_steps, int checkpoint_every, int mode,
                    const double* target, double* grad, double* out);
-/* WENO-Z epsilon of the 2D face reconstructions: the public member WENOZ5::eps (WENOZ.h:13-18),
- * 1e-40 by default as in the reference.  With 1e-40 the Z weights tau/(b + eps) jump between
- * regimes wherever the smoothness indicators b are near zero (uniform far fields, exponential
- * tails), so the map is not differentiable at the scale of a finite-difference check; the
- * gradient checks run the forward and the adjoint with eps = 1e-6 (the differentiable mode). */
-int awcm2d_set_wenoz_eps(awcm2d_t h, double eps);
+/* WENO-Z parameters of the 2D face reconstructions (forward and adjoint): eps is the public
+ * member WENOZ5::eps (WENOZ.h:13-18), 1e-40 by default as in the reference; tau_delta > 0
+ * replaces tau = |b0 - b2| (WENOZ.h:84) by sqrt((b0 - b2)^2 + tau_delta^2), 0 by default (no
+ * counterpart in the reference).  With the reference's values the Z weights tau/(b + eps) jump
+ * between regimes wherever the smoothness indicators b are near zero (uniform far fields,
+ * exponential tails) and |.| has a kink at b0 = b2, so the map is not differentiable at the scale
+ * of a finite-difference check; the gradient checks run the differentiable mode
+ * eps = tau_delta = 1e-6. */
+int awcm2d_set_wenoz(awcm2d_t h, double eps, double tau_delta);
 /* Copy the first n_steps steps of the LF-speed tape out of / into the instance. */
 int awcm2d_get_alpha_tape(awcm2d_t h, int n_steps, double* tape);
 int awcm2d_set_alpha_tape(awcm2d_t h, int n_steps, const double* tape);

@@ -184,7 +184,10 @@ class Oracle2D:
         self._apply_bc = b("apply_bc", None, [_vp, _c_double])
         self._step = b("step", None, [_vp] + [_c_double] * 5 + [_dp, _dp])
         self._set_freeze = b("set_freeze", None, [_vp, _c_int])
-        self._set_wenoz_eps = b("set_wenoz_eps", None, [_vp, _c_double])
+        if kind == "port":
+            self._set_wenoz = b("set_wenoz", None, [_vp, _c_double, _c_double])
+        else:
+            self._set_wenoz_eps = b("set_wenoz_eps", None, [_vp, _c_double])
         self._run = b("run", _c_int, [_vp, _c_double, _c_double, _c_double, _c_int, _dp])
         self._threads = b("threads", _c_int, [])
         self.h = self._create(num_levels, nx_coarse, ny_coarse, x_min, x_max, y_min, y_max, bc_kind)
@@ -254,10 +257,16 @@ class Oracle2D:
         recorded into the alpha buffer given to step(); 2 frozen mask with the LF speeds replayed."""
         self._set_freeze(self.h, int(mode))
 
-    def set_wenoz_eps(self, eps: float):
-        """WENO-Z epsilon of the face reconstructions (WENOZ5::eps; the reference's default is
-        1e-40, the differentiable mode of the gradient checks uses 1e-6)."""
-        self._set_wenoz_eps(self.h, float(eps))
+    def set_wenoz(self, eps: float, tau_delta: float = 0.0):
+        """WENO-Z epsilon of the face reconstructions (WENOZ5::eps, a public member of the
+        reference solver, 1e-40 by default) and, for the restatement only, the smoothing
+        tau = sqrt((b0-b2)^2 + tau_delta^2) of the differentiable mode (the reference has |.|)."""
+        if self.kind == "port":
+            self._set_wenoz(self.h, float(eps), float(tau_delta))
+        else:
+            if tau_delta != 0.0:
+                raise ValueError("the reference's WENO-Z has no smoothed |b0 - b2|")
+            self._set_wenoz_eps(self.h, float(eps))
 
     def step(self, tol, cfl, t, t_next, dt_fixed=0.0, alpha=None):
         out = np.zeros(8)

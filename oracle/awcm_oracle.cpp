@@ -54,7 +54,8 @@ inline double maxd(double a, double b) { return a > b ? a : b; }
 // Reconstruction.  WENOZ5::ReconstructLeft (WENOZ.h:75-104): Z weights with tau = |b0 - b2| and
 // exponent 1, eps 1e-40.  WENO5::ReconstructLeft (WENO.h:71-99): classic weights, eps 1e-6.
 // ReconstructRight(a,b,c,d,e) is ReconstructLeft(e,d,c,b,a) in both (WENOZ.h:106-108, WENO.h:101-104).
-inline double recon_left(double ll, double l, double c, double r, double rr, int scheme, double wz_eps = 1e-40)
+inline double recon_left(double ll, double l, double c, double r, double rr, int scheme, double wz_eps = 1e-40,
+                          double wz_delta = 0.0)
 {
     const double b0 = C13_12 * sqr(c - 2 * r + rr) + 0.25 * sqr(3 * c - 4 * r + rr);
     const double b1 = C13_12 * sqr(l - 2 * c + r) + 0.25 * sqr(l - r);
@@ -67,7 +68,7 @@ inline double recon_left(double ll, double l, double c, double r, double rr, int
         a2 = 0.3 / sqr(eps + b2);
     } else {
         const double eps = wz_eps;
-        const double tau = absd(b0 - b2);
+        const double tau = wz_delta > 0 ? std::sqrt(sqr(b0 - b2) + sqr(wz_delta)) : absd(b0 - b2);
         a0 = 0.1 * (1 + tau / (b0 + eps));
         a1 = 0.6 * (1 + tau / (b1 + eps));
         a2 = 0.3 * (1 + tau / (b2 + eps));
@@ -542,7 +543,7 @@ inline void invy(double u, double v, double H, double c, const double* b, double
 }
 
 // WENOZ_EULER_SOLVER_2D::ComputeFluxX / ComputeFluxY (WENOZ.h:236-320); s[0..5] = cells -3..+2.
-V4 face_flux_2d(const double* const* s, double alpha, double g, int dir, double wz_eps)
+V4 face_flux_2d(const double* const* s, double alpha, double g, int dir, double wz_eps, double wz_delta)
 {
     double f[6][4], RQ[6][4], RF[6][4], fp[6][4], fm[6][4];
     for (int p = 0; p < 6; ++p) {
@@ -591,8 +592,8 @@ V4 face_flux_2d(const double* const* s, double alpha, double g, int dir, double 
         }
     double S[4];
     for (int k = 0; k < 4; ++k) {
-        const double lr = recon_left(fp[4][k], fp[3][k], fp[2][k], fp[1][k], fp[0][k], 0, wz_eps);
-        const double rl = recon_left(fm[1][k], fm[2][k], fm[3][k], fm[4][k], fm[5][k], 0, wz_eps);
+        const double lr = recon_left(fp[4][k], fp[3][k], fp[2][k], fp[1][k], fp[0][k], 0, wz_eps, wz_delta);
+        const double rl = recon_left(fm[1][k], fm[2][k], fm[3][k], fm[4][k], fm[5][k], 0, wz_eps, wz_delta);
         S[k] = lr + rl;
     }
     V4 out;
@@ -611,6 +612,7 @@ struct O2D {
     int bc_kind = BC_QUAD;
     int freeze = 0;
     double wz_eps = 1e-40;  // WENOZ5::eps (WENOZ.h:13-18), a public member of the reference solver
+    double wz_delta = 0.0;  // > 0: smoothed tau = sqrt((b0-b2)^2 + delta^2) (no reference counterpart)
     std::vector<double> q[4], q2[4], q1[4], q0[4];
     std::vector<uint8_t> m;
     std::vector<int> lv[4];
@@ -1104,10 +1106,11 @@ void stage2d(O2D& s, std::vector<double>* in, std::vector<double>* out, int b, i
                     px[o] = bx[o];
                     py[o] = by[o];
                 }
-                V4 a = face_flux_2d(px, ax[j], g, 0, s.wz_eps), bb = face_flux_2d(px + 1, ax[j], g, 0, s.wz_eps);
+                V4 a = face_flux_2d(px, ax[j], g, 0, s.wz_eps, s.wz_delta);
+                V4 bb = face_flux_2d(px + 1, ax[j], g, 0, s.wz_eps, s.wz_delta);
                 for (int p = 0; p < 4; ++p) dF[p] = bb.v[p] - a.v[p];
-                a = face_flux_2d(py, ay[i], g, 1, s.wz_eps);
-                bb = face_flux_2d(py + 1, ay[i], g, 1, s.wz_eps);
+                a = face_flux_2d(py, ay[i], g, 1, s.wz_eps, s.wz_delta);
+                bb = face_flux_2d(py + 1, ay[i], g, 1, s.wz_eps, s.wz_delta);
                 for (int p = 0; p < 4; ++p) dG[p] = bb.v[p] - a.v[p];
             } else {
                 double b5[5][4];
@@ -1505,7 +1508,11 @@ void or2d_step(void* h, double tol, double cfl, double t, double t_next, double 
 }
 
 void or2d_set_freeze(void* h, int freeze) { static_cast<O2D*>(h)->freeze = freeze; }
-void or2d_set_wenoz_eps(void* h, double eps) { static_cast<O2D*>(h)->wz_eps = eps; }
+void or2d_set_wenoz(void* h, double eps, double tau_delta)
+{
+    static_cast<O2D*>(h)->wz_eps = eps;
+    static_cast<O2D*>(h)->wz_delta = tau_delta;
+}
 
 int or2d_run(void* h, double tol, double cfl, double t_end, int max_steps, double* out)
 {

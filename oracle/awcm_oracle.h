@@ -53,8 +53,9 @@ void or2d_apply_bc(void* h, double t);
 void or2d_step(void* h, double tol, double cfl, double t, double t_next, double dt_fixed, double* alpha_io,
                double* out);
 void or2d_set_freeze(void* h, int freeze);
-/* WENO-Z epsilon of the face reconstructions (the reference solver's WENOZ5::eps, default 1e-40). */
-void or2d_set_wenoz_eps(void* h, double eps);
+/* WENO-Z epsilon of the face reconstructions (the reference solver's WENOZ5::eps, default 1e-40)
+ * and the smoothing of tau = |b0 - b2| (0: none, as in the reference). */
+void or2d_set_wenoz(void* h, double eps, double tau_delta);
 int or2d_run(void* h, double tol, double cfl, double t_end, int max_steps, double* out);
 int or2d_threads(void);
 

@@ -95,7 +95,7 @@ def frozen_replay(kind, q, masks, levels, tape, dt, eps, nl, nxc):
     r.set_q(q)
     r.set_masks(masks)
     r.set_levels(levels)
-    r.set_wenoz_eps(eps)
+    r.set_wenoz(eps)
     r.set_freeze(2)
     t = 0.0
     tp = np.array(tape, copy=True)
@@ -117,7 +117,7 @@ def gen_adjoint():
     r.prepare(c["tol"])
     qp, masks, levels = r.get_q(), r.get_masks(), r.get_levels()
     # recording run (LF speeds computed), then central differences with the speeds replayed
-    r.set_wenoz_eps(c["eps"])
+    r.set_wenoz(c["eps"])
     r.set_freeze(1)
     tape = np.zeros((c["steps"], 3 * (r.nx + r.ny)))
     t = 0.0
@@ -130,7 +130,7 @@ def gen_adjoint():
     for d in dirs:
         a = frozen_replay("reference", qp + c["h"] * d, masks, levels, tape, dt, c["eps"], nl, nxc)
         b = frozen_replay("reference", qp - c["h"] * d, masks, levels, tape, dt, c["eps"], nl, nxc)
-        fd.append(G.loss_difference(a, b, target) / (2 * c["h"]))
+        fd.append(G.loss_difference(a, b, target, G.active_points(masks)) / (2 * c["h"]))
     return {"adjoint_vortex65": dict(q=qp, masks=masks, levels=levels, tape=tape, target=target, q_end=q_end,
                                      fd=np.array(fd), dt=dt,
                                      params=np.array([nl, nxc, c["tol"], c["eps"], c["steps"], c["n_dirs"],

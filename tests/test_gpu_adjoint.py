@@ -3,9 +3,18 @@
 * The frozen-mask forward (no PrepareEuler / residue removal, fixed dt, LF speeds recorded or
   replayed) is bit-identical to the CPU restatement and to the reference's own code, and its
   central differences equal the reference's (tests/golden/adjoint_vortex65.npz) bit for bit.
-* The adjoint's directional derivatives agree with FP64 central finite differences (h = 1e-6,
-  16 seeded unit directions) to 1e-6 relative, in the differentiable mode (WENO-Z eps = 1e-6),
-  on the small fixture grid and on the 513^2 / 200-step gradient workload.
+* The adjoint's directional derivatives agree with FP64 central finite differences (16 seeded
+  directions of unit L2 norm) to 1e-6 relative in the differentiable mode (WENO-Z eps = 1e-6 and
+  tau = sqrt((b0-b2)^2 + delta^2), delta = 1e-6): with h = 1e-6 on the fixture grid (65^2,
+  10 steps), and on the 513^2 / 200-step gradient workload with h = 1e-5.  There a unit direction
+  spreads over 10^6 values (1e-9 each at h = 1e-6), and the rounding of the 200-step run moves the
+  loss difference by ~6e-15, i.e. ~3e-9 on a directional derivative of 2e-4: differences at
+  h = 1e-6 of the weakest directions scatter by up to 1.5e-5 relative around the h = 1e-5 value,
+  which itself agrees with the adjoint to better than 5e-7 in all 16 directions.
+* Against the reference solver's own central differences (eps = 1e-6, exact |b0 - b2|, which the
+  reference cannot smooth) the agreement is bounded by the differences' own noise: with |.| the
+  map has kinks, and central differences at h = 1e-6 and 1e-7 of the same direction differ by
+  up to 7e-5 relative (CPU restatement, 16 directions); the bound used is 2e-4.
 * Checkpoint intervals (every step, sqrt(N), keep-all) give the same gradient.
 * The torch.autograd.Function harness passes torch.autograd.gradcheck (fast mode).
 """
@@ -21,7 +30,9 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FD_REL_TOL = 1e-6
-EPS_DIFF = 1e-6  # WENO-Z epsilon of the differentiable mode
+REF_FD_REL_TOL = 2e-4
+EPS_DIFF = 1e-6    # WENO-Z epsilon of the differentiable mode
+DELTA_DIFF = 1e-6  # smoothing of |b0 - b2| in the differentiable mode
 
 
 def fixture():
@@ -59,24 +70,24 @@ def test_prepared_state_matches_fixture(awcm_lib):
     assert np.array_equal(s.get_levels(), g["levels"])
 
 
-@pytest.mark.parametrize("eps", [1e-40, EPS_DIFF])
-def test_frozen_run_bitexact_vs_checkers(awcm_lib, eps):
+@pytest.mark.parametrize("eps,delta", [(1e-40, 0.0), (EPS_DIFF, 0.0), (EPS_DIFF, DELTA_DIFF)])
+def test_frozen_run_bitexact_vs_checkers(awcm_lib, eps, delta):
     """Recording run: end state and LF-speed tape equal the restatement's (and the reference's,
-    when its build is present) bit for bit."""
+    when its build is present and the mode is one it has) bit for bit."""
     s, g = prepared_small(awcm_lib)
-    s.set_wenoz_eps(eps)
+    s.set_wenoz(eps, delta)
     nl, nxc, steps = int(g["params"][0]), int(g["params"][1]), int(g["params"][4])
     dt = float(g["dt"])
     qp = s.get_q()
     s.frozen_run(0.0, dt, steps)
     q_gpu, tape_gpu = s.get_q(), s.get_alpha_tape(steps)
-    kinds = ["port"] + (["reference"] if oracle.reference_available() else [])
+    kinds = ["port"] + (["reference"] if oracle.reference_available() and delta == 0 else [])
     for kind in kinds:
         o = Oracle2D(nl, nxc, nxc, 0.0, 10.0, 0.0, 10.0, bc_kind=2, kind=kind)
         o.set_q(qp)
         o.set_masks(g["masks"])
         o.set_levels(g["levels"])
-        o.set_wenoz_eps(eps)
+        o.set_wenoz(eps, delta)
         o.set_freeze(1)
         tape = np.zeros_like(tape_gpu)
         t = 0.0
@@ -87,7 +98,7 @@ def test_frozen_run_bitexact_vs_checkers(awcm_lib, eps):
         qo = o.get_q()
         inner = (slice(3, -3), slice(3, -3))
         assert np.array_equal(q_gpu[inner], qo[inner]), kind
-    if eps == EPS_DIFF:
+    if eps == EPS_DIFF and delta == 0:
         assert np.array_equal(tape_gpu, g["tape"])
         assert np.array_equal(q_gpu[3:-3, 3:-3], g["q_end"][3:-3, 3:-3])
 
@@ -97,7 +108,7 @@ def test_gpu_finite_differences_equal_reference(awcm_lib):
     from awcm import gradient as G
 
     s, g = prepared_small(awcm_lib)
-    s.set_wenoz_eps(EPS_DIFF)
+    s.set_wenoz(EPS_DIFF)
     _, _, _, _, steps, n_dirs, seed, h = g["params"]
     steps, n_dirs, seed = int(steps), int(n_dirs), int(seed)
     s.set_alpha_tape(g["tape"])
@@ -105,7 +116,7 @@ def test_gpu_finite_differences_equal_reference(awcm_lib):
     for k in range(n_dirs):
         a = replay_q(s, g["q"] + h * dirs[k], float(g["dt"]), steps)
         b = replay_q(s, g["q"] - h * dirs[k], float(g["dt"]), steps)
-        assert G.loss_difference(a, b, g["target"]) / (2 * h) == g["fd"][k], k
+        assert G.loss_difference(a, b, g["target"], G.active_points(g["masks"])) / (2 * h) == g["fd"][k], k
 
 
 def directional_errors(grad, dirs, fd):
@@ -114,26 +125,46 @@ def directional_errors(grad, dirs, fd):
 
 
 def test_adjoint_vs_reference_directional_gradient(awcm_lib):
-    """Adjoint directional derivatives against the reference solver's central differences."""
+    """Adjoint directional derivatives against the reference solver's central differences
+    (WENO-Z eps 1e-6, exact |b0 - b2|)."""
     from awcm import gradient as G
 
     s, g = prepared_small(awcm_lib)
-    s.set_wenoz_eps(EPS_DIFF)
+    s.set_wenoz(EPS_DIFF)
     _, _, _, _, steps, n_dirs, seed, h = g["params"]
     s.set_alpha_tape(g["tape"])
     loss, grad, info = s.adjoint(0.0, float(g["dt"]), int(steps), g["target"], replay=True)
     dirs = G.unit_directions(g["q"].shape, int(n_dirs), int(seed))
     ad, rel = directional_errors(grad, dirs, g["fd"])
-    assert rel.max() <= FD_REL_TOL, (rel, ad, g["fd"])
+    print("adjoint vs reference differences: max rel %.2e" % rel.max())
+    assert rel.max() <= REF_FD_REL_TOL, (rel, ad, g["fd"])
     # loss of the replayed run, same value as the recording run's
-    qe = g["q_end"][3:-3, 3:-3, 0] - g["target"]
-    assert loss == pytest.approx(0.5 * float(np.sum(qe * qe)), rel=1e-13)
+    assert loss == pytest.approx(G.loss(g["q_end"], g["target"], G.active_points(g["masks"])), rel=1e-13)
     assert np.all(grad[:3] == 0) and np.all(grad[-3:] == 0) and np.all(grad[:, :3] == 0) and np.all(grad[:, -3:] == 0)
+
+
+def test_adjoint_vs_differences_differentiable_mode(awcm_lib):
+    """Differentiable mode on the fixture grid: 16 directions, h = 1e-6, GPU frozen replay."""
+    from awcm import gradient as G
+
+    s, g = prepared_small(awcm_lib)
+    s.set_wenoz(EPS_DIFF, DELTA_DIFF)
+    _, _, _, _, steps, n_dirs, seed, h = g["params"]
+    steps, dt = int(steps), float(g["dt"])
+    s.set_q(g["q"])
+    loss, grad, info = s.adjoint(0.0, dt, steps, g["target"])
+    dirs = G.unit_directions(g["q"].shape, int(n_dirs), int(seed))
+    act = G.active_points(g["masks"])
+    fd = np.array([G.loss_difference(replay_q(s, g["q"] + h * d, dt, steps), replay_q(s, g["q"] - h * d, dt, steps),
+                                     g["target"], act) / (2 * h) for d in dirs])
+    ad, rel = directional_errors(grad, dirs, fd)
+    print("adjoint vs differences (differentiable mode, 65^2): max rel %.2e" % rel.max())
+    assert rel.max() <= FD_REL_TOL, (rel, ad, fd)
 
 
 def test_checkpoint_intervals_agree(awcm_lib):
     s, g = prepared_small(awcm_lib)
-    s.set_wenoz_eps(EPS_DIFF)
+    s.set_wenoz(EPS_DIFF)
     steps, dt = int(g["params"][4]), float(g["dt"])
     s.set_alpha_tape(g["tape"])
     grads = []
@@ -154,7 +185,7 @@ def test_checkpoint_intervals_agree(awcm_lib):
 def test_adjoint_recording_equals_replay(awcm_lib):
     """mode 1 (record during the adjoint's forward) and mode 2 (replay) give the same result."""
     s, g = prepared_small(awcm_lib)
-    s.set_wenoz_eps(EPS_DIFF)
+    s.set_wenoz(EPS_DIFF)
     steps, dt = int(g["params"][4]), float(g["dt"])
     s.set_q(g["q"])
     l1, g1, _ = s.adjoint(0.0, dt, steps, g["target"])
@@ -167,7 +198,8 @@ def test_adjoint_recording_equals_replay(awcm_lib):
 
 def test_gradient_workload_full_size(awcm_lib):
     """513^2 periodic vortex + bumps, 200 frozen steps, sqrt(N) checkpoints: 16 seeded unit
-    directions against central differences of the GPU frozen replay (h = 1e-6)."""
+    directions against central differences of the GPU frozen replay (h = 1e-5, the smallest step
+    above the run's rounding floor)."""
     from awcm import gradient as G
 
     s = awcm_lib.AWCM2D(6, 17, 17, 0.0, 10.0, 0.0, 10.0, bc_kind=awcm_lib.BC_PERIODIC)
@@ -177,19 +209,20 @@ def test_gradient_workload_full_size(awcm_lib):
     dt = G.stable_dt(q0, 10.0 / 512)
     s.set_q(q0)
     s.prepare(1e-3)
-    s.set_wenoz_eps(EPS_DIFF)
+    s.set_wenoz(EPS_DIFF, DELTA_DIFF)
     qp = s.get_q()
     n = 200
     loss, grad, info = s.adjoint(0.0, dt, n, target)
     assert info["checkpoint_every"] == 15
     assert np.isfinite(loss) and np.isfinite(grad).all()
-    h = 1e-6
+    h = 1e-5
+    act = G.active_points(s.get_masks())
     dirs = G.unit_directions(qp.shape, 16, 11)
     fd = []
     for d in dirs:
         a = replay_q(s, qp + h * d, dt, n)
         b = replay_q(s, qp - h * d, dt, n)
-        fd.append(G.loss_difference(a, b, target) / (2 * h))
+        fd.append(G.loss_difference(a, b, target, act) / (2 * h))
     ad, rel = directional_errors(grad, dirs, np.array(fd))
     print("full-size adjoint: loss %.6e fwd %.1f ms rev %.1f ms max rel %.2e" %
           (loss, info["forward_ms"], info["reverse_ms"], rel.max()))
@@ -207,7 +240,7 @@ def test_torch_autograd_harness(awcm_lib):
     dt = G.stable_dt(q0, 10.0 / (s.nx - 1))
     s.set_q(q0)
     s.prepare(1e-3)
-    s.set_wenoz_eps(EPS_DIFF)
+    s.set_wenoz(EPS_DIFF, DELTA_DIFF)
     qp = s.get_q()
     s.frozen_run(0.0, dt, 4)  # records the LF-speed tape the harness replays
     F = G.frozen_loss_function()
