@@ -104,6 +104,40 @@ __device__ __forceinline__ bool union_point(const Grid2& g, int lev, const int (
     return false;
 }
 
+// Mask words: the plane-wide passes and the fine-level row scans work one 32-bit word of the mask
+// plane (four consecutive points of one row: the pitch is a multiple of 32) per virtual thread,
+// test the word's bits of interest at once and skip empty words, which is most of them.
+constexpr unsigned kLaneBits = 0x01010101u;  // bit 0 of each of the four bytes
+
+struct MaskWord {
+    unsigned w;  // word index; bytes 4w .. 4w+3 of the plane
+    int i0, j;   // grid coordinates of byte 0 (ghosts negative / beyond the grid)
+};
+__device__ __forceinline__ MaskWord mask_word(const Grid2& g, unsigned w)
+{
+    const unsigned a = 4u * w, row = a / (unsigned)g.pitch;
+    return MaskWord{w, (int)(a - row * (unsigned)g.pitch) - kGhost, (int)row - kGhost};
+}
+__device__ __forceinline__ unsigned plane_words(const Grid2& g) { return (unsigned)g.pitch * (unsigned)g.rows / 4u; }
+// Lanes (bit L = byte L) whose column i0 + L lies in [lo, hi].
+__device__ __forceinline__ unsigned lanes_in(int i0, int lo, int hi)
+{
+    unsigned r = 0;
+#pragma unroll
+    for (int L = 0; L < 4; ++L) r |= (unsigned)(i0 + L >= lo && i0 + L <= hi) << L;
+    return r;
+}
+// Lane set -> bit 0 of each selected byte.
+__device__ __forceinline__ unsigned lane_bits(unsigned lanes)
+{
+    return (lanes & 1u) | ((lanes & 2u) << 7) | ((lanes & 4u) << 14) | ((lanes & 8u) << 21);
+}
+// Lanes that are grid points (0 <= i < nx, 0 <= j < ny).
+__device__ __forceinline__ unsigned grid_lanes(const Grid2& g, const MaskWord& mw)
+{
+    return (mw.j >= 0 && mw.j < g.ny) ? lanes_in(mw.i0, 0, g.nx - 1) : 0u;
+}
+
 // ------------------------------------------------------------------------------- phase bodies
 // Every PrepareEuler pass is a device function over a virtual thread range (t0, stride), so the
 // same body runs as a standalone kernel (one thread per point) or inside the persistent prepare
@@ -267,9 +301,28 @@ __device__ void ph_iwt(const Grid2& g, double* __restrict__ q, const uint8_t* __
 // d3 -> d1 -> d2 so that d1/d2 points switched on by a d3 point also mark their stencils; those
 // stencils ((is..is+3D, n) for a d1 point (i, n), (m, js..js+3D) for a d2 point (m, j)) lie inside
 // the d3 point's own 4x4 block of marks, so all three sub-bands can run concurrently.
-__device__ void ph_cr(const Grid2& g, uint8_t* __restrict__ m, int lev, int bit, Span sp)
+__device__ __forceinline__ void cr_push(const Grid2& g, uint8_t* m, int i, int j, int D, int w, int bit)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
+    int is, js, k;
+    if (w == 2) {
+        predict_stencil(i, D, NX, is, k);
+        predict_stencil(j, D, NY, js, k);
+        for (int c = 0; c < 4; ++c) push_bit(g, m, is + c * D, j, bit);
+        for (int c = 0; c < 4; ++c) push_bit(g, m, i, js + c * D, bit);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) push_bit(g, m, is + c1 * D, js + c2 * D, bit);
+    } else if (w == 0) {
+        predict_stencil(i, D, NX, is, k);
+        for (int c = 0; c < 4; ++c) push_bit(g, m, is + c * D, j, bit);
+    } else {
+        predict_stencil(j, D, NY, js, k);
+        for (int c = 0; c < 4; ++c) push_bit(g, m, i, js + c * D, bit);
+    }
+}
+
+__device__ void ph_cr(const Grid2& g, uint8_t* __restrict__ m, int lev, int bit, Span sp)
+{
     const int which[3] = {2, 0, 1};
     const unsigned n = band_n(g, lev, 0) + band_n(g, lev, 1) + band_n(g, lev, 2);
     const int D = g.D(lev);
@@ -277,30 +330,112 @@ __device__ void ph_cr(const Grid2& g, uint8_t* __restrict__ m, int lev, int bit,
         int i, j, w;
         union_point(g, lev, which, t, i, j, w);
         if (!((m[g.at(i, j)] >> bit) & 1u)) continue;
-        int is, js, k;
-        if (w == 2) {
-            predict_stencil(i, D, NX, is, k);
-            predict_stencil(j, D, NY, js, k);
-            for (int c = 0; c < 4; ++c) push_bit(g, m, is + c * D, j, bit);
-            for (int c = 0; c < 4; ++c) push_bit(g, m, i, js + c * D, bit);
-            for (int c2 = 0; c2 < 4; ++c2)
-                for (int c1 = 0; c1 < 4; ++c1) push_bit(g, m, is + c1 * D, js + c2 * D, bit);
-        } else if (w == 0) {
-            predict_stencil(i, D, NX, is, k);
-            for (int c = 0; c < 4; ++c) push_bit(g, m, is + c * D, j, bit);
-        } else {
-            predict_stencil(j, D, NY, js, k);
-            for (int c = 0; c < 4; ++c) push_bit(g, m, i, js + c * D, bit);
+        cr_push(g, m, i, j, D, w, bit);
+    }
+}
+
+// Row-scan form of a fine level (point spacing h = D/2 <= kRowScanMaxH): the rows j = 0, h, 2h ..
+// of the level are scanned one mask word (four columns) per virtual thread and the set lanes are
+// classified by position: d1 = (odd, even) multiples of h off the top/bottom rows, d2 = (even,
+// odd) off the left/right columns, d3 = (odd, odd) -- exactly the sub-band extents of band_of.
+// Rows with parity `rows` (0 even, 1 odd, 2 both) in units of h.
+constexpr int kRowScanMaxH = 2;
+__device__ __forceinline__ unsigned rowscan_n(const Grid2& g, int lev, int rows)
+{
+    const int h = g.D(lev) >> 1;
+    const unsigned nr = (unsigned)((g.ny - 1) / h) + 1u;  // rows 0, h, .., NY
+    const unsigned wpr = (unsigned)g.pitch / 4u;
+    return (rows == 2 ? nr : (rows == 0 ? (nr + 1u) / 2u : nr / 2u)) * wpr;
+}
+// Decodes virtual thread t of a row scan into the row j and the word (its first column i0, its
+// mask bits v) ; returns the set of lanes that are points of this level (columns multiple of h in
+// [0, NX]).
+__device__ __forceinline__ unsigned rowscan_word(const Grid2& g, int lev, int rows, unsigned t, int& j, int& i0,
+                                                 unsigned& widx)
+{
+    const int h = g.D(lev) >> 1;
+    const unsigned wpr = (unsigned)g.pitch / 4u;
+    const unsigned r = t / wpr, wi = t - r * wpr;
+    const unsigned rr = rows == 2 ? r : 2u * r + (unsigned)rows;
+    j = (int)rr * h;
+    i0 = 4 * (int)wi - kGhost;
+    widx = (unsigned)(j + kGhost) * wpr + wi;
+    unsigned lanes = lanes_in(i0, 0, g.nx - 1);
+    if (h == 2) lanes &= (i0 & 1) ? 0xAu : 0x5u;  // even columns
+    return lanes;
+}
+// Sub-band of the level point (i, j) (h = spacing): 2 = d3, 0 = d1, 1 = d2, -1 = none.
+__device__ __forceinline__ int rowscan_band(const Grid2& g, int i, int j, int h)
+{
+    const bool io = (i / h) & 1, jo = (j / h) & 1;
+    if (io && jo) return 2;
+    if (io) return (j == 0 || j == g.ny - 1) ? -1 : 0;
+    if (jo) return (i == 0 || i == g.nx - 1) ? -1 : 1;
+    return -1;
+}
+
+__device__ void ph_cr_rows(const Grid2& g, uint8_t* __restrict__ m, int lev, int bit, Span sp)
+{
+    const int D = g.D(lev), h = D >> 1;
+    const unsigned n = rowscan_n(g, lev, 2);
+    const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int j, i0;
+        unsigned wdx;
+        const unsigned lanes = rowscan_word(g, lev, 2, t, j, i0, wdx);
+        unsigned hit = (mp[wdx] >> bit) & lane_bits(lanes);
+        while (hit) {
+            const int L = (__ffs(hit) - 1) >> 3;
+            hit &= hit - 1;
+            const int i = i0 + L;
+            const int w = rowscan_band(g, i, j, h);
+            if (w >= 0) cr_push(g, m, i, j, D, w, bit);
         }
     }
 }
 
 // InterpolateEuler, one phase of one level (WAVELET_2D.h:784-907): PH 0 = d1 and d2, PH 1 = d3;
 // components 1..3 at points of the work mask that were not active before (`from_bit`).
+__device__ __forceinline__ void interp_point(const Grid2& g, Field4 q, int i, int j, size_t a, int D, int w)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    if (w == 0) {
+        int s0, k;
+        predict_stencil(i, D, NX, s0, k);
+        for (int p = 1; p < 4; ++p) {
+            const double* qp = q.p[p];
+            double v = 0.0;
+            for (int c = 0; c < 4; ++c) v += qp[g.at(s0 + c * D, j)] * g.w(c, k);
+            q.p[p][a] = v;
+        }
+    } else if (w == 1) {
+        int s0, k;
+        predict_stencil(j, D, NY, s0, k);
+        for (int p = 1; p < 4; ++p) {
+            const double* qp = q.p[p];
+            double v = 0.0;
+            for (int c = 0; c < 4; ++c) v += qp[g.at(i, s0 + c * D)] * g.w(c, k);
+            q.p[p][a] = v;
+        }
+    } else {
+        int is, k1, js, k2;
+        predict_stencil(i, D, NX, is, k1);
+        predict_stencil(j, D, NY, js, k2);
+        for (int p = 1; p < 4; ++p) {
+            const double* qp = q.p[p];
+            double v = 0.0;
+            for (int c = 0; c < 4; ++c) v += qp[g.at(is + c * D, j)] * g.w(c, k1);
+            for (int c = 0; c < 4; ++c) v += qp[g.at(i, js + c * D)] * g.w(c, k2);
+            for (int c2 = 0; c2 < 4; ++c2)
+                for (int c1 = 0; c1 < 4; ++c1) v -= qp[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+            q.p[p][a] = v;
+        }
+    }
+}
+
 template <int PH>
 __device__ void ph_interp(const Grid2& g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit, Span sp)
 {
-    const int NX = g.nx - 1, NY = g.ny - 1;
     const int D = g.D(lev);
     const unsigned n = PH == 0 ? band_n(g, lev, 0) + band_n(g, lev, 1) : band_n(g, lev, 2);
     for (unsigned t = sp.t0; t < n; t += sp.stride) {
@@ -315,71 +450,66 @@ __device__ void ph_interp(const Grid2& g, Field4 q, const uint8_t* __restrict__ 
         const size_t a = g.at(i, j);
         const unsigned mb = m[a];
         if (!((mb >> kBitInterp) & 1u) || ((mb >> from_bit) & 1u)) continue;
-        if (w == 0) {
-            int s0, k;
-            predict_stencil(i, D, NX, s0, k);
-            for (int p = 1; p < 4; ++p) {
-                const double* qp = q.p[p];
-                double v = 0.0;
-                for (int c = 0; c < 4; ++c) v += qp[g.at(s0 + c * D, j)] * g.w(c, k);
-                q.p[p][a] = v;
-            }
-        } else if (w == 1) {
-            int s0, k;
-            predict_stencil(j, D, NY, s0, k);
-            for (int p = 1; p < 4; ++p) {
-                const double* qp = q.p[p];
-                double v = 0.0;
-                for (int c = 0; c < 4; ++c) v += qp[g.at(i, s0 + c * D)] * g.w(c, k);
-                q.p[p][a] = v;
-            }
-        } else {
-            int is, k1, js, k2;
-            predict_stencil(i, D, NX, is, k1);
-            predict_stencil(j, D, NY, js, k2);
-            for (int p = 1; p < 4; ++p) {
-                const double* qp = q.p[p];
-                double v = 0.0;
-                for (int c = 0; c < 4; ++c) v += qp[g.at(is + c * D, j)] * g.w(c, k1);
-                for (int c = 0; c < 4; ++c) v += qp[g.at(i, js + c * D)] * g.w(c, k2);
-                for (int c2 = 0; c2 < 4; ++c2)
-                    for (int c1 = 0; c1 < 4; ++c1) v -= qp[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-                q.p[p][a] = v;
-            }
+        interp_point(g, q, i, j, a, D, w);
+    }
+}
+
+// Row-scan form of ph_interp for the fine levels: PH 0 scans every row of the level (d1 on the
+// even ones, d2 on the odd ones), PH 1 only the odd rows (d3).
+template <int PH>
+__device__ void ph_interp_rows(const Grid2& g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit, Span sp)
+{
+    const int D = g.D(lev), h = D >> 1;
+    const int rows = PH == 0 ? 2 : 1;
+    const unsigned n = rowscan_n(g, lev, rows);
+    const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        int j, i0;
+        unsigned wdx;
+        const unsigned lanes = rowscan_word(g, lev, rows, t, j, i0, wdx);
+        const unsigned v = mp[wdx];
+        unsigned hit = (v >> kBitInterp) & ~(v >> from_bit) & lane_bits(lanes);
+        while (hit) {
+            const int L = (__ffs(hit) - 1) >> 3;
+            hit &= hit - 1;
+            const int i = i0 + L;
+            const int w = rowscan_band(g, i, j, h);
+            if (w < 0 || (PH == 0) == (w == 2)) continue;
+            interp_point(g, q, i, j, 4u * wdx + L, D, w);
         }
     }
 }
 
 // ------------------------------------------------------------------------------- dense mask passes
-__device__ __forceinline__ bool grid_point(const Grid2& g, unsigned t, int& i, int& j)
-{
-    if (t >= (unsigned)g.nx * (unsigned)g.ny) return false;
-    i = (int)(t % (unsigned)g.nx);
-    j = (int)(t / (unsigned)g.nx);
-    return true;
-}
-
 __device__ void ph_copy_bit_all(uint8_t* m, size_t n, int from, int to, Span sp)
 {
-    for (unsigned a = sp.t0; a < n; a += sp.stride) {
-        const unsigned v = m[a];
-        m[a] = (uint8_t)((v & ~(1u << to)) | (((v >> from) & 1u) << to));
+    unsigned* mw = reinterpret_cast<unsigned*>(m);
+    const unsigned nw = (unsigned)(n / 4);
+    for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const unsigned v = mw[w];
+        const unsigned nv = (v & ~(kLaneBits << to)) | (((v >> from) & kLaneBits) << to);
+        if (nv != v) mw[w] = nv;
     }
 }
 
 // BandingMask (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:205-213) on `bit`, then copies the
-// result into the work bit read by the following add-adjacent-zone pass.
+// result into the work bit read by the following add-adjacent-zone pass (grid points only).
 __device__ void ph_band_copy(const Grid2& g, uint8_t* m, int bit, int copy_to, Span sp)
 {
-    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
-    for (unsigned t = sp.t0; t < n; t += sp.stride) {
-        int i, j;
-        grid_point(g, t, i, j);
-        const size_t a = g.at(i, j);
-        unsigned v = m[a];
-        if (!(2 <= i && i <= g.nx - 3 && j >= 2 && j <= g.ny - 3)) v |= 1u << bit;
-        if (copy_to >= 0) v = (v & ~(1u << copy_to)) | (((v >> bit) & 1u) << copy_to);
-        m[a] = (uint8_t)v;
+    unsigned* mp = reinterpret_cast<unsigned*>(m);
+    const unsigned nw = plane_words(g);
+    for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const MaskWord mw = mask_word(g, w);
+        const unsigned G = grid_lanes(g, mw);
+        if (!G) continue;
+        const unsigned inner = (mw.j >= 2 && mw.j <= g.ny - 3) ? lanes_in(mw.i0, 2, g.nx - 3) : 0u;
+        const unsigned v = mp[w];
+        unsigned nv = v | (lane_bits(G & ~inner) << bit);
+        if (copy_to >= 0) {
+            const unsigned gb = lane_bits(G);
+            nv = (nv & ~(gb << copy_to)) | (((nv >> bit) & gb) << copy_to);
+        }
+        if (nv != v) mp[w] = nv;
     }
 }
 
@@ -390,32 +520,39 @@ __device__ void ph_band_copy(const Grid2& g, uint8_t* m, int bit, int copy_to, S
 __device__ void ph_aaz(const Grid2& g, uint8_t* m, int bit, int src, Span sp)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
-    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
-    for (unsigned t = sp.t0; t < n; t += sp.stride) {
-        int i, j;
-        grid_point(g, t, i, j);
-        const int ti = ctz_or(i, 64), tj = ctz_or(j, 64);
-        const int mn = ti < tj ? ti : tj;
-        if (mn >= g.maxl) continue;
-        if (ti < tj && (j == 0 || j == NY)) continue;
-        if (tj < ti && (i == 0 || i == NX)) continue;
-        if (!((m[g.at(i, j)] >> src) & 1u)) continue;
-        const int lev = g.maxl - 1 - mn;
-        if (lev == g.maxl - 1) {
-            push_bit(g, m, i - 1, j, bit);
-            push_bit(g, m, i + 1, j, bit);
-            push_bit(g, m, i, j - 1, bit);
-            push_bit(g, m, i, j + 1, bit);
-        } else {
-            const int D = g.D(lev), h = D / 2, q4 = D / 4;
-            push_bit(g, m, i - q4, j, bit);
-            push_bit(g, m, i + q4, j, bit);
-            push_bit(g, m, i, j - q4, bit);
-            push_bit(g, m, i, j + q4, bit);
-            push_bit(g, m, i - h, j, bit);
-            push_bit(g, m, i + h, j, bit);
-            push_bit(g, m, i, j - h, bit);
-            push_bit(g, m, i, j + h, bit);
+    const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    const unsigned nw = plane_words(g);
+    for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const MaskWord mw = mask_word(g, w);
+        const unsigned G = grid_lanes(g, mw);
+        if (!G) continue;
+        unsigned hit = (mp[w] >> src) & lane_bits(G);
+        while (hit) {
+            const int L = (__ffs(hit) - 1) >> 3;
+            hit &= hit - 1;
+            const int i = mw.i0 + L, j = mw.j;
+            const int ti = ctz_or(i, 64), tj = ctz_or(j, 64);
+            const int mn = ti < tj ? ti : tj;
+            if (mn >= g.maxl) continue;
+            if (ti < tj && (j == 0 || j == NY)) continue;
+            if (tj < ti && (i == 0 || i == NX)) continue;
+            const int lev = g.maxl - 1 - mn;
+            if (lev == g.maxl - 1) {
+                push_bit(g, m, i - 1, j, bit);
+                push_bit(g, m, i + 1, j, bit);
+                push_bit(g, m, i, j - 1, bit);
+                push_bit(g, m, i, j + 1, bit);
+            } else {
+                const int D = g.D(lev), h = D / 2, q4 = D / 4;
+                push_bit(g, m, i - q4, j, bit);
+                push_bit(g, m, i + q4, j, bit);
+                push_bit(g, m, i, j - q4, bit);
+                push_bit(g, m, i, j + q4, bit);
+                push_bit(g, m, i - h, j, bit);
+                push_bit(g, m, i + h, j, bit);
+                push_bit(g, m, i, j - h, bit);
+                push_bit(g, m, i, j + h, bit);
+            }
         }
     }
 }
@@ -433,26 +570,42 @@ __device__ __forceinline__ bool mask_or_ghost(const Grid2& g, const uint8_t* m, 
 // runs for grid points only.
 __device__ void ph_cl(const Grid2& g, uint8_t* m, int8_t* lvl, int bit, int copy_to, size_t plane, Span sp)
 {
-    for (unsigned a = sp.t0; a < plane; a += sp.stride) {
-        const int i = (int)(a % (unsigned)g.pitch) - kGhost, j = (int)(a / (unsigned)g.pitch) - kGhost;
-        const unsigned v = m[a];
-        const bool on = (v >> bit) & 1u;
-        if (i >= 0 && i < g.nx && j >= 0 && j < g.ny) {
-            if (!on) {
-                lvl[a] = 0;
-            } else {
+    unsigned* mp = reinterpret_cast<unsigned*>(m);
+    unsigned* lp = reinterpret_cast<unsigned*>(lvl);
+    const unsigned nw = (unsigned)(plane / 4);
+    for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const MaskWord mw = mask_word(g, w);
+        const unsigned v = mp[w];
+        const unsigned G = grid_lanes(g, mw);
+        if (G) {
+            const unsigned lv0 = lp[w];
+            unsigned lv = lv0;
+            const unsigned on = (v >> bit) & kLaneBits;
+#pragma unroll
+            for (int L = 0; L < 4; ++L) {
+                if (!((G >> L) & 1u)) continue;
+                const unsigned sh = 8u * L;
+                if (!((on >> sh) & 1u)) {
+                    lv &= ~(0xffu << sh);
+                    continue;
+                }
+                const int i = mw.i0 + L, j = mw.j;
                 int dx = 1;
                 for (int lev = g.maxl; lev >= 0; --lev) {
                     if (mask_or_ghost(g, m, i - dx, j, bit) || mask_or_ghost(g, m, i + dx, j, bit) ||
                         mask_or_ghost(g, m, i, j - dx, bit) || mask_or_ghost(g, m, i, j + dx, bit)) {
-                        lvl[a] = (int8_t)lev;
+                        lv = (lv & ~(0xffu << sh)) | ((unsigned)(uint8_t)(int8_t)lev << sh);
                         break;
                     }
                     dx *= 2;
                 }
             }
+            if (lv != lv0) lp[w] = lv;
         }
-        if (copy_to >= 0) m[a] = (uint8_t)((v & ~(1u << copy_to)) | ((on ? 1u : 0u) << copy_to));
+        if (copy_to >= 0) {
+            const unsigned nv = (v & ~(kLaneBits << copy_to)) | (((v >> bit) & kLaneBits) << copy_to);
+            if (nv != v) mp[w] = nv;
+        }
     }
 }
 
@@ -461,44 +614,53 @@ __device__ void ph_cl(const Grid2& g, uint8_t* m, int8_t* lvl, int bit, int copy
 __device__ void ph_apd(const Grid2& g, uint8_t* m, const int8_t* lvl, int bit, int src, Span sp)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
-    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
-    for (unsigned t = sp.t0; t < n; t += sp.stride) {
-        int i, j;
-        grid_point(g, t, i, j);
-        if (i < 1 || i > NX - 1 || j < 1 || j > NY - 1) continue;
-        const size_t a = g.at(i, j);
-        if (!((m[a] >> src) & 1u)) continue;
-        const int lev = lvl[a];
-        if (lev == g.maxl) {
-            for (int c = -3; c <= 3; ++c) {
-                push_bit(g, m, i + c, j, bit);
-                push_bit(g, m, i, j + c, bit);
+    const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    const unsigned nw = plane_words(g);
+    for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const MaskWord mw = mask_word(g, w);
+        if (mw.j < 1 || mw.j > NY - 1) continue;
+        const unsigned I = lanes_in(mw.i0, 1, NX - 1);
+        if (!I) continue;
+        unsigned hit = (mp[w] >> src) & lane_bits(I);
+        while (hit) {
+            const int L = (__ffs(hit) - 1) >> 3;
+            hit &= hit - 1;
+            const int i = mw.i0 + L, j = mw.j;
+            const int lev = lvl[4u * w + L];
+            if (lev == g.maxl) {
+                for (int c = -3; c <= 3; ++c) {
+                    push_bit(g, m, i + c, j, bit);
+                    push_bit(g, m, i, j + c, bit);
+                }
+                continue;
             }
-            continue;
+            const int D = g.D(lev);
+            int lo = -2, hi = 2;
+            if (i - 2 * D < 0) lo = -1;
+            else if (i + 2 * D > NX) hi = 1;
+            for (int c = lo; c <= hi; ++c) push_bit(g, m, i + D * c, j, bit);
+            lo = -2, hi = 2;
+            if (j - 2 * D < 0) lo = -1;
+            else if (j + 2 * D > NY) hi = 1;
+            for (int c = lo; c <= hi; ++c) push_bit(g, m, i, j + D * c, bit);
         }
-        const int D = g.D(lev);
-        int lo = -2, hi = 2;
-        if (i - 2 * D < 0) lo = -1;
-        else if (i + 2 * D > NX) hi = 1;
-        for (int c = lo; c <= hi; ++c) push_bit(g, m, i + D * c, j, bit);
-        lo = -2, hi = 2;
-        if (j - 2 * D < 0) lo = -1;
-        else if (j + 2 * D > NY) hi = 1;
-        for (int c = lo; c <= hi; ++c) push_bit(g, m, i, j + D * c, bit);
     }
 }
 
 // Work mask of InterpolateEuler: `to` minus `from` over the grid points (ghost bits untouched).
 __device__ void ph_interp_init(const Grid2& g, uint8_t* m, int from, int to, Span sp)
 {
-    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
-    for (unsigned t = sp.t0; t < n; t += sp.stride) {
-        int i, j;
-        grid_point(g, t, i, j);
-        const size_t a = g.at(i, j);
-        const unsigned v = m[a];
-        const unsigned on = ((v >> to) & 1u) & ~((v >> from) & 1u);
-        m[a] = (uint8_t)((v & ~(1u << kBitInterp)) | (on << kBitInterp));
+    unsigned* mp = reinterpret_cast<unsigned*>(m);
+    const unsigned nw = plane_words(g);
+    for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const MaskWord mw = mask_word(g, w);
+        const unsigned G = grid_lanes(g, mw);
+        if (!G) continue;
+        const unsigned gb = lane_bits(G);
+        const unsigned v = mp[w];
+        const unsigned on = (v >> to) & ~(v >> from) & gb;
+        const unsigned nv = (v & ~(gb << kBitInterp)) | (on << kBitInterp);
+        if (nv != v) mp[w] = nv;
     }
 }
 
@@ -506,19 +668,26 @@ __device__ void ph_interp_init(const Grid2& g, uint8_t* m, int from, int to, Spa
 // step only points that can hold non-zero values (in mask3 or in the previous mask0) are written.
 __device__ void ph_remove_residue(const Grid2& g, Field4 q, const uint8_t* m, int bit, bool full, Span sp)
 {
-    const unsigned n = (unsigned)g.nx * (unsigned)g.ny;
-    for (unsigned t = sp.t0; t < n; t += sp.stride) {
-        int i, j;
-        grid_point(g, t, i, j);
-        if (i < 1 || i > g.nx - 2 || j < 1 || j > g.ny - 2) continue;
-        const size_t a = g.at(i, j);
-        const unsigned v = m[a];
-        if ((v >> bit) & 1u) continue;
-        if (!full && !(v & ((1u << 3) | (1u << kBitTemp)))) continue;
-        q.p[0][a] = 0.0;
-        q.p[1][a] = 0.0;
-        q.p[2][a] = 0.0;
-        q.p[3][a] = 0.0;
+    const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    const unsigned nw = plane_words(g);
+    for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const MaskWord mw = mask_word(g, w);
+        if (mw.j < 1 || mw.j > g.ny - 2) continue;
+        const unsigned I = lanes_in(mw.i0, 1, g.nx - 2);
+        if (!I) continue;
+        const unsigned v = mp[w];
+        unsigned hit = ~(v >> bit) & lane_bits(I);
+        if (!full) hit &= (v >> 3) | (v >> kBitTemp);
+        hit &= kLaneBits;
+        while (hit) {
+            const int L = (__ffs(hit) - 1) >> 3;
+            hit &= hit - 1;
+            const size_t a = 4u * w + L;
+            q.p[0][a] = 0.0;
+            q.p[1][a] = 0.0;
+            q.p[2][a] = 0.0;
+            q.p[3][a] = 0.0;
+        }
     }
 }
 
@@ -547,11 +716,22 @@ __global__ void k_cr(Grid2 g, uint8_t* m, int lev, int bit, const StepState* st)
     AWCM_SKIP_IF_DONE(st);
     ph_cr(g, m, lev, bit, grid_span());
 }
+__global__ void k_cr_rows(Grid2 g, uint8_t* m, int lev, int bit, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_cr_rows(g, m, lev, bit, grid_span());
+}
 template <int PH>
 __global__ void k_interp(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, const StepState* st)
 {
     AWCM_SKIP_IF_DONE(st);
     ph_interp<PH>(g, q, m, lev, from_bit, grid_span());
+}
+template <int PH>
+__global__ void k_interp_rows(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, const StepState* st)
+{
+    AWCM_SKIP_IF_DONE(st);
+    ph_interp_rows<PH>(g, q, m, lev, from_bit, grid_span());
 }
 __global__ void k_copy_bit_all(uint8_t* m, size_t n, int from, int to, const StepState* st)
 {
@@ -796,40 +976,54 @@ __global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host)
 // ------------------------------------------------------------------------- CFL and LF reductions
 // Per-row alpha_x[j] = max |u|+c and per-column alpha_y[i] = max |v|+c over the points of mask
 // `bit` (main_2d_euler(quad).cpp:86-104); with mv != null also the CFL speed
-// max (|u|+c)+(|v|+c) (:61-76).  Tiles of 32 columns x 32 rows; maxima are order-independent.
+// max (|u|+c)+(|v|+c) (:61-76).  A CTA covers 128 columns (one mask word of four points per
+// lane) x 32 rows (four per warp); empty words cost one load.  Maxima are order-independent.
+constexpr int kAlphaRows = 4;
 __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t* __restrict__ m, int bit,
                                                double* ax, double* ay, double* mv, const StepState* st)
 {
     if (st && st->done) return;
-    __shared__ double col[8][32];
+    __shared__ double col[8][128];
     __shared__ double cfl[8];
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    double cmax = 0, vmax = 0;
-    for (int r = 0; r < 4; ++r) {
-        const int j = blockIdx.y * 32 + threadIdx.y * 4 + r;
-        double sx = 0;
-        if (i < g.nx && j < g.ny) {
-            const size_t a = g.at(i, j);
-            if ((m[a] >> bit) & 1u) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned wpr = (unsigned)g.pitch / 4u;  // mask words per plane row
+    const unsigned wi = blockIdx.x * 32u + lane;
+    const int i0 = 4 * (int)wi - kGhost;
+    const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    double cm[4] = {0, 0, 0, 0};
+    double vmax = 0;
+    for (int r = 0; r < kAlphaRows; ++r) {
+        const int j = (int)blockIdx.y * (8 * kAlphaRows) + warp * kAlphaRows + r;
+        double sx_row = 0;
+        if (j < g.ny && wi < wpr) {
+            const unsigned lanes = lanes_in(i0, 0, g.nx - 1);
+            const unsigned hit = (mp[(size_t)(j + kGhost) * wpr + wi] >> bit) & lane_bits(lanes);
+#pragma unroll
+            for (int L = 0; L < 4; ++L) {
+                if (!((hit >> (8 * L)) & 1u)) continue;
+                const size_t a = g.at(i0 + L, j);
                 const double q[4] = {f.p[0][a], f.p[1][a], f.p[2][a], f.p[3][a]};
                 const double c = sound2(q, g.gamma);
-                sx = absd(q[1] / q[0]) + c;
+                const double sx = absd(q[1] / q[0]) + c;
                 const double sy = absd(q[2] / q[0]) + c;
-                cmax = maxd(cmax, sy);
+                sx_row = maxd(sx_row, sx);
+                cm[L] = maxd(cm[L], sy);
                 vmax = maxd(vmax, sx + sy);
             }
         }
-        const double rowmax = warp_max(sx);
-        if (threadIdx.x == 0 && j < g.ny && rowmax > 0) atomic_max_nonneg(&ax[j], rowmax);
+        const double rowmax = warp_max(sx_row);
+        if (lane == 0 && j < g.ny && rowmax > 0) atomic_max_nonneg(&ax[j], rowmax);
     }
-    col[threadIdx.y][threadIdx.x] = cmax;
+#pragma unroll
+    for (int L = 0; L < 4; ++L) col[warp][4 * lane + L] = cm[L];
     vmax = warp_max(vmax);
-    if (threadIdx.x == 0) cfl[threadIdx.y] = vmax;
+    if (lane == 0) cfl[warp] = vmax;
     __syncthreads();
-    if (threadIdx.y == 0) {
+    if (threadIdx.x < 128) {
         double c = col[0][threadIdx.x];
         for (int y = 1; y < 8; ++y) c = maxd(c, col[y][threadIdx.x]);
-        if (i < g.nx && c > 0) atomic_max_nonneg(&ay[i], c);
+        const int i = 4 * ((int)blockIdx.x * 32) - kGhost + (int)threadIdx.x;
+        if (i >= 0 && i < g.nx && c > 0) atomic_max_nonneg(&ay[i], c);
         if (mv && threadIdx.x == 0) {
             double v = cfl[0];
             for (int y = 1; y < 8; ++y) v = maxd(v, cfl[y]);
@@ -896,11 +1090,35 @@ struct ListArgs {
     uint32_t* list[kNumLists];
 };
 
-__device__ __forceinline__ bool fin_at(const Grid2& g, const uint8_t* m, const int8_t* lvl, int i, int j, int bit)
+// Stage predicates of the point (i, j) (i from -1, j from -1): per stage s (bits 4s..4s+3):
+// finest-level point, coarse point, x face (i+1/2, j) needed, y face (i, j+1/2) needed.
+__device__ __forceinline__ unsigned list_preds(const Grid2& g, const uint8_t* __restrict__ m,
+                                               const int8_t* const (&lvls)[kStages], int i, int j, unsigned& mbits)
 {
-    if (i < 0 || i >= g.nx || j < 0 || j >= g.ny) return false;
-    const size_t a = g.at(i, j);
-    return ((m[a] >> bit) & 1u) && lvl[a] == g.maxl;
+    const bool row_in = j >= 0 && j < g.ny, col_in = i >= 0 && i < g.nx;
+    const bool inside = row_in && col_in;
+    const bool right_in = row_in && i + 1 >= 0 && i + 1 < g.nx;
+    const bool up_in = col_in && j + 1 >= 0 && j + 1 < g.ny;
+    const unsigned here = inside ? m[g.at(i, j)] : 0u;
+    const unsigned right = right_in ? m[g.at(i + 1, j)] : 0u;
+    const unsigned up = up_in ? m[g.at(i, j + 1)] : 0u;
+    mbits = here & 15u;
+    if (!((here | right | up) & 7u)) return 0u;
+    const bool xface = row_in && i <= g.nx - 1, yface = col_in && j <= g.ny - 1;
+    unsigned p = 0;
+#pragma unroll
+    for (int s = 0; s < kStages; ++s) {
+        const int bit = 2 - s;
+        const int8_t* lvl = lvls[s];
+        const bool act = (here >> bit) & 1u;
+        const bool fin = act && lvl[g.at(i, j)] == g.maxl;
+        const bool fin_r = ((right >> bit) & 1u) && lvl[g.at(i + 1, j)] == g.maxl;
+        const bool fin_u = ((up >> bit) & 1u) && lvl[g.at(i, j + 1)] == g.maxl;
+        p |= ((unsigned)fin | ((unsigned)(act && !fin) << 1) | ((unsigned)(xface && (fin || fin_r)) << 2) |
+              ((unsigned)(yface && (fin || fin_u)) << 3))
+             << (4 * s);
+    }
+    return p;
 }
 
 __global__ void __launch_bounds__(256) k_lists(Grid2 g, const uint8_t* __restrict__ m, const int8_t* __restrict__ l2,
@@ -913,53 +1131,41 @@ __global__ void __launch_bounds__(256) k_lists(Grid2 g, const uint8_t* __restric
     __shared__ unsigned mcnt[4];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int i = (int)blockIdx.x * 256 + threadIdx.x - 1;  // -1 .. nx-1 (+ padding)
-    const int8_t* lvls[3] = {l2, l1, l0};
-    const int bits[3] = {2, 1, 0};
+    const int8_t* const lvls[kStages] = {l2, l1, l0};
     if (threadIdx.x < kNumLists)
         for (int w = 0; w < 8; ++w) wcnt[w][threadIdx.x] = 0;
     if (threadIdx.x < 4) mcnt[threadIdx.x] = 0;
     __syncthreads();
 
-    auto preds = [&](int j, bool* p, unsigned& mbits) {
-        mbits = 0;
-        const bool inside = i >= 0 && i < g.nx && j >= 0 && j < g.ny;
-        if (inside) mbits = m[g.at(i, j)] & 15u;
-#pragma unroll
-        for (int s = 0; s < kStages; ++s) {
-            const int bit = bits[s];
-            const int8_t* lvl = lvls[s];
-            bool act = false, fin = false;
-            if (inside) {
-                act = (mbits >> bit) & 1u;
-                fin = act && lvl[g.at(i, j)] == g.maxl;
-            }
-            p[4 * s + 0] = fin;
-            p[4 * s + 1] = act && !fin;
-            p[4 * s + 2] = j >= 0 && j < g.ny && i <= g.nx - 1 && (fin || fin_at(g, m, lvl, i + 1, j, bit));
-            p[4 * s + 3] = i >= 0 && i < g.nx && j <= g.ny - 1 && (fin || fin_at(g, m, lvl, i, j + 1, bit));
-        }
-    };
-
+    // predicates of the kListRows rows, kept in registers for the write pass
     const int j0 = (int)blockIdx.y * kListRows - 1;
+    unsigned pm[kListRows];
     unsigned mloc[4] = {0, 0, 0, 0};
-    for (int r = 0; r < kListRows; ++r) {
-        const int j = j0 + r;
-        bool p[kNumLists];
-        unsigned mb;
-        preds(j, p, mb);
-        if (j >= 0 && i >= 0)
-            for (int k = 0; k < 4; ++k) mloc[k] += (mb >> k) & 1u;
+    unsigned any = 0;
 #pragma unroll
-        for (int L = 0; L < kNumLists; ++L) {
-            const unsigned bal = __ballot_sync(0xffffffffu, p[L]);
-            if (lane == 0) wcnt[warp][L] += __popc(bal);
-        }
+    for (int r = 0; r < kListRows; ++r) {
+        unsigned mb;
+        pm[r] = list_preds(g, m, lvls, i, j0 + r, mb);
+        any |= pm[r];
+        if (j0 + r >= 0 && i >= 0)
+            for (int k = 0; k < 4; ++k) mloc[k] += (mb >> k) & 1u;
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        unsigned v = mloc[k];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        const unsigned v = __reduce_add_sync(0xffffffffu, mloc[k]);
         if (lane == 0 && v) atomicAdd(&mcnt[k], v);
+    }
+    const bool warp_any = __any_sync(0xffffffffu, any != 0);
+    if (warp_any) {
+#pragma unroll
+        for (int r = 0; r < kListRows; ++r) {
+            if (!__any_sync(0xffffffffu, pm[r] != 0)) continue;
+#pragma unroll
+            for (int L = 0; L < kNumLists; ++L) {
+                const unsigned bal = __ballot_sync(0xffffffffu, (pm[r] >> L) & 1u);
+                if (lane == 0) wcnt[warp][L] += __popc(bal);
+            }
+        }
     }
     __syncthreads();
     if (threadIdx.x < kNumLists) {
@@ -974,20 +1180,21 @@ __global__ void __launch_bounds__(256) k_lists(Grid2 g, const uint8_t* __restric
     }
     if (threadIdx.x < 4 && mcnt[threadIdx.x]) atomicAdd(&st->mask_cnt[threadIdx.x], mcnt[threadIdx.x]);
     __syncthreads();
+    if (!warp_any) return;
     unsigned run[kNumLists];
 #pragma unroll
     for (int L = 0; L < kNumLists; ++L) run[L] = woff[warp][L];
     const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
     for (int r = 0; r < kListRows; ++r) {
+        if (!__any_sync(0xffffffffu, pm[r] != 0)) continue;
         const int j = j0 + r;
-        bool p[kNumLists];
-        unsigned mb;
-        preds(j, p, mb);
         const uint32_t idx = (uint32_t)((size_t)(j + kGhost) * g.pitch + (size_t)(i + kGhost));
 #pragma unroll
         for (int L = 0; L < kNumLists; ++L) {
-            const unsigned bal = __ballot_sync(0xffffffffu, p[L]);
-            if (p[L]) la.list[L][run[L] + __popc(bal & lt)] = idx;
+            const bool p = (pm[r] >> L) & 1u;
+            const unsigned bal = __ballot_sync(0xffffffffu, p);
+            if (p) la.list[L][run[L] + __popc(bal & lt)] = idx;
             run[L] += __popc(bal);
         }
     }
@@ -1486,6 +1693,7 @@ struct Solver2D {
 
     // ---------------------------------------------------------------- enqueue helpers
     long grid_points() const { return (long)g.nx * g.ny; }
+    long words() const { return (long)(plane / 4); }  // 32-bit words of a mask/level plane
 
     long band_count(int lev, int which) const
     {
@@ -1494,11 +1702,26 @@ struct Solver2D {
     }
     long details(int lev) const { return band_count(lev, 0) + band_count(lev, 1) + band_count(lev, 2); }
 
+    // Fine levels (point spacing <= kRowScanMaxH) scan mask words row by row and skip empty words;
+    // coarser levels enumerate their sub-band points.
+    bool row_scan(int lev) const { return (g.D(lev) >> 1) <= kRowScanMaxH; }
+    long rowscan_threads(int lev, int rows) const
+    {
+        const int h = g.D(lev) >> 1;
+        const long nr = (g.ny - 1) / h + 1, wpr = g.pitch / 4;
+        return (rows == 2 ? nr : (rows == 0 ? (nr + 1) / 2 : nr / 2)) * wpr;
+    }
+
     void enq_cr(int bit, const StepState* s)
     {
         for (int lev = g.maxl - 1; lev >= 0; --lev) {
-            k_cr<<<blocks_for(details(lev), 256), 256, 0, stream>>>(g, m, lev, bit, s);
-            after("k_cr");
+            if (row_scan(lev)) {
+                k_cr_rows<<<blocks_for(rowscan_threads(lev, 2), 256), 256, 0, stream>>>(g, m, lev, bit, s);
+                after("k_cr_rows");
+            } else {
+                k_cr<<<blocks_for(details(lev), 256), 256, 0, stream>>>(g, m, lev, bit, s);
+                after("k_cr");
+            }
             launches += 1;
         }
     }
@@ -1533,24 +1756,31 @@ struct Solver2D {
 
     void enq_interp(int from, int to, const StepState* s)
     {
-        k_interp_init<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, m, from, to, s);
+        k_interp_init<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, from, to, s);
         after("k_interp_init");
         launches += 1;
         enq_cr(kBitInterp, s);
         for (int lev = 0; lev < g.maxl; ++lev) {
-            k_interp<0><<<blocks_for(band_count(lev, 0) + band_count(lev, 1), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
-            after("k_interp<0>");
-            k_interp<1><<<blocks_for(band_count(lev, 2), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
-            after("k_interp<1>");
+            if (row_scan(lev)) {
+                k_interp_rows<0><<<blocks_for(rowscan_threads(lev, 2), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+                after("k_interp_rows<0>");
+                k_interp_rows<1><<<blocks_for(rowscan_threads(lev, 1), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+                after("k_interp_rows<1>");
+            } else {
+                k_interp<0><<<blocks_for(band_count(lev, 0) + band_count(lev, 1), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+                after("k_interp<0>");
+                k_interp<1><<<blocks_for(band_count(lev, 2), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+                after("k_interp<1>");
+            }
             launches += 2;
         }
     }
 
     void enq_aaz(int bit, const StepState* s)
     {
-        k_copy_bit_all<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, bit, kBitCopy, s);
+        k_copy_bit_all<<<blocks_for(words(), 256), 256, 0, stream>>>(m, plane, bit, kBitCopy, s);
         after("k_copy_bit_all");
-        k_aaz<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, m, bit, kBitCopy, s);
+        k_aaz<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, bit, kBitCopy, s);
         after("k_aaz");
         launches += 2;
     }
@@ -1588,21 +1818,20 @@ struct Solver2D {
             launches += 1;
             return;
         }
-        const long np = grid_points();
-        k_copy_bit_all<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, 0, kBitTemp, s);
+        k_copy_bit_all<<<blocks_for(words(), 256), 256, 0, stream>>>(m, plane, 0, kBitTemp, s);
         after("k_copy_bit_all");
         launches += 1;
         enq_fwt(s);
-        k_band_copy<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
+        k_band_copy<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
         after("k_band_copy");
-        k_aaz<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
+        k_aaz<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
         after("k_aaz");
         launches += 2;
         enq_cr(0, s);
         for (int k = 1; k <= 3; ++k) {
-            k_cl<<<blocks_for((long)plane, 256), 256, 0, stream>>>(g, m, lvl[k - 1], k - 1, k, plane, s);
+            k_cl<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, lvl[k - 1], k - 1, k, plane, s);
             after("k_cl");
-            k_apd<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, lvl[k - 1], k, k - 1, s);
+            k_apd<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, lvl[k - 1], k, k - 1, s);
             after("k_apd");
             launches += 2;
             enq_cr(k, s);
@@ -1623,8 +1852,8 @@ struct Solver2D {
     {
         cudaMemsetAsync(ax[stage], 0, sizeof(double) * g.ny, stream);
         cudaMemsetAsync(ay[stage], 0, sizeof(double) * g.nx, stream);
-        dim3 grid((g.nx + 31) / 32, (g.ny + 31) / 32), block(32, 8);
-        k_alpha<<<grid, block, 0, stream>>>(g, f, m, bit, ax[stage], ay[stage], with_cfl ? &st->mv : nullptr, st);
+        dim3 grid((unsigned)(g.pitch / 4 + 31) / 32, (unsigned)(g.ny + 8 * kAlphaRows - 1) / (8 * kAlphaRows));
+        k_alpha<<<grid, 256, 0, stream>>>(g, f, m, bit, ax[stage], ay[stage], with_cfl ? &st->mv : nullptr, st);
         after("k_alpha");
         launches += 1;
     }
@@ -1691,7 +1920,7 @@ struct Solver2D {
         enq_bc(q1, st);
         enq_alpha(q1, 1, 2, false);
         enq_faces_update(2, q1, q1);
-        k_remove_residue<<<blocks_for(grid_points(), 256), 256, 0, stream>>>(g, q, m, 0, 1, st);
+        k_remove_residue<<<blocks_for(words(), 256), 256, 0, stream>>>(g, q, m, 0, 1, st);
         after("k_remove_residue");
         k_finish<<<1, 1, 0, stream>>>(st);
         after("k_finish");
@@ -1910,18 +2139,17 @@ struct Solver2D {
     int manager(int op, int mask_id, int level_id)
     {
         const int b = bit_of(mask_id);
-        const long np = grid_points();
         if (level_id < 0 || level_id > 3) return kErrArg;
         switch (op) {
             case 0: enq_aaz(b, nullptr); break;
             case 1: enq_cr(b, nullptr); break;
             case 2:
-                k_copy_bit_all<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, b, kBitCopy, nullptr);
-                k_apd<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, lvl[level_id], b, kBitCopy, nullptr);
+                k_copy_bit_all<<<blocks_for(words(), 256), 256, 0, stream>>>(m, plane, b, kBitCopy, nullptr);
+                k_apd<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, lvl[level_id], b, kBitCopy, nullptr);
                 break;
-            case 3: k_cl<<<blocks_for((long)plane, 256), 256, 0, stream>>>(g, m, lvl[level_id], b, -1, plane, nullptr); break;
-            case 4: k_remove_residue<<<blocks_for(np, 256), 256, 0, stream>>>(g, q, m, b, 0, nullptr); break;
-            case 5: k_band_copy<<<blocks_for(np, 256), 256, 0, stream>>>(g, m, b, -1, nullptr); break;
+            case 3: k_cl<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, lvl[level_id], b, -1, plane, nullptr); break;
+            case 4: k_remove_residue<<<blocks_for(words(), 256), 256, 0, stream>>>(g, q, m, b, 0, nullptr); break;
+            case 5: k_band_copy<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, b, -1, nullptr); break;
             default: return kErrArg;
         }
         AWCM_CUDA_TRY(cudaGetLastError());

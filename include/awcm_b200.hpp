@@ -85,6 +85,25 @@ public:
         const int plane = mask_id == 4 ? 0 : mask_id + 1;
         return std::vector<uint8_t>(all.begin() + plane * n, all.begin() + (plane + 1) * n);
     }
+    // Frozen-mask run and discrete adjoint (no reference counterpart): n_steps steps at fixed dt
+    // on the masks of the last PrepareEuler; Adjoint returns the loss and fills grad (the
+    // SetField layout) with dLoss/dQ(t0).  SetWenoZ(1e-6, 1e-6) selects the differentiable mode.
+    void SetWenoZ(double eps, double tau_delta = 0) { check(awcm2d_set_wenoz(h_, eps, tau_delta), "awcm2d_set_wenoz"); }
+    double FrozenRun(double t0, double dt, int n_steps, bool replay = false)
+    {
+        double out[3];
+        check(awcm2d_frozen_run(h_, t0, dt, n_steps, replay ? 2 : 1, out), "awcm2d_frozen_run");
+        return out[0];
+    }
+    double Adjoint(double t0, double dt, int n_steps, const double* target, double* grad, int checkpoint_every = 0,
+                   bool replay = false)
+    {
+        double out[5];
+        check(awcm2d_adjoint(h_, t0, dt, n_steps, checkpoint_every, replay ? 2 : 1, target, grad, out),
+              "awcm2d_adjoint");
+        return out[0];
+    }
+
     std::vector<int> Level(int level_id) const
     {
         const size_t n = (size_t)nx_ * ny_;
