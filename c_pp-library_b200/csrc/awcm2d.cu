@@ -72,6 +72,18 @@ __host__ __device__ __forceinline__ Band band_of(const Grid2& g, int lev, int wh
 // the emulated 64-bit division).
 __device__ __forceinline__ unsigned gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 
+// Programmatic dependent launch: the kernels of a step are launched with programmatic stream
+// serialisation, so the next kernel's CTAs are scheduled once every CTA of the current one is
+// running and then wait in griddepcontrol.wait (a hardware wait on the predecessor grid's
+// completion and memory flush, not a software spin) before their first access.  This hides the
+// launch latency between the ~100 short dependent kernels of a step.  Launched without the
+// attribute, both instructions are no-ops.
+__device__ __forceinline__ void pdl_begin()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // Push of a mask bit at (i,j).  Under the reference's mask invariants every push lands on the
 // ghosted grid; pushes that would leave it (possible only for inconsistent user-set masks/levels,
 // where the reference itself writes out of bounds) are dropped.
@@ -697,74 +709,88 @@ __device__ void ph_remove_residue(const Grid2& g, Field4 q, const uint8_t* m, in
 
 __global__ void k_fwt_a(Grid2 g, double* q, double* tb, uint8_t* m, int lev, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_fwt_a(g, q, tb, m, lev, st->tol, grid_span());
 }
 __global__ void k_fwt_b(Grid2 g, double* q, const double* tb, const uint8_t* m, int lev, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_fwt_b(g, q, tb, m, lev, grid_span());
 }
 template <int PH>
 __global__ void k_iwt(Grid2 g, double* q, const uint8_t* m, int lev, int bit, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_iwt<PH>(g, q, m, lev, bit, grid_span());
 }
 __global__ void k_cr(Grid2 g, uint8_t* m, int lev, int bit, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_cr(g, m, lev, bit, grid_span());
 }
 __global__ void k_cr_rows(Grid2 g, uint8_t* m, int lev, int bit, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_cr_rows(g, m, lev, bit, grid_span());
 }
 template <int PH>
 __global__ void k_interp(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_interp<PH>(g, q, m, lev, from_bit, grid_span());
 }
 template <int PH>
 __global__ void k_interp_rows(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_interp_rows<PH>(g, q, m, lev, from_bit, grid_span());
 }
 __global__ void k_copy_bit_all(uint8_t* m, size_t n, int from, int to, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_copy_bit_all(m, n, from, to, grid_span());
 }
 __global__ void k_band_copy(Grid2 g, uint8_t* m, int bit, int copy_to, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_band_copy(g, m, bit, copy_to, grid_span());
 }
 __global__ void k_aaz(Grid2 g, uint8_t* m, int bit, int src, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_aaz(g, m, bit, src, grid_span());
 }
 __global__ void k_cl(Grid2 g, uint8_t* m, int8_t* lvl, int bit, int copy_to, size_t plane, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_cl(g, m, lvl, bit, copy_to, plane, grid_span());
 }
 __global__ void k_apd(Grid2 g, uint8_t* m, const int8_t* lvl, int bit, int src, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_apd(g, m, lvl, bit, src, grid_span());
 }
 __global__ void k_interp_init(Grid2 g, uint8_t* m, int from, int to, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_interp_init(g, m, from, to, grid_span());
 }
 __global__ void k_remove_residue(Grid2 g, Field4 q, const uint8_t* m, int bit, int sparse, const StepState* st)
 {
+    pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     const bool full = !sparse || (st && st->full_zero);
     ph_remove_residue(g, q, m, bit, full, grid_span());
@@ -898,11 +924,15 @@ __device__ __forceinline__ double euler_E(double g, double rho, double u, double
 // transmissive BOUNDARY_MANAGER_QUAD (Problems/2D/PROBLEM_QUADRANTS.h:123-203), double Mach
 // BOUNDARY_MANAGER_DMACH(t) (Problems/2D/PROBLEM_DOUBLEMACH.h:106-245) and periodic
 // BOUNDARY_MANAGER_ISENVORTEX (Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h:107-171).
-__global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host)
+__global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, double* zx, double* zy)
 {
+    pdl_begin();
     if (st && st->done) return;
     const double t = st ? st->t : t_host;
     const long tid = gtid();
+    // zero the LF-speed accumulators of the stage this fill feeds (the grid covers nx and ny)
+    if (zx && tid < g.ny) zx[tid] = 0.0;
+    if (zy && tid < g.nx) zy[tid] = 0.0;
     const int NX = g.nx - 1, NY = g.ny - 1;
     const long nside = (long)kGhost * g.ny, nbt = (long)kGhost * g.nx;
     int i, j, si, sj;  // ghost point and source point
@@ -982,6 +1012,7 @@ constexpr int kAlphaRows = 4;
 __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t* __restrict__ m, int bit,
                                                double* ax, double* ay, double* mv, const StepState* st)
 {
+    pdl_begin();
     if (st && st->done) return;
     __shared__ double col[8][128];
     __shared__ double cfl[8];
@@ -1036,6 +1067,7 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
 // per-level stage factor dt / (dx 2^(maxl-lev)) of the RK updates.
 __global__ void k_dt(Grid2 g, StepState* st)
 {
+    pdl_begin();
     if (st->done) return;
     double dt = st->cfl * g.dx / st->mv;
     if (st->dt_fixed > 0) dt = st->dt_fixed;
@@ -1053,6 +1085,7 @@ __global__ void k_dt(Grid2 g, StepState* st)
 
 __global__ void k_begin(StepState* st)
 {
+    pdl_begin();
     st->done = (st->t >= st->t_end || st->error) ? 1 : 0;
     if (st->done) return;
     st->bar[0] = 0;
@@ -1064,6 +1097,7 @@ __global__ void k_begin(StepState* st)
 
 __global__ void k_finish(StepState* st)
 {
+    pdl_begin();
     if (st->done) return;
     if (st->bar_err) {
         st->error = st->bar_err;
@@ -1125,6 +1159,7 @@ __global__ void __launch_bounds__(256) k_lists(Grid2 g, const uint8_t* __restric
                                                const int8_t* __restrict__ l1, const int8_t* __restrict__ l0,
                                                ListArgs la, StepState* st)
 {
+    pdl_begin();
     if (st->done) return;
     __shared__ unsigned wcnt[8][kNumLists];
     __shared__ unsigned woff[8][kNumLists];
@@ -1208,6 +1243,7 @@ __global__ void __launch_bounds__(128) k_face(Grid2 g, Field4 f, Field4 out, con
                                               const unsigned* __restrict__ count, const double* __restrict__ alpha,
                                               const StepState* st)
 {
+    pdl_begin();
     if (st->done) return;
     const unsigned n = *count;
     const long stride = (long)gridDim.x * blockDim.x;
@@ -1252,6 +1288,7 @@ __global__ void __launch_bounds__(256) k_update_fin(Grid2 g, Field4 in, Field4 o
                                                     const uint32_t* __restrict__ list,
                                                     const unsigned* __restrict__ count, const StepState* st)
 {
+    pdl_begin();
     if (st->done) return;
     const unsigned n = *count;
     const double sc = st->sc[g.maxl];
@@ -1277,6 +1314,7 @@ __global__ void __launch_bounds__(256) k_update_crs(Grid2 g, Field4 in, Field4 o
                                                     const uint32_t* __restrict__ list,
                                                     const unsigned* __restrict__ count, const StepState* st)
 {
+    pdl_begin();
     if (st->done) return;
     const unsigned n = *count;
     const long stride = (long)gridDim.x * blockDim.x;
@@ -1344,6 +1382,7 @@ __global__ void __launch_bounds__(256) k_update_crs(Grid2 g, Field4 in, Field4 o
 // ------------------------------------------------------------------------- layout conversions
 __global__ void k_aos_to_soa(Grid2 g, const double* __restrict__ aos, Field4 f)
 {
+    pdl_begin();
     const long t = gtid();
     const int w = g.nx + 2 * kGhost;
     if (t >= (long)w * (g.ny + 2 * kGhost)) return;
@@ -1354,6 +1393,7 @@ __global__ void k_aos_to_soa(Grid2 g, const double* __restrict__ aos, Field4 f)
 
 __global__ void k_soa_to_aos(Grid2 g, Field4 f, double* __restrict__ aos)
 {
+    pdl_begin();
     const long t = gtid();
     const int w = g.nx + 2 * kGhost;
     if (t >= (long)w * (g.ny + 2 * kGhost)) return;
@@ -1365,6 +1405,7 @@ __global__ void k_soa_to_aos(Grid2 g, Field4 f, double* __restrict__ aos)
 // masks: 5 planes (mask_temp, mask0..mask3) of (ny+6) x (nx+6) bytes <-> bit byte per point.
 __global__ void k_pack_masks(Grid2 g, const uint8_t* __restrict__ planes, uint8_t* m)
 {
+    pdl_begin();
     const long t = gtid();
     const int w = g.nx + 2 * kGhost;
     const long n = (long)w * (g.ny + 2 * kGhost);
@@ -1380,6 +1421,7 @@ __global__ void k_pack_masks(Grid2 g, const uint8_t* __restrict__ planes, uint8_
 
 __global__ void k_unpack_masks(Grid2 g, const uint8_t* m, uint8_t* __restrict__ planes)
 {
+    pdl_begin();
     const long t = gtid();
     const int w = g.nx + 2 * kGhost;
     const long n = (long)w * (g.ny + 2 * kGhost);
@@ -1392,6 +1434,7 @@ __global__ void k_unpack_masks(Grid2 g, const uint8_t* m, uint8_t* __restrict__ 
 
 __global__ void k_levels_in(Grid2 g, const int* __restrict__ lv, int8_t* l0, int8_t* l1, int8_t* l2, int8_t* l3)
 {
+    pdl_begin();
     const long t = gtid();
     const long n = (long)g.nx * g.ny;
     if (t >= n) return;
@@ -1405,6 +1448,7 @@ __global__ void k_levels_in(Grid2 g, const int* __restrict__ lv, int8_t* l0, int
 __global__ void k_levels_out(Grid2 g, const int8_t* l0, const int8_t* l1, const int8_t* l2, const int8_t* l3,
                              int* __restrict__ lv)
 {
+    pdl_begin();
     const long t = gtid();
     const long n = (long)g.nx * g.ny;
     if (t >= n) return;
@@ -1417,12 +1461,14 @@ __global__ void k_levels_out(Grid2 g, const int8_t* l0, const int8_t* l1, const 
 
 __global__ void k_fill_u8(uint8_t* p, size_t n, uint8_t v)
 {
+    pdl_begin();
     const size_t a = (size_t)gtid();
     if (a < n) p[a] = v;
 }
 
 __global__ void k_fill_i8(int8_t* p, size_t n, int8_t v)
 {
+    pdl_begin();
     const size_t a = (size_t)gtid();
     if (a < n) p[a] = v;
 }
@@ -1430,6 +1476,7 @@ __global__ void k_fill_i8(int8_t* p, size_t n, int8_t v)
 // EULER_EQUATION_2D batch entry points.
 __global__ void k_euler_flux(const double* q, double* f, int n, int dir, double gamma)
 {
+    pdl_begin();
     const long t = gtid();
     if (t >= n) return;
     double s[4] = {q[4 * t], q[4 * t + 1], q[4 * t + 2], q[4 * t + 3]}, o[4];
@@ -1440,6 +1487,7 @@ __global__ void k_euler_flux(const double* q, double* f, int n, int dir, double 
 
 __global__ void k_euler_sr(const double* q, double* out, int n, int dir, double gamma)
 {
+    pdl_begin();
     const long t = gtid();
     if (t >= n) return;
     const double s[4] = {q[4 * t], q[4 * t + 1], q[4 * t + 2], q[4 * t + 3]};
@@ -1486,6 +1534,25 @@ struct Solver2D {
         cudaEventCreate(&e);
         cudaEventRecord(e, stream);
         fine->emplace_back(name, e);
+    }
+
+    // Kernel launch on the instance's stream with programmatic stream serialisation (see
+    // pdl_begin); `pdl` false gives plain launches.
+    bool pdl = true;
+    template <typename... P, typename... A>
+    void launch(void (*kern)(P...), dim3 grid, dim3 block, A&&... args)
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = pdl ? 1 : 0;
+        cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
     }
 
     ~Solver2D() { release(); }
@@ -1570,8 +1637,8 @@ struct Solver2D {
         for (auto& l : lists) AWCM_CUDA_TRY(cudaMalloc(&l, cap * sizeof(uint32_t)));
         // AWCM_2D's constructor: every mask byte all ones on the ghosts, mask0 true inside, all
         // levels at the finest level (Wavelet/AWCM_2D.h:26-41).
-        k_fill_u8<<<blocks_for((long)plane, 256), 256, 0, stream>>>(m, plane, 0xff);
-        for (int k = 0; k < 4; ++k) k_fill_i8<<<blocks_for((long)plane, 256), 256, 0, stream>>>(lvl[k], plane, (int8_t)g.maxl);
+        launch(k_fill_u8, blocks_for((long)plane, 256), 256, m, plane, 0xff);
+        for (int k = 0; k < 4; ++k) launch(k_fill_i8, blocks_for((long)plane, 256), 256, lvl[k], plane, (int8_t)g.maxl);
         AWCM_CUDA_TRY(cudaGetLastError());
         {
             // AWCM_2D's constructor (Wavelet/AWCM_2D.h:26-37): mask0 true on every point, ghosts
@@ -1615,7 +1682,7 @@ struct Solver2D {
         int rc = ensure_staging(n * 4 * sizeof(double));
         if (rc) return rc;
         AWCM_CUDA_TRY(cudaMemcpyAsync(staging, host, n * 4 * sizeof(double), cudaMemcpyHostToDevice, stream));
-        k_aos_to_soa<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, (const double*)staging, q);
+        launch(k_aos_to_soa, blocks_for((long)n, 256), 256, g, (const double*)staging, q);
         AWCM_CUDA_TRY(cudaGetLastError());
         mark_full_zero();
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1627,7 +1694,7 @@ struct Solver2D {
         const size_t n = ghosted_points();
         int rc = ensure_staging(n * 4 * sizeof(double));
         if (rc) return rc;
-        k_soa_to_aos<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, q, (double*)staging);
+        launch(k_soa_to_aos, blocks_for((long)n, 256), 256, g, q, (double*)staging);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaMemcpyAsync(host, staging, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, stream));
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1640,7 +1707,7 @@ struct Solver2D {
         int rc = ensure_staging(5 * n);
         if (rc) return rc;
         AWCM_CUDA_TRY(cudaMemcpyAsync(staging, host, 5 * n, cudaMemcpyHostToDevice, stream));
-        k_pack_masks<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, (const uint8_t*)staging, m);
+        launch(k_pack_masks, blocks_for((long)n, 256), 256, g, (const uint8_t*)staging, m);
         AWCM_CUDA_TRY(cudaGetLastError());
         mark_full_zero();
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1652,7 +1719,7 @@ struct Solver2D {
         const size_t n = ghosted_points();
         int rc = ensure_staging(5 * n);
         if (rc) return rc;
-        k_unpack_masks<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, m, (uint8_t*)staging);
+        launch(k_unpack_masks, blocks_for((long)n, 256), 256, g, m, (uint8_t*)staging);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaMemcpyAsync(host, staging, 5 * n, cudaMemcpyDeviceToHost, stream));
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1665,7 +1732,7 @@ struct Solver2D {
         int rc = ensure_staging(4 * n * sizeof(int));
         if (rc) return rc;
         AWCM_CUDA_TRY(cudaMemcpyAsync(staging, host, 4 * n * sizeof(int), cudaMemcpyHostToDevice, stream));
-        k_levels_in<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, (const int*)staging, lvl[0], lvl[1], lvl[2], lvl[3]);
+        launch(k_levels_in, blocks_for((long)n, 256), 256, g, (const int*)staging, lvl[0], lvl[1], lvl[2], lvl[3]);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
@@ -1676,7 +1743,7 @@ struct Solver2D {
         const size_t n = (size_t)g.nx * g.ny;
         int rc = ensure_staging(4 * n * sizeof(int));
         if (rc) return rc;
-        k_levels_out<<<blocks_for((long)n, 256), 256, 0, stream>>>(g, lvl[0], lvl[1], lvl[2], lvl[3], (int*)staging);
+        launch(k_levels_out, blocks_for((long)n, 256), 256, g, lvl[0], lvl[1], lvl[2], lvl[3], (int*)staging);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaMemcpyAsync(host, staging, 4 * n * sizeof(int), cudaMemcpyDeviceToHost, stream));
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1716,10 +1783,10 @@ struct Solver2D {
     {
         for (int lev = g.maxl - 1; lev >= 0; --lev) {
             if (row_scan(lev)) {
-                k_cr_rows<<<blocks_for(rowscan_threads(lev, 2), 256), 256, 0, stream>>>(g, m, lev, bit, s);
+                launch(k_cr_rows, blocks_for(rowscan_threads(lev, 2), 256), 256, g, m, lev, bit, s);
                 after("k_cr_rows");
             } else {
-                k_cr<<<blocks_for(details(lev), 256), 256, 0, stream>>>(g, m, lev, bit, s);
+                launch(k_cr, blocks_for(details(lev), 256), 256, g, m, lev, bit, s);
                 after("k_cr");
             }
             launches += 1;
@@ -1731,10 +1798,10 @@ struct Solver2D {
     void enq_fwt(const StepState* s)
     {
         for (int lev = g.maxl - 1; lev >= 0; --lev) {
-            k_fwt_a<<<blocks_for(details(lev), 256), 256, 0, stream>>>(g, q.p[0], fx.p[0], m, lev, s);
+            launch(k_fwt_a, blocks_for(details(lev), 256), 256, g, q.p[0], fx.p[0], m, lev, s);
             after("k_fwt_a");
             const long nb = band_count(lev, 3) + band_count(lev, 0) + band_count(lev, 1);
-            k_fwt_b<<<blocks_for(nb, 256), 256, 0, stream>>>(g, q.p[0], fx.p[0], m, lev, s);
+            launch(k_fwt_b, blocks_for(nb, 256), 256, g, q.p[0], fx.p[0], m, lev, s);
             after("k_fwt_b");
             launches += 2;
         }
@@ -1744,11 +1811,11 @@ struct Solver2D {
     {
         for (int lev = 0; lev < g.maxl; ++lev) {
             const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1), bc = band_of(g, lev, 3);
-            k_iwt<0><<<blocks_for((long)bc.cx * bc.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            launch(k_iwt<0>, blocks_for((long)bc.cx * bc.cy, 256), 256, g, q.p[0], m, lev, bit, s);
             after("k_iwt<0>");
-            k_iwt<1><<<blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            launch(k_iwt<1>, blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, g, q.p[0], m, lev, bit, s);
             after("k_iwt<1>");
-            k_iwt<2><<<blocks_for((long)b3.cx * b3.cy, 256), 256, 0, stream>>>(g, q.p[0], m, lev, bit, s);
+            launch(k_iwt<2>, blocks_for((long)b3.cx * b3.cy, 256), 256, g, q.p[0], m, lev, bit, s);
             after("k_iwt<2>");
             launches += 3;
         }
@@ -1756,20 +1823,20 @@ struct Solver2D {
 
     void enq_interp(int from, int to, const StepState* s)
     {
-        k_interp_init<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, from, to, s);
+        launch(k_interp_init, blocks_for(words(), 256), 256, g, m, from, to, s);
         after("k_interp_init");
         launches += 1;
         enq_cr(kBitInterp, s);
         for (int lev = 0; lev < g.maxl; ++lev) {
             if (row_scan(lev)) {
-                k_interp_rows<0><<<blocks_for(rowscan_threads(lev, 2), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+                launch(k_interp_rows<0>, blocks_for(rowscan_threads(lev, 2), 256), 256, g, q, m, lev, from, s);
                 after("k_interp_rows<0>");
-                k_interp_rows<1><<<blocks_for(rowscan_threads(lev, 1), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+                launch(k_interp_rows<1>, blocks_for(rowscan_threads(lev, 1), 256), 256, g, q, m, lev, from, s);
                 after("k_interp_rows<1>");
             } else {
-                k_interp<0><<<blocks_for(band_count(lev, 0) + band_count(lev, 1), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+                launch(k_interp<0>, blocks_for(band_count(lev, 0) + band_count(lev, 1), 256), 256, g, q, m, lev, from, s);
                 after("k_interp<0>");
-                k_interp<1><<<blocks_for(band_count(lev, 2), 256), 256, 0, stream>>>(g, q, m, lev, from, s);
+                launch(k_interp<1>, blocks_for(band_count(lev, 2), 256), 256, g, q, m, lev, from, s);
                 after("k_interp<1>");
             }
             launches += 2;
@@ -1778,9 +1845,9 @@ struct Solver2D {
 
     void enq_aaz(int bit, const StepState* s)
     {
-        k_copy_bit_all<<<blocks_for(words(), 256), 256, 0, stream>>>(m, plane, bit, kBitCopy, s);
+        launch(k_copy_bit_all, blocks_for(words(), 256), 256, m, plane, bit, kBitCopy, s);
         after("k_copy_bit_all");
-        k_aaz<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, bit, kBitCopy, s);
+        launch(k_aaz, blocks_for(words(), 256), 256, g, m, bit, kBitCopy, s);
         after("k_aaz");
         launches += 2;
     }
@@ -1818,20 +1885,20 @@ struct Solver2D {
             launches += 1;
             return;
         }
-        k_copy_bit_all<<<blocks_for(words(), 256), 256, 0, stream>>>(m, plane, 0, kBitTemp, s);
+        launch(k_copy_bit_all, blocks_for(words(), 256), 256, m, plane, 0, kBitTemp, s);
         after("k_copy_bit_all");
         launches += 1;
         enq_fwt(s);
-        k_band_copy<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
+        launch(k_band_copy, blocks_for(words(), 256), 256, g, m, 0, kBitCopy, s);
         after("k_band_copy");
-        k_aaz<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, 0, kBitCopy, s);
+        launch(k_aaz, blocks_for(words(), 256), 256, g, m, 0, kBitCopy, s);
         after("k_aaz");
         launches += 2;
         enq_cr(0, s);
         for (int k = 1; k <= 3; ++k) {
-            k_cl<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, lvl[k - 1], k - 1, k, plane, s);
+            launch(k_cl, blocks_for(words(), 256), 256, g, m, lvl[k - 1], k - 1, k, plane, s);
             after("k_cl");
-            k_apd<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, lvl[k - 1], k, k - 1, s);
+            launch(k_apd, blocks_for(words(), 256), 256, g, m, lvl[k - 1], k, k - 1, s);
             after("k_apd");
             launches += 2;
             enq_cr(k, s);
@@ -1840,20 +1907,23 @@ struct Solver2D {
         enq_interp(kBitTemp, 3, s);
     }
 
-    void enq_bc(Field4 f, const StepState* s)
+    // Boundary fill of a stage input; with zero_stage >= 0 it also zeroes that stage's LF-speed
+    // accumulators for the k_alpha that follows.
+    void enq_bc(Field4 f, const StepState* s, int zero_stage = -1)
     {
         const long n = 2L * kGhost * g.ny + 2L * kGhost * g.nx;
-        k_bc<<<blocks_for(n, 256), 256, 0, stream>>>(g, f, s, 0.0);
+        double* zx = zero_stage >= 0 ? ax[zero_stage] : nullptr;
+        double* zy = zero_stage >= 0 ? ay[zero_stage] : nullptr;
+        launch(k_bc, blocks_for(n, 256), 256, g, f, s, 0.0, zx, zy);
         after("k_bc");
         launches += 1;
     }
 
     void enq_alpha(Field4 f, int bit, int stage, bool with_cfl)
     {
-        cudaMemsetAsync(ax[stage], 0, sizeof(double) * g.ny, stream);
-        cudaMemsetAsync(ay[stage], 0, sizeof(double) * g.nx, stream);
+        // ax[stage] / ay[stage] were zeroed by the boundary fill before this launch
         dim3 grid((unsigned)(g.pitch / 4 + 31) / 32, (unsigned)(g.ny + 8 * kAlphaRows - 1) / (8 * kAlphaRows));
-        k_alpha<<<grid, 256, 0, stream>>>(g, f, m, bit, ax[stage], ay[stage], with_cfl ? &st->mv : nullptr, st);
+        launch(k_alpha, grid, 256, g, f, m, bit, ax[stage], ay[stage], with_cfl ? &st->mv : nullptr, st);
         after("k_alpha");
         launches += 1;
     }
@@ -1863,27 +1933,27 @@ struct Solver2D {
         uint32_t* const* L = lists + 4 * stage;
         const unsigned* C = st->cnt + 4 * stage;
         mark();
-        k_face<0><<<face_blocks, 128, 0, stream>>>(g, in, fx, L[2], C + 2, ax[stage], st);
+        launch(k_face<0>, face_blocks, 128, g, in, fx, L[2], C + 2, ax[stage], st);
         after("k_face<0>");
-        k_face<1><<<face_blocks, 128, 0, stream>>>(g, in, fy, L[3], C + 3, ay[stage], st);
+        launch(k_face<1>, face_blocks, 128, g, in, fy, L[3], C + 3, ay[stage], st);
         after("k_face<1>");
         launches += 2;
         mark();
         const int ub = face_blocks / 2;
         if (stage == 0) {
-            k_update_fin<1><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            launch(k_update_fin<1>, ub, 256, g, in, out, q, fx, fy, L[0], C + 0, st);
             after("k_update_fin<1>");
-            k_update_crs<1><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[2], L[1], C + 1, st);
+            launch(k_update_crs<1>, ub, 256, g, in, out, q, lvl[2], L[1], C + 1, st);
             after("k_update_crs<1>");
         } else if (stage == 1) {
-            k_update_fin<2><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            launch(k_update_fin<2>, ub, 256, g, in, out, q, fx, fy, L[0], C + 0, st);
             after("k_update_fin<2>");
-            k_update_crs<2><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[1], L[1], C + 1, st);
+            launch(k_update_crs<2>, ub, 256, g, in, out, q, lvl[1], L[1], C + 1, st);
             after("k_update_crs<2>");
         } else {
-            k_update_fin<3><<<ub, 256, 0, stream>>>(g, in, out, q, fx, fy, L[0], C + 0, st);
+            launch(k_update_fin<3>, ub, 256, g, in, out, q, fx, fy, L[0], C + 0, st);
             after("k_update_fin<3>");
-            k_update_crs<3><<<ub, 256, 0, stream>>>(g, in, out, q, lvl[0], L[1], C + 1, st);
+            launch(k_update_crs<3>, ub, 256, g, in, out, q, lvl[0], L[1], C + 1, st);
             after("k_update_crs<3>");
         }
         launches += 2;
@@ -1895,34 +1965,34 @@ struct Solver2D {
     {
         launches = 0;
         mark();
-        k_begin<<<1, 1, 0, stream>>>(st);
+        launch(k_begin, 1, 1, st);
         after("k_begin");
         launches += 1;
         enq_prepare(st);
         mark();
-        enq_bc(q, st);
+        enq_bc(q, st, 0);
         enq_alpha(q, 3, 0, true);
-        k_dt<<<1, 1, 0, stream>>>(g, st);
+        launch(k_dt, 1, 1, g, st);
         after("k_dt");
         launches += 1;
         {
             ListArgs la;
             for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
             dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
-            k_lists<<<grid, 256, 0, stream>>>(g, m, lvl[2], lvl[1], lvl[0], la, st);
+            launch(k_lists, grid, 256, g, m, lvl[2], lvl[1], lvl[0], la, st);
             after("k_lists");
             launches += 1;
         }
         enq_faces_update(0, q, q2);
-        enq_bc(q2, st);
+        enq_bc(q2, st, 1);
         enq_alpha(q2, 2, 1, false);
         enq_faces_update(1, q2, q1);
-        enq_bc(q1, st);
+        enq_bc(q1, st, 2);
         enq_alpha(q1, 1, 2, false);
         enq_faces_update(2, q1, q1);
-        k_remove_residue<<<blocks_for(words(), 256), 256, 0, stream>>>(g, q, m, 0, 1, st);
+        launch(k_remove_residue, blocks_for(words(), 256), 256, g, q, m, 0, 1, st);
         after("k_remove_residue");
-        k_finish<<<1, 1, 0, stream>>>(st);
+        launch(k_finish, 1, 1, st);
         after("k_finish");
         launches += 2;
         mark();
@@ -2100,7 +2170,7 @@ struct Solver2D {
     {
         int rc = write_params(tol, 0, 0, 1, 0);
         if (rc) return rc;
-        k_begin<<<1, 1, 0, stream>>>(st);
+        launch(k_begin, 1, 1, st);
         enq_prepare(st);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -2111,7 +2181,7 @@ struct Solver2D {
     {
         int rc = write_params(tol, 0, 0, 1, 0);
         if (rc) return rc;
-        k_begin<<<1, 1, 0, stream>>>(st);
+        launch(k_begin, 1, 1, st);
         enq_fwt(st);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -2144,12 +2214,12 @@ struct Solver2D {
             case 0: enq_aaz(b, nullptr); break;
             case 1: enq_cr(b, nullptr); break;
             case 2:
-                k_copy_bit_all<<<blocks_for(words(), 256), 256, 0, stream>>>(m, plane, b, kBitCopy, nullptr);
-                k_apd<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, lvl[level_id], b, kBitCopy, nullptr);
+                launch(k_copy_bit_all, blocks_for(words(), 256), 256, m, plane, b, kBitCopy, nullptr);
+                launch(k_apd, blocks_for(words(), 256), 256, g, m, lvl[level_id], b, kBitCopy, nullptr);
                 break;
-            case 3: k_cl<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, lvl[level_id], b, -1, plane, nullptr); break;
-            case 4: k_remove_residue<<<blocks_for(words(), 256), 256, 0, stream>>>(g, q, m, b, 0, nullptr); break;
-            case 5: k_band_copy<<<blocks_for(words(), 256), 256, 0, stream>>>(g, m, b, -1, nullptr); break;
+            case 3: launch(k_cl, blocks_for(words(), 256), 256, g, m, lvl[level_id], b, -1, plane, nullptr); break;
+            case 4: launch(k_remove_residue, blocks_for(words(), 256), 256, g, q, m, b, 0, nullptr); break;
+            case 5: launch(k_band_copy, blocks_for(words(), 256), 256, g, m, b, -1, nullptr); break;
             default: return kErrArg;
         }
         AWCM_CUDA_TRY(cudaGetLastError());
@@ -2160,7 +2230,7 @@ struct Solver2D {
     int apply_bc(double t)
     {
         const long n = 2L * kGhost * g.ny + 2L * kGhost * g.nx;
-        k_bc<<<blocks_for(n, 256), 256, 0, stream>>>(g, q, nullptr, t);
+        launch(k_bc, blocks_for(n, 256), 256, g, q, nullptr, t, nullptr, nullptr);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
@@ -2197,27 +2267,27 @@ struct Solver2D {
 
     void enq_frozen_step(const double* tin, double* tout, const Field4* save)
     {
-        k_begin<<<1, 1, 0, stream>>>(st);
-        enq_bc(q, st);
+        launch(k_begin, 1, 1, st);
+        enq_bc(q, st, 0);
         if (save) copy_field(save[0], q);
         enq_alpha_frozen(q, 3, 0, tin, tout);
-        k_dt<<<1, 1, 0, stream>>>(g, st);
+        launch(k_dt, 1, 1, g, st);
         {
             ListArgs la;
             for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
             dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
-            k_lists<<<grid, 256, 0, stream>>>(g, m, lvl[2], lvl[1], lvl[0], la, st);
+            launch(k_lists, grid, 256, g, m, lvl[2], lvl[1], lvl[0], la, st);
         }
         enq_faces_update(0, q, q2);
-        enq_bc(q2, st);
+        enq_bc(q2, st, 1);
         if (save) copy_field(save[1], q2);
         enq_alpha_frozen(q2, 2, 1, tin, tout);
         enq_faces_update(1, q2, q1);
-        enq_bc(q1, st);
+        enq_bc(q1, st, 2);
         if (save) copy_field(save[2], q1);
         enq_alpha_frozen(q1, 1, 2, tin, tout);
         enq_faces_update(2, q1, q1);
-        k_finish<<<1, 1, 0, stream>>>(st);
+        launch(k_finish, 1, 1, st);
     }
 
     // Device buffers of the frozen run and the adjoint, grown on demand and kept.
@@ -2433,7 +2503,7 @@ struct Solver2D {
         if (grad_host) {
             const size_t np = ghosted_points();
             if ((rc = ensure_staging(np * 4 * sizeof(double)))) return rc;
-            k_soa_to_aos<<<blocks_for((long)np, 256), 256, 0, stream>>>(g, lam, (double*)staging);
+            launch(k_soa_to_aos, blocks_for((long)np, 256), 256, g, lam, (double*)staging);
             AWCM_CUDA_TRY(cudaGetLastError());
             AWCM_CUDA_TRY(cudaMemcpyAsync(grad_host, staging, np * 4 * sizeof(double), cudaMemcpyDeviceToHost, stream));
         }
