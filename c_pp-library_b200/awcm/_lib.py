@@ -49,6 +49,9 @@ _SIGS = {
     "awcm2d_frozen_run": [c_void_p, c_double, c_double, c_int, c_int, P_double],
     "awcm2d_adjoint": [c_void_p, c_double, c_double, c_int, c_int, c_int, P_double, P_double, P_double],
     "awcm2d_set_wenoz": [c_void_p, c_double, c_double],
+    "awcm2d_get_geometry": [c_void_p, c_void_p],
+    "awcm2d_save_state": [c_void_p, ctypes.c_char_p, c_double, ctypes.c_longlong],
+    "awcm2d_load_state": [c_void_p, ctypes.c_char_p, P_double, ctypes.POINTER(ctypes.c_longlong)],
     "awcm2d_get_alpha_tape": [c_void_p, c_int, P_double],
     "awcm2d_set_alpha_tape": [c_void_p, c_int, P_double],
     "awcm1d_batch_create": [c_int, P_int, P_int, P_double, P_double, c_double, c_int, ctypes.POINTER(c_void_p)],

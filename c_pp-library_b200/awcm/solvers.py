@@ -162,6 +162,28 @@ class AWCM2D:
         call("awcm2d_stream", self.h, ctypes.byref(s))
         return s.value or 0
 
+    # state file -------------------------------------------------------------------------------
+    def geometry(self):
+        """(num_levels, nx_coarse, ny_coarse, bc_kind, x_min, x_max, y_min, y_max, gamma)."""
+        class _G(ctypes.Structure):
+            _fields_ = [("num_levels", ctypes.c_int), ("nx_coarse", ctypes.c_int), ("ny_coarse", ctypes.c_int),
+                        ("bc_kind", ctypes.c_int), ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+                        ("y_min", ctypes.c_double), ("y_max", ctypes.c_double), ("gamma", ctypes.c_double)]
+        gm = _G()
+        call("awcm2d_get_geometry", self.h, ctypes.byref(gm))
+        return (gm.num_levels, gm.nx_coarse, gm.ny_coarse, gm.bc_kind, gm.x_min, gm.x_max, gm.y_min, gm.y_max,
+                gm.gamma)
+
+    def save_state(self, path, t=0.0, step=0):
+        """Binary state file: masks, levels and the state on mask0 (awcm2d_save_state)."""
+        call("awcm2d_save_state", self.h, str(path).encode(), float(t), int(step))
+
+    def load_state(self, path):
+        """Restores state, masks and levels from a state file; returns (t, step)."""
+        t, step = ctypes.c_double(), ctypes.c_longlong()
+        call("awcm2d_load_state", self.h, str(path).encode(), ctypes.byref(t), ctypes.byref(step))
+        return t.value, step.value
+
     # frozen-mask run and adjoint --------------------------------------------------------------
     @property
     def tape_stride(self) -> int:

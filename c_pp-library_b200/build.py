@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libawcm_b200.so")
-SOURCES = ["awcm_common.cu", "awcm2d.cu", "awcm1d.cu", "awcm2d_adjoint.cu"]
+SOURCES = ["awcm_common.cu", "awcm2d.cu", "awcm1d.cu", "awcm2d_adjoint.cu", "awcm_state.cpp"]
 HEADERS = ["awcm_common.cuh", "awcm_numerics.cuh", "awcm2d_types.cuh"]
 # per-file overrides of the contraction flags
 FMA_SOURCES = {"awcm2d_adjoint.cu"}
@@ -51,7 +51,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(objdir, exist_ok=True)
     objs = []
     for src in SOURCES:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         flags = NVCC_FLAGS
         if src in FMA_SOURCES:
             flags = [f.replace("--fmad=false", "--fmad=true").replace("-ffp-contract=off", "-ffp-contract=fast")

@@ -1588,10 +1588,13 @@ struct Solver2D {
         stream = nullptr;
     }
 
+    awcm2d_geometry geo{};
+
     int create(int num_levels, int nxc, int nyc, double x_min, double x_max, double y_min, double y_max, int bc)
     {
         if (num_levels < 2 || num_levels > kMaxLevels - 1 || nxc < 5 || nyc < 5) return kErrArg;
         if (bc < 0 || bc > 2) return kErrArg;
+        geo = awcm2d_geometry{num_levels, nxc, nyc, bc, x_min, x_max, y_min, y_max, 1.4};
         const long nx = (long)(nxc - 1) * (1L << (num_levels - 1)) + 1;
         const long ny = (long)(nyc - 1) * (1L << (num_levels - 1)) + 1;
         const long pitch = ((nx + 2 * kGhost + 31) / 32) * 32;
@@ -2609,6 +2612,12 @@ int awcm2d_dims(awcm2d_t h, int* nx, int* ny)
     return awcm::kOk;
 }
 
+int awcm2d_get_geometry(awcm2d_t h, awcm2d_geometry* out)
+{
+    if (!h || !out) return awcm::kErrArg;
+    *out = h->s.geo;
+    return awcm::kOk;
+}
 int awcm2d_set_q(awcm2d_t h, const double* q)
 {
     AWCM_H(h);

@@ -77,6 +77,12 @@ int awcm2d_create(int num_levels, int nx_coarse, int ny_coarse, double x_min, do
                   double y_max, int bc_kind, awcm2d_t* out);
 int awcm2d_destroy(awcm2d_t h);
 int awcm2d_dims(awcm2d_t h, int* nx, int* ny);
+/* The creation arguments of the instance (and its gas constant). */
+typedef struct awcm2d_geometry {
+    int num_levels, nx_coarse, ny_coarse, bc_kind;
+    double x_min, x_max, y_min, y_max, gamma;
+} awcm2d_geometry;
+int awcm2d_get_geometry(awcm2d_t h, awcm2d_geometry* out);
 /* Conserved state in the reference layout (host memory), ghosts included. */
 int awcm2d_set_q(awcm2d_t h, const double* q);
 int awcm2d_get_q(awcm2d_t h, double* q);
@@ -125,6 +131,16 @@ int awcm2d_launches_per_step(awcm2d_t h, int* n);
 int awcm2d_set_prepare_mode(awcm2d_t h, int mode);
 /* CUDA stream the instance runs on (cudaStream_t), for event timing by the caller. */
 int awcm2d_stream(awcm2d_t h, void** stream);
+
+/* Binary state file (no counterpart in the reference, whose only output is the write-only text
+ * dump of AWCM_MANAGER_2D::Print, Wavelet/AWCM_MANAGER_2D.h:243-255): a 128-byte header (magic
+ * "AWCMST2D", version 1, the geometry, t, step, |mask0|, payload size, CRC-32 of the payload),
+ * then the five mask planes bit-packed, the four level planes as bytes and the conserved state
+ * of the mask0 points (between steps every other point holds zero).  Loading checks magic,
+ * version, geometry, sizes and CRC (AWCM_ERR_STATE otherwise) and replaces state, masks and
+ * levels; t and step are returned as stored.  The CPU checker reads and writes the same format. */
+int awcm2d_save_state(awcm2d_t h, const char* path, double t, long long step);
+int awcm2d_load_state(awcm2d_t h, const char* path, double* t, long long* step);
 
 /* ---------------------------------------------------------------- 2D frozen-mask run and adjoint
  * No counterpart in the reference (it has no derivative code).  The frozen-mask step is the

@@ -85,6 +85,16 @@ public:
         const int plane = mask_id == 4 ? 0 : mask_id + 1;
         return std::vector<uint8_t>(all.begin() + plane * n, all.begin() + (plane + 1) * n);
     }
+    // Binary state file (awcm2d_save_state / awcm2d_load_state): resume a run bit for bit.
+    void SaveState(const char* path, double t, long long step) const
+    {
+        check(awcm2d_save_state(h_, path, t, step), "awcm2d_save_state");
+    }
+    void LoadState(const char* path, double* t = nullptr, long long* step = nullptr)
+    {
+        check(awcm2d_load_state(h_, path, t, step), "awcm2d_load_state");
+    }
+
     // Frozen-mask run and discrete adjoint (no reference counterpart): n_steps steps at fixed dt
     // on the masks of the last PrepareEuler; Adjoint returns the loss and fills grad (the
     // SetField layout) with dLoss/dQ(t0).  SetWenoZ(1e-6, 1e-6) selects the differentiable mode.

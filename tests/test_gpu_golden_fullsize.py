@@ -72,8 +72,12 @@ def test_fullsize_first_steps_bit_exact(case, awcm_lib):
     gpu = awcm_lib.AWCM2D(nl, nxc, nyc, *dom, bc)
     ref.init_problem(prob, a, b)
     gpu.init_problem(prob, a, b)
+    from near_threshold import near_threshold
+
     t = 0.0
     for k in range(2):
+        n_k, e_k = near_threshold((nl, nxc, nyc, *dom, bc), ref.get_q(), ref.get_masks(), tol)
+        print(f"{case} step {k}: {n_k} of {e_k} active details within 1e-12 relative of the threshold")
         o_r = ref.step(tol, cfl, t, 10.0)
         o_g = gpu.step(tol, cfl, t, 10.0)
         assert o_g[0] == o_r[0] and np.array_equal(o_g[2:6], o_r[2:6]), (k, o_g, o_r)

@@ -128,3 +128,24 @@ def test_frozen_gradient_workload_builder():
     o.prepare(tol)
     assert np.array_equal(o.get_q(), g["q"])
     assert np.array_equal(o.get_masks(), g["masks"])
+
+
+def test_near_threshold_report():
+    """The near-threshold counter finds a detail placed exactly on the threshold and none on a
+    state whose details are far from it."""
+    from near_threshold import detail_ratios, near_threshold
+
+    g = load("quad65")
+    nl, nxc, nyc, x0, x1, y0, y1, bc = g["params"][:8]
+    geom = (int(nl), int(nxc), int(nyc), x0, x1, y0, y1, int(bc))
+    o = Oracle2D(*geom[:7], bc_kind=geom[7], kind="port")
+    o.set_q(g["q0"])
+    masks = o.get_masks()
+    r = detail_ratios(geom, g["q0"], masks, 1.0)
+    nz = r[r > 0]
+    assert nz.size > 0
+    tol = float(nz[0])  # a threshold equal to one detail's magnitude
+    n, examined = near_threshold(geom, g["q0"], masks, tol)
+    assert n >= 1 and examined == r.size
+    n2, _ = near_threshold(geom, g["q0"], masks, tol * 1.5)
+    assert n2 <= n
