@@ -36,6 +36,7 @@ _SIGS = {
     "awcm2d_fwt": [c_void_p, c_double],
     "awcm2d_iwt": [c_void_p, c_int],
     "awcm2d_interpolate": [c_void_p, c_int, c_int],
+    "awcm2d_interpolate_all": [c_void_p, c_int],
     "awcm2d_manager": [c_void_p, c_int, c_int, c_int],
     "awcm2d_apply_bc": [c_void_p, c_double],
     "awcm2d_step": [c_void_p, c_double, c_double, c_double, c_double, c_double, P_double],

@@ -96,6 +96,11 @@ class AWCM2D:
     def iwt(self, mask_id=3):
         call("awcm2d_iwt", self.h, mask_id)
 
+    def interpolate_all(self, from_id=0):
+        """InterpolateAllGridEuler: interpolate all four components at every grid point outside
+        mask `from_id` (the dense field)."""
+        call("awcm2d_interpolate_all", self.h, from_id)
+
     def interpolate(self, from_id=4, to_id=3):
         call("awcm2d_interpolate", self.h, from_id, to_id)
 

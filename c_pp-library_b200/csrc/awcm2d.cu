@@ -408,13 +408,13 @@ __device__ void ph_cr_rows(const Grid2& g, uint8_t* __restrict__ m, int lev, int
 
 // InterpolateEuler, one phase of one level (WAVELET_2D.h:784-907): PH 0 = d1 and d2, PH 1 = d3;
 // components 1..3 at points of the work mask that were not active before (`from_bit`).
-__device__ __forceinline__ void interp_point(const Grid2& g, Field4 q, int i, int j, size_t a, int D, int w)
+__device__ __forceinline__ void interp_point(const Grid2& g, Field4 q, int i, int j, size_t a, int D, int w, int p0)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
     if (w == 0) {
         int s0, k;
         predict_stencil(i, D, NX, s0, k);
-        for (int p = 1; p < 4; ++p) {
+        for (int p = p0; p < 4; ++p) {
             const double* qp = q.p[p];
             double v = 0.0;
             for (int c = 0; c < 4; ++c) v += qp[g.at(s0 + c * D, j)] * g.w(c, k);
@@ -423,7 +423,7 @@ __device__ __forceinline__ void interp_point(const Grid2& g, Field4 q, int i, in
     } else if (w == 1) {
         int s0, k;
         predict_stencil(j, D, NY, s0, k);
-        for (int p = 1; p < 4; ++p) {
+        for (int p = p0; p < 4; ++p) {
             const double* qp = q.p[p];
             double v = 0.0;
             for (int c = 0; c < 4; ++c) v += qp[g.at(i, s0 + c * D)] * g.w(c, k);
@@ -433,7 +433,7 @@ __device__ __forceinline__ void interp_point(const Grid2& g, Field4 q, int i, in
         int is, k1, js, k2;
         predict_stencil(i, D, NX, is, k1);
         predict_stencil(j, D, NY, js, k2);
-        for (int p = 1; p < 4; ++p) {
+        for (int p = p0; p < 4; ++p) {
             const double* qp = q.p[p];
             double v = 0.0;
             for (int c = 0; c < 4; ++c) v += qp[g.at(is + c * D, j)] * g.w(c, k1);
@@ -446,7 +446,8 @@ __device__ __forceinline__ void interp_point(const Grid2& g, Field4 q, int i, in
 }
 
 template <int PH>
-__device__ void ph_interp(const Grid2& g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit, Span sp)
+__device__ void ph_interp(const Grid2& g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit, int p0,
+                          Span sp)
 {
     const int D = g.D(lev);
     const unsigned n = PH == 0 ? band_n(g, lev, 0) + band_n(g, lev, 1) : band_n(g, lev, 2);
@@ -462,14 +463,15 @@ __device__ void ph_interp(const Grid2& g, Field4 q, const uint8_t* __restrict__ 
         const size_t a = g.at(i, j);
         const unsigned mb = m[a];
         if (!((mb >> kBitInterp) & 1u) || ((mb >> from_bit) & 1u)) continue;
-        interp_point(g, q, i, j, a, D, w);
+        interp_point(g, q, i, j, a, D, w, p0);
     }
 }
 
 // Row-scan form of ph_interp for the fine levels: PH 0 scans every row of the level (d1 on the
 // even ones, d2 on the odd ones), PH 1 only the odd rows (d3).
 template <int PH>
-__device__ void ph_interp_rows(const Grid2& g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit, Span sp)
+__device__ void ph_interp_rows(const Grid2& g, Field4 q, const uint8_t* __restrict__ m, int lev, int from_bit, int p0,
+                               Span sp)
 {
     const int D = g.D(lev), h = D >> 1;
     const int rows = PH == 0 ? 2 : 1;
@@ -487,7 +489,7 @@ __device__ void ph_interp_rows(const Grid2& g, Field4 q, const uint8_t* __restri
             const int i = i0 + L;
             const int w = rowscan_band(g, i, j, h);
             if (w < 0 || (PH == 0) == (w == 2)) continue;
-            interp_point(g, q, i, j, 4u * wdx + L, D, w);
+            interp_point(g, q, i, j, 4u * wdx + L, D, w, p0);
         }
     }
 }
@@ -659,7 +661,8 @@ __device__ void ph_apd(const Grid2& g, uint8_t* m, const int8_t* lvl, int bit, i
     }
 }
 
-// Work mask of InterpolateEuler: `to` minus `from` over the grid points (ghost bits untouched).
+// Work mask of InterpolateEuler: `to` minus `from` over the grid points (ghost bits untouched);
+// to < 0 stands for every grid point (InterpolateAllGridEuler).
 __device__ void ph_interp_init(const Grid2& g, uint8_t* m, int from, int to, Span sp)
 {
     unsigned* mp = reinterpret_cast<unsigned*>(m);
@@ -670,7 +673,7 @@ __device__ void ph_interp_init(const Grid2& g, uint8_t* m, int from, int to, Spa
         if (!G) continue;
         const unsigned gb = lane_bits(G);
         const unsigned v = mp[w];
-        const unsigned on = (v >> to) & ~(v >> from) & gb;
+        const unsigned on = (to >= 0 ? (v >> to) : ~0u) & ~(v >> from) & gb;
         const unsigned nv = (v & ~(gb << kBitInterp)) | (on << kBitInterp);
         if (nv != v) mp[w] = nv;
     }
@@ -739,18 +742,19 @@ __global__ void k_cr_rows(Grid2 g, uint8_t* m, int lev, int bit, const StepState
     ph_cr_rows(g, m, lev, bit, grid_span());
 }
 template <int PH>
-__global__ void k_interp(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, const StepState* st)
+__global__ void k_interp(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, int p0, const StepState* st)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_interp<PH>(g, q, m, lev, from_bit, grid_span());
+    ph_interp<PH>(g, q, m, lev, from_bit, p0, grid_span());
 }
 template <int PH>
-__global__ void k_interp_rows(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, const StepState* st)
+__global__ void k_interp_rows(Grid2 g, Field4 q, const uint8_t* m, int lev, int from_bit, int p0,
+                              const StepState* st)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_interp_rows<PH>(g, q, m, lev, from_bit, grid_span());
+    ph_interp_rows<PH>(g, q, m, lev, from_bit, p0, grid_span());
 }
 __global__ void k_copy_bit_all(uint8_t* m, size_t n, int from, int to, const StepState* st)
 {
@@ -906,9 +910,9 @@ __global__ void __launch_bounds__(kPrepThreads, 1) k_prepare(PrepArgs A)
         SYNC_OR_LEAVE;
     }
     for (int lev = 0; lev < g.maxl; ++lev) {
-        ph_interp<0>(g, A.q, A.m, lev, kBitTemp, sp);
+        ph_interp<0>(g, A.q, A.m, lev, kBitTemp, 1, sp);
         SYNC_OR_LEAVE;
-        ph_interp<1>(g, A.q, A.m, lev, kBitTemp, sp);
+        ph_interp<1>(g, A.q, A.m, lev, kBitTemp, 1, sp);
         if (lev + 1 < g.maxl) SYNC_OR_LEAVE;
     }
 #undef SYNC_OR_LEAVE
@@ -1824,7 +1828,7 @@ struct Solver2D {
         }
     }
 
-    void enq_interp(int from, int to, const StepState* s)
+    void enq_interp(int from, int to, const StepState* s, int p0 = 1)
     {
         launch(k_interp_init, blocks_for(words(), 256), 256, g, m, from, to, s);
         after("k_interp_init");
@@ -1832,14 +1836,14 @@ struct Solver2D {
         enq_cr(kBitInterp, s);
         for (int lev = 0; lev < g.maxl; ++lev) {
             if (row_scan(lev)) {
-                launch(k_interp_rows<0>, blocks_for(rowscan_threads(lev, 2), 256), 256, g, q, m, lev, from, s);
+                launch(k_interp_rows<0>, blocks_for(rowscan_threads(lev, 2), 256), 256, g, q, m, lev, from, p0, s);
                 after("k_interp_rows<0>");
-                launch(k_interp_rows<1>, blocks_for(rowscan_threads(lev, 1), 256), 256, g, q, m, lev, from, s);
+                launch(k_interp_rows<1>, blocks_for(rowscan_threads(lev, 1), 256), 256, g, q, m, lev, from, p0, s);
                 after("k_interp_rows<1>");
             } else {
-                launch(k_interp<0>, blocks_for(band_count(lev, 0) + band_count(lev, 1), 256), 256, g, q, m, lev, from, s);
+                launch(k_interp<0>, blocks_for(band_count(lev, 0) + band_count(lev, 1), 256), 256, g, q, m, lev, from, p0, s);
                 after("k_interp<0>");
-                launch(k_interp<1>, blocks_for(band_count(lev, 2), 256), 256, g, q, m, lev, from, s);
+                launch(k_interp<1>, blocks_for(band_count(lev, 2), 256), 256, g, q, m, lev, from, p0, s);
                 after("k_interp<1>");
             }
             launches += 2;
@@ -2205,6 +2209,20 @@ struct Solver2D {
     {
         enq_interp(bit_of(from_id), bit_of(to_id), nullptr);
         AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    // WAVELET_2D::InterpolateAllGridEuler (Wavelet/WAVELET_2D.h:912-1044): every grid point outside
+    // mask `from_id` gets all four components interpolated, coarse to fine, from the active ones:
+    // the dense field.  Same work mask (all points minus `from`, closed by CheckReconstruction) and
+    // the same interpolation bodies as InterpolateEuler, with density included.  The field then
+    // holds values off mask0, so the next step zeroes densely.
+    int interpolate_all(int from_id)
+    {
+        enq_interp(bit_of(from_id), -1, nullptr, 0);
+        AWCM_CUDA_TRY(cudaGetLastError());
+        mark_full_zero();
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
     }
@@ -2672,6 +2690,12 @@ int awcm2d_interpolate(awcm2d_t h, int from_id, int to_id)
 {
     AWCM_H(h);
     return h->s.interpolate(from_id, to_id);
+}
+int awcm2d_interpolate_all(awcm2d_t h, int from_id)
+{
+    AWCM_H(h);
+    if (from_id < 0 || from_id > 4) return awcm::kErrArg;
+    return h->s.interpolate_all(from_id);
 }
 int awcm2d_manager(awcm2d_t h, int op, int mask_id, int level_id)
 {

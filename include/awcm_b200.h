@@ -101,6 +101,10 @@ int awcm2d_fwt(awcm2d_t h, double tol);
 int awcm2d_iwt(awcm2d_t h, int mask_id);
 /* WAVELET_2D::InterpolateEuler(Q, mra, mask_from, mask_to) (Wavelet/WAVELET_2D.h:784-907). */
 int awcm2d_interpolate(awcm2d_t h, int from_id, int to_id);
+/* WAVELET_2D::InterpolateAllGridEuler(Q, mra, mask_from) (Wavelet/WAVELET_2D.h:912-1044): every grid
+ * point outside mask `from_id` gets all four components interpolated from the active points,
+ * coarse to fine (the dense field behind Q.Print, main_2d_euler.cpp:334). */
+int awcm2d_interpolate_all(awcm2d_t h, int from_id);
 /* AWCM_MANAGER_2D passes (Wavelet/AWCM_MANAGER_2D.h:14-280) and the banding of AWCM_2D.h:122-124. */
 int awcm2d_manager(awcm2d_t h, int op, int mask_id, int level_id);
 /* BOUNDARY_MANAGER_{QUAD,DMACH,ISENVORTEX}::SetBoundaryCondition([t]) on the conserved field. */

@@ -85,6 +85,10 @@ public:
         const int plane = mask_id == 4 ? 0 : mask_id + 1;
         return std::vector<uint8_t>(all.begin() + plane * n, all.begin() + (plane + 1) * n);
     }
+    // WAVELET_2D::InterpolateAllGridEuler(Q, mra, mask_from) (Wavelet/WAVELET_2D.h:912-1044): the dense
+    // field, interpolated at every grid point outside mask `from_id` (0 = mask0).
+    void InterpolateAllGridEuler(int from_id = 0) { check(awcm2d_interpolate_all(h_, from_id), "awcm2d_interpolate_all"); }
+
     // Binary state file (awcm2d_save_state / awcm2d_load_state): resume a run bit for bit.
     void SaveState(const char* path, double t, long long step) const
     {

@@ -180,6 +180,7 @@ class Oracle2D:
         self._fwt = b("fwt", None, [_vp, _c_double])
         self._iwt = b("iwt", None, [_vp, _c_int])
         self._interpolate = b("interpolate", None, [_vp, _c_int, _c_int])
+        self._interpolate_all = b("interpolate_all", None, [_vp, _c_int])
         self._manager = b("manager", None, [_vp, _c_int, _c_int, _c_int])
         self._apply_bc = b("apply_bc", None, [_vp, _c_double])
         self._step = b("step", None, [_vp] + [_c_double] * 5 + [_dp, _dp])
@@ -245,6 +246,10 @@ class Oracle2D:
 
     def interpolate(self, from_id=4, to_id=3):
         self._interpolate(self.h, from_id, to_id)
+
+    def interpolate_all(self, from_id=0):
+        """InterpolateAllGridEuler: the dense field from the points of mask `from_id`."""
+        self._interpolate_all(self.h, from_id)
 
     def manager(self, op, mask_id, level_id=0):
         self._manager(self.h, op, mask_id, level_id)

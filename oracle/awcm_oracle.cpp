@@ -906,10 +906,15 @@ void band2d(O2D& s, int b)
 }
 
 // WAVELET_2D::InterpolateEuler (Wavelet/WAVELET_2D.h:784-907): components 1..3 at new points.
-void interp2d(O2D& s, int from, int to)
+// to < 0: every grid point (InterpolateAllGridEuler, WAVELET_2D.h:912-1044, mask_temp all true
+// minus mask_from); p0: first interpolated component (1 for InterpolateEuler, 0 for the dense
+// field).
+void interp2d(O2D& s, int from, int to, int p0 = 1)
 {
     const int NX = s.nx - 1, NY = s.ny - 1;
-    copy_bit(s.m, to, 5);
+    if (to >= 0) copy_bit(s.m, to, 5);
+    else
+        for (auto& b : s.m) b |= (uint8_t)(1u << 5);
     for (int j = 0; j <= NY; ++j)
         for (int i = 0; i <= NX; ++i)
             if (s.get(i, j, from)) s.clr(i, j, 5);
@@ -917,7 +922,7 @@ void interp2d(O2D& s, int from, int to)
     auto need = [&](int i, int j) { return s.get(i, j, 5) && !s.get(i, j, from); };
     for (int lev = 0; lev < s.maxl; ++lev) {
         const int D = s.D(lev), h = D / 2;
-        for (int p = 1; p < 4; ++p) {
+        for (int p = p0; p < 4; ++p) {
             std::vector<double>& q = s.q[p];
             auto Q = [&](int i, int j) -> double& { return q[s.at(i, j)]; };
             for (int j = D; j <= NY - D; j += D)
@@ -939,7 +944,7 @@ void interp2d(O2D& s, int from, int to)
                     Q(i, j) = v;
                 }
         }
-        for (int p = 1; p < 4; ++p) {
+        for (int p = p0; p < 4; ++p) {
             std::vector<double>& q = s.q[p];
             auto Q = [&](int i, int j) -> double& { return q[s.at(i, j)]; };
             for (int j = h; j <= NY - h; j += D)
@@ -1478,6 +1483,11 @@ void or2d_iwt(void* h, int mask_id) { iwt2d(*static_cast<O2D*>(h), bit_of(mask_i
 void or2d_interpolate(void* h, int from_id, int to_id)
 {
     interp2d(*static_cast<O2D*>(h), bit_of(from_id), bit_of(to_id));
+}
+
+void or2d_interpolate_all(void* h, int from_id)
+{
+    interp2d(*static_cast<O2D*>(h), bit_of(from_id), -1, 0);
 }
 
 void or2d_manager(void* h, int op, int mask_id, int level_id)

@@ -48,6 +48,8 @@ void or2d_prepare(void* h, double tol);
 void or2d_fwt(void* h, double tol);
 void or2d_iwt(void* h, int mask_id);
 void or2d_interpolate(void* h, int from_id, int to_id);
+/* WAVELET_2D::InterpolateAllGridEuler (Wavelet/WAVELET_2D.h:912-1044). */
+void or2d_interpolate_all(void* h, int from_id);
 void or2d_manager(void* h, int op, int mask_id, int level_id);
 void or2d_apply_bc(void* h, double t);
 void or2d_step(void* h, double tol, double cfl, double t, double t_next, double dt_fixed, double* alpha_io,

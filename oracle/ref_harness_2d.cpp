@@ -375,6 +375,12 @@ void ref2d_interpolate(void* h, int from_id, int to_id)
     s->awcm->wavelet.InterpolateEuler(s->Q, s->mra, mask_ref(s, from_id), mask_ref(s, to_id));
 }
 
+void ref2d_interpolate_all(void* h, int from_id)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    s->awcm->wavelet.InterpolateAllGridEuler(s->Q, s->mra, mask_ref(s, from_id));
+}
+
 // AWCM_MANAGER_2D passes on one of the facade's masks.
 // op 0 AddAdjacentZone, 1 CheckReconstruction, 2 AddPointForDifferentiation(level_id),
 // 3 ComputeLevel(level_id <- mask), 4 RemoveResidueEuler(Q, mask), 5 BandingMask.
