@@ -926,8 +926,10 @@ __device__ __forceinline__ double euler_E(double g, double rho, double u, double
 
 // Ghost fill of the edge strips (corners are never read by the axis-aligned stencils):
 // transmissive BOUNDARY_MANAGER_QUAD (Problems/2D/PROBLEM_QUADRANTS.h:123-203), double Mach
-// BOUNDARY_MANAGER_DMACH(t) (Problems/2D/PROBLEM_DOUBLEMACH.h:106-245) and periodic
-// BOUNDARY_MANAGER_ISENVORTEX (Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h:107-171).
+// BOUNDARY_MANAGER_DMACH(t) (Problems/2D/PROBLEM_DOUBLEMACH.h:106-245), periodic
+// BOUNDARY_MANAGER_ISENVORTEX (Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h:107-171) and
+// BOUNDARY_MANAGER_SHOCK_VORTEX (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:118-201:
+// transmissive left/right, bottom/top walls reflecting rho v).
 __global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, double* zx, double* zy)
 {
     pdl_begin();
@@ -1004,6 +1006,13 @@ __global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, doub
         return;
     }
     const size_t s = g.at(i, sj);
+    if (g.bc_kind == AWCM_BC_SHOCK_VORTEX) {
+        f.p[0][a] = f.p[0][s];
+        f.p[1][a] = f.p[1][s];
+        f.p[2][a] = -f.p[2][s];
+        f.p[3][a] = f.p[3][s];
+        return;
+    }
     for (int k = 0; k < 4; ++k) f.p[k][a] = f.p[k][s];
 }
 
@@ -1597,7 +1606,7 @@ struct Solver2D {
     int create(int num_levels, int nxc, int nyc, double x_min, double x_max, double y_min, double y_max, int bc)
     {
         if (num_levels < 2 || num_levels > kMaxLevels - 1 || nxc < 5 || nyc < 5) return kErrArg;
-        if (bc < 0 || bc > 2) return kErrArg;
+        if (bc < 0 || bc > 3) return kErrArg;
         geo = awcm2d_geometry{num_levels, nxc, nyc, bc, x_min, x_max, y_min, y_max, 1.4};
         const long nx = (long)(nxc - 1) * (1L << (num_levels - 1)) + 1;
         const long ny = (long)(nyc - 1) * (1L << (num_levels - 1)) + 1;
@@ -2576,6 +2585,23 @@ struct Solver2D {
                     rhov *= rho;
                     p = std::pow(rho, gam);
                     Q[0] = rho, Q[1] = rhou, Q[2] = rhov, Q[3] = E(rho, rhou / rho, rhov / rho, p);
+                } else if (kind == AWCM_PROBLEM_SHOCK_VORTEX) {
+                    // SHOCK_VORTEX::Initialize (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:32-66):
+                    // post-shock state for x <= 0, vortex of Mach 0.5 centred at (a, b) ahead of it.
+                    const double Mv = 0.5;
+                    const double r = std::sqrt((x - a) * (x - a) + (y - b) * (y - b));
+                    if (x <= 0) {
+                        rho = 1.394708041144614, u = -0.860403729339060, v = 0, p = 1.121834000000000;
+                    } else {
+                        rho = 1 - (gam - 1) / 2 * (Mv * Mv) * std::exp(1 - r * r);
+                        rho = std::pow(rho, 1 / (gam - 1));
+                        p = 1 - (gam - 1) / 2 * (Mv * Mv) * std::exp(1 - r * r);
+                        p = std::pow(p, gam / (gam - 1));
+                        p = 1 / gam * p;
+                        u = Mv * std::exp(0.5 * (1 - r * r)) * (-y) - 1.200011999940001;
+                        v = Mv * std::exp(0.5 * (1 - r * r)) * (x - a);
+                    }
+                    Q[0] = rho, Q[1] = rho * u, Q[2] = rho * v, Q[3] = E(rho, u, v, p);
                 } else {
                     return kErrArg;
                 }

@@ -467,14 +467,15 @@ __global__ void k_adj_rk(int stage, Grid2 g, size_t plane, const uint8_t* __rest
 
 // Adjoint of the boundary fill: every ghost's adjoint moves to the interior point it was copied
 // from (transmissive: the edge point; periodic: the wrapped point; double Mach: the transmissive
-// right edge and the reflecting bottom for x > 1/6, sign flip on rho v; prescribed states carry
-// no adjoint).  One thread per edge line; a corner source is shared by a row thread and a column
+// right edge and the reflecting bottom for x > 1/6, sign flip on rho v; shock-vortex: the
+// reflecting bottom and top, sign flip on rho v; prescribed states carry no adjoint).  One thread per edge line; a corner source is shared by a row thread and a column
 // thread, so sources are updated atomically.
 __global__ void k_adj_fold(Grid2 g, Field4 lam)
 {
     const int t = (int)gtid();
     const int NX = g.nx - 1, NY = g.ny - 1;
     const bool per = g.bc_kind == AWCM_BC_PERIODIC, dm = g.bc_kind == AWCM_BC_DOUBLE_MACH;
+    const bool sv = g.bc_kind == AWCM_BC_SHOCK_VORTEX;  // walls at the bottom and top: rho v flips
     if (t < g.ny) {
         const int j = t;
         for (int c = 0; c < kGhost; ++c) {
@@ -497,8 +498,9 @@ __global__ void k_adj_fold(Grid2 g, Field4 lam)
                 if (dm) {
                     if (x > 1.0 / 6.0) atomic_add(&lam.p[k][sb], (k == 2 ? -1.0 : 1.0) * lam.p[k][gb]);
                 } else {
-                    atomic_add(&lam.p[k][sb], lam.p[k][gb]);
-                    atomic_add(&lam.p[k][st], lam.p[k][gt]);
+                    const double sg = (sv && k == 2) ? -1.0 : 1.0;
+                    atomic_add(&lam.p[k][sb], sg * lam.p[k][gb]);
+                    atomic_add(&lam.p[k][st], sg * lam.p[k][gt]);
                 }
                 lam.p[k][gb] = 0;
                 lam.p[k][gt] = 0;

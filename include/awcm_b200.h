@@ -52,11 +52,14 @@ extern "C" {
 #define AWCM_BC_TRANSMISSIVE 0 /* BOUNDARY_MANAGER (1D), BOUNDARY_MANAGER_QUAD (2D)   */
 #define AWCM_BC_DOUBLE_MACH 1  /* BOUNDARY_MANAGER_DMACH::SetBoundaryCondition(t)      */
 #define AWCM_BC_PERIODIC 2     /* BOUNDARY_MANAGER_ISENVORTEX                          */
+#define AWCM_BC_SHOCK_VORTEX 3 /* BOUNDARY_MANAGER_SHOCK_VORTEX: transmissive left/right,
+                                  reflecting bottom/top (PROBLEM_SHOCK_VORTEX_INTERACTION.h:78-201) */
 
 /* 2D problem initial states (Problems/2D/*::Initialize). */
 #define AWCM_PROBLEM_QUADRANTS 0   /* a, b = split point                      */
 #define AWCM_PROBLEM_DOUBLE_MACH 1 /* a = pre-shock density                   */
 #define AWCM_PROBLEM_VORTEX 2      /* a, b = vortex centre                    */
+#define AWCM_PROBLEM_SHOCK_VORTEX 3 /* SHOCK_VORTEX: Mach 1.2 shock at x = 0, vortex at (a, b) */
 
 /* Last error message of the calling thread ("" if none). */
 const char* awcm_last_error(void);

@@ -603,7 +603,7 @@ V4 face_flux_2d(const double* const* s, double alpha, double g, int dir, double 
 
 // =============================================================================================
 // 2D AWCM state.
-enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2 };
+enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2, BC_SHOCK_VORTEX = 3 };
 
 struct O2D {
     int L = 0, maxl = 0, nx = 0, ny = 0, w = 0;
@@ -1052,6 +1052,16 @@ void bc2d(O2D& s, std::vector<double>* f, double t)
             for (int j = NY + 1; j <= NY + G; ++j)
                 for (int k = 0; k < 4; ++k) F(k, i, j) = x < xs ? post[k] : pre[k];
         }
+    } else if (s.bc_kind == BC_SHOCK_VORTEX) {
+        // BOUNDARY_MANAGER_SHOCK_VORTEX::SetBottom/TopBoundaryCondition
+        // (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:145-175): walls, rho v reflected.
+        for (int i = 0; i <= NX; ++i)
+            for (int c = 1; c <= G; ++c)
+                for (int k = 0; k < 4; ++k) {
+                    const double sg = k == 2 ? -1.0 : 1.0;
+                    F(k, i, -c) = sg * F(k, i, 0);
+                    F(k, i, NY + c) = sg * F(k, i, NY);
+                }
     } else {
         for (int i = 0; i <= NX; ++i)
             for (int c = 1; c <= G; ++c)
@@ -1428,7 +1438,7 @@ void or2d_init_problem(void* h, int kind, double a, double b)
                 if (y > std::sqrt(3.0) * (x - 1.0 / 6.0)) { rho = 8; u = 8.25 * std::sqrt(3.0) * 0.5; v = -8.25 * 0.5; p = 116.5; }
                 else { rho = a; u = 0; v = 0; p = 1; }
                 Q[0] = rho, Q[1] = rho * u, Q[2] = rho * v, Q[3] = euler_E(g, rho, u, v, p);
-            } else {
+            } else if (kind == 2) {
                 const double rr = sqr(x - a) + sqr(y - b);
                 const double beta = 5;
                 rho = 1 - (g - 1) * sqr(beta) / (8 * g * PI * PI) * std::exp(1 - rr);
@@ -1439,6 +1449,23 @@ void or2d_init_problem(void* h, int kind, double a, double b)
                 rhov *= rho;
                 p = std::pow(rho, g);
                 Q[0] = rho, Q[1] = rhou, Q[2] = rhov, Q[3] = euler_E(g, rho, rhou / rho, rhov / rho, p);
+            }
+            if (kind == 3) {
+                // SHOCK_VORTEX::Initialize (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:32-66)
+                const double Mv = 0.5;
+                const double r = std::sqrt(sqr(x - a) + sqr(y - b));
+                if (x <= 0) {
+                    rho = 1.394708041144614, u = -0.860403729339060, v = 0, p = 1.121834000000000;
+                } else {
+                    rho = 1 - (g - 1) / 2 * sqr(Mv) * std::exp(1 - r * r);
+                    rho = std::pow(rho, 1 / (g - 1));
+                    p = 1 - (g - 1) / 2 * sqr(Mv) * std::exp(1 - r * r);
+                    p = std::pow(p, g / (g - 1));
+                    p = 1 / g * p;
+                    u = Mv * std::exp(0.5 * (1 - r * r)) * (-y) - 1.200011999940001;
+                    v = Mv * std::exp(0.5 * (1 - r * r)) * (x - a);
+                }
+                Q[0] = rho, Q[1] = rho * u, Q[2] = rho * v, Q[3] = euler_E(g, rho, u, v, p);
             }
             for (int k = 0; k < 4; ++k) s->q[k][s->at(i, j)] = Q[k];
         }

@@ -20,7 +20,7 @@
 
 namespace {
 
-enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2 };
+enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2, BC_SHOCK_VORTEX = 3 };
 
 // One boundary manager per field, of the kind the problem uses.
 struct BC2D {
@@ -28,10 +28,12 @@ struct BC2D {
     BOUNDARY_MANAGER_QUAD* quad = nullptr;
     BOUNDARY_MANAGER_DMACH* dmach = nullptr;
     BOUNDARY_MANAGER_ISENVORTEX* periodic = nullptr;
+    BOUNDARY_MANAGER_SHOCK_VORTEX* shock_vortex = nullptr;
     BC2D(int k, FIELD_UNIFORM_2D<VECTOR_4D<double>>& Q) : kind(k)
     {
         if (k == BC_DMACH) dmach = new BOUNDARY_MANAGER_DMACH(Q);
         else if (k == BC_PERIODIC) periodic = new BOUNDARY_MANAGER_ISENVORTEX(Q);
+        else if (k == BC_SHOCK_VORTEX) shock_vortex = new BOUNDARY_MANAGER_SHOCK_VORTEX(Q);
         else quad = new BOUNDARY_MANAGER_QUAD(Q);
     }
     ~BC2D()
@@ -39,11 +41,13 @@ struct BC2D {
         delete quad;
         delete dmach;
         delete periodic;
+        delete shock_vortex;
     }
     void apply(double t)
     {
         if (dmach) dmach->SetBoundaryCondition(t);
         else if (periodic) periodic->SetBoundaryCondition();
+        else if (shock_vortex) shock_vortex->SetBoundaryCondition();
         else quad->SetBoundaryCondition();
     }
 };
@@ -277,6 +281,24 @@ void ref2d_init_problem(void* h, int kind, double a, double b)
         } else if (kind == 1) {
             if (y > sqrt(3.0) * (x - 1.0 / 6.0)) { rho = 8; u = 8.25 * sqrt(3.0) * 0.5; v = -8.25 * 0.5; p = 116.5; }
             else { rho = a; u = 0; v = 0; p = 1; }
+            Q(i, j)[0] = rho;
+            Q(i, j)[1] = rho * u;
+            Q(i, j)[2] = rho * v;
+            Q(i, j)[3] = EOS.E(rho, u, v, p);
+        } else if (kind == 3) {
+            // SHOCK_VORTEX::Initialize (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:32-66), vortex at (a, b)
+            const double M_v = 0.5;
+            const double r = sqrt(SQR(x - a) + SQR(y - b));
+            if (x <= 0) { rho = 1.394708041144614; u = -0.860403729339060; v = 0; p = 1.121834000000000; }
+            else {
+                rho = 1 - (gamma - 1) / 2 * SQR(M_v) * exp(1 - r * r);
+                rho = pow(rho, 1 / (gamma - 1));
+                p = 1 - (gamma - 1) / 2 * SQR(M_v) * exp(1 - r * r);
+                p = pow(p, gamma / (gamma - 1));
+                p = 1 / gamma * p;
+                u = M_v * exp(0.5 * (1 - r * r)) * (-y) - 1.200011999940001;
+                v = M_v * exp(0.5 * (1 - r * r)) * (x - a);
+            }
             Q(i, j)[0] = rho;
             Q(i, j)[1] = rho * u;
             Q(i, j)[2] = rho * v;

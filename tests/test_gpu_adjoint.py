@@ -250,3 +250,41 @@ def test_torch_autograd_harness(awcm_lib):
     assert x.grad is not None and torch.isfinite(x.grad).all()
     assert torch.autograd.gradcheck(lambda y: F.apply(y, s, target, 0.0, dt, 4, 0), (x,), eps=1e-6, atol=1e-8,
                                     rtol=1e-5, fast_mode=True)
+
+
+@pytest.mark.parametrize("bc", [0, 1, 3])
+def test_adjoint_boundary_folds(awcm_lib, bc):
+    """Transposed boundary fills of the transmissive, double-Mach and wall managers: the adjoint
+    against central differences (h = 1e-6), differentiable mode.  The transmissive and wall
+    managers run on the vortex + bumps state (bound 1e-6); the double-Mach manager on its own
+    initial state (129 x 33 nodes, 6 steps at a quarter of the CFL limit, target 1.01 rho0), whose
+    shock leaves central differences at h = 1e-6 and 1e-7 up to 1.5e-6 apart (CPU restatement),
+    so the bound there is 2e-5."""
+    from awcm import gradient as G
+
+    if bc == 1:
+        s = awcm_lib.AWCM2D(4, 17, 5, 0.0, 4.0, 0.0, 1.0, bc_kind=1)
+        s.init_problem(awcm_lib.PROBLEM_DOUBLE_MACH, 1.4, 0.0)
+        q0 = s.get_q()
+        target = 1.01 * q0[3:-3, 3:-3, 0]
+        dt = 0.25 * (4.0 / (s.nx - 1)) / 22.0
+        tol_rel = 2e-5
+    else:
+        s = awcm_lib.AWCM2D(4, 9, 9, 0.0, 10.0, 0.0, 10.0, bc_kind=bc)
+        q0, target = G.vortex_bumps(s), G.target_density(s)
+        dt = G.stable_dt(q0, 10.0 / (s.nx - 1))
+        tol_rel = FD_REL_TOL
+    s.set_q(q0)
+    s.prepare(1e-3)
+    s.set_wenoz(EPS_DIFF, DELTA_DIFF)
+    qp = s.get_q()
+    n = 6
+    loss, grad, _ = s.adjoint(0.0, dt, n, target)
+    act = G.active_points(s.get_masks())
+    dirs = G.unit_directions(qp.shape, 8, 5)
+    h = 1e-6
+    fd = np.array([G.loss_difference(replay_q(s, qp + h * d, dt, n), replay_q(s, qp - h * d, dt, n), target, act)
+                   / (2 * h) for d in dirs])
+    ad, rel = directional_errors(grad, dirs, fd)
+    print(f"adjoint vs differences, boundary kind {bc}: max rel {rel.max():.2e}")
+    assert rel.max() <= tol_rel, (rel, ad, fd)

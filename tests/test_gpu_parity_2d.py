@@ -23,6 +23,7 @@ CASES = {
     "quad_ref_split": (5, 9, 9, (0.0, 1.0, 0.0, 1.0), 0, 0, 0.8, 0.8, 1e-4, 0.5),
     "dmach": (4, 17, 5, (0.0, 4.0, 0.0, 1.0), 1, 1, 1.4, 0.0, 1e-3, 0.5),
     "vortex": (4, 9, 9, (0.0, 10.0, 0.0, 10.0), 2, 2, 5.0, 5.0, 1e-3, 0.4),
+    "shock_vortex": (5, 9, 9, (-16.0, 8.0, -12.0, 12.0), 3, 3, 2.0, 0.0, 1e-3, 0.4),
 }
 
 

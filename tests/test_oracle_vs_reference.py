@@ -52,6 +52,7 @@ def test_1d_shipped_driver_geometry():
     (6, 17, 17, (0.0, 1.0, 0.0, 1.0), 0, 0, 0.5, 0.5, 1e-3, 0.4, 2),   # 513^2 quadrants
     (5, 17, 5, (0.0, 4.0, 0.0, 1.0), 1, 1, 1.5, 0.0, 1e-3, 0.5, 3),   # double Mach, reference IC density 1.5
     (5, 9, 9, (0.0, 10.0, -5.0, 5.0), 2, 2, 5.0, 0.0, 1e-3, 0.4, 3),  # vortex at the reference's centre
+    (5, 9, 9, (-16.0, 8.0, -12.0, 12.0), 3, 3, 2.0, 0.0, 1e-3, 0.4, 4),  # shock-vortex, reference domain
 ])
 def test_2d_cases(case):
     nl, nxc, nyc, dom, bc, prob, a_, b_, tol, cfl, steps = case
