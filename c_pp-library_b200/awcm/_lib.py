@@ -37,6 +37,10 @@ _SIGS = {
     "awcm2d_iwt": [c_void_p, c_int],
     "awcm2d_interpolate": [c_void_p, c_int, c_int],
     "awcm2d_interpolate_all": [c_void_p, c_int],
+    "awcm2d_create_scalar": [c_int, c_int, c_int, c_double, c_double, c_double, c_double, ctypes.POINTER(c_void_p)],
+    "awcm2d_scalar_set_q": [c_void_p, P_double],
+    "awcm2d_scalar_get_q": [c_void_p, P_double],
+    "awcm2d_scalar_advance": [c_void_p, c_double, c_double, c_double, c_int, P_double],
     "awcm2d_manager": [c_void_p, c_int, c_int, c_int],
     "awcm2d_apply_bc": [c_void_p, c_double],
     "awcm2d_step": [c_void_p, c_double, c_double, c_double, c_double, c_double, P_double],

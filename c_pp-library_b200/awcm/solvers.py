@@ -231,6 +231,62 @@ class AWCM2D:
         call("awcm2d_set_alpha_tape", self.h, t.shape[0], ptr(t, ctypes.c_double))
 
 
+class AWCM2DScalar:
+    """Scalar AWCM instance (the path of Wavelet/main_2d_advect.cpp): one field advected with unit
+    velocity, periodic; masks and levels as for AWCM2D."""
+
+    def __init__(self, num_levels: int, nx_coarse: int, ny_coarse: int, x_min: float, x_max: float,
+                 y_min: float, y_max: float):
+        h = c_void_p()
+        call("awcm2d_create_scalar", num_levels, nx_coarse, ny_coarse, x_min, x_max, y_min, y_max, ctypes.byref(h))
+        self.h = h
+        nx, ny = ctypes.c_int(), ctypes.c_int()
+        call("awcm2d_dims", self.h, ctypes.byref(nx), ctypes.byref(ny))
+        self.nx, self.ny = nx.value, ny.value
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            call("awcm2d_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_q(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.ny + 6, self.nx + 6)
+        call("awcm2d_scalar_set_q", self.h, ptr(q, ctypes.c_double))
+
+    def get_q(self):
+        q = np.empty((self.ny + 6, self.nx + 6), np.float64)
+        call("awcm2d_scalar_get_q", self.h, ptr(q, ctypes.c_double))
+        return q
+
+    def get_masks(self):
+        m = np.empty((5, self.ny + 6, self.nx + 6), np.uint8)
+        call("awcm2d_get_masks", self.h, ptr(m, ctypes.c_uint8))
+        return m
+
+    def get_levels(self):
+        lv = np.empty((4, self.ny, self.nx), np.int32)
+        call("awcm2d_get_levels", self.h, ptr(lv, ctypes.c_int))
+        return lv
+
+    def advance(self, tol, dt, t, n_steps):
+        """n_steps driver passes at the fixed dt; returns (t, steps, sum |mask0|)."""
+        out = np.zeros(3)
+        call("awcm2d_scalar_advance", self.h, tol, dt, t, n_steps, ptr(out, ctypes.c_double))
+        return out[0], int(out[1]), out[2]
+
+    @property
+    def stream(self) -> int:
+        s = c_void_p()
+        call("awcm2d_stream", self.h, ctypes.byref(s))
+        return s.value or 0
+
+
 class AWCM1DBatch:
     """Independent 1D AWCM instances advanced together (one persistent launch per RK3 step)."""
 

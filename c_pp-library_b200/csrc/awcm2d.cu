@@ -1393,6 +1393,90 @@ __global__ void __launch_bounds__(256) k_update_crs(Grid2 g, Field4 in, Field4 o
 }
 
 // ------------------------------------------------------------------------- layout conversions
+// ------------------------------------------------------------------- scalar AWCM (advection)
+// The scalar path of Wavelet/main_2d_advect.cpp:33-205 (AWCM_2D::Prepare on FIELD_UNIFORM_2D<double>,
+// linear advection with unit velocity in x and y): finest-level points take the upwind WENO5 face
+// values F(i+1/2) = WENO5::ReconstructRight(q[i-2..i+2]) (WENO.h:101-104) and dF = F(i+1/2) -
+// F(i-1/2); coarser points the 4th-order central differences of q itself
+// (AWCM_2D::Differentiate*, Wavelet/AWCM_2D.h:95-109) with the same edge forms as the Euler path.
+template <int DIR>
+__global__ void __launch_bounds__(256) k_face_scalar(Grid2 g, const double* __restrict__ f, double* __restrict__ out,
+                                                     const uint32_t* __restrict__ list,
+                                                     const unsigned* __restrict__ count, const StepState* st)
+{
+    pdl_begin();
+    if (st->done) return;
+    const unsigned n = *count;
+    const long step = DIR == 0 ? 1 : g.pitch;
+    for (unsigned e = gtid(); e < n; e += gridDim.x * blockDim.x) {
+        const long a = list[e];
+        out[a] = recon_left<kWeno5>(f[a + 2 * step], f[a + step], f[a], f[a - step], f[a - 2 * step]);
+    }
+}
+
+// Stage combinations of main_2d_advect.cpp:65, 121, 177 and 183-189: KIND 1: out = in - sc (dF+dG);
+// KIND 2: out = 0.75 qn + 0.25 (in - sc (dF+dG)); KIND 4: qn = 1/3 qn + 2/3 (in - sc (dF+dG)).
+template <int KIND>
+__device__ __forceinline__ void rk_store_scalar(const double* in, double* out, double* qn, size_t a, double d,
+                                                double sc)
+{
+    const double r = in[a] - sc * d;
+    if (KIND == 1) out[a] = r;
+    else if (KIND == 2) out[a] = 0.75 * qn[a] + 0.25 * r;
+    else qn[a] = kC1_3 * qn[a] + kD1 * r;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(256) k_update_fin_scalar(Grid2 g, const double* in, double* out, double* qn,
+                                                           const double* fx, const double* fy,
+                                                           const uint32_t* __restrict__ list,
+                                                           const unsigned* __restrict__ count, const StepState* st)
+{
+    pdl_begin();
+    if (st->done) return;
+    const unsigned n = *count;
+    const double sc = st->sc[g.maxl];
+    for (unsigned e = gtid(); e < n; e += gridDim.x * blockDim.x) {
+        const size_t a = list[e];
+        const double dF = fx[a] - fx[a - 1];
+        const double dG = fy[a] - fy[a - g.pitch];
+        rk_store_scalar<KIND>(in, out, qn, a, dF + dG, sc);
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(256) k_update_crs_scalar(Grid2 g, const double* in, double* out, double* qn,
+                                                           const int8_t* __restrict__ lvl,
+                                                           const uint32_t* __restrict__ list,
+                                                           const unsigned* __restrict__ count, const StepState* st)
+{
+    pdl_begin();
+    if (st->done) return;
+    const unsigned n = *count;
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    for (unsigned e = gtid(); e < n; e += gridDim.x * blockDim.x) {
+        const size_t a = list[e];
+        const int i = (int)((unsigned)a % (unsigned)g.pitch) - kGhost;
+        const int j = (int)((unsigned)a / (unsigned)g.pitch) - kGhost;
+        const int lev = lvl[a];
+        if (lev < 0 || lev > g.maxl) continue;
+        const int d = g.D(lev);
+        const int lo_x = i <= d ? i - d : i - 2 * d, hi_x = i >= NX - d && !(i <= d) ? i + d : i + 2 * d;
+        const int lo_y = j <= d ? j - d : j - 2 * d, hi_y = j >= NY - d && !(j <= d) ? j + d : j + 2 * d;
+        if (lo_x < -kGhost || hi_x > NX + kGhost || lo_y < -kGhost || hi_y > NY + kGhost) continue;
+        auto X = [&](long o) { return in[(long)a + o]; };
+        auto Y = [&](long o) { return in[(long)a + o * g.pitch]; };
+        double dF, dG;
+        if (i <= d) dF = kD1 * (X(d) - X(-d)) + kD2 * (X(2 * d) - X(-d));
+        else if (i >= NX - d) dF = kD1 * (X(d) - X(-d)) + kD2 * (X(d) - X(-2 * d));
+        else dF = kD1 * (X(d) - X(-d)) + kD2 * (X(2 * d) - X(-2 * d));
+        if (j <= d) dG = kD1 * (Y(d) - Y(-d)) + kD2 * (Y(2 * d) - Y(-d));
+        else if (j >= NY - d) dG = kD1 * (Y(d) - Y(-d)) + kD2 * (Y(d) - Y(-2 * d));
+        else dG = kD1 * (Y(d) - Y(-d)) + kD2 * (Y(2 * d) - Y(-2 * d));
+        rk_store_scalar<KIND>(in, out, qn, a, dF + dG, st->sc[lev]);
+    }
+}
+
 __global__ void k_aos_to_soa(Grid2 g, const double* __restrict__ aos, Field4 f)
 {
     pdl_begin();
@@ -1873,6 +1957,8 @@ struct Solver2D {
     // (prep_mode 0) the persistent cooperative kernel with grid barriers.
     int prep_mode = 1;
     int prep_blocks = 0;
+    // Scalar AWCM instance (Wavelet/main_2d_advect.cpp): plane 0 of q, q2, q1 carries the field.
+    bool scalar = false;
 
     void enq_prepare(const StepState* s)
     {
@@ -1901,7 +1987,7 @@ struct Solver2D {
             launches += 1;
             return;
         }
-        launch(k_copy_bit_all, blocks_for(words(), 256), 256, m, plane, 0, kBitTemp, s);
+        if (!scalar) launch(k_copy_bit_all, blocks_for(words(), 256), 256, m, plane, 0, kBitTemp, s);
         after("k_copy_bit_all");
         launches += 1;
         enq_fwt(s);
@@ -1920,7 +2006,8 @@ struct Solver2D {
             enq_cr(k, s);
         }
         enq_iwt(3, s);
-        enq_interp(kBitTemp, 3, s);
+        // AWCM_2D::Prepare (the scalar form, Wavelet/AWCM_2D.h:52-79) ends with the inverse transform
+        if (!scalar) enq_interp(kBitTemp, 3, s);
     }
 
     // Boundary fill of a stage input; with zero_stage >= 0 it also zeroes that stage's LF-speed
@@ -2014,12 +2101,66 @@ struct Solver2D {
         mark();
     }
 
+    // One pass of the scalar driver loop (Wavelet/main_2d_advect.cpp:48-190): Prepare (no
+    // interpolation), periodic fill, three SSP-RK3 stages at the fixed dt with WENO5 upwind faces
+    // on the finest level and central differences below, PostProcess.
+    static Field4 alias(double* p) { return Field4{{p, p, p, p}}; }
+    void enq_stage_scalar(int stage, const double* in, double* out)
+    {
+        uint32_t* const* L = lists + 4 * stage;
+        const unsigned* C = st->cnt + 4 * stage;
+        launch(k_face_scalar<0>, face_blocks, 256, g, in, fx.p[0], L[2], C + 2, st);
+        after("k_face_scalar<0>");
+        launch(k_face_scalar<1>, face_blocks, 256, g, in, fy.p[0], L[3], C + 3, st);
+        after("k_face_scalar<1>");
+        const int ub = face_blocks / 2;
+        double* qn = q.p[0];
+        if (stage == 0) {
+            launch(k_update_fin_scalar<1>, ub, 256, g, in, out, qn, fx.p[0], fy.p[0], L[0], C + 0, st);
+            launch(k_update_crs_scalar<1>, ub, 256, g, in, out, qn, lvl[2], L[1], C + 1, st);
+        } else if (stage == 1) {
+            launch(k_update_fin_scalar<2>, ub, 256, g, in, out, qn, fx.p[0], fy.p[0], L[0], C + 0, st);
+            launch(k_update_crs_scalar<2>, ub, 256, g, in, out, qn, lvl[1], L[1], C + 1, st);
+        } else {
+            launch(k_update_fin_scalar<4>, ub, 256, g, in, out, qn, fx.p[0], fy.p[0], L[0], C + 0, st);
+            launch(k_update_crs_scalar<4>, ub, 256, g, in, out, qn, lvl[0], L[1], C + 1, st);
+        }
+        after("k_update_scalar");
+        launches += 4;
+    }
+
+    void enq_step_scalar()
+    {
+        launches = 0;
+        launch(k_begin, 1, 1, st);
+        launches += 1;
+        enq_prepare(st);
+        enq_bc(alias(q.p[0]), st);
+        launch(k_dt, 1, 1, g, st);
+        {
+            ListArgs la;
+            for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
+            dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
+            launch(k_lists, grid, 256, g, m, lvl[2], lvl[1], lvl[0], la, st);
+        }
+        launches += 2;
+        enq_stage_scalar(0, q.p[0], q2.p[0]);
+        enq_bc(alias(q2.p[0]), st);
+        enq_stage_scalar(1, q2.p[0], q1.p[0]);
+        enq_bc(alias(q1.p[0]), st);
+        enq_stage_scalar(2, q1.p[0], q1.p[0]);
+        launch(k_remove_residue, blocks_for(words(), 256), 256, g, q, m, 0, 1, st);
+        launch(k_finish, 1, 1, st);
+        launches += 2;
+    }
+
     int build_graph()
     {
         if (graph) return kOk;
         cudaGraph_t gr;
         AWCM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        enq_step();
+        if (scalar) enq_step_scalar();
+        else enq_step();
         cudaError_t e = cudaStreamEndCapture(stream, &gr);
         if (e != cudaSuccess) {
             set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
@@ -2233,6 +2374,44 @@ struct Solver2D {
         AWCM_CUDA_TRY(cudaGetLastError());
         mark_full_zero();
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
+    // Scalar field in the reference's FIELD_UNIFORM_2D<double> layout ((Ny+6) x (Nx+6) doubles).
+    int scalar_set_q(const double* host)
+    {
+        const size_t w = (size_t)g.nx + 2 * kGhost;
+        AWCM_CUDA_TRY(cudaMemcpy2DAsync(q.p[0], (size_t)g.pitch * sizeof(double), host, w * sizeof(double),
+                                        w * sizeof(double), (size_t)g.rows, cudaMemcpyHostToDevice, stream));
+        mark_full_zero();
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+    int scalar_get_q(double* host)
+    {
+        const size_t w = (size_t)g.nx + 2 * kGhost;
+        AWCM_CUDA_TRY(cudaMemcpy2DAsync(host, w * sizeof(double), q.p[0], (size_t)g.pitch * sizeof(double),
+                                        w * sizeof(double), (size_t)g.rows, cudaMemcpyDeviceToHost, stream));
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+    // n scalar steps at the fixed dt from t (graph replays); out[3]: t, steps, sum |mask0|.
+    int scalar_advance(double tol, double dt, double t, int n, double* out)
+    {
+        if (!(dt > 0) || n < 0) return kErrArg;
+        int rc = build_graph();
+        if (rc) return rc;
+        if ((rc = write_params(tol, 1.0, t, 1e300, dt))) return rc;
+        StepState h0;
+        if ((rc = read_state(&h0))) return rc;
+        for (int k = 0; k < n; ++k) AWCM_CUDA_TRY(cudaGraphLaunch(graph, stream));
+        StepState h;
+        if ((rc = read_state(&h))) return rc;
+        if (out) {
+            out[0] = h.t;
+            out[1] = h.steps - h0.steps;
+            out[2] = (double)(h.upd - h0.upd);
+        }
         return kOk;
     }
 
@@ -2638,6 +2817,15 @@ int awcm2d_create(int num_levels, int nx_coarse, int ny_coarse, double x_min, do
     return awcm::kOk;
 }
 
+int awcm2d_create_scalar(int num_levels, int nx_coarse, int ny_coarse, double x_min, double x_max, double y_min,
+                         double y_max, awcm2d_t* out)
+{
+    const int rc = awcm2d_create(num_levels, nx_coarse, ny_coarse, x_min, x_max, y_min, y_max, AWCM_BC_PERIODIC, out);
+    if (rc) return rc;
+    (*out)->s.scalar = true;
+    return awcm::kOk;
+}
+
 int awcm2d_destroy(awcm2d_t h)
 {
     delete h;
@@ -2647,6 +2835,18 @@ int awcm2d_destroy(awcm2d_t h)
 #define AWCM_H(h)                         \
     if (!(h)) return awcm::kErrArg;       \
     cudaSetDevice((h)->s.device)
+
+#define AWCM_EULER_ONLY(h)                                                                  \
+    if ((h)->s.scalar) {                                                                    \
+        awcm::set_last_error("Euler entry point called on a scalar instance", __FILE__, __LINE__); \
+        return awcm::kErrState;                                                             \
+    }
+#define AWCM_SCALAR_ONLY(h)                                                                 \
+    if (!(h)->s.scalar) {                                                                   \
+        awcm::set_last_error("scalar entry point called on an Euler instance", __FILE__, __LINE__); \
+        return awcm::kErrState;                                                             \
+    }
+
 
 int awcm2d_dims(awcm2d_t h, int* nx, int* ny)
 {
@@ -2665,11 +2865,13 @@ int awcm2d_get_geometry(awcm2d_t h, awcm2d_geometry* out)
 int awcm2d_set_q(awcm2d_t h, const double* q)
 {
     AWCM_H(h);
+    AWCM_EULER_ONLY(h);
     return q ? h->s.set_q(q) : awcm::kErrArg;
 }
 int awcm2d_get_q(awcm2d_t h, double* q)
 {
     AWCM_H(h);
+    AWCM_EULER_ONLY(h);
     return q ? h->s.get_q(q) : awcm::kErrArg;
 }
 int awcm2d_get_masks(awcm2d_t h, uint8_t* m)
@@ -2695,6 +2897,7 @@ int awcm2d_set_levels(awcm2d_t h, const int* lv)
 int awcm2d_init_problem(awcm2d_t h, int kind, double a, double b)
 {
     AWCM_H(h);
+    AWCM_EULER_ONLY(h);
     return h->s.init_problem(kind, a, b);
 }
 int awcm2d_prepare(awcm2d_t h, double tol)
@@ -2733,14 +2936,34 @@ int awcm2d_apply_bc(awcm2d_t h, double t)
     AWCM_H(h);
     return h->s.apply_bc(t);
 }
+int awcm2d_scalar_set_q(awcm2d_t h, const double* q)
+{
+    AWCM_H(h);
+    AWCM_SCALAR_ONLY(h);
+    return q ? h->s.scalar_set_q(q) : awcm::kErrArg;
+}
+int awcm2d_scalar_get_q(awcm2d_t h, double* q)
+{
+    AWCM_H(h);
+    AWCM_SCALAR_ONLY(h);
+    return q ? h->s.scalar_get_q(q) : awcm::kErrArg;
+}
+int awcm2d_scalar_advance(awcm2d_t h, double tol, double dt, double t, int n_steps, double* out)
+{
+    AWCM_H(h);
+    AWCM_SCALAR_ONLY(h);
+    return h->s.scalar_advance(tol, dt, t, n_steps, out);
+}
 int awcm2d_step(awcm2d_t h, double tol, double cfl, double t, double t_next, double dt_fixed, double* out)
 {
     AWCM_H(h);
+    AWCM_EULER_ONLY(h);
     return h->s.step(tol, cfl, t, t_next, dt_fixed, out);
 }
 int awcm2d_advance(awcm2d_t h, double tol, double cfl, double t_start, double t_end, int n_steps, double* out)
 {
     AWCM_H(h);
+    AWCM_EULER_ONLY(h);
     if (n_steps < 0) return awcm::kErrArg;
     return h->s.advance(tol, cfl, t_start, t_end, n_steps, out);
 }
@@ -2786,12 +3009,14 @@ int awcm2d_set_prepare_mode(awcm2d_t h, int mode)
 int awcm2d_frozen_run(awcm2d_t h, double t0, double dt, int n_steps, int mode, double* out)
 {
     AWCM_H(h);
+    AWCM_EULER_ONLY(h);
     return h->s.frozen_run(t0, dt, n_steps, mode, out);
 }
 int awcm2d_adjoint(awcm2d_t h, double t0, double dt, int n_steps, int checkpoint_every, int mode,
                    const double* target, double* grad, double* out)
 {
     AWCM_H(h);
+    AWCM_EULER_ONLY(h);
     return h->s.adjoint(t0, dt, n_steps, checkpoint_every, mode, target, grad, out);
 }
 int awcm2d_set_wenoz(awcm2d_t h, double eps, double tau_delta)

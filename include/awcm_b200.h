@@ -149,6 +149,24 @@ int awcm2d_stream(awcm2d_t h, void** stream);
 int awcm2d_save_state(awcm2d_t h, const char* path, double t, long long step);
 int awcm2d_load_state(awcm2d_t h, const char* path, double* t, long long* step);
 
+/* ------------------------------------------------------------------- 2D scalar AWCM (advection)
+ * The scalar path of Wavelet/main_2d_advect.cpp:33-205: one scalar field on the same dyadic grid,
+ * AWCM_2D::Prepare(FIELD_UNIFORM_2D<double>&, tol) (Wavelet/AWCM_2D.h:52-79: the Euler adaptation
+ * without the interpolation of new points), linear advection with unit velocity in x and y,
+ * WENO5::ReconstructRight upwind faces (WENO.h:101-104) on the finest level and
+ * AWCM_2D::Differentiate* (Wavelet/AWCM_2D.h:95-109) below, SSP-RK3 at a fixed dt with the final
+ * combination 1/3 q + 2/3 q0, AWCM_2D::PostProcess, and the periodic BOUNDARY_MANAGER of
+ * Problems/2D/PROBLEM_BOX_ADVECTION.h.  Masks, levels and the manager passes of the 2D instance
+ * apply; the Euler entry points (state, steps, adjoint) return AWCM_ERR_STATE on it. */
+int awcm2d_create_scalar(int num_levels, int nx_coarse, int ny_coarse, double x_min, double x_max, double y_min,
+                         double y_max, awcm2d_t* out);
+/* The field in the FIELD_UNIFORM_2D<double> layout: (Ny+6) x (Nx+6) doubles, ghosts included. */
+int awcm2d_scalar_set_q(awcm2d_t h, const double* q);
+int awcm2d_scalar_get_q(awcm2d_t h, double* q);
+/* n_steps passes of the driver loop from t at the fixed dt (one CUDA graph per step).
+ * out[3]: final t, steps, sum |mask0| over the steps. */
+int awcm2d_scalar_advance(awcm2d_t h, double tol, double dt, double t, int n_steps, double* out);
+
 /* ---------------------------------------------------------------- 2D frozen-mask run and adjoint
  * No counterpart in the reference (it has no derivative code).  The frozen-mask step is the
  * driver loop of Wavelet/main_2d_euler(quad).cpp:58-334 with PrepareEuler and PostProcessEuler

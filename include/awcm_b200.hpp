@@ -132,6 +132,37 @@ private:
     long last_mask_sizes_[4] = {0, 0, 0, 0};
 };
 
+// The scalar AWCM path of Wavelet/main_2d_advect.cpp (AWCM_2D::Prepare/PostProcess on a
+// FIELD_UNIFORM_2D<double>, unit-velocity advection, periodic box manager).
+class AWCM_2D_SCALAR {
+public:
+    AWCM_2D_SCALAR(int num_levels, int nx_coarse, int ny_coarse, double x_min, double x_max, double y_min, double y_max)
+    {
+        check(awcm2d_create_scalar(num_levels, nx_coarse, ny_coarse, x_min, x_max, y_min, y_max, &h_),
+              "awcm2d_create_scalar");
+        check(awcm2d_dims(h_, &nx_, &ny_), "awcm2d_dims");
+    }
+    ~AWCM_2D_SCALAR() { awcm2d_destroy(h_); }
+    AWCM_2D_SCALAR(const AWCM_2D_SCALAR&) = delete;
+    AWCM_2D_SCALAR& operator=(const AWCM_2D_SCALAR&) = delete;
+    int Nx() const { return nx_; }
+    int Ny() const { return ny_; }
+    // (Ny+6) x (Nx+6) doubles, the FIELD_UNIFORM_2D<double> storage with its ghost ring of 3.
+    void SetField(const double* q) { check(awcm2d_scalar_set_q(h_, q), "awcm2d_scalar_set_q"); }
+    void GetField(double* q) const { check(awcm2d_scalar_get_q(h_, q), "awcm2d_scalar_get_q"); }
+    // n passes of the driver loop at the fixed dt; returns the new time.
+    double Advance(double tol, double dt, double t, int n)
+    {
+        double out[3];
+        check(awcm2d_scalar_advance(h_, tol, dt, t, n, out), "awcm2d_scalar_advance");
+        return out[0];
+    }
+
+private:
+    awcm2d_t h_ = nullptr;
+    int nx_ = 0, ny_ = 0;
+};
+
 // AWCM_MANAGER_2D (Wavelet/AWCM_MANAGER_2D.h): static passes on one of the facade's masks.
 struct AWCM_MANAGER_2D {
     static void AddAdjacentZone(AWCM_2D& a, int mask_id)

@@ -181,6 +181,10 @@ class Oracle2D:
         self._iwt = b("iwt", None, [_vp, _c_int])
         self._interpolate = b("interpolate", None, [_vp, _c_int, _c_int])
         self._interpolate_all = b("interpolate_all", None, [_vp, _c_int])
+        self._set_scalar = b("set_scalar", None, [_vp, _c_int])
+        self._scalar_set_q = b("scalar_set_q", None, [_vp, _dp])
+        self._scalar_get_q = b("scalar_get_q", None, [_vp, _dp])
+        self._scalar_step = b("scalar_step", None, [_vp, _c_double, _c_double, _dp])
         self._manager = b("manager", None, [_vp, _c_int, _c_int, _c_int])
         self._apply_bc = b("apply_bc", None, [_vp, _c_double])
         self._step = b("step", None, [_vp] + [_c_double] * 5 + [_dp, _dp])
@@ -246,6 +250,25 @@ class Oracle2D:
 
     def interpolate(self, from_id=4, to_id=3):
         self._interpolate(self.h, from_id, to_id)
+
+    # scalar AWCM (Wavelet/main_2d_advect.cpp) ------------------------------------------------
+    def set_scalar(self):
+        """Switches the instance to the scalar advection path (field (Ny+6, Nx+6))."""
+        self._set_scalar(self.h, 1)
+
+    def scalar_set_q(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.ny + 6, self.nx + 6)
+        self._scalar_set_q(self.h, _ptr(q, ctypes.c_double))
+
+    def scalar_get_q(self):
+        q = np.empty((self.ny + 6, self.nx + 6), np.float64)
+        self._scalar_get_q(self.h, _ptr(q, ctypes.c_double))
+        return q
+
+    def scalar_step(self, tol, dt):
+        out = np.zeros(4)
+        self._scalar_step(self.h, tol, dt, _ptr(out, ctypes.c_double))
+        return out
 
     def interpolate_all(self, from_id=0):
         """InterpolateAllGridEuler: the dense field from the points of mask `from_id`."""

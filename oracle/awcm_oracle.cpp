@@ -616,6 +616,7 @@ struct O2D {
     std::vector<double> q[4], q2[4], q1[4], q0[4];
     std::vector<uint8_t> m;
     std::vector<int> lv[4];
+    bool scalar = false;  // scalar AWCM (main_2d_advect.cpp): q[0] carries the field
     int D(int lev) const { return 1 << (maxl - lev); }
     size_t at(int i, int j) const { return (size_t)(j + G) * w + (i + G); }
     bool get(int i, int j, int b) const { return (m[at(i, j)] >> b) & 1; }
@@ -976,7 +977,7 @@ void remove_residue_2d(O2D& s, int b)
 // AWCM_2D::PrepareEuler (Wavelet/AWCM_2D.h:114-147).
 void prepare2d(O2D& s, double tol)
 {
-    copy_bit(s.m, 0, 4);
+    if (!s.scalar) copy_bit(s.m, 0, 4);  // the scalar Prepare keeps no previous mask0
     fwt2d(s, tol);
     band2d(s, 0);
     aaz2d(s, 0);
@@ -988,7 +989,8 @@ void prepare2d(O2D& s, double tol)
         cr2d(s, k);
     }
     iwt2d(s, 3);
-    interp2d(s, 4, 3);
+    // AWCM_2D::Prepare, the scalar form (Wavelet/AWCM_2D.h:52-79), stops after the inverse transform
+    if (!s.scalar) interp2d(s, 4, 3);
 }
 
 double euler_E(double g, double rho, double u, double v, double p) { return p / (g - 1) + 0.5 * rho * (u * u + v * v); }
@@ -1511,6 +1513,102 @@ void or2d_interpolate(void* h, int from_id, int to_id)
 {
     interp2d(*static_cast<O2D*>(h), bit_of(from_id), bit_of(to_id));
 }
+
+// Scalar AWCM driver loop (Wavelet/main_2d_advect.cpp:48-190): Prepare, the periodic
+// BOUNDARY_MANAGER of Problems/2D/PROBLEM_BOX_ADVECTION.h (edge ghosts), three SSP-RK3 stages of
+// linear advection with unit velocity (finest level: WENO5::ReconstructRight upwind faces, WENO.h:101-104,
+// both faces per point as the driver computes them; coarser levels: AWCM_2D::Differentiate*,
+// Wavelet/AWCM_2D.h:95-109), q = 1/3 q + 2/3 q0 on mask0, PostProcess (RemoveResidue on mask0).
+void scalar_bc2d(O2D& s, std::vector<double>& f)
+{
+    const int NX = s.nx - 1, NY = s.ny - 1;
+    for (int j = 0; j <= NY; ++j)
+        for (int c = 0; c < G; ++c) {
+            f[s.at(-1 - c, j)] = f[s.at(NX - c, j)];
+            f[s.at(NX + 1 + c, j)] = f[s.at(c, j)];
+        }
+    for (int i = 0; i <= NX; ++i)
+        for (int c = 0; c < G; ++c) {
+            f[s.at(i, -1 - c)] = f[s.at(i, NY - c)];
+            f[s.at(i, NY + 1 + c)] = f[s.at(i, c)];
+        }
+}
+
+void scalar_stage2d(O2D& s, const std::vector<double>& in, std::vector<double>& out, int bit, int l, double dt,
+                    int kind)
+{
+    const int NX = s.nx - 1, NY = s.ny - 1;
+    const double d1 = 2.0 / 3.0, d2 = -1.0 / 12.0;
+    const std::vector<double>& qn = s.q[0];
+    auto Q = [&](int i, int j) { return in[s.at(i, j)]; };
+    for (int j = 0; j <= NY; ++j)
+        for (int i = 0; i <= NX; ++i) {
+            if (!s.get(i, j, bit)) continue;
+            const int lev = s.LV(l, i, j);
+            const int d = s.D(lev);
+            const double dxl = s.dx * d;
+            double dF, dG;
+            if (lev == s.maxl) {
+                double a = recon_left(Q(i + 1, j), Q(i, j), Q(i - 1, j), Q(i - 2, j), Q(i - 3, j), 1);
+                double b = recon_left(Q(i + 2, j), Q(i + 1, j), Q(i, j), Q(i - 1, j), Q(i - 2, j), 1);
+                dF = b - a;
+                a = recon_left(Q(i, j + 1), Q(i, j), Q(i, j - 1), Q(i, j - 2), Q(i, j - 3), 1);
+                b = recon_left(Q(i, j + 2), Q(i, j + 1), Q(i, j), Q(i, j - 1), Q(i, j - 2), 1);
+                dG = b - a;
+            } else {
+                if (i <= d) dF = d1 * (Q(i + d, j) - Q(i - d, j)) + d2 * (Q(i + 2 * d, j) - Q(i - d, j));
+                else if (i >= NX - d) dF = d1 * (Q(i + d, j) - Q(i - d, j)) + d2 * (Q(i + d, j) - Q(i - 2 * d, j));
+                else dF = d1 * (Q(i + d, j) - Q(i - d, j)) + d2 * (Q(i + 2 * d, j) - Q(i - 2 * d, j));
+                if (j <= d) dG = d1 * (Q(i, j + d) - Q(i, j - d)) + d2 * (Q(i, j + 2 * d) - Q(i, j - d));
+                else if (j >= NY - d) dG = d1 * (Q(i, j + d) - Q(i, j - d)) + d2 * (Q(i, j + d) - Q(i, j - 2 * d));
+                else dG = d1 * (Q(i, j + d) - Q(i, j - d)) + d2 * (Q(i, j + 2 * d) - Q(i, j - 2 * d));
+            }
+            const size_t a = s.at(i, j);
+            if (kind == 2) out[a] = 0.75 * qn[a] + 0.25 * (in[a] - dt / dxl * (dF + dG));
+            else out[a] = in[a] - dt / dxl * (dF + dG);
+        }
+}
+
+void scalar_step2d(O2D& s, double tol, double dt, double* out)
+{
+    prepare2d(s, tol);
+    scalar_bc2d(s, s.q[0]);
+    scalar_stage2d(s, s.q[0], s.q2[0], 2, 2, dt, 1);
+    scalar_bc2d(s, s.q2[0]);
+    scalar_stage2d(s, s.q2[0], s.q1[0], 1, 1, dt, 2);
+    scalar_bc2d(s, s.q1[0]);
+    scalar_stage2d(s, s.q1[0], s.q0[0], 0, 0, dt, 3);
+    const int NX = s.nx - 1, NY = s.ny - 1;
+    for (int j = 0; j <= NY; ++j)
+        for (int i = 0; i <= NX; ++i)
+            if (s.get(i, j, 0)) {
+                const size_t a = s.at(i, j);
+                s.q[0][a] = 1.0 / 3.0 * s.q[0][a] + 2.0 / 3.0 * s.q0[0][a];
+            }
+    for (int j = 1; j <= NY - 1; ++j)
+        for (int i = 1; i <= NX - 1; ++i)
+            if (!s.get(i, j, 0)) s.q[0][s.at(i, j)] = 0.0;
+    if (out)
+        for (int k = 0; k < 4; ++k) {
+            long c = 0;
+            for (int j = 0; j <= NY; ++j)
+                for (int i = 0; i <= NX; ++i) c += s.get(i, j, k);
+            out[k] = (double)c;
+        }
+}
+
+void or2d_set_scalar(void* h, int on) { static_cast<O2D*>(h)->scalar = on != 0; }
+void or2d_scalar_set_q(void* h, const double* q)
+{
+    O2D* s = static_cast<O2D*>(h);
+    for (size_t a = 0; a < s->plane; ++a) s->q[0][a] = q[a];
+}
+void or2d_scalar_get_q(void* h, double* q)
+{
+    O2D* s = static_cast<O2D*>(h);
+    for (size_t a = 0; a < s->plane; ++a) q[a] = s->q[0][a];
+}
+void or2d_scalar_step(void* h, double tol, double dt, double* out) { scalar_step2d(*static_cast<O2D*>(h), tol, dt, out); }
 
 void or2d_interpolate_all(void* h, int from_id)
 {

@@ -48,6 +48,12 @@ void or2d_prepare(void* h, double tol);
 void or2d_fwt(void* h, double tol);
 void or2d_iwt(void* h, int mask_id);
 void or2d_interpolate(void* h, int from_id, int to_id);
+/* Scalar AWCM (Wavelet/main_2d_advect.cpp): mode switch, field (ny+6)x(nx+6) doubles, one driver pass;
+ * out[4] = |mask0..mask3|. */
+void or2d_set_scalar(void* h, int on);
+void or2d_scalar_set_q(void* h, const double* q);
+void or2d_scalar_get_q(void* h, double* q);
+void or2d_scalar_step(void* h, double tol, double dt, double* out);
 /* WAVELET_2D::InterpolateAllGridEuler (Wavelet/WAVELET_2D.h:912-1044). */
 void or2d_interpolate_all(void* h, int from_id);
 void or2d_manager(void* h, int op, int mask_id, int level_id);

@@ -9,6 +9,7 @@
 #include "OMP_MANAGER.h"
 #include "Problems/2D/PROBLEM_QUADRANTS.h"
 #include "Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h"
+#include "Problems/2D/PROBLEM_BOX_ADVECTION.h"
 #include "AWCM_2D.h"
 #include "WENO.h"
 #include "WENOZ.h"
@@ -67,6 +68,10 @@ struct Ref2D {
     // Value given to the public member WENOZ5::eps (WENOZ.h:13-18) of every WENOZ_EULER_SOLVER_2D
     // the stages construct; the solver's own default is 1e-40.
     double wenoz_eps = 1e-40;
+    // Scalar AWCM (Wavelet/main_2d_advect.cpp): the field and its stage copies, each with the
+    // periodic BOUNDARY_MANAGER of Problems/2D/PROBLEM_BOX_ADVECTION.h; created by ref2d_set_scalar.
+    FIELD_UNIFORM_2D<double> S, S_0, S_1, S_2;
+    BOUNDARY_MANAGER *bs = nullptr, *bs1 = nullptr, *bs2 = nullptr;
 };
 
 FIELD_UNIFORM_2D<bool>& mask_ref(Ref2D* s, int id)
@@ -220,6 +225,9 @@ void ref2d_destroy(void* h)
     delete s->bc0;
     delete s->bc1;
     delete s->bc2;
+    delete s->bs;
+    delete s->bs1;
+    delete s->bs2;
     delete s->awcm;
     delete s;
 }
@@ -401,6 +409,104 @@ void ref2d_interpolate_all(void* h, int from_id)
 {
     Ref2D* s = static_cast<Ref2D*>(h);
     s->awcm->wavelet.InterpolateAllGridEuler(s->Q, s->mra, mask_ref(s, from_id));
+}
+
+// Scalar AWCM: one pass of the loop of Wavelet/main_2d_advect.cpp:48-190 (AWCM_2D::Prepare, the box
+// manager's periodic fill, three SSP-RK3 stages of unit-velocity advection with WENO5 upwind faces on
+// the finest level and AWCM_2D::Differentiate* below, 1/3 Q + 2/3 Q_0 on mask0, PostProcess),
+// restated as a function with the same calls, order and arithmetic.  out[4] = |mask0..mask3|.
+void ref2d_set_scalar(void* h, int on)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    if (!on || s->bs) return;
+    for (FIELD_UNIFORM_2D<double>* f : {&s->S, &s->S_0, &s->S_1, &s->S_2}) {
+        f->Initialize(s->grid, 3);
+        f->AssignAllValues(0.0);
+    }
+    s->bs = new BOUNDARY_MANAGER(s->S);
+    s->bs1 = new BOUNDARY_MANAGER(s->S_1);
+    s->bs2 = new BOUNDARY_MANAGER(s->S_2);
+}
+
+void ref2d_scalar_set_q(void* h, const double* q)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const int w = s->nx + 6;
+    for (int j = -3; j < s->ny + 3; ++j)
+        for (int i = -3; i < s->nx + 3; ++i) s->S(i, j) = q[(size_t)(j + 3) * w + (i + 3)];
+}
+
+void ref2d_scalar_get_q(void* h, double* q)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    const int w = s->nx + 6;
+    for (int j = -3; j < s->ny + 3; ++j)
+        for (int i = -3; i < s->nx + 3; ++i) q[(size_t)(j + 3) * w + (i + 3)] = s->S(i, j);
+}
+
+void ref2d_scalar_step(void* h, double tol, double dt, double* out)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    AWCM_2D& awcm = *s->awcm;
+    const GRID_UNIFORM_2D& grid = s->grid;
+    MRA_GRID_INT_2D& mra_grid = s->mra;
+    const int max_lev = mra_grid.num_levels - 1;
+    FIELD_UNIFORM_2D<double>& Q = s->S;
+    WENO5 weno;
+    auto stage = [&](FIELD_UNIFORM_2D<double>& in, FIELD_UNIFORM_2D<double>& res, FIELD_UNIFORM_2D<bool>& mask,
+                     FIELD_UNIFORM_2D<int>& level, int kind) {
+        ITERATION_GRID_2D(grid, 0)
+        {
+            double dF = 0, dG = 0;
+            if (mask(i, j) == false) continue;
+            const int lev = level(i, j);
+            const int d = mra_grid.grid[lev].dx;
+            const double dx = grid.dx * d;
+            if (lev == max_lev) {
+                double a, b;
+                weno.ReconstructRight(in(i - 3, j), in(i - 2, j), in(i - 1, j), in(i, j), in(i + 1, j), a);
+                weno.ReconstructRight(in(i - 2, j), in(i - 1, j), in(i, j), in(i + 1, j), in(i + 2, j), b);
+                dF = b - a;
+                weno.ReconstructRight(in(i, j - 3), in(i, j - 2), in(i, j - 1), in(i, j), in(i, j + 1), a);
+                weno.ReconstructRight(in(i, j - 2), in(i, j - 1), in(i, j), in(i, j + 1), in(i, j + 2), b);
+                dG = b - a;
+            } else {
+                if (i <= d) awcm.DifferentiateAtLeftBoundary(in(i - d, j), in(i, j), in(i + d, j), in(i + 2 * d, j), dF);
+                else if (i >= grid.i_end - d)
+                    awcm.DifferentiateAtRightBoundary(in(i - 2 * d, j), in(i - d, j), in(i, j), in(i + d, j), dF);
+                else awcm.Differentiate(in(i - 2 * d, j), in(i - d, j), in(i, j), in(i + d, j), in(i + 2 * d, j), dF);
+                if (j <= d) awcm.DifferentiateAtLeftBoundary(in(i, j - d), in(i, j), in(i, j + d), in(i, j + 2 * d), dG);
+                else if (j >= grid.j_end - d)
+                    awcm.DifferentiateAtRightBoundary(in(i, j - 2 * d), in(i, j - d), in(i, j), in(i, j + d), dG);
+                else awcm.Differentiate(in(i, j - 2 * d), in(i, j - d), in(i, j), in(i, j + d), in(i, j + 2 * d), dG);
+            }
+            if (kind == 2) res(i, j) = 0.75 * Q(i, j) + 0.25 * (in(i, j) - dt / dx * (dF + dG));
+            else res(i, j) = in(i, j) - dt / dx * (dF + dG);
+        }
+    };
+    awcm.Prepare(Q, tol);
+    s->bs->SetBoundaryCondition();
+    stage(Q, s->S_2, awcm.mask2, awcm.level2, 1);
+    s->bs2->SetBoundaryCondition();
+    stage(s->S_2, s->S_1, awcm.mask1, awcm.level1, 2);
+    s->bs1->SetBoundaryCondition();
+    stage(s->S_1, s->S_0, awcm.mask0, awcm.level0, 3);
+    ITERATION_GRID_2D(grid, 0)
+    {
+        if (awcm.mask0(i, j) == true) Q(i, j) = (1.0 / 3.0 * Q(i, j) + 2.0 / 3.0 * s->S_0(i, j));
+    }
+    awcm.PostProcess(Q);
+    if (out) {
+        long cnt[4] = {0, 0, 0, 0};
+        for (int j = 0; j < s->ny; ++j)
+            for (int i = 0; i < s->nx; ++i) {
+                cnt[0] += awcm.mask0(i, j);
+                cnt[1] += awcm.mask1(i, j);
+                cnt[2] += awcm.mask2(i, j);
+                cnt[3] += awcm.mask3(i, j);
+            }
+        for (int k = 0; k < 4; ++k) out[k] = (double)cnt[k];
+    }
 }
 
 // AWCM_MANAGER_2D passes on one of the facade's masks.
