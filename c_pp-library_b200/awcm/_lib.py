@@ -46,6 +46,7 @@ _SIGS = {
     "awcm2d_step": [c_void_p, c_double, c_double, c_double, c_double, c_double, P_double],
     "awcm2d_advance": [c_void_p, c_double, c_double, c_double, c_double, c_int, P_double],
     "awcm2d_launches_per_step": [c_void_p, P_int],
+    "awcm2d_step_io_bytes": [c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
     "awcm2d_stream": [c_void_p, ctypes.POINTER(c_void_p)],
     "awcm2d_set_prepare_mode": [c_void_p, c_int],
     "awcm2d_profile_step": [c_void_p, c_double, c_double, c_double, c_double, P_double],

@@ -1096,7 +1096,8 @@ __global__ void k_dt(Grid2 g, StepState* st)
     }
 }
 
-__global__ void k_begin(StepState* st)
+// keep_lists: the step reuses the worklists (and mask counts) of the previous one (frozen masks).
+__global__ void k_begin(StepState* st, int keep_lists)
 {
     pdl_begin();
     st->done = (st->t >= st->t_end || st->error) ? 1 : 0;
@@ -1104,8 +1105,16 @@ __global__ void k_begin(StepState* st)
     st->bar[0] = 0;
     st->bar_err = 0;
     st->mv = 0;
+    if (keep_lists) return;
     for (int k = 0; k < 4 * kStages; ++k) st->cnt[k] = 0;
     for (int k = 0; k < 4; ++k) st->mask_cnt[k] = 0;
+}
+
+__global__ void k_copy4(Field4 dst, Field4 src, size_t n)
+{
+    pdl_begin();
+    for (size_t a = gtid(); a < n; a += (size_t)gridDim.x * blockDim.x)
+        for (int k = 0; k < 4; ++k) dst.p[k][a] = src.p[k][a];
 }
 
 __global__ void k_finish(StepState* st)
@@ -1251,10 +1260,15 @@ __global__ void __launch_bounds__(256) k_lists(Grid2 g, const uint8_t* __restric
 // --------------------------------------------------------------------------------- stage kernels
 // Face flux from the compacted face list: x faces (DIR 0) read cells i-2..i+3 of row j, y faces
 // (DIR 1) cells j-2..j+3 of column i (WENOZ_EULER_SOLVER_2D::ComputeFluxX/Y, WENOZ.h:236-320).
-template <int DIR>
-__global__ void __launch_bounds__(128) k_face(Grid2 g, Field4 f, Field4 out, const uint32_t* __restrict__ list,
-                                              const unsigned* __restrict__ count, const double* __restrict__ alpha,
-                                              const StepState* st)
+// CUSTOM false: the reference's WENO-Z parameters as compile-time constants (eps 1e-40, exact
+// |b0 - b2|); true: the instance's runtime parameters (the differentiable mode).
+#ifndef AWCM_FACE_MIN_CTAS
+#define AWCM_FACE_MIN_CTAS 4
+#endif
+template <int DIR, bool CUSTOM>
+__global__ void __launch_bounds__(128, AWCM_FACE_MIN_CTAS)
+    k_face(Grid2 g, Field4 f, Field4 out, const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
+           const double* __restrict__ alpha, const StepState* st)
 {
     pdl_begin();
     if (st->done) return;
@@ -1274,7 +1288,8 @@ __global__ void __launch_bounds__(128) k_face(Grid2 g, Field4 f, Field4 out, con
         }
         const double al = DIR == 0 ? alpha[jj] : alpha[ii];
         double o[4];
-        face_flux_2d<DIR>(s, al, g.gamma, o, g.wz_eps, g.wz_delta);
+        if (CUSTOM) face_flux_2d<DIR>(s, al, g.gamma, o, g.wz_eps, g.wz_delta);
+        else face_flux_2d<DIR>(s, al, g.gamma, o);
 #pragma unroll
         for (int k = 0; k < 4; ++k) out.p[k][idx] = o[k];
     }
@@ -2012,34 +2027,47 @@ struct Solver2D {
 
     // Boundary fill of a stage input; with zero_stage >= 0 it also zeroes that stage's LF-speed
     // accumulators for the k_alpha that follows.
-    void enq_bc(Field4 f, const StepState* s, int zero_stage = -1)
+    void enq_bc(Field4 f, const StepState* s, int zero_stage = -1, double* zx_in = nullptr, double* zy_in = nullptr)
     {
         const long n = 2L * kGhost * g.ny + 2L * kGhost * g.nx;
-        double* zx = zero_stage >= 0 ? ax[zero_stage] : nullptr;
-        double* zy = zero_stage >= 0 ? ay[zero_stage] : nullptr;
+        double* zx = zx_in ? zx_in : (zero_stage >= 0 ? ax[zero_stage] : nullptr);
+        double* zy = zy_in ? zy_in : (zero_stage >= 0 ? ay[zero_stage] : nullptr);
         launch(k_bc, blocks_for(n, 256), 256, g, f, s, 0.0, zx, zy);
         after("k_bc");
         launches += 1;
     }
 
-    void enq_alpha(Field4 f, int bit, int stage, bool with_cfl)
+    // Accumulates into ax[stage] / ay[stage], or into (axp, ayp) when given; the accumulators were
+    // zeroed by the boundary fill before this launch.
+    void enq_alpha(Field4 f, int bit, int stage, bool with_cfl, double* axp = nullptr, double* ayp = nullptr)
     {
-        // ax[stage] / ay[stage] were zeroed by the boundary fill before this launch
         dim3 grid((unsigned)(g.pitch / 4 + 31) / 32, (unsigned)(g.ny + 8 * kAlphaRows - 1) / (8 * kAlphaRows));
-        launch(k_alpha, grid, 256, g, f, m, bit, ax[stage], ay[stage], with_cfl ? &st->mv : nullptr, st);
+        launch(k_alpha, grid, 256, g, f, m, bit, axp ? axp : ax[stage], ayp ? ayp : ay[stage],
+               with_cfl ? &st->mv : nullptr, st);
         after("k_alpha");
         launches += 1;
     }
 
-    void enq_faces_update(int stage, Field4 in, Field4 out)
+    // Face fluxes and point updates of one stage; the LF speeds come from ax[stage] / ay[stage],
+    // or from (axp, ayp) when given.
+    void enq_faces_update(int stage, Field4 in, Field4 out, const double* axp = nullptr, const double* ayp = nullptr)
     {
         uint32_t* const* L = lists + 4 * stage;
         const unsigned* C = st->cnt + 4 * stage;
+        const double* sx = axp ? axp : ax[stage];
+        const double* sy = ayp ? ayp : ay[stage];
         mark();
-        launch(k_face<0>, face_blocks, 128, g, in, fx, L[2], C + 2, ax[stage], st);
-        after("k_face<0>");
-        launch(k_face<1>, face_blocks, 128, g, in, fy, L[3], C + 3, ay[stage], st);
-        after("k_face<1>");
+        if (g.wz_eps == 1e-40 && g.wz_delta == 0.0) {
+            launch(k_face<0, false>, face_blocks, 128, g, in, fx, L[2], C + 2, sx, st);
+            after("k_face<0>");
+            launch(k_face<1, false>, face_blocks, 128, g, in, fy, L[3], C + 3, sy, st);
+            after("k_face<1>");
+        } else {
+            launch(k_face<0, true>, face_blocks, 128, g, in, fx, L[2], C + 2, sx, st);
+            after("k_face<0>");
+            launch(k_face<1, true>, face_blocks, 128, g, in, fy, L[3], C + 3, sy, st);
+            after("k_face<1>");
+        }
         launches += 2;
         mark();
         const int ub = face_blocks / 2;
@@ -2068,7 +2096,7 @@ struct Solver2D {
     {
         launches = 0;
         mark();
-        launch(k_begin, 1, 1, st);
+        launch(k_begin, 1, 1, st, 0);
         after("k_begin");
         launches += 1;
         enq_prepare(st);
@@ -2132,7 +2160,7 @@ struct Solver2D {
     void enq_step_scalar()
     {
         launches = 0;
-        launch(k_begin, 1, 1, st);
+        launch(k_begin, 1, 1, st, 0);
         launches += 1;
         enq_prepare(st);
         enq_bc(alias(q.p[0]), st);
@@ -2327,7 +2355,7 @@ struct Solver2D {
     {
         int rc = write_params(tol, 0, 0, 1, 0);
         if (rc) return rc;
-        launch(k_begin, 1, 1, st);
+        launch(k_begin, 1, 1, st, 0);
         enq_prepare(st);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -2338,7 +2366,7 @@ struct Solver2D {
     {
         int rc = write_params(tol, 0, 0, 1, 0);
         if (rc) return rc;
-        launch(k_begin, 1, 1, st);
+        launch(k_begin, 1, 1, st, 0);
         enq_fwt(st);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -2455,47 +2483,40 @@ struct Solver2D {
 
     void copy_field(Field4 dst, Field4 src)
     {
-        for (int k = 0; k < 4; ++k)
-            cudaMemcpyAsync(dst.p[k], src.p[k], plane * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+        launch(k_copy4, blocks_for((long)plane, 256), 256, dst, src, plane);
     }
 
-    void enq_alpha_frozen(Field4 f, int bit, int stage, const double* tin, double* tout)
+    // One frozen step.  The LF speeds of stage k live in the tape row itself: recorded there by
+    // k_alpha (zeroed by the boundary fill before it), or read from it when replaying, so neither
+    // way copies them.  The worklists are built by the first step of a run (masks and levels are
+    // frozen) and kept by the later ones.
+    void enq_frozen_step(const double* tin, double* tout, const Field4* save, bool build_lists)
     {
-        const size_t o = (size_t)stage * (g.nx + g.ny);
-        if (tin) {
-            cudaMemcpyAsync(ax[stage], tin + o, sizeof(double) * g.ny, cudaMemcpyDeviceToDevice, stream);
-            cudaMemcpyAsync(ay[stage], tin + o + g.ny, sizeof(double) * g.nx, cudaMemcpyDeviceToDevice, stream);
-            return;
+        launch(k_begin, 1, 1, st, build_lists ? 0 : 1);
+        const size_t stride = (size_t)g.nx + g.ny;
+        Field4 ins[3] = {q, q2, q1};
+        for (int fs = 0; fs < kStages; ++fs) {
+            const double* rin = tin ? tin + fs * stride : nullptr;
+            double* rout = tout ? tout + fs * stride : nullptr;
+            double* rx = rout ? rout : ax[fs];
+            double* ry = rout ? rout + g.ny : ay[fs];
+            if (tin) enq_bc(ins[fs], st);
+            else enq_bc(ins[fs], st, -1, rx, ry);
+            if (save) copy_field(save[fs], ins[fs]);
+            if (!tin) enq_alpha(ins[fs], 3 - fs, fs, false, rx, ry);
+            if (fs == 0) {
+                launch(k_dt, 1, 1, g, st);
+                if (build_lists) {
+                    ListArgs la;
+                    for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
+                    dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
+                    launch(k_lists, grid, 256, g, m, lvl[2], lvl[1], lvl[0], la, st);
+                }
+            }
+            const double* fx_a = tin ? rin : rx;
+            const double* fy_a = tin ? rin + g.ny : ry;
+            enq_faces_update(fs, ins[fs], fs == 0 ? q2 : q1, fx_a, fy_a);
         }
-        enq_alpha(f, bit, stage, false);
-        if (tout) {
-            cudaMemcpyAsync(tout + o, ax[stage], sizeof(double) * g.ny, cudaMemcpyDeviceToDevice, stream);
-            cudaMemcpyAsync(tout + o + g.ny, ay[stage], sizeof(double) * g.nx, cudaMemcpyDeviceToDevice, stream);
-        }
-    }
-
-    void enq_frozen_step(const double* tin, double* tout, const Field4* save)
-    {
-        launch(k_begin, 1, 1, st);
-        enq_bc(q, st, 0);
-        if (save) copy_field(save[0], q);
-        enq_alpha_frozen(q, 3, 0, tin, tout);
-        launch(k_dt, 1, 1, g, st);
-        {
-            ListArgs la;
-            for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
-            dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
-            launch(k_lists, grid, 256, g, m, lvl[2], lvl[1], lvl[0], la, st);
-        }
-        enq_faces_update(0, q, q2);
-        enq_bc(q2, st, 1);
-        if (save) copy_field(save[1], q2);
-        enq_alpha_frozen(q2, 2, 1, tin, tout);
-        enq_faces_update(1, q2, q1);
-        enq_bc(q1, st, 2);
-        if (save) copy_field(save[2], q1);
-        enq_alpha_frozen(q1, 1, 2, tin, tout);
-        enq_faces_update(2, q1, q1);
         launch(k_finish, 1, 1, st);
     }
 
@@ -2591,7 +2612,7 @@ struct Solver2D {
         cudaEventRecord(e0, stream);
         for (int s = 0; s < n; ++s) {
             double* row = tape + (size_t)s * tape_stride();
-            enq_frozen_step(mode == 2 ? row : nullptr, mode == 1 ? row : nullptr, nullptr);
+            enq_frozen_step(mode == 2 ? row : nullptr, mode == 1 ? row : nullptr, nullptr, s == 0);
         }
         cudaEventRecord(e1, stream);
         AWCM_CUDA_TRY(cudaGetLastError());
@@ -2675,7 +2696,8 @@ struct Solver2D {
         for (int s = 0; s < n; ++s) {
             if (!keep_all && s % every == 0) copy_field(ckpt[s / every], q);
             double* row = tape + (size_t)s * tape_stride();
-            enq_frozen_step(mode == 2 ? row : nullptr, mode == 1 ? row : nullptr, keep_all ? &seg[3 * s] : nullptr);
+            enq_frozen_step(mode == 2 ? row : nullptr, mode == 1 ? row : nullptr, keep_all ? &seg[3 * s] : nullptr,
+                            s == 0);
         }
         adj_launch_seed(g, q, m, target, lam, rowsum, loss_dev, stream);
         cudaEventRecord(ev[1], stream);
@@ -2689,7 +2711,7 @@ struct Solver2D {
                 const double tk = t0 + s0 * dt;
                 cudaMemcpyAsync(&st->t, &tk, sizeof(double), cudaMemcpyHostToDevice, stream);
                 for (int s = s0; s < s1; ++s)
-                    enq_frozen_step(tape + (size_t)s * tape_stride(), nullptr, &seg[3 * (s - s0)]);
+                    enq_frozen_step(tape + (size_t)s * tape_stride(), nullptr, &seg[3 * (s - s0)], false);
             }
             for (int s = s1 - 1; s >= s0; --s)
                 enq_adjoint_step(&seg[3 * (s - s0)], tape + (size_t)s * tape_stride());
@@ -2966,6 +2988,15 @@ int awcm2d_advance(awcm2d_t h, double tol, double cfl, double t_start, double t_
     AWCM_EULER_ONLY(h);
     if (n_steps < 0) return awcm::kErrArg;
     return h->s.advance(tol, cfl, t_start, t_end, n_steps, out);
+}
+int awcm2d_step_io_bytes(awcm2d_t h, long long* h2d, long long* d2h)
+{
+    if (!h || !h2d || !d2h) return awcm::kErrArg;
+    // awcm2d_step: the step scalars are read back, updated and written (one copy each way), and
+    // the step's results read after the graph (a second copy back)
+    *h2d = (long long)sizeof(awcm::StepState);
+    *d2h = 2LL * (long long)sizeof(awcm::StepState);
+    return awcm::kOk;
 }
 int awcm2d_launches_per_step(awcm2d_t h, int* n)
 {

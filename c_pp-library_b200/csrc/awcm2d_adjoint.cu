@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <utility>
 
 #include "awcm_b200.h"
 #include "awcm2d_types.cuh"
@@ -25,6 +26,30 @@ namespace awcm {
 namespace {
 
 __device__ __forceinline__ unsigned gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+
+// Programmatic dependent launch, as for the forward kernels: the successor's CTAs are scheduled
+// once all of this kernel's CTAs run and wait in griddepcontrol.wait (a hardware wait on the
+// predecessor's completion) before their first access; no-ops without the launch attribute.
+__device__ __forceinline__ void pdl_begin()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... P, typename... A>
+void launch_pdl(void (*kern)(P...), dim3 grid, dim3 block, cudaStream_t s, A&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
 
 __device__ __forceinline__ void atomic_sub(double* p, double v)
 {
@@ -332,6 +357,7 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjStage A, const uint32_t* __
                                                   const unsigned* __restrict__ count,
                                                   const double* __restrict__ alpha)
 {
+    pdl_begin();
     const Grid2& g = A.g;
     const unsigned n = *count;
     const unsigned stride = gridDim.x * blockDim.x;
@@ -378,6 +404,7 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjStage A, const uint32_t* __
 // one-sided forms at the edges; same branch selection as the forward).
 __global__ void __launch_bounds__(256) k_adj_coarse(AdjStage A)
 {
+    pdl_begin();
     const Grid2& g = A.g;
     const unsigned n = *A.ncrs;
     const unsigned stride = gridDim.x * blockDim.x;
@@ -438,6 +465,7 @@ __global__ void k_adj_rk(int stage, Grid2 g, size_t plane, const uint8_t* __rest
                          const int8_t* __restrict__ lvl, const double* __restrict__ sc, Field4 lam_next, Field4 lam_n,
                          Field4 lam_in, Field4 nu)
 {
+    pdl_begin();
     const unsigned a = gtid();
     if (a >= plane) return;
     const int i = (int)(a % (unsigned)g.pitch) - kGhost, j = (int)(a / (unsigned)g.pitch) - kGhost;
@@ -472,6 +500,7 @@ __global__ void k_adj_rk(int stage, Grid2 g, size_t plane, const uint8_t* __rest
 // thread, so sources are updated atomically.
 __global__ void k_adj_fold(Grid2 g, Field4 lam)
 {
+    pdl_begin();
     const int t = (int)gtid();
     const int NX = g.nx - 1, NY = g.ny - 1;
     const bool per = g.bc_kind == AWCM_BC_PERIODIC, dm = g.bc_kind == AWCM_BC_DOUBLE_MACH;
@@ -515,6 +544,7 @@ __global__ void k_adj_fold(Grid2 g, Field4 lam)
 __global__ void k_adj_seed(Grid2 g, Field4 q, const uint8_t* __restrict__ m, const double* __restrict__ target,
                            Field4 lam, double* rowsum)
 {
+    pdl_begin();
     const int j = (int)gtid();
     if (j >= g.ny) return;
     double acc = 0;
@@ -530,6 +560,7 @@ __global__ void k_adj_seed(Grid2 g, Field4 q, const uint8_t* __restrict__ m, con
 
 __global__ void k_sum_rows(const double* rowsum, int n, double* loss)
 {
+    pdl_begin();
     if (gtid() != 0) return;
     double s = 0;
     for (int j = 0; j < n; ++j) s += rowsum[j];
@@ -540,28 +571,28 @@ __global__ void k_sum_rows(const double* rowsum, int n, double* loss)
 
 void adj_launch_stage(const AdjStage& a, int face_blocks, cudaStream_t s)
 {
-    k_adj_face<0><<<face_blocks, 128, 0, s>>>(a, a.xf, a.nxf, a.ax);
-    k_adj_face<1><<<face_blocks, 128, 0, s>>>(a, a.yf, a.nyf, a.ay);
-    k_adj_coarse<<<face_blocks / 2, 256, 0, s>>>(a);
+    launch_pdl(k_adj_face<0>, face_blocks, 128, s, a, a.xf, a.nxf, a.ax);
+    launch_pdl(k_adj_face<1>, face_blocks, 128, s, a, a.yf, a.nyf, a.ay);
+    launch_pdl(k_adj_coarse, face_blocks / 2, 256, s, a);
 }
 
 void adj_launch_rk(int stage, const Grid2& g, size_t plane, const uint8_t* m, const int8_t* lvl, const double* sc,
                    Field4 lam_next, Field4 lam_n, Field4 lam_in, Field4 nu, cudaStream_t s)
 {
-    k_adj_rk<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(stage, g, plane, m, lvl, sc, lam_next, lam_n, lam_in, nu);
+    launch_pdl(k_adj_rk, (unsigned)((plane + 255) / 256), 256, s, stage, g, plane, m, lvl, sc, lam_next, lam_n, lam_in, nu);
 }
 
 void adj_launch_fold(const Grid2& g, Field4 lam, cudaStream_t s)
 {
     const int n = g.nx + g.ny;
-    k_adj_fold<<<(n + 127) / 128, 128, 0, s>>>(g, lam);
+    launch_pdl(k_adj_fold, (n + 127) / 128, 128, s, g, lam);
 }
 
 void adj_launch_seed(const Grid2& g, Field4 q, const uint8_t* m, const double* target, Field4 lam, double* rowsum,
                      double* loss, cudaStream_t s)
 {
-    k_adj_seed<<<(g.ny + 127) / 128, 128, 0, s>>>(g, q, m, target, lam, rowsum);
-    k_sum_rows<<<1, 32, 0, s>>>(rowsum, g.ny, loss);
+    launch_pdl(k_adj_seed, (g.ny + 127) / 128, 128, s, g, q, m, target, lam, rowsum);
+    launch_pdl(k_sum_rows, 1, 32, s, (const double*)rowsum, g.ny, loss);
 }
 
 }  // namespace awcm

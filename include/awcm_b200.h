@@ -131,6 +131,8 @@ int awcm2d_profile_step(awcm2d_t h, double tol, double cfl, double t, double t_e
  * cap launches in launch order; *n = launches recorded.  Instrumentation only. */
 int awcm2d_profile_kernels(awcm2d_t h, double tol, double cfl, double t, double t_end, int cap, char* names,
                            double* ms, int* n);
+/* Host<->device bytes one awcm2d_step call moves (step scalars in, results out; instrumentation). */
+int awcm2d_step_io_bytes(awcm2d_t h, long long* h2d, long long* d2h);
 /* Kernel launches enqueued by one step (for instrumentation). */
 int awcm2d_launches_per_step(awcm2d_t h, int* n);
 /* PrepareEuler execution: 1 = one kernel launch per pass (default), 0 = one persistent
