@@ -496,75 +496,102 @@ __global__ void k_adj_rk(int stage, Grid2 g, size_t plane, const uint8_t* __rest
 // Adjoint of the boundary fill: every ghost's adjoint moves to the interior point it was copied
 // from (transmissive: the edge point; periodic: the wrapped point; double Mach: the transmissive
 // right edge and the reflecting bottom for x > 1/6, sign flip on rho v; shock-vortex: the
-// reflecting bottom and top, sign flip on rho v; prescribed states carry no adjoint).  One thread per edge line; a corner source is shared by a row thread and a column
-// thread, so sources are updated atomically.
+// reflecting bottom and top, sign flip on rho v; prescribed states carry no adjoint).  One thread
+// per ghost cell of the edge strips; several ghosts share a source (and the corner points are the
+// source of a row ghost and a column ghost), so sources are updated atomically.
 __global__ void k_adj_fold(Grid2 g, Field4 lam)
 {
     pdl_begin();
-    const int t = (int)gtid();
+    const long t = (long)gtid();
     const int NX = g.nx - 1, NY = g.ny - 1;
     const bool per = g.bc_kind == AWCM_BC_PERIODIC, dm = g.bc_kind == AWCM_BC_DOUBLE_MACH;
     const bool sv = g.bc_kind == AWCM_BC_SHOCK_VORTEX;  // walls at the bottom and top: rho v flips
-    if (t < g.ny) {
-        const int j = t;
-        for (int c = 0; c < kGhost; ++c) {
-            const size_t gl = g.at(-1 - c, j), gr = g.at(NX + 1 + c, j);
-            const size_t sl = g.at(per ? NX - c : 0, j), sr = g.at(per ? c : NX, j);
-            for (int k = 0; k < 4; ++k) {
-                if (!dm) atomic_add(&lam.p[k][sl], lam.p[k][gl]);
-                lam.p[k][gl] = 0;
-                atomic_add(&lam.p[k][sr], lam.p[k][gr]);
-                lam.p[k][gr] = 0;
-            }
+    const long nside = (long)kGhost * g.ny, nbt = (long)kGhost * g.nx;
+    size_t gh, src;
+    bool take = true;    // false: a prescribed state, the adjoint is dropped
+    double sg2 = 1.0;    // sign applied to component 2 (rho v)
+    if (t < 2 * nside) {
+        const bool right = t >= nside;
+        const long r = right ? t - nside : t;
+        const int j = (int)(r / kGhost), c = (int)(r % kGhost);
+        if (!right) {
+            gh = g.at(-1 - c, j);
+            src = g.at(per ? NX - c : 0, j);
+            take = !dm;
+        } else {
+            gh = g.at(NX + 1 + c, j);
+            src = g.at(per ? c : NX, j);
         }
-    } else if (t < g.ny + g.nx) {
-        const int i = t - g.ny;
-        const double x = g.x_min + i * g.dx;
-        for (int c = 0; c < kGhost; ++c) {
-            const size_t gb = g.at(i, -1 - c), gt = g.at(i, NY + 1 + c);
-            const size_t sb = g.at(i, per ? NY - c : 0), st = g.at(i, per ? c : NY);
-            for (int k = 0; k < 4; ++k) {
-                if (dm) {
-                    if (x > 1.0 / 6.0) atomic_add(&lam.p[k][sb], (k == 2 ? -1.0 : 1.0) * lam.p[k][gb]);
-                } else {
-                    const double sg = (sv && k == 2) ? -1.0 : 1.0;
-                    atomic_add(&lam.p[k][sb], sg * lam.p[k][gb]);
-                    atomic_add(&lam.p[k][st], sg * lam.p[k][gt]);
-                }
-                lam.p[k][gb] = 0;
-                lam.p[k][gt] = 0;
-            }
+    } else if (t < 2 * nside + 2 * nbt) {
+        const long r0 = t - 2 * nside;
+        const bool top = r0 >= nbt;
+        const long r = top ? r0 - nbt : r0;
+        const int i = (int)(r / kGhost), c = (int)(r % kGhost);
+        if (!top) {
+            gh = g.at(i, -1 - c);
+            src = g.at(i, per ? NY - c : 0);
+            if (dm) take = g.x_min + i * g.dx > 1.0 / 6.0;
+            if (dm || sv) sg2 = -1.0;
+        } else {
+            gh = g.at(i, NY + 1 + c);
+            src = g.at(i, per ? c : NY);
+            take = !dm;
+            if (sv) sg2 = -1.0;
         }
+    } else {
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double v = lam.p[k][gh];
+        if (take) atomic_add(&lam.p[k][src], (k == 2 ? sg2 : 1.0) * v);
+        lam.p[k][gh] = 0;
     }
 }
 
 // Loss and seed over the active points (mask0; the other points carry no solution value):
-// rowsum[j] = sum_i (rho - target)^2 / 2 in order of i; lam = rho - target on mask0 points
-// (component 0), 0 elsewhere.
-__global__ void k_adj_seed(Grid2 g, Field4 q, const uint8_t* __restrict__ m, const double* __restrict__ target,
-                           Field4 lam, double* rowsum)
+// lam = rho - target on mask0 points (component 0), 0 elsewhere on the grid; the loss
+// 1/2 sum (rho - target)^2 is reduced in a fixed order (one CTA per row: strided partial sums, then
+// a shared-memory tree; the rows likewise), so it is reproducible from run to run.
+constexpr int kSeedThreads = 256;
+__device__ __forceinline__ double block_sum_fixed(double v, double* sh)
+{
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = kSeedThreads / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    return sh[0];
+}
+
+__global__ void __launch_bounds__(kSeedThreads) k_adj_seed(Grid2 g, Field4 q, const uint8_t* __restrict__ m,
+                                                            const double* __restrict__ target, Field4 lam,
+                                                            double* rowsum)
 {
     pdl_begin();
-    const int j = (int)gtid();
-    if (j >= g.ny) return;
+    __shared__ double sh[kSeedThreads];
+    const int j = (int)blockIdx.x;
     double acc = 0;
-    for (int i = 0; i < g.nx; ++i) {
+    for (int i = threadIdx.x; i < g.nx; i += kSeedThreads) {
         const size_t a = g.at(i, j);
         const double d = (m[a] & 1u) ? q.p[0][a] - target[(size_t)j * g.nx + i] : 0.0;
         acc += 0.5 * d * d;
         lam.p[0][a] = d;
         lam.p[1][a] = lam.p[2][a] = lam.p[3][a] = 0;
     }
-    rowsum[j] = acc;
+    const double r = block_sum_fixed(acc, sh);
+    if (threadIdx.x == 0) rowsum[j] = r;
 }
 
-__global__ void k_sum_rows(const double* rowsum, int n, double* loss)
+__global__ void __launch_bounds__(kSeedThreads) k_sum_rows(const double* rowsum, int n, double* loss)
 {
     pdl_begin();
-    if (gtid() != 0) return;
-    double s = 0;
-    for (int j = 0; j < n; ++j) s += rowsum[j];
-    *loss = s;
+    __shared__ double sh[kSeedThreads];
+    double acc = 0;
+    for (int j = threadIdx.x; j < n; j += kSeedThreads) acc += rowsum[j];
+    const double r = block_sum_fixed(acc, sh);
+    if (threadIdx.x == 0) *loss = r;
 }
 
 }  // namespace
@@ -584,15 +611,15 @@ void adj_launch_rk(int stage, const Grid2& g, size_t plane, const uint8_t* m, co
 
 void adj_launch_fold(const Grid2& g, Field4 lam, cudaStream_t s)
 {
-    const int n = g.nx + g.ny;
-    launch_pdl(k_adj_fold, (n + 127) / 128, 128, s, g, lam);
+    const long n = 2L * kGhost * (g.nx + g.ny);
+    launch_pdl(k_adj_fold, (unsigned)((n + 255) / 256), 256, s, g, lam);
 }
 
 void adj_launch_seed(const Grid2& g, Field4 q, const uint8_t* m, const double* target, Field4 lam, double* rowsum,
                      double* loss, cudaStream_t s)
 {
-    launch_pdl(k_adj_seed, (g.ny + 127) / 128, 128, s, g, q, m, target, lam, rowsum);
-    launch_pdl(k_sum_rows, 1, 32, s, (const double*)rowsum, g.ny, loss);
+    launch_pdl(k_adj_seed, (unsigned)g.ny, kSeedThreads, s, g, q, m, target, lam, rowsum);
+    launch_pdl(k_sum_rows, 1, kSeedThreads, s, (const double*)rowsum, g.ny, loss);
 }
 
 }  // namespace awcm

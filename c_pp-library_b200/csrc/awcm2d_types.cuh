@@ -52,8 +52,8 @@ void adj_launch_stage(const AdjStage& a, int face_blocks, cudaStream_t s);
 void adj_launch_rk(int stage, const Grid2& g, size_t plane, const uint8_t* m, const int8_t* lvl, const double* sc,
                    Field4 lam_next, Field4 lam_n, Field4 lam_in, Field4 nu, cudaStream_t s);
 void adj_launch_fold(const Grid2& g, Field4 lam, cudaStream_t s);
-// Loss 1/2 sum over the mask0 points of (rho - target)^2 (rows summed in order, then rows in
-// order) and its gradient seed; target: Ny x Nx doubles on the device; rowsum: Ny doubles scratch.
+// Loss 1/2 sum over the mask0 points of (rho - target)^2 (reduced in a fixed order) and its
+// gradient seed; target: Ny x Nx doubles on the device; rowsum: Ny doubles scratch.
 void adj_launch_seed(const Grid2& g, Field4 q, const uint8_t* m, const double* target, Field4 lam, double* rowsum,
                      double* loss, cudaStream_t s);
 
