@@ -62,10 +62,10 @@ __device__ __forceinline__ void atomic_add(double* p, double v)
 
 // ---------------------------------------------------------------------------- WENO-Z reverse
 // Reverse of recon_left<kWenoZ> (WENOZ5::ReconstructLeft, WENOZ.h:75-104): adds d(out)/d(input)
-// times ob to g[0..4] for the inputs (ll, l, c, r, rr).  tau = |b0 - b2| is differentiated as
+// times ob to g[0..4] for the inputs (ll, l, c, r, rr) and returns out itself.  tau = |b0 - b2| is differentiated as
 // sign(b0 - b2); with delta > 0, tau = sqrt((b0 - b2)^2 + delta^2) and dtau = (b0 - b2) / tau.
-__device__ __forceinline__ void recon_left_vjp(double ll, double l, double c, double r, double rr, double ob,
-                                               double eps, double delta, double* g)
+__device__ __forceinline__ double recon_left_vjp(double ll, double l, double c, double r, double rr, double ob,
+                                                 double eps, double delta, double* g)
 {
     const double A0 = c - 2 * r + rr, B0 = 3 * c - 4 * r + rr;
     const double A1 = l - 2 * c + r, B1 = l - r;
@@ -108,6 +108,7 @@ __device__ __forceinline__ void recon_left_vjp(double ll, double l, double c, do
     g[2] += Ab0 + 3 * Bb0 - 2 * Ab1 + Ab2 + 3 * Bb2 + kC11_6 * Pb0 + kC5_6 * Pb1 + kC1_3 * Pb2;
     g[3] += -2 * Ab0 - 4 * Bb0 + Ab1 - Bb1 + kCm7_6 * Pb0 + kCm1_6 * Pb1;
     g[4] += Ab0 + Bb0 + kC1_3 * Pb0;
+    return w0 * P0 + w1 * P1 + w2 * P2;  // the forward value (FMA-contracted: a derivative input only)
 }
 
 // ---------------------------------------------------------------------- physical flux reverse
@@ -214,11 +215,16 @@ __device__ __forceinline__ void inv2_vjp(const RoeAdj& R, const double* b, const
 }
 
 // d(face flux)/d(six cells)^T ob (WENOZ_EULER_SOLVER_2D::ComputeFluxX/Y, WENOZ.h:236-320).
-// Forward values are recomputed here; alpha (the frozen LF speed) has no adjoint.
+// Forward values are recomputed here; alpha (the frozen LF speed) has no adjoint.  The 6 x 4
+// characteristic states and fluxes (and, in place, their adjoints) live in shared memory:
+// `sh` points at this thread's slot, element e at sh[e * kAdjThreads].
+constexpr int kAdjThreads = 128;
 template <int DIR>
 __device__ void face_flux_2d_vjp(const double (&s)[6][4], double alpha, double g, const double* ob, double eps,
-                                 double delta, double (&gs)[6][4])
+                                 double delta, double (&gs)[6][4], double* sh)
 {
+    auto RQs = [&](int p, int k) -> double& { return sh[(p * 4 + k) * kAdjThreads]; };
+    auto RFs = [&](int p, int k) -> double& { return sh[(24 + p * 4 + k) * kAdjThreads]; };
     // ---- forward: Roe average of the face states s[2], s[3] (ROESOLVER.h:49-70)
     const double* L = s[2];
     const double* Rr = s[3];
@@ -238,75 +244,79 @@ __device__ void face_flux_2d_vjp(const double (&s)[6][4], double alpha, double g
     R.c = sqrt(0.4 * (R.H - 0.5 * q2));
     R.kc = 0.4 / (R.c * R.c);
     // ---- forward: characteristic variables and LF split of the six cells
-    double RQ[6][4], RF[6][4], f[6][4];
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
-        flux2<DIR>(s[p], g, f[p]);
-        inv2<DIR>(R.u, R.v, R.H, R.c, R.kc, s[p], RQ[p]);
-        inv2<DIR>(R.u, R.v, R.H, R.c, R.kc, f[p], RF[p]);
-    }
-    // ---- reverse: back-projection out = sum_k S_k r_k
-    double S[4];
+        double f[4], rq[4], rf[4];
+        flux2<DIR>(s[p], g, f);
+        inv2<DIR>(R.u, R.v, R.H, R.c, R.kc, s[p], rq);
+        inv2<DIR>(R.u, R.v, R.H, R.c, R.kc, f, rf);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        double fp[6], fm[6];
-#pragma unroll
-        for (int p = 0; p < 6; ++p) {
-            fp[p] = 0.5 * (RF[p][k] + alpha * RQ[p][k]);
-            fm[p] = 0.5 * (RF[p][k] - alpha * RQ[p][k]);
+        for (int k = 0; k < 4; ++k) {
+            RQs(p, k) = rq[k];
+            RFs(p, k) = rf[k];
         }
-        S[k] = recon_left<kWenoZ>(fp[4], fp[3], fp[2], fp[1], fp[0], eps, delta) +
-               recon_left<kWenoZ>(fm[1], fm[2], fm[3], fm[4], fm[5], eps, delta);
     }
+    // ---- reverse: back-projection out = sum_k S_k r_k.  The adjoints of S depend only on ob
+    // and the Roe state; S itself (needed for the Roe-state adjoints) comes out of the WENO-Z
+    // reverse below, which recomputes the reconstructions anyway.
     const double u = R.u, v = R.v, H = R.H, c = R.c;
     double Sb[4];
-    RoeAdj P{0, 0, 0, 0, 0};
     if (DIR == 0) {
         Sb[0] = ob[0] + ob[1] * (u - c) + ob[2] * v + ob[3] * (H - u * c);
         Sb[1] = ob[2] + ob[3] * v;
         Sb[2] = ob[0] + ob[1] * u + ob[2] * v + ob[3] * 0.5 * q2;
         Sb[3] = ob[0] + ob[1] * (u + c) + ob[2] * v + ob[3] * (H + u * c);
-        P.u += ob[1] * (S[0] + S[2] + S[3]) + ob[3] * (-S[0] * c + S[2] * u + S[3] * c);
-        P.v += ob[2] * (S[0] + S[2] + S[3]) + ob[3] * (S[1] + S[2] * v);
-        P.c += ob[1] * (S[3] - S[0]) + ob[3] * u * (S[3] - S[0]);
     } else {
         Sb[0] = ob[0] + ob[1] * u + ob[2] * (v - c) + ob[3] * (H - v * c);
         Sb[1] = ob[1] + ob[3] * u;
         Sb[2] = ob[0] + ob[1] * u + ob[2] * v + ob[3] * 0.5 * q2;
         Sb[3] = ob[0] + ob[1] * u + ob[2] * (v + c) + ob[3] * (H + v * c);
-        P.u += ob[1] * (S[0] + S[2] + S[3]) + ob[3] * (S[1] + S[2] * u);
-        P.v += ob[2] * (S[0] + S[2] + S[3]) + ob[3] * (-S[0] * c + S[2] * v + S[3] * c);
-        P.c += ob[2] * (S[3] - S[0]) + ob[3] * v * (S[3] - S[0]);
     }
-    P.H += ob[3] * (S[0] + S[3]);
     // ---- reverse: WENO-Z reconstructions and the LF split, per characteristic field
-    double RQb[6][4], RFb[6][4];
+    double S[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         double fp[6], fm[6], fpb[6] = {0, 0, 0, 0, 0, 0}, fmb[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int p = 0; p < 6; ++p) {
-            fp[p] = 0.5 * (RF[p][k] + alpha * RQ[p][k]);
-            fm[p] = 0.5 * (RF[p][k] - alpha * RQ[p][k]);
+            fp[p] = 0.5 * (RFs(p, k) + alpha * RQs(p, k));
+            fm[p] = 0.5 * (RFs(p, k) - alpha * RQs(p, k));
         }
         // left_r = ReconstructLeft(fp4, fp3, fp2, fp1, fp0); right_l = ReconstructLeft(fm1..fm5)
         double gl[5] = {0, 0, 0, 0, 0}, gr[5] = {0, 0, 0, 0, 0};
-        recon_left_vjp(fp[4], fp[3], fp[2], fp[1], fp[0], Sb[k], eps, delta, gl);
-        recon_left_vjp(fm[1], fm[2], fm[3], fm[4], fm[5], Sb[k], eps, delta, gr);
+        S[k] = recon_left_vjp(fp[4], fp[3], fp[2], fp[1], fp[0], Sb[k], eps, delta, gl) +
+               recon_left_vjp(fm[1], fm[2], fm[3], fm[4], fm[5], Sb[k], eps, delta, gr);
         fpb[4] += gl[0], fpb[3] += gl[1], fpb[2] += gl[2], fpb[1] += gl[3], fpb[0] += gl[4];
         fmb[1] += gr[0], fmb[2] += gr[1], fmb[3] += gr[2], fmb[4] += gr[3], fmb[5] += gr[4];
 #pragma unroll
-        for (int p = 0; p < 6; ++p) {
-            RFb[p][k] = 0.5 * (fpb[p] + fmb[p]);
-            RQb[p][k] = 0.5 * alpha * (fpb[p] - fmb[p]);
+        for (int p = 0; p < 6; ++p) {  // column k is not read again: its adjoints replace it
+            RFs(p, k) = 0.5 * (fpb[p] + fmb[p]);
+            RQs(p, k) = 0.5 * alpha * (fpb[p] - fmb[p]);
         }
     }
+    RoeAdj P{0, 0, 0, 0, 0};
+    if (DIR == 0) {
+        P.u += ob[1] * (S[0] + S[2] + S[3]) + ob[3] * (-S[0] * c + S[2] * u + S[3] * c);
+        P.v += ob[2] * (S[0] + S[2] + S[3]) + ob[3] * (S[1] + S[2] * v);
+        P.c += ob[1] * (S[3] - S[0]) + ob[3] * u * (S[3] - S[0]);
+    } else {
+        P.u += ob[1] * (S[0] + S[2] + S[3]) + ob[3] * (S[1] + S[2] * u);
+        P.v += ob[2] * (S[0] + S[2] + S[3]) + ob[3] * (-S[0] * c + S[2] * v + S[3] * c);
+        P.c += ob[2] * (S[3] - S[0]) + ob[3] * v * (S[3] - S[0]);
+    }
+    P.H += ob[3] * (S[0] + S[3]);
     // ---- reverse: characteristic projections and physical fluxes
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
-        double fb[4] = {0, 0, 0, 0};
-        inv2_vjp<DIR>(R, s[p], RQb[p], gs[p], P);
-        inv2_vjp<DIR>(R, f[p], RFb[p], fb, P);
+        double f[4], fb[4] = {0, 0, 0, 0}, rqb[4], rfb[4];
+        flux2<DIR>(s[p], g, f);  // recomputed rather than kept live across the WENO-Z reverse
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            rqb[k] = RQs(p, k);
+            rfb[k] = RFs(p, k);
+        }
+        inv2_vjp<DIR>(R, s[p], rqb, gs[p], P);
+        inv2_vjp<DIR>(R, f, rfb, fb, P);
         flux2_vjp<DIR>(s[p], g, fb, gs[p]);
     }
     // ---- reverse: Roe average (kc = 0.4 / c^2, c = sqrt(0.4 (H - q2/2)))
@@ -352,12 +362,16 @@ __device__ __forceinline__ bool fin_point(const Grid2& g, const uint8_t* m, cons
 // Face VJP over the stage's face list: the weight of face f (between f and f+1 along DIR) is
 // nu(f) for a finest-level point f (R_f += F_f) minus nu(f+1) for a finest point f+1
 // (R_{f+1} -= F_f); lam -= weight . dF_f/dcells.
+#ifndef AWCM_ADJ_MIN_CTAS
+#define AWCM_ADJ_MIN_CTAS 1  // 255 registers and 2 CTAs per SM; forcing more CTAs spills and runs slower
+#endif
 template <int DIR>
-__global__ void __launch_bounds__(128) k_adj_face(AdjStage A, const uint32_t* __restrict__ list,
+__global__ void __launch_bounds__(kAdjThreads, AWCM_ADJ_MIN_CTAS) k_adj_face(AdjStage A, const uint32_t* __restrict__ list,
                                                   const unsigned* __restrict__ count,
                                                   const double* __restrict__ alpha)
 {
     pdl_begin();
+    __shared__ double sh[48 * kAdjThreads];
     const Grid2& g = A.g;
     const unsigned n = *count;
     const unsigned stride = gridDim.x * blockDim.x;
@@ -390,7 +404,7 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjStage A, const uint32_t* __
             }
         }
         const double al = DIR == 0 ? alpha[jj] : alpha[ii];
-        face_flux_2d_vjp<DIR>(s, al, g.gamma, w, g.wz_eps, g.wz_delta, gs);
+        face_flux_2d_vjp<DIR>(s, al, g.gamma, w, g.wz_eps, g.wz_delta, gs, sh + threadIdx.x);
 #pragma unroll
         for (int p = 0; p < 6; ++p) {
             const long a = (long)idx + (p - 2) * step;
@@ -598,8 +612,8 @@ __global__ void __launch_bounds__(kSeedThreads) k_sum_rows(const double* rowsum,
 
 void adj_launch_stage(const AdjStage& a, int face_blocks, cudaStream_t s)
 {
-    launch_pdl(k_adj_face<0>, face_blocks, 128, s, a, a.xf, a.nxf, a.ax);
-    launch_pdl(k_adj_face<1>, face_blocks, 128, s, a, a.yf, a.nyf, a.ay);
+    launch_pdl(k_adj_face<0>, face_blocks, kAdjThreads, s, a, a.xf, a.nxf, a.ax);
+    launch_pdl(k_adj_face<1>, face_blocks, kAdjThreads, s, a, a.yf, a.nyf, a.ay);
     launch_pdl(k_adj_coarse, face_blocks / 2, 256, s, a);
 }
 
