@@ -56,9 +56,17 @@ __device__ __forceinline__ double recon_left(double ll, double l, double c, doub
     } else {
         const double eps = wz_eps;
         const double tau = wz_delta > 0 ? sqrt(sqr(b0 - b2) + sqr(wz_delta)) : absd(b0 - b2);
-        a0 = 0.1 * (1 + tau / (b0 + eps));
-        a1 = 0.6 * (1 + tau / (b1 + eps));
-        a2 = 0.3 * (1 + tau / (b2 + eps));
+        const double d0 = b0 + eps, d1 = b1 + eps, d2 = b2 + eps;
+        if (tau == 0 && d0 > 0 && d1 > 0 && d2 > 0) {
+            // tau / d_k is a signed zero and 1 + (+-0) = 1, so a_k = d_k exactly: the three
+            // divisions are skipped (a zero quotient sends IEEE division down its slow path,
+            // and piecewise-constant stencils make tau = 0 common).
+            a0 = 0.1, a1 = 0.6, a2 = 0.3;
+        } else {
+            a0 = 0.1 * (1 + tau / d0);
+            a1 = 0.6 * (1 + tau / d1);
+            a2 = 0.3 * (1 + tau / d2);
+        }
     }
     const double s = a0 + a1 + a2;
     const double w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
