@@ -1076,6 +1076,52 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
     }
 }
 
+// The same LF speeds over a mask whose points are already listed: the union of a stage's
+// finest-level and coarse point lists is exactly the grid points of that stage's mask, so stage 2
+// (mask2) reads the lists of stage 1's update and stage 3 (mask1) those of stage 2's.  One point
+// per lane; the row maximum is a segmented max-scan over runs of equal rows in the warp (lists
+// are row-ordered within each warp segment) with one atomic per run, the column maximum one
+// atomic per point.  Maxima are order-independent, so the result equals k_alpha's.
+__global__ void __launch_bounds__(256) k_alpha_list(Grid2 g, Field4 f, const uint32_t* __restrict__ la,
+                                                    const unsigned* __restrict__ na,
+                                                    const uint32_t* __restrict__ lb,
+                                                    const unsigned* __restrict__ nb, double* ax, double* ay,
+                                                    const StepState* st)
+{
+    pdl_begin();
+    if (st->done) return;
+    const unsigned n0 = *na, n = n0 + *nb;
+    const int lane = threadIdx.x & 31;
+    const unsigned stride = gridDim.x * blockDim.x;
+    for (unsigned base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const unsigned e = base + (unsigned)lane;
+        const bool on = e < n;
+        int j = -1;
+        double sx = 0;
+        if (on) {
+            const uint32_t idx = e < n0 ? la[e] : lb[e - n0];
+            const int i = (int)(idx % (uint32_t)g.pitch) - kGhost;
+            j = (int)(idx / (uint32_t)g.pitch) - kGhost;
+            const double q[4] = {f.p[0][idx], f.p[1][idx], f.p[2][idx], f.p[3][idx]};
+            const double c = sound2(q, g.gamma);
+            sx = absd(q[1] / q[0]) + c;
+            const double sy = absd(q[2] / q[0]) + c;
+            if (sy > 0) atomic_max_nonneg(&ay[i], sy);
+        }
+        const int jp = __shfl_up_sync(0xffffffffu, j, 1);
+        const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || j != jp);
+        const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+        double v = sx;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const double o = __shfl_up_sync(0xffffffffu, v, off);
+            if (lane - off >= start) v = maxd(v, o);
+        }
+        const int jn = __shfl_down_sync(0xffffffffu, j, 1);
+        if (on && (lane == 31 || jn != j) && v > 0) atomic_max_nonneg(&ax[j], v);
+    }
+}
+
 // dt = cfl dx / max speed, clipped to the output time (main_2d_euler(quad).cpp:76-83), and the
 // per-level stage factor dt / (dx 2^(maxl-lev)) of the RK updates.
 __global__ void k_dt(Grid2 g, StepState* st)
@@ -2047,6 +2093,16 @@ struct Solver2D {
         after("k_alpha");
         launches += 1;
     }
+    // Stage `stage` (1 or 2) over the points of the previous stage's update lists (its mask).
+    void enq_alpha_listed(Field4 f, int stage, double* axp = nullptr, double* ayp = nullptr)
+    {
+        const int ls = stage - 1;
+        const unsigned* C = st->cnt + 4 * ls;
+        launch(k_alpha_list, face_blocks / 2, 256, g, f, lists[4 * ls], C, lists[4 * ls + 1], C + 1,
+               axp ? axp : ax[stage], ayp ? ayp : ay[stage], st);
+        after("k_alpha_list");
+        launches += 1;
+    }
 
     // Face fluxes and point updates of one stage; the LF speeds come from ax[stage] / ay[stage],
     // or from (axp, ayp) when given.
@@ -2116,10 +2172,10 @@ struct Solver2D {
         }
         enq_faces_update(0, q, q2);
         enq_bc(q2, st, 1);
-        enq_alpha(q2, 2, 1, false);
+        enq_alpha_listed(q2, 1);
         enq_faces_update(1, q2, q1);
         enq_bc(q1, st, 2);
-        enq_alpha(q1, 1, 2, false);
+        enq_alpha_listed(q1, 2);
         enq_faces_update(2, q1, q1);
         launch(k_remove_residue, blocks_for(words(), 256), 256, g, q, m, 0, 1, st);
         after("k_remove_residue");
@@ -2503,7 +2559,10 @@ struct Solver2D {
             if (tin) enq_bc(ins[fs], st);
             else enq_bc(ins[fs], st, -1, rx, ry);
             if (save) copy_field(save[fs], ins[fs]);
-            if (!tin) enq_alpha(ins[fs], 3 - fs, fs, false, rx, ry);
+            if (!tin) {
+                if (fs == 0) enq_alpha(ins[fs], 3, fs, false, rx, ry);
+                else enq_alpha_listed(ins[fs], fs, rx, ry);
+            }
             if (fs == 0) {
                 launch(k_dt, 1, 1, g, st);
                 if (build_lists) {
