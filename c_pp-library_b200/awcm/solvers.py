@@ -21,6 +21,8 @@ AAZ, CR, APD, CL, RR, BAND = 0, 1, 2, 3, 4, 5
 BC_TRANSMISSIVE, BC_DOUBLE_MACH, BC_PERIODIC = 0, 1, 2
 PROBLEM_QUADRANTS, PROBLEM_DOUBLE_MACH, PROBLEM_VORTEX = 0, 1, 2
 WENOZ, WENO5 = 0, 1
+# 1D scalar AWCM (the path of Wavelet/main_1d_advect.cpp): a batch scheme like the two above.
+SCALAR_ADVECTION = 2
 
 
 def measure_fp64_peak(iters: int = 20000, repeats: int = 5) -> float:
@@ -383,6 +385,47 @@ class AWCM1DBatch:
         s = c_void_p()
         call("awcm1d_batch_stream", self.h, ctypes.byref(s))
         return s.value or 0
+
+
+class AWCM1DScalar:
+    """Scalar 1D AWCM instances (the path of Wavelet/main_1d_advect.cpp:48-224): one field advected
+    with unit speed at a fixed dt, batched like the Euler instances (scheme SCALAR_ADVECTION)."""
+
+    def __init__(self, num_levels, nx_coarse, x_min, x_max):
+        self.b = AWCM1DBatch(num_levels, nx_coarse, x_min, x_max, 1.4, SCALAR_ADVECTION)
+        self.n, self.nx = self.b.n, self.b.nx
+        self._t = np.zeros(self.n)
+
+    def set_q(self, k, q):
+        """q: the field at the Nx + 6 points -3 .. Nx+2 (ghosts included)."""
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.nx[k] + 6)
+        full = np.zeros((self.nx[k] + 6, 3))
+        full[:, 0] = q
+        self.b.set_q(k, full)
+
+    def get_q(self, k):
+        return np.ascontiguousarray(self.b.get_q(k)[:, 0])
+
+    def get_masks(self, k):
+        return self.b.get_masks(k)
+
+    def get_levels(self, k):
+        return self.b.get_levels(k)
+
+    def advance(self, tol, dt: float, n_steps: int):
+        """n_steps driver passes of every instance at the fixed dt (one dt for the batch: the
+        driver's 0.5 dx is the caller's choice); returns the per-instance time."""
+        self.b.set_run(tol, 0.0, self._t, np.inf, float(dt))
+        self.b.steps(n_steps)
+        self.b.sync()
+        self._t = np.array([self.b.status(k)[0] for k in range(self.n)])
+        return self._t.copy()
+
+    def status(self, k):
+        return self.b.status(k)
+
+    def totals(self):
+        return self.b.totals()
 
 
 class AWCM1D:

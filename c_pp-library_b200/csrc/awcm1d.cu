@@ -513,6 +513,143 @@ __device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, u
     __syncthreads();
 }
 
+// ------------------------------------------------------------------- scalar AWCM (advection)
+// The scalar path of Wavelet/main_1d_advect.cpp:48-224: one field q advected with unit speed at a
+// fixed dt, on the same masks and levels.  q lives in plane 0 of the instance's field; the stage
+// outputs q_2, q_1, q_0 in the three planes of the stage-start copy.
+
+// AWCM_1D::Prepare (Wavelet/AWCM_1D.h:45-72): WAVELET_1D::ForwardWaveletTransform
+// (WAVELET_1D.h:90-144, the arithmetic of the Euler form on its density), banding, then the
+// mask/level chain without PrepareEuler's adjacent zones on mask1..mask3, the inverse transform
+// (WAVELET_1D.h:146-196) and no interpolation of new points.
+__device__ void prepare1_scalar(const Ctx& c)
+{
+    fwt1(c);
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
+        if (!(3 <= i && i <= c.N1 - 3)) c.set(i, 0);
+    __syncthreads();
+    copy_bit1(c, 0, kBitCopy, false);
+    aaz1(c, 0, kBitCopy);
+    cr1(c, 0);
+    for (int k = 1; k <= 3; ++k) {
+        cl1(c, k - 1, k - 1, k);  // level_{k-1} of mask_{k-1}; mask_k = mask_{k-1}
+        copy_bit1(c, k, kBitCopy, false);
+        apd1(c, k, k - 1);        // AddPointForDifferentiation(mask_k, level_{k-1})
+        cr1(c, k);
+    }
+    cl1(c, 3, 3, -1);
+    iwt1(c, 3);
+}
+
+// Coarse-level derivative of the field with the driver's branch selection (main_1d_advect.cpp:
+// 62-83): AWCM_1D::Differentiate and the 4-point DifferentiateAtLeftBoundary (Wavelet/AWCM_1D.h:
+// 127-135), the right edge by the left form on the mirrored stencil as the driver calls it.  The
+// driver's two 6-argument DifferentiateAtLeftBoundary calls (i == 2 dx_, i + 2 dx_ == i_end) name
+// no scalar overload of AWCM_1D (the driver does not compile as shipped); they take the 5-point
+// form of the vector counterpart, DifferentiateEulerAtLeftBoundary (AWCM_1D.h:174-185), with the
+// identity flux of unit-speed advection.
+__device__ double coarse_d1_scalar(const Ctx& c, const double* in, int i, int d)
+{
+    auto Q = [&](int ii) { return in[ii + kGhost]; };
+    const int iend = c.N1;
+    if (i - 2 * d > 0 && i + 2 * d < iend) return kD1 * (Q(i + d) - Q(i - d)) + kD2 * (Q(i + 2 * d) - Q(i - 2 * d));
+    if (i - 2 * d < 0) return kD1 * (Q(i + d) - Q(i - d)) + kD2 * (Q(i + 2 * d) - Q(i - d));
+    if (i == 2 * d)
+        return kD02 * Q(i - 2 * d) + kD12 * Q(i - d) + kD22 * Q(i) + kD32 * Q(i + d) + kD2 * Q(i + 2 * d);
+    if (i + 2 * d > iend) return kD1 * (Q(i - d) - Q(i + d)) + kD2 * (Q(i - 2 * d) - Q(i + d));
+    return kD02 * Q(i + 2 * d) + kD12 * Q(i + d) + kD22 * Q(i) + kD32 * Q(i - d) + kD2 * Q(i - 2 * d);
+}
+
+// One scalar stage (main_1d_advect.cpp:50-99, :100-155, :164-212): out = in (the whole line),
+// then at the points of mask b (level set l) out(i) -= dt (F_r - F_l) / (dx dx_) on the finest
+// level, F_r = WENO5::ReconstructRight(in(i-2..i+2)) (WENO.h:101-104; the face i+1/2 is shared by
+// points i and i+1, which the reference evaluates twice identically), or out(i) -= dt / (dx dx_)
+// dF below it; then the driver's ghost copies of the end points.
+__device__ void stage1_scalar(const Ctx& c, const double* in, double* out, int b, int l, double dt, uint32_t* list,
+                              unsigned* ured)
+{
+    for (int t = threadIdx.x; t < c.w; t += blockDim.x) out[t] = in[t];
+    __syncthreads();
+    auto fin = [&](int i) { return i >= 0 && i <= c.N1 && c.bit(i, b) && c.L(l, i) == c.maxl; };
+    const int nf = block_compact(-1, c.N1, [&](int f) { return fin(f) || fin(f + 1); }, list, ured);
+    for (int e = threadIdx.x; e < nf; e += blockDim.x) {
+        const int f = (int)list[e];
+        const double* v = in + f + kGhost;
+        c.fl[f + kGhost] = recon_left<kWeno5>(v[2], v[1], v[0], v[-1], v[-2]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
+        if (!c.bit(i, b)) continue;
+        const int lev = c.L(l, i);
+        if (lev < 0 || lev > c.maxl) continue;
+        const int d = c.D(lev);
+        if (lev != c.maxl && (i - 2 * d < -kGhost || i + 2 * d > c.N1 + kGhost)) continue;
+        double& o = out[i + kGhost];
+        if (lev == c.maxl) o = o - dt * (c.fl[i + kGhost] - c.fl[i - 1 + kGhost]) / (c.I.dx * d);
+        else o = o - dt / (c.I.dx * d) * coarse_d1_scalar(c, in, i, d);
+    }
+    __syncthreads();
+    if (threadIdx.x < kGhost) {
+        const int g = threadIdx.x + 1;
+        out[kGhost - g] = out[kGhost];
+        out[kGhost + c.N1 + g] = out[kGhost + c.N1];
+    }
+    __syncthreads();
+}
+
+// One pass of the scalar driver loop: Prepare, the three stages at dt = dt_fixed (the driver's
+// 0.5 dx is the caller's choice), the combinations q_1 = 3/4 q + 1/4 q_1 on mask1 (after q_1's
+// ghost copies) and q = 1/3 q + 2/3 q_0 on mask0, and PostProcess (RemoveResidue on mask0).  The
+// ghosts of q itself are never rewritten, as in the driver.
+__device__ void step_ctx_scalar(Inst1& I, const Ctx& c, uint32_t* list, unsigned* ured)
+{
+    prepare1_scalar(c);
+    const double dt = I.dt_fixed;
+    unsigned cnt[4];
+    for (int k = 0; k < 4; ++k) {
+        unsigned v = 0;
+        for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) v += c.bit(i, k);
+        cnt[k] = block_sum(v, ured);
+    }
+    double* q = c.q;
+    double* q2 = c.qc;
+    double* q1 = c.qc + c.w;
+    double* q0 = c.qc + 2 * c.w;
+    stage1_scalar(c, q, q2, 2, 2, dt, list, ured);
+    stage1_scalar(c, q2, q1, 1, 1, dt, list, ured);
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
+        if (c.bit(i, 1)) q1[i + kGhost] = 0.75 * q[i + kGhost] + 0.25 * q1[i + kGhost];
+    __syncthreads();
+    stage1_scalar(c, q1, q0, 0, 0, dt, list, ured);
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
+        if (c.bit(i, 0)) q[i + kGhost] = kC1_3 * q[i + kGhost] + kD1 * q0[i + kGhost];
+    __syncthreads();
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
+        if (!c.bit(i, 0)) q[i + kGhost] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        I.dt = dt;
+        I.mv = 0;
+        I.alpha[0] = I.alpha[1] = I.alpha[2] = 0;
+        I.do_print = 0;
+        for (int k = 0; k < 4; ++k) I.mask_cnt[k] = cnt[k];
+        I.upd += cnt[0];
+        I.steps += 1;
+        I.t += dt;
+        I.done = I.t >= I.t_end;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
+{
+    const int w = I.nx + 2 * kGhost;
+    double* base = P.q + I.q_off;
+    uint8_t* mb = P.m + I.m_off;
+    return Ctx{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + w), P.W, w, I.nx, I.nx - 1,
+               I.maxl};
+}
+
 template <int SCHEME>
 __device__ void step_instance(Inst1& I, const Pool& P, uint32_t* list, double* dred, unsigned* ured)
 {
@@ -542,8 +679,17 @@ __global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, uns
         __syncthreads();
         if (k >= n) break;
         Inst1& I = insts[order[k]];
-        if (I.scheme == kWeno5) step_instance<kWeno5>(I, P, list, dred, ured);
-        else step_instance<kWenoZ>(I, P, list, dred, ured);
+        if (I.scheme == kScalarAdvection) {
+            if (I.t >= I.t_end) {
+                if (threadIdx.x == 0) I.done = 1;
+            } else {
+                step_ctx_scalar(I, make_ctx(I, P), list, ured);
+            }
+        } else if (I.scheme == kWeno5) {
+            step_instance<kWeno5>(I, P, list, dred, ured);
+        } else {
+            step_instance<kWenoZ>(I, P, list, dred, ured);
+        }
         __syncthreads();
     }
 }
@@ -576,7 +722,10 @@ __global__ void k_pass1d(Inst1* insts, int inst, Pool P, int op, int bit, int le
             for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
                 if (!(3 <= i && i <= c.N1 - 3)) c.set(i, bit);
             break;
-        case 10: prepare1(c); break;
+        case 10:
+            if (I.scheme == kScalarAdvection) prepare1_scalar(c);
+            else prepare1(c);
+            break;
         case 11: fwt1(c); break;
         case 12: iwt1(c, bit); break;
         default: break;
@@ -618,7 +767,7 @@ struct Batch1D {
                double gamma, int scheme)
     {
         if (count <= 0 || !num_levels || !nx_coarse || !x_min || !x_max) return kErrArg;
-        if (scheme != kWenoZ && scheme != kWeno5) return kErrArg;
+        if (scheme != kWenoZ && scheme != kWeno5 && scheme != kScalarAdvection) return kErrArg;
         AWCM_CUDA_TRY(cudaGetDevice(&device));
         n = count;
         host.assign(n, Inst1{});

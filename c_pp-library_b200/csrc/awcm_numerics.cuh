@@ -29,7 +29,7 @@ constexpr double kD12 = -0x1.5555555555555p-1;  // -2/3
 constexpr double kD22 = 0.0;
 constexpr double kD32 = 0x1.5555555555555p-1;   // 2/3
 
-enum Scheme : int { kWenoZ = 0, kWeno5 = 1 };
+enum Scheme : int { kWenoZ = 0, kWeno5 = 1, kScalarAdvection = 2 };  // 2: the 1D scalar path only
 
 __device__ __forceinline__ double sqr(double x) { return x * x; }
 __device__ __forceinline__ double absd(double x) { return x < 0 ? -x : x; }

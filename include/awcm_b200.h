@@ -212,7 +212,18 @@ int awcm2d_set_alpha_tape(awcm2d_t h, int n_steps, const double* tape);
  * one instance through PrepareEuler, the three stages and PostProcessEuler); a batch of one is the
  * plain single-instance form of Wavelet/main_1d_euler.cpp:61-260.  Instances are indexed 0..count-1.
  * scheme 0 = WENO-Z face fluxes (WENOZ_EULER_SOLVER_1D::ComputeFlux, WENOZ.h:160-205),
- * scheme 1 = the shipped driver's WENO5 ComputedF (WENO.h:176-184). */
+ * scheme 1 = the shipped driver's WENO5 ComputedF (WENO.h:176-184),
+ * scheme 2 = the scalar AWCM path of Wavelet/main_1d_advect.cpp:48-224 (AWCM_SCALAR_ADVECTION):
+ *   one field advected with unit speed, AWCM_1D::Prepare (Wavelet/AWCM_1D.h:45-72, no adjacent
+ *   zones on mask1..3, no interpolation), WENO5::ReconstructRight faces (WENO.h:101-104) on the
+ *   finest level and AWCM_1D::Differentiate* (AWCM_1D.h:127-140) below it, the driver's stage
+ *   combinations and ghost copies, AWCM_1D::PostProcess.  The field is component 0 of set_q /
+ *   get_q (components 1 and 2 are unused); every step uses dt = dt_fixed of set_run (the driver's
+ *   0.5 dx is the caller's choice) with no CFL and no clipping to t_end, and an instance stops once
+ *   t >= t_end.  The driver's 6-argument DifferentiateAtLeftBoundary calls (:74, :82), which name
+ *   no scalar overload (the driver does not compile as shipped), take the 5-point form of
+ *   DifferentiateEulerAtLeftBoundary (AWCM_1D.h:174-185) on the field. */
+#define AWCM_SCALAR_ADVECTION 2
 typedef struct awcm1d_batch_s* awcm1d_batch_t;
 
 /* x_min/x_max: first and last node of each instance's cell-centred grid (GRID_UNIFORM_1D). */

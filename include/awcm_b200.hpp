@@ -224,6 +224,8 @@ struct EULER_EQUATION_2D {
 
 // ------------------------------------------------------------------------------------------ 1D
 // AWCM_1D (Wavelet/AWCM_1D.h) as a batch of one instance, and the batch itself.
+// scheme AWCM_SCALAR_ADVECTION gives the scalar path of Wavelet/main_1d_advect.cpp (the field in
+// component 0 of SetField/GetField, dt = SetRun's dt_fixed).
 class AWCM_1D_BATCH {
 public:
     AWCM_1D_BATCH(const std::vector<int>& num_levels, const std::vector<int>& nx_coarse, const std::vector<double>& x_min,

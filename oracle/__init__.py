@@ -96,6 +96,7 @@ class Oracle1D:
         self._manager = b("manager", None, [_vp, _c_int, _c_int, _c_int])
         self._step = b("step", None, [_vp, _c_double, _c_double, _c_double, _c_double, _dp])
         self._run = b("run", _c_int, [_vp, _c_double, _c_double, _c_double, _c_int, _dp])
+        self._scalar_step = b("scalar_step", None, [_vp, _c_double, _c_double, _dp])
         self.h = self._create(num_levels, nx_coarse, x_min, x_max, gamma, scheme)
         self.nx = self._nx(self.h)
 
@@ -155,6 +156,13 @@ class Oracle1D:
         out = np.zeros(2)
         n = self._run(self.h, tol, cfl, t_end, max_steps, _ptr(out, ctypes.c_double))
         return n, out[0], out[1]
+
+    def scalar_step(self, tol, dt):
+        """Scheme 2 (the scalar path of Wavelet/main_1d_advect.cpp): one driver pass at the fixed dt;
+        returns [dt, |mask0|, |mask1|, |mask2|, |mask3|].  The field is column 0 of set_q/get_q."""
+        out = np.zeros(5)
+        self._scalar_step(self.h, tol, dt, _ptr(out, ctypes.c_double))
+        return out
 
 
 class Oracle2D:

@@ -489,6 +489,104 @@ void step1d(O1D& s, double tol, double cfl, double t, double t_next, double* out
     out[9] = mv;
 }
 
+// ---------------------------------------------------------------------------------------------
+// 1D scalar AWCM, the path of Wavelet/main_1d_advect.cpp:48-224 (scheme 2): the field in plane 0
+// of q, the stage outputs q_2, q_1, q_0 in the three planes of qc.
+
+// AWCM_1D::Prepare (Wavelet/AWCM_1D.h:45-72): the scalar transforms (WAVELET_1D.h:90-196) are the
+// Euler ones on plane 0; no mask_temp, no adjacent zones on mask1..mask3, no interpolation.
+void prepare1d_scalar(O1D& s, double tol)
+{
+    fwt1d(s, tol);
+    band1d(s, 0);
+    aaz1d(s, 0);
+    cr1d(s, 0);
+    for (int k = 1; k <= 3; ++k) {
+        copy_bit(s.m, k - 1, k);
+        cl1d(s, k - 1, k - 1);
+        apd1d(s, k, k - 1);
+        cr1d(s, k);
+    }
+    cl1d(s, 3, 3);
+    iwt1d(s, 3);
+}
+
+// Coarse-level derivative with the driver's branches (main_1d_advect.cpp:62-83):
+// AWCM_1D::Differentiate, the 4-point DifferentiateAtLeftBoundary (Wavelet/AWCM_1D.h:127-135)
+// and, at the right edge, the same on the mirrored stencil.  The driver's 6-argument
+// DifferentiateAtLeftBoundary calls (i == 2 dx_, i + 2 dx_ == i_end) have no scalar overload in
+// AWCM_1D; they evaluate the 5-point form of DifferentiateEulerAtLeftBoundary (AWCM_1D.h:174-185)
+// with the identity flux.
+double coarse_d_scalar_1d(const O1D& s, const std::vector<double>& in, int i, int d)
+{
+    auto Q = [&](int ii) { return in[ii + G]; };
+    const double d1 = 2.0 / 3.0, d2 = -1.0 / 12.0;
+    const double d02 = 1.0 / 12.0, d12 = -2.0 / 3.0, d22 = 0, d32 = 2.0 / 3.0;
+    const int iend = s.nx - 1;
+    if (i - 2 * d > 0 && i + 2 * d < iend) return d1 * (Q(i + d) - Q(i - d)) + d2 * (Q(i + 2 * d) - Q(i - 2 * d));
+    if (i - 2 * d < 0) return d1 * (Q(i + d) - Q(i - d)) + d2 * (Q(i + 2 * d) - Q(i - d));
+    if (i == 2 * d) return d02 * Q(i - 2 * d) + d12 * Q(i - d) + d22 * Q(i) + d32 * Q(i + d) + d2 * Q(i + 2 * d);
+    if (i + 2 * d > iend) return d1 * (Q(i - d) - Q(i + d)) + d2 * (Q(i - 2 * d) - Q(i + d));
+    return d02 * Q(i + 2 * d) + d12 * Q(i + d) + d22 * Q(i) + d32 * Q(i - d) + d2 * Q(i - 2 * d);
+}
+
+// One stage: out = in (ghosts included), then on the points of mask b with level set l
+// out(i) -= dt (F_r - F_l) / (dx dx_) on the finest level (F = WENO5::ReconstructRight, WENO.h:
+// 101-104) or out(i) -= dt / (dx dx_) dF below it, then the ghost copies of the end points.
+// Stencils that would leave the ghosted line (only reachable from inconsistent user-set
+// masks/levels) are skipped.
+void scalar_stage1d(O1D& s, const std::vector<double>& in, std::vector<double>& out, int b, int l, double dt)
+{
+    out = in;
+    auto right = [&](int c) {  // ReconstructRight(in(c-2..c+2)) = ReconstructLeft(in(c+2..c-2))
+        return recon_left(in[c + 2 + G], in[c + 1 + G], in[c + G], in[c - 1 + G], in[c - 2 + G], 1);
+    };
+    for (int i = 0; i < s.nx; ++i) {
+        if (!s.get(i, b)) continue;
+        const int lev = s.lv[l][i];
+        if (lev < 0 || lev > s.maxl) continue;
+        const int d = s.D(lev);
+        if (lev != s.maxl && (i - 2 * d < -G || i + 2 * d > s.nx - 1 + G)) continue;
+        double& o = out[i + G];
+        if (lev == s.maxl) {
+            const double F_l = right(i - 1), F_r = right(i);
+            o = o - dt * (F_r - F_l) / (s.dx * d);
+        } else {
+            o = o - dt / (s.dx * d) * coarse_d_scalar_1d(s, in, i, d);
+        }
+    }
+    for (int g = 1; g <= G; ++g) {
+        out[G - g] = out[G];
+        out[s.nx - 1 + g + G] = out[s.nx - 1 + G];
+    }
+}
+
+// One pass of the driver loop: Prepare, the stages at the fixed dt with the combinations
+// q_1 = 3/4 q + 1/4 q_1 on mask1 (after q_1's ghost copies) and q = 1/3 q + 2/3 q_0 on mask0,
+// then PostProcess (RemoveResidue on mask0).  q's own ghosts are never rewritten.
+void scalar_step1d(O1D& s, double tol, double dt, double* out)
+{
+    prepare1d_scalar(s, tol);
+    long cnt[4] = {0, 0, 0, 0};
+    for (int i = 0; i < s.nx; ++i)
+        for (int k = 0; k < 4; ++k) cnt[k] += s.get(i, k);
+    std::vector<double>& q = s.q[0];
+    std::vector<double>& q2 = s.qc[0];
+    std::vector<double>& q1 = s.qc[1];
+    std::vector<double>& q0 = s.qc[2];
+    scalar_stage1d(s, q, q2, 2, 2, dt);
+    scalar_stage1d(s, q2, q1, 1, 1, dt);
+    for (int i = 0; i < s.nx; ++i)
+        if (s.get(i, 1)) q1[i + G] = 0.75 * q[i + G] + 0.25 * q1[i + G];
+    scalar_stage1d(s, q1, q0, 0, 0, dt);
+    for (int i = 0; i < s.nx; ++i)
+        if (s.get(i, 0)) q[i + G] = 1.0 / 3.0 * q[i + G] + 2.0 / 3.0 * q0[i + G];
+    for (int i = 0; i < s.nx; ++i)
+        if (!s.get(i, 0)) q[i + G] = 0;
+    out[0] = dt;
+    for (int k = 0; k < 4; ++k) out[1 + k] = (double)cnt[k];
+}
+
 // =============================================================================================
 // 2D physics: IDEAL_GAS_2D (IDEAL_GAS_EQUATIONS.h:60-111), EULER_EQUATION_2D (EULER_EQUATION.h:64-156),
 // ROE_SOLVER_2D (ROESOLVER.h:43-110).
@@ -1327,7 +1425,12 @@ void or1d_set_levels(void* h, const int* lv)
     for (int r = 0; r < 4; ++r) std::memcpy(s->lv[r].data(), lv + r * s->nx, sizeof(int) * s->nx);
 }
 
-void or1d_prepare(void* h, double tol) { prepare1d(*static_cast<O1D*>(h), tol); }
+void or1d_prepare(void* h, double tol)
+{
+    O1D& s = *static_cast<O1D*>(h);
+    if (s.scheme == 2) prepare1d_scalar(s, tol);
+    else prepare1d(s, tol);
+}
 void or1d_fwt(void* h, double tol) { fwt1d(*static_cast<O1D*>(h), tol); }
 void or1d_iwt(void* h, int mask_id) { iwt1d(*static_cast<O1D*>(h), bit_of(mask_id)); }
 
@@ -1349,6 +1452,11 @@ void or1d_manager(void* h, int op, int mask_id, int level_id)
 void or1d_step(void* h, double tol, double cfl, double t, double t_next, double* out)
 {
     step1d(*static_cast<O1D*>(h), tol, cfl, t, t_next, out);
+}
+
+void or1d_scalar_step(void* h, double tol, double dt, double* out)
+{
+    scalar_step1d(*static_cast<O1D*>(h), tol, dt, out);
 }
 
 int or1d_run(void* h, double tol, double cfl, double t_end, int max_steps, double* out)

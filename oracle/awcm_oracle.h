@@ -31,6 +31,9 @@ void or1d_fwt(void* h, double tol);
 void or1d_iwt(void* h, int mask_id);
 void or1d_manager(void* h, int op, int mask_id, int level_id);
 void or1d_step(void* h, double tol, double cfl, double t, double t_next, double* out);
+/* scheme 2 (scalar path of Wavelet/main_1d_advect.cpp): one driver pass at the fixed dt;
+ * out[0] = dt, out[1..4] = |mask0..mask3|.  The field is component 0 of set_q/get_q. */
+void or1d_scalar_step(void* h, double tol, double dt, double* out);
 int or1d_run(void* h, double tol, double cfl, double t_end, int max_steps, double* out);
 
 void* or2d_create(int num_levels, int nx_coarse, int ny_coarse, double x_min, double x_max, double y_min,

@@ -9,7 +9,9 @@
 //   scheme 0: WENO-Z face fluxes, WENOZ_EULER_SOLVER_1D::ComputeFlux (WENOZ.h:160-205),
 //             applied to the two faces of a point the way WENO_EULER_SOLVER_1D::ComputedF
 //             (WENO.h:176-184) does it -- the 1D Sod configuration of the benchmark;
-//   scheme 1: the shipped driver's classic WENO5 ComputedF (WENO.h:176-184).
+//   scheme 1: the shipped driver's classic WENO5 ComputedF (WENO.h:176-184);
+//   scheme 2: the scalar path of Wavelet/main_1d_advect.cpp:48-224 (AWCM_1D::Prepare and
+//             PostProcess, WENO5::ReconstructRight, AWCM_1D::Differentiate*), ref1d_scalar_step.
 #include "FIELD_UNIFORM_1D.h"
 
 // The reference's ARRAY_1D has no AssignAllValue(), which FIELD_UNIFORM_1D<T>::AssignAllValues
@@ -42,6 +44,8 @@ struct Ref1D {
     BOUNDARY_MANAGER* bc = nullptr;
     WENO_EULER_SOLVER_1D* weno = nullptr;
     WENOZ_EULER_SOLVER_1D* wenoz = nullptr;
+    FIELD_UNIFORM_1D<double> sq, sq_0, sq_1, sq_2;  // scheme 2: q and the stage fields q_0, q_1, q_2
+    WENO5 weno5;
     double gamma = 1.4;
     int scheme = 0;
     int nx = 0;
@@ -124,6 +128,60 @@ void stage1d(Ref1D* s, const FIELD_UNIFORM_1D<bool>& mask, const FIELD_UNIFORM_1
     }
 }
 
+// The 5-point form of AWCM_1D::DifferentiateEulerAtLeftBoundary (Wavelet/AWCM_1D.h:174-185) on
+// scalars, with AWCM_1D's own coefficients: main_1d_advect.cpp calls a 6-argument scalar
+// DifferentiateAtLeftBoundary (:74, :82 and the same lines of the later stages) that AWCM_1D does
+// not declare, so the driver does not compile as shipped; the flux of unit-speed advection is
+// the field itself, which makes this the vector form's meaning for a scalar.
+double left5(const AWCM_1D& a, double ll, double l, double c, double r, double rr)
+{
+    return a.d02 * ll + a.d12 * l + a.d22 * c + a.d32 * r + a.d2 * rr;
+}
+
+// One stage of Wavelet/main_1d_advect.cpp (:50-99, :100-155, :164-212): out = q, the update of
+// the points of the mask, the ghost copies of the end points.
+void scalar_stage1d(Ref1D* s, const FIELD_UNIFORM_1D<double>& q, FIELD_UNIFORM_1D<double>& out,
+                    const FIELD_UNIFORM_1D<bool>& mask, const FIELD_UNIFORM_1D<int>& level, double dt)
+{
+    AWCM_1D& awcm = *s->awcm;
+    const MRA_GRID_INT_1D& mra = s->mra;
+    const int max_lev = mra.num_levels - 1;
+    const double dx = s->grid.dx;
+    const int i_res = s->nx;
+    out = q;
+    double dF = 0;
+    ITERATION_GRID_1D(s->grid, 0)
+    {
+        if (mask(i) == false) continue;
+        const int lev = level(i);
+        const int dx_ = mra.grid[lev].dx;
+        if (lev == max_lev) {
+            double F_r, F_l;
+            s->weno5.ReconstructRight(q(i - 3), q(i - 2), q(i - 1), q(i), q(i + 1), F_l);
+            s->weno5.ReconstructRight(q(i - 2), q(i - 1), q(i), q(i + 1), q(i + 2), F_r);
+            out(i) = out(i) - dt * (F_r - F_l) / (dx * dx_);
+        } else {
+            if (i - 2 * dx_ > 0 && i + 2 * dx_ < s->grid.i_end)
+                awcm.Differentiate(q(i - 2 * dx_), q(i - dx_), q(i), q(i + dx_), q(i + 2 * dx_), dF);
+            else if (i - 2 * dx_ < 0)
+                awcm.DifferentiateAtLeftBoundary(q(i - dx_), q(i), q(i + dx_), q(i + 2 * dx_), dF);
+            else if (i == 2 * dx_)
+                dF = left5(awcm, q(i - 2 * dx_), q(i - dx_), q(i), q(i + dx_), q(i + 2 * dx_));
+            else if (i + 2 * dx_ > s->grid.i_end)
+                awcm.DifferentiateAtLeftBoundary(q(i + dx_), q(i), q(i - dx_), q(i - 2 * dx_), dF);
+            else
+                dF = left5(awcm, q(i + 2 * dx_), q(i + dx_), q(i), q(i - dx_), q(i - 2 * dx_));
+            out(i) = out(i) - dt / (dx * dx_) * dF;
+        }
+    }
+    out(-1) = out(0);
+    out(-2) = out(0);
+    out(-3) = out(0);
+    out(i_res) = out(i_res - 1);
+    out(i_res + 1) = out(i_res - 1);
+    out(i_res + 2) = out(i_res - 1);
+}
+
 // LF-splitting speed over the finest-level points of a mask (main_1d_euler.cpp:86-95).
 double alpha1d(Ref1D* s, const FIELD_UNIFORM_1D<bool>& mask, const FIELD_UNIFORM_1D<int>& level)
 {
@@ -159,6 +217,7 @@ void* ref1d_create(int num_levels, int nx_coarse, double x_min, double x_max, do
     s->scheme = scheme;
     s->weno = new WENO_EULER_SOLVER_1D(gamma);
     s->wenoz = new WENOZ_EULER_SOLVER_1D(gamma);
+    if (scheme == 2) s->sq.Initialize(s->grid, 3);
     return s;
 }
 
@@ -175,18 +234,22 @@ void ref1d_destroy(void* h)
 int ref1d_nx(void* h) { return static_cast<Ref1D*>(h)->nx; }
 
 // q: (Nx+6) x 3 doubles, point i (ghosts -3..Nx+2) at row i+3.
+// Scheme 2: the field is component 0 (components 1 and 2 are ignored, and read back as 0).
 void ref1d_set_q(void* h, const double* q)
 {
     Ref1D* s = static_cast<Ref1D*>(h);
-    for (int i = -3; i < s->nx + 3; ++i)
-        for (int p = 0; p < 3; ++p) s->Q(i)[p] = q[(i + 3) * 3 + p];
+    for (int i = -3; i < s->nx + 3; ++i) {
+        if (s->scheme == 2) s->sq(i) = q[(i + 3) * 3];
+        else
+            for (int p = 0; p < 3; ++p) s->Q(i)[p] = q[(i + 3) * 3 + p];
+    }
 }
 
 void ref1d_get_q(void* h, double* q)
 {
     Ref1D* s = static_cast<Ref1D*>(h);
     for (int i = -3; i < s->nx + 3; ++i)
-        for (int p = 0; p < 3; ++p) q[(i + 3) * 3 + p] = s->Q(i)[p];
+        for (int p = 0; p < 3; ++p) q[(i + 3) * 3 + p] = s->scheme == 2 ? (p == 0 ? s->sq(i) : 0.0) : s->Q(i)[p];
 }
 
 // Sod-type initial state on the cell-centred grid, as SHOCKTUBE::Initialize builds it
@@ -250,23 +313,60 @@ void ref1d_set_levels(void* h, const int* lv)
     }
 }
 
-// AWCM_1D::PrepareEuler (Wavelet/AWCM_1D.h:86-120).
+// AWCM_1D::PrepareEuler (Wavelet/AWCM_1D.h:86-120); scheme 2: AWCM_1D::Prepare (:45-72).
 void ref1d_prepare(void* h, double tol)
 {
     Ref1D* s = static_cast<Ref1D*>(h);
-    s->awcm->PrepareEuler(s->Q, tol);
+    if (s->scheme == 2) s->awcm->Prepare(s->sq, tol);
+    else s->awcm->PrepareEuler(s->Q, tol);
 }
 
 void ref1d_fwt(void* h, double tol)
 {
     Ref1D* s = static_cast<Ref1D*>(h);
-    s->awcm->wavelet.ForwardWaveletTransformEuler(s->Q, s->mra, s->awcm->mask0, tol);
+    if (s->scheme == 2) s->awcm->wavelet.ForwardWaveletTransform(s->sq, s->mra, s->awcm->mask0, tol);
+    else s->awcm->wavelet.ForwardWaveletTransformEuler(s->Q, s->mra, s->awcm->mask0, tol);
 }
 
 void ref1d_iwt(void* h, int mask_id)
 {
     Ref1D* s = static_cast<Ref1D*>(h);
-    s->awcm->wavelet.InverseWaveletTransformEuler(s->Q, s->mra, mask_ref(s, mask_id));
+    if (s->scheme == 2) s->awcm->wavelet.InverseWaveletTransform(s->sq, s->mra, mask_ref(s, mask_id));
+    else s->awcm->wavelet.InverseWaveletTransformEuler(s->Q, s->mra, mask_ref(s, mask_id));
+}
+
+// One pass of the loop body of Wavelet/main_1d_advect.cpp:48-224 (it lives inside the driver's
+// main()) at the fixed dt.  out[0] = dt, out[1..4] = |mask0..mask3| after Prepare.
+void ref1d_scalar_step(void* h, double tol, double dt, double* out)
+{
+    Ref1D* s = static_cast<Ref1D*>(h);
+    AWCM_1D& awcm = *s->awcm;
+    FIELD_UNIFORM_1D<double>& q = s->sq;
+    awcm.Prepare(q, tol);
+    long cnt[4] = {0, 0, 0, 0};
+    ITERATION_GRID_1D(s->grid, 0)
+    {
+        cnt[0] += awcm.mask0(i);
+        cnt[1] += awcm.mask1(i);
+        cnt[2] += awcm.mask2(i);
+        cnt[3] += awcm.mask3(i);
+    }
+    scalar_stage1d(s, q, s->sq_2, awcm.mask2, awcm.level2, dt);
+    scalar_stage1d(s, s->sq_2, s->sq_1, awcm.mask1, awcm.level1, dt);
+    ITERATION_GRID_1D(s->grid, 0)
+    {
+        if (awcm.mask1(i) == false) continue;
+        s->sq_1(i) = 0.75 * q(i) + 0.25 * s->sq_1(i);
+    }
+    scalar_stage1d(s, s->sq_1, s->sq_0, awcm.mask0, awcm.level0, dt);
+    ITERATION_GRID_1D(s->grid, 0)
+    {
+        if (awcm.mask0(i) == false) continue;
+        q(i) = 1.0 / 3.0 * q(i) + 2.0 / 3.0 * s->sq_0(i);
+    }
+    awcm.PostProcess(q);
+    out[0] = dt;
+    for (int k = 0; k < 4; ++k) out[1 + k] = (double)cnt[k];
 }
 
 // AWCM_MANAGER_1D passes on one of the facade's masks.
