@@ -1676,6 +1676,17 @@ struct Solver2D {
     int device = 0;
     int list_rows_blocks = 0;
     int face_blocks = 0;
+    // Grid of a grid-stride phase kernel: at most two waves (16 CTAs of 256 threads per SM).  The
+    // passes are short and latency-bound: fewer CTAs leave too few warps in flight (8 per SM:
+    // +1.2 % step time, 4: +7 %), while the uncapped grids of up to 12k CTAs spend microseconds
+    // per launch on block scheduling (+2.6 %; measured on the 2049^2 four-quadrant step).
+#ifndef AWCM_PHASE_CTAS_PER_SM
+#define AWCM_PHASE_CTAS_PER_SM 16
+#endif
+    unsigned pb(long n) const
+    {
+        return std::min(blocks_for(n, 256), (unsigned)(face_blocks / 8 * AWCM_PHASE_CTAS_PER_SM));
+    }
     // Phase marks of a profiled step (null while capturing the graph).
     cudaEvent_t* prof_ev = nullptr;
     int prof_n = 0;
@@ -1944,10 +1955,10 @@ struct Solver2D {
     {
         for (int lev = g.maxl - 1; lev >= 0; --lev) {
             if (row_scan(lev)) {
-                launch(k_cr_rows, blocks_for(rowscan_threads(lev, 2), 256), 256, g, m, lev, bit, s);
+                launch(k_cr_rows, pb(rowscan_threads(lev, 2)), 256, g, m, lev, bit, s);
                 after("k_cr_rows");
             } else {
-                launch(k_cr, blocks_for(details(lev), 256), 256, g, m, lev, bit, s);
+                launch(k_cr, pb(details(lev)), 256, g, m, lev, bit, s);
                 after("k_cr");
             }
             launches += 1;
@@ -1959,10 +1970,10 @@ struct Solver2D {
     void enq_fwt(const StepState* s)
     {
         for (int lev = g.maxl - 1; lev >= 0; --lev) {
-            launch(k_fwt_a, blocks_for(details(lev), 256), 256, g, q.p[0], fx.p[0], m, lev, s);
+            launch(k_fwt_a, pb(details(lev)), 256, g, q.p[0], fx.p[0], m, lev, s);
             after("k_fwt_a");
             const long nb = band_count(lev, 3) + band_count(lev, 0) + band_count(lev, 1);
-            launch(k_fwt_b, blocks_for(nb, 256), 256, g, q.p[0], fx.p[0], m, lev, s);
+            launch(k_fwt_b, pb(nb), 256, g, q.p[0], fx.p[0], m, lev, s);
             after("k_fwt_b");
             launches += 2;
         }
@@ -1972,11 +1983,11 @@ struct Solver2D {
     {
         for (int lev = 0; lev < g.maxl; ++lev) {
             const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1), bc = band_of(g, lev, 3);
-            launch(k_iwt<0>, blocks_for((long)bc.cx * bc.cy, 256), 256, g, q.p[0], m, lev, bit, s);
+            launch(k_iwt<0>, pb((long)bc.cx * bc.cy), 256, g, q.p[0], m, lev, bit, s);
             after("k_iwt<0>");
-            launch(k_iwt<1>, blocks_for((long)b1.cx * b1.cy + (long)b2.cx * b2.cy, 256), 256, g, q.p[0], m, lev, bit, s);
+            launch(k_iwt<1>, pb((long)b1.cx * b1.cy + (long)b2.cx * b2.cy), 256, g, q.p[0], m, lev, bit, s);
             after("k_iwt<1>");
-            launch(k_iwt<2>, blocks_for((long)b3.cx * b3.cy, 256), 256, g, q.p[0], m, lev, bit, s);
+            launch(k_iwt<2>, pb((long)b3.cx * b3.cy), 256, g, q.p[0], m, lev, bit, s);
             after("k_iwt<2>");
             launches += 3;
         }
@@ -1984,20 +1995,20 @@ struct Solver2D {
 
     void enq_interp(int from, int to, const StepState* s, int p0 = 1)
     {
-        launch(k_interp_init, blocks_for(words(), 256), 256, g, m, from, to, s);
+        launch(k_interp_init, pb(words()), 256, g, m, from, to, s);
         after("k_interp_init");
         launches += 1;
         enq_cr(kBitInterp, s);
         for (int lev = 0; lev < g.maxl; ++lev) {
             if (row_scan(lev)) {
-                launch(k_interp_rows<0>, blocks_for(rowscan_threads(lev, 2), 256), 256, g, q, m, lev, from, p0, s);
+                launch(k_interp_rows<0>, pb(rowscan_threads(lev, 2)), 256, g, q, m, lev, from, p0, s);
                 after("k_interp_rows<0>");
-                launch(k_interp_rows<1>, blocks_for(rowscan_threads(lev, 1), 256), 256, g, q, m, lev, from, p0, s);
+                launch(k_interp_rows<1>, pb(rowscan_threads(lev, 1)), 256, g, q, m, lev, from, p0, s);
                 after("k_interp_rows<1>");
             } else {
-                launch(k_interp<0>, blocks_for(band_count(lev, 0) + band_count(lev, 1), 256), 256, g, q, m, lev, from, p0, s);
+                launch(k_interp<0>, pb(band_count(lev, 0) + band_count(lev, 1)), 256, g, q, m, lev, from, p0, s);
                 after("k_interp<0>");
-                launch(k_interp<1>, blocks_for(band_count(lev, 2), 256), 256, g, q, m, lev, from, p0, s);
+                launch(k_interp<1>, pb(band_count(lev, 2)), 256, g, q, m, lev, from, p0, s);
                 after("k_interp<1>");
             }
             launches += 2;
@@ -2006,9 +2017,9 @@ struct Solver2D {
 
     void enq_aaz(int bit, const StepState* s)
     {
-        launch(k_copy_bit_all, blocks_for(words(), 256), 256, m, plane, bit, kBitCopy, s);
+        launch(k_copy_bit_all, pb(words()), 256, m, plane, bit, kBitCopy, s);
         after("k_copy_bit_all");
-        launch(k_aaz, blocks_for(words(), 256), 256, g, m, bit, kBitCopy, s);
+        launch(k_aaz, pb(words()), 256, g, m, bit, kBitCopy, s);
         after("k_aaz");
         launches += 2;
     }
@@ -2048,20 +2059,20 @@ struct Solver2D {
             launches += 1;
             return;
         }
-        if (!scalar) launch(k_copy_bit_all, blocks_for(words(), 256), 256, m, plane, 0, kBitTemp, s);
+        if (!scalar) launch(k_copy_bit_all, pb(words()), 256, m, plane, 0, kBitTemp, s);
         after("k_copy_bit_all");
         launches += 1;
         enq_fwt(s);
-        launch(k_band_copy, blocks_for(words(), 256), 256, g, m, 0, kBitCopy, s);
+        launch(k_band_copy, pb(words()), 256, g, m, 0, kBitCopy, s);
         after("k_band_copy");
-        launch(k_aaz, blocks_for(words(), 256), 256, g, m, 0, kBitCopy, s);
+        launch(k_aaz, pb(words()), 256, g, m, 0, kBitCopy, s);
         after("k_aaz");
         launches += 2;
         enq_cr(0, s);
         for (int k = 1; k <= 3; ++k) {
-            launch(k_cl, blocks_for(words(), 256), 256, g, m, lvl[k - 1], k - 1, k, plane, s);
+            launch(k_cl, pb(words()), 256, g, m, lvl[k - 1], k - 1, k, plane, s);
             after("k_cl");
-            launch(k_apd, blocks_for(words(), 256), 256, g, m, lvl[k - 1], k, k - 1, s);
+            launch(k_apd, pb(words()), 256, g, m, lvl[k - 1], k, k - 1, s);
             after("k_apd");
             launches += 2;
             enq_cr(k, s);
@@ -2177,7 +2188,7 @@ struct Solver2D {
         enq_bc(q1, st, 2);
         enq_alpha_listed(q1, 2);
         enq_faces_update(2, q1, q1);
-        launch(k_remove_residue, blocks_for(words(), 256), 256, g, q, m, 0, 1, st);
+        launch(k_remove_residue, pb(words()), 256, g, q, m, 0, 1, st);
         after("k_remove_residue");
         launch(k_finish, 1, 1, st);
         after("k_finish");
@@ -2233,7 +2244,7 @@ struct Solver2D {
         enq_stage_scalar(1, q2.p[0], q1.p[0]);
         enq_bc(alias(q1.p[0]), st);
         enq_stage_scalar(2, q1.p[0], q1.p[0]);
-        launch(k_remove_residue, blocks_for(words(), 256), 256, g, q, m, 0, 1, st);
+        launch(k_remove_residue, pb(words()), 256, g, q, m, 0, 1, st);
         launch(k_finish, 1, 1, st);
         launches += 2;
     }
@@ -2507,12 +2518,12 @@ struct Solver2D {
             case 0: enq_aaz(b, nullptr); break;
             case 1: enq_cr(b, nullptr); break;
             case 2:
-                launch(k_copy_bit_all, blocks_for(words(), 256), 256, m, plane, b, kBitCopy, nullptr);
-                launch(k_apd, blocks_for(words(), 256), 256, g, m, lvl[level_id], b, kBitCopy, nullptr);
+                launch(k_copy_bit_all, pb(words()), 256, m, plane, b, kBitCopy, nullptr);
+                launch(k_apd, pb(words()), 256, g, m, lvl[level_id], b, kBitCopy, nullptr);
                 break;
-            case 3: launch(k_cl, blocks_for(words(), 256), 256, g, m, lvl[level_id], b, -1, plane, nullptr); break;
-            case 4: launch(k_remove_residue, blocks_for(words(), 256), 256, g, q, m, b, 0, nullptr); break;
-            case 5: launch(k_band_copy, blocks_for(words(), 256), 256, g, m, b, -1, nullptr); break;
+            case 3: launch(k_cl, pb(words()), 256, g, m, lvl[level_id], b, -1, plane, nullptr); break;
+            case 4: launch(k_remove_residue, pb(words()), 256, g, q, m, b, 0, nullptr); break;
+            case 5: launch(k_band_copy, pb(words()), 256, g, m, b, -1, nullptr); break;
             default: return kErrArg;
         }
         AWCM_CUDA_TRY(cudaGetLastError());
