@@ -407,42 +407,54 @@ __device__ void ph_cr_rows(const Grid2& g, uint8_t* __restrict__ m, int lev, int
 }
 
 // InterpolateEuler, one phase of one level (WAVELET_2D.h:784-907): PH 0 = d1 and d2, PH 1 = d3;
-// components 1..3 at points of the work mask that were not active before (`from_bit`).
+// components 1..3 at points of the work mask that were not active before (`from_bit`).  All
+// components are computed before any is stored: a store of one component plane could alias the
+// stencil loads of the next as far as the compiler knows, which would serialize their gathers.
 __device__ __forceinline__ void interp_point(const Grid2& g, Field4 q, int i, int j, size_t a, int D, int w, int p0)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
+    double out[4] = {0, 0, 0, 0};
     if (w == 0) {
         int s0, k;
         predict_stencil(i, D, NX, s0, k);
-        for (int p = p0; p < 4; ++p) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (p < p0) continue;
             const double* qp = q.p[p];
             double v = 0.0;
             for (int c = 0; c < 4; ++c) v += qp[g.at(s0 + c * D, j)] * g.w(c, k);
-            q.p[p][a] = v;
+            out[p] = v;
         }
     } else if (w == 1) {
         int s0, k;
         predict_stencil(j, D, NY, s0, k);
-        for (int p = p0; p < 4; ++p) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (p < p0) continue;
             const double* qp = q.p[p];
             double v = 0.0;
             for (int c = 0; c < 4; ++c) v += qp[g.at(i, s0 + c * D)] * g.w(c, k);
-            q.p[p][a] = v;
+            out[p] = v;
         }
     } else {
         int is, k1, js, k2;
         predict_stencil(i, D, NX, is, k1);
         predict_stencil(j, D, NY, js, k2);
-        for (int p = p0; p < 4; ++p) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (p < p0) continue;
             const double* qp = q.p[p];
             double v = 0.0;
             for (int c = 0; c < 4; ++c) v += qp[g.at(is + c * D, j)] * g.w(c, k1);
             for (int c = 0; c < 4; ++c) v += qp[g.at(i, js + c * D)] * g.w(c, k2);
             for (int c2 = 0; c2 < 4; ++c2)
                 for (int c1 = 0; c1 < 4; ++c1) v -= qp[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-            q.p[p][a] = v;
+            out[p] = v;
         }
     }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+        if (p >= p0) q.p[p][a] = out[p];
 }
 
 template <int PH>
@@ -966,7 +978,9 @@ __global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, doub
             return;
         }
         const size_t s = g.at(si, sj);
-        for (int k = 0; k < 4; ++k) f.p[k][a] = f.p[k][s];
+        double v[4];
+        for (int k = 0; k < 4; ++k) v[k] = f.p[k][s];
+        for (int k = 0; k < 4; ++k) f.p[k][a] = v[k];
         return;
     }
     const long r0 = tid - 2 * nside;
@@ -1006,14 +1020,10 @@ __global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, doub
         return;
     }
     const size_t s = g.at(i, sj);
-    if (g.bc_kind == AWCM_BC_SHOCK_VORTEX) {
-        f.p[0][a] = f.p[0][s];
-        f.p[1][a] = f.p[1][s];
-        f.p[2][a] = -f.p[2][s];
-        f.p[3][a] = f.p[3][s];
-        return;
-    }
-    for (int k = 0; k < 4; ++k) f.p[k][a] = f.p[k][s];
+    double v[4];
+    for (int k = 0; k < 4; ++k) v[k] = f.p[k][s];
+    if (g.bc_kind == AWCM_BC_SHOCK_VORTEX) v[2] = -v[2];
+    for (int k = 0; k < 4; ++k) f.p[k][a] = v[k];
 }
 
 // ------------------------------------------------------------------------- CFL and LF reductions
@@ -1159,8 +1169,11 @@ __global__ void k_begin(StepState* st, int keep_lists)
 __global__ void k_copy4(Field4 dst, Field4 src, size_t n)
 {
     pdl_begin();
-    for (size_t a = gtid(); a < n; a += (size_t)gridDim.x * blockDim.x)
-        for (int k = 0; k < 4; ++k) dst.p[k][a] = src.p[k][a];
+    for (size_t a = gtid(); a < n; a += (size_t)gridDim.x * blockDim.x) {
+        double v[4];
+        for (int k = 0; k < 4; ++k) v[k] = src.p[k][a];
+        for (int k = 0; k < 4; ++k) dst.p[k][a] = v[k];
+    }
 }
 
 __global__ void k_finish(StepState* st)
@@ -1344,16 +1357,29 @@ __global__ void __launch_bounds__(128, AWCM_FACE_MIN_CTAS)
 // RK combinations of the three stages (main_2d_euler(quad).cpp:162, 242, 321 and 325-332):
 // KIND 1: out = in - sc (dF+dG); KIND 2: out = 0.75 qn + 0.25 (in - sc (dF+dG));
 // KIND 3: qn = (qn + 2 (in - sc (dF+dG))) / 3.
+// All four components are loaded before any is stored (a store to one plane could alias the
+// next plane's load as far as the compiler knows, which would serialize the round trips).
 template <int KIND>
 __device__ __forceinline__ void rk_store(Field4 in, Field4 out, Field4 qn, size_t a, const double* dF,
                                          const double* dG, double sc)
 {
+    double x[4], y[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const double r = in.p[k][a] - sc * (dF[k] + dG[k]);
-        if (KIND == 1) out.p[k][a] = r;
-        else if (KIND == 2) out.p[k][a] = 0.75 * qn.p[k][a] + 0.25 * r;
-        else qn.p[k][a] = (qn.p[k][a] + 2.0 * r) / 3.0;
+        x[k] = in.p[k][a];
+        y[k] = KIND == 1 ? 0.0 : qn.p[k][a];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double r = x[k] - sc * (dF[k] + dG[k]);
+        if (KIND == 1) y[k] = r;
+        else if (KIND == 2) y[k] = 0.75 * y[k] + 0.25 * r;
+        else y[k] = (y[k] + 2.0 * r) / 3.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (KIND == 3) qn.p[k][a] = y[k];
+        else out.p[k][a] = y[k];
     }
 }
 
