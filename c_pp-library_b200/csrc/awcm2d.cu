@@ -942,12 +942,10 @@ __device__ __forceinline__ double euler_E(double g, double rho, double u, double
 // BOUNDARY_MANAGER_ISENVORTEX (Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h:107-171) and
 // BOUNDARY_MANAGER_SHOCK_VORTEX (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:118-201:
 // transmissive left/right, bottom/top walls reflecting rho v).
-__global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, double* zx, double* zy)
+__device__ void bc_fill(const Grid2& g, Field4 f, const StepState* st, double t_host, double* zx, double* zy,
+                        long tid)
 {
-    pdl_begin();
-    if (st && st->done) return;
     const double t = st ? st->t : t_host;
-    const long tid = gtid();
     // zero the LF-speed accumulators of the stage this fill feeds (the grid covers nx and ny)
     if (zx && tid < g.ny) zx[tid] = 0.0;
     if (zy && tid < g.nx) zy[tid] = 0.0;
@@ -1026,6 +1024,13 @@ __global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, doub
     for (int k = 0; k < 4; ++k) f.p[k][a] = v[k];
 }
 
+__global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, double* zx, double* zy)
+{
+    pdl_begin();
+    if (st && st->done) return;
+    bc_fill(g, f, st, t_host, zx, zy, gtid());
+}
+
 // ------------------------------------------------------------------------- CFL and LF reductions
 // Per-row alpha_x[j] = max |u|+c and per-column alpha_y[i] = max |v|+c over the points of mask
 // `bit` (main_2d_euler(quad).cpp:86-104); with mv != null also the CFL speed
@@ -1092,18 +1097,15 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
 // per lane; the row maximum is a segmented max-scan over runs of equal rows in the warp (lists
 // are row-ordered within each warp segment) with one atomic per run, the column maximum one
 // atomic per point.  Maxima are order-independent, so the result equals k_alpha's.
-__global__ void __launch_bounds__(256) k_alpha_list(Grid2 g, Field4 f, const uint32_t* __restrict__ la,
-                                                    const unsigned* __restrict__ na,
-                                                    const uint32_t* __restrict__ lb,
-                                                    const unsigned* __restrict__ nb, double* ax, double* ay,
-                                                    const StepState* st)
+// first: this CTA's first thread in the launch's range of LF-speed threads, stride: that range's size.
+__device__ void alpha_list_run(const Grid2& g, Field4 f, const uint32_t* __restrict__ la,
+                               const unsigned* __restrict__ na, const uint32_t* __restrict__ lb,
+                               const unsigned* __restrict__ nb, double* ax, double* ay, unsigned first,
+                               unsigned stride)
 {
-    pdl_begin();
-    if (st->done) return;
     const unsigned n0 = *na, n = n0 + *nb;
     const int lane = threadIdx.x & 31;
-    const unsigned stride = gridDim.x * blockDim.x;
-    for (unsigned base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    for (unsigned base = first + (threadIdx.x & ~31u); base < n; base += stride) {
         const unsigned e = base + (unsigned)lane;
         const bool on = e < n;
         int j = -1;
@@ -1132,12 +1134,40 @@ __global__ void __launch_bounds__(256) k_alpha_list(Grid2 g, Field4 f, const uin
     }
 }
 
-// dt = cfl dx / max speed, clipped to the output time (main_2d_euler(quad).cpp:76-83), and the
-// per-level stage factor dt / (dx 2^(maxl-lev)) of the RK updates.
-__global__ void k_dt(Grid2 g, StepState* st)
+__global__ void __launch_bounds__(256) k_alpha_list(Grid2 g, Field4 f, const uint32_t* __restrict__ la,
+                                                    const unsigned* __restrict__ na,
+                                                    const uint32_t* __restrict__ lb,
+                                                    const unsigned* __restrict__ nb, double* ax, double* ay,
+                                                    const StepState* st)
 {
     pdl_begin();
     if (st->done) return;
+    alpha_list_run(g, f, la, na, lb, nb, ax, ay, blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
+}
+
+// Boundary fill and LF speeds of stage 2 or 3 in one launch: the fill writes only ghost cells and
+// the speeds read only listed grid points, so neither waits for the other (the accumulators were
+// zeroed by the worklist builder).  CTAs [0, bc_blocks) fill, the others compute the speeds.
+__global__ void __launch_bounds__(256) k_bc_alpha(Grid2 g, Field4 f, const uint32_t* __restrict__ la,
+                                                  const unsigned* __restrict__ na,
+                                                  const uint32_t* __restrict__ lb,
+                                                  const unsigned* __restrict__ nb, double* ax, double* ay,
+                                                  const StepState* st, unsigned bc_blocks)
+{
+    pdl_begin();
+    if (st->done) return;
+    if (blockIdx.x < bc_blocks) {
+        bc_fill(g, f, st, 0.0, nullptr, nullptr, (long)blockIdx.x * blockDim.x + threadIdx.x);
+        return;
+    }
+    alpha_list_run(g, f, la, na, lb, nb, ax, ay, (blockIdx.x - bc_blocks) * blockDim.x,
+                   (gridDim.x - bc_blocks) * blockDim.x);
+}
+
+// dt = cfl dx / max speed, clipped to the output time (main_2d_euler(quad).cpp:76-83), and the
+// per-level stage factor dt / (dx 2^(maxl-lev)) of the RK updates.
+__device__ void compute_dt(const Grid2& g, StepState* st)
+{
     double dt = st->cfl * g.dx / st->mv;
     if (st->dt_fixed > 0) dt = st->dt_fixed;
     st->do_print = 0;
@@ -1150,6 +1180,12 @@ __global__ void k_dt(Grid2 g, StepState* st)
         const double dxl = g.dx * g.D(lev);
         st->sc[lev] = dt / dxl;
     }
+}
+__global__ void k_dt(Grid2 g, StepState* st)
+{
+    pdl_begin();
+    if (st->done) return;
+    compute_dt(g, st);
 }
 
 // keep_lists: the step reuses the worklists (and mask counts) of the previous one (frozen masks).
@@ -1198,11 +1234,15 @@ __global__ void k_finish(StepState* st)
 // finest-level point needs.  A CTA covers 256 consecutive columns of kListRows rows of the grid
 // extended by one row/column on the low side (faces -1/2); compaction is a warp ballot, a
 // per-block prefix over warps and one atomicAdd per list per block.
-constexpr int kListRows = 8;
+constexpr int kListRows = 8;  // 16 or 32 rows per CTA measured slower (+2 %, +3 % step time)
 constexpr int kNumLists = 4 * kStages;
 
 struct ListArgs {
     uint32_t* list[kNumLists];
+    // optional: LF-speed accumulators of stages 2 and 3 to zero, and the dt computation (both need
+    // only to happen after stage 1's speeds and before their own use)
+    double *zx1 = nullptr, *zy1 = nullptr, *zx2 = nullptr, *zy2 = nullptr;
+    int with_dt = 0;
 };
 
 // Stage predicates of the point (i, j) (i from -1, j from -1): per stage s (bits 4s..4s+3):
@@ -1242,6 +1282,12 @@ __global__ void __launch_bounds__(256) k_lists(Grid2 g, const uint8_t* __restric
 {
     pdl_begin();
     if (st->done) return;
+    {
+        const unsigned lin = (blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+        if (la.zx1 && lin < (unsigned)g.ny) la.zx1[lin] = la.zx2[lin] = 0.0;
+        if (la.zy1 && lin < (unsigned)g.nx) la.zy1[lin] = la.zy2[lin] = 0.0;
+        if (la.with_dt && lin == 0) compute_dt(g, st);
+    }
     __shared__ unsigned wcnt[8][kNumLists];
     __shared__ unsigned woff[8][kNumLists];
     __shared__ unsigned mcnt[4];
@@ -1383,99 +1429,102 @@ __device__ __forceinline__ void rk_store(Field4 in, Field4 out, Field4 qn, size_
     }
 }
 
+// Finest-level point: dF = F(i+1/2) - F(i-1/2), dG likewise, from the face planes.
 template <int KIND>
-__global__ void __launch_bounds__(256) k_update_fin(Grid2 g, Field4 in, Field4 out, Field4 qn, Field4 fx, Field4 fy,
-                                                    const uint32_t* __restrict__ list,
-                                                    const unsigned* __restrict__ count, const StepState* st)
+__device__ __forceinline__ void update_fin_point(const Grid2& g, Field4 in, Field4 out, Field4 qn, Field4 fx,
+                                                 Field4 fy, size_t a, double sc)
 {
-    pdl_begin();
-    if (st->done) return;
-    const unsigned n = *count;
-    const double sc = st->sc[g.maxl];
-    const long stride = (long)gridDim.x * blockDim.x;
-    for (long e = gtid(); e < n; e += stride) {
-        const size_t a = list[e];
-        double dF[4], dG[4];
+    double dF[4], dG[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            dF[k] = fx.p[k][a] - fx.p[k][a - 1];
-            dG[k] = fy.p[k][a] - fy.p[k][a - g.pitch];
-        }
-        rk_store<KIND>(in, out, qn, a, dF, dG, sc);
+    for (int k = 0; k < 4; ++k) {
+        dF[k] = fx.p[k][a] - fx.p[k][a - 1];
+        dG[k] = fy.p[k][a] - fy.p[k][a - g.pitch];
     }
+    rk_store<KIND>(in, out, qn, a, dF, dG, sc);
 }
+
 
 // Coarse-level points: 4th-order central differences of F and G at spacing d = 2^(maxl-lev), with
 // the reference's one-sided forms next to the boundary (AWCM_2D::Differentiate*, Wavelet/AWCM_2D.h:154-187,
 // branch selection main_2d_euler(quad).cpp:132-160).
 template <int KIND>
-__global__ void __launch_bounds__(256) k_update_crs(Grid2 g, Field4 in, Field4 out, Field4 qn,
-                                                    const int8_t* __restrict__ lvl,
-                                                    const uint32_t* __restrict__ list,
-                                                    const unsigned* __restrict__ count, const StepState* st)
+__device__ __forceinline__ void update_crs_point(const Grid2& g, Field4 in, Field4 out, Field4 qn,
+                                                 const int8_t* __restrict__ lvl, size_t a, const StepState* st)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    const int i = (int)((unsigned)a % (unsigned)g.pitch) - kGhost;
+    const int j = (int)((unsigned)a / (unsigned)g.pitch) - kGhost;
+    const int lev = lvl[a];
+    if (lev < 0 || lev > g.maxl) return;
+    const int d = g.D(lev);
+    // Coarse stencils stay on the ghosted grid whenever the levels come from ComputeLevel on
+    // a reconstruction-closed mask; any other point is skipped rather than read out of bounds.
+    const int lo_x = i <= d ? i - d : i - 2 * d, hi_x = i >= NX - d && !(i <= d) ? i + d : i + 2 * d;
+    const int lo_y = j <= d ? j - d : j - 2 * d, hi_y = j >= NY - d && !(j <= d) ? j + d : j + 2 * d;
+    if (lo_x < -kGhost || hi_x > NX + kGhost || lo_y < -kGhost || hi_y > NY + kGhost) return;
+    double dF[4], dG[4];
+    {
+        double fl[4], fr[4], fo[4], q[4];
+        auto load = [&](long off, double* o) {
+            for (int k = 0; k < 4; ++k) q[k] = in.p[k][(long)a + off];
+            flux2<0>(q, g.gamma, o);
+        };
+        load(-d, fl);
+        load(d, fr);
+        if (i <= d) {
+            load(2 * d, fo);
+            for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fo[k] - fl[k]);
+        } else if (i >= NX - d) {
+            load(-2 * d, fo);
+            for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fr[k] - fo[k]);
+        } else {
+            double fll[4];
+            load(-2 * d, fll);
+            load(2 * d, fo);
+            for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fo[k] - fll[k]);
+        }
+    }
+    {
+        const long P = g.pitch;
+        double gb[4], gt[4], go[4], q[4];
+        auto load = [&](long off, double* o) {
+            for (int k = 0; k < 4; ++k) q[k] = in.p[k][(long)a + off * P];
+            flux2<1>(q, g.gamma, o);
+        };
+        load(-d, gb);
+        load(d, gt);
+        if (j <= d) {
+            load(2 * d, go);
+            for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (go[k] - gb[k]);
+        } else if (j >= NY - d) {
+            load(-2 * d, go);
+            for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (gt[k] - go[k]);
+        } else {
+            double gbb[4];
+            load(-2 * d, gbb);
+            load(2 * d, go);
+            for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (go[k] - gbb[k]);
+        }
+    }
+    rk_store<KIND>(in, out, qn, a, dF, dG, st->sc[lev]);
+}
+
+// The finest-level and the coarse points of a stage in one launch: the two sets are disjoint and
+// neither reads what the other writes (the stage output, or qn at the point itself).
+template <int KIND>
+__global__ void __launch_bounds__(256) k_update(Grid2 g, Field4 in, Field4 out, Field4 qn, Field4 fx, Field4 fy,
+                                                const int8_t* __restrict__ lvl, const uint32_t* __restrict__ lf,
+                                                const unsigned* __restrict__ nf, const uint32_t* __restrict__ lc,
+                                                const unsigned* __restrict__ nc, const StepState* st)
 {
     pdl_begin();
     if (st->done) return;
-    const unsigned n = *count;
+    const unsigned n0 = *nf, n = n0 + *nc;
+    const double sc = st->sc[g.maxl];
     const long stride = (long)gridDim.x * blockDim.x;
-    const int NX = g.nx - 1, NY = g.ny - 1;
     for (long e = gtid(); e < n; e += stride) {
-        const size_t a = list[e];
-        const int i = (int)((unsigned)a % (unsigned)g.pitch) - kGhost;
-        const int j = (int)((unsigned)a / (unsigned)g.pitch) - kGhost;
-        const int lev = lvl[a];
-        if (lev < 0 || lev > g.maxl) continue;
-        const int d = g.D(lev);
-        // Coarse stencils stay on the ghosted grid whenever the levels come from ComputeLevel on
-        // a reconstruction-closed mask; any other point is skipped rather than read out of bounds.
-        const int lo_x = i <= d ? i - d : i - 2 * d, hi_x = i >= NX - d && !(i <= d) ? i + d : i + 2 * d;
-        const int lo_y = j <= d ? j - d : j - 2 * d, hi_y = j >= NY - d && !(j <= d) ? j + d : j + 2 * d;
-        if (lo_x < -kGhost || hi_x > NX + kGhost || lo_y < -kGhost || hi_y > NY + kGhost) continue;
-        double dF[4], dG[4];
-        {
-            double fl[4], fr[4], fo[4], q[4];
-            auto load = [&](long off, double* o) {
-                for (int k = 0; k < 4; ++k) q[k] = in.p[k][(long)a + off];
-                flux2<0>(q, g.gamma, o);
-            };
-            load(-d, fl);
-            load(d, fr);
-            if (i <= d) {
-                load(2 * d, fo);
-                for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fo[k] - fl[k]);
-            } else if (i >= NX - d) {
-                load(-2 * d, fo);
-                for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fr[k] - fo[k]);
-            } else {
-                double fll[4];
-                load(-2 * d, fll);
-                load(2 * d, fo);
-                for (int k = 0; k < 4; ++k) dF[k] = kD1 * (fr[k] - fl[k]) + kD2 * (fo[k] - fll[k]);
-            }
-        }
-        {
-            const long P = g.pitch;
-            double gb[4], gt[4], go[4], q[4];
-            auto load = [&](long off, double* o) {
-                for (int k = 0; k < 4; ++k) q[k] = in.p[k][(long)a + off * P];
-                flux2<1>(q, g.gamma, o);
-            };
-            load(-d, gb);
-            load(d, gt);
-            if (j <= d) {
-                load(2 * d, go);
-                for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (go[k] - gb[k]);
-            } else if (j >= NY - d) {
-                load(-2 * d, go);
-                for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (gt[k] - go[k]);
-            } else {
-                double gbb[4];
-                load(-2 * d, gbb);
-                load(2 * d, go);
-                for (int k = 0; k < 4; ++k) dG[k] = kD1 * (gt[k] - gb[k]) + kD2 * (go[k] - gbb[k]);
-            }
-        }
-        rk_store<KIND>(in, out, qn, a, dF, dG, st->sc[lev]);
+        if (e < n0) update_fin_point<KIND>(g, in, out, qn, fx, fy, lf[e], sc);
+        else update_crs_point<KIND>(g, in, out, qn, lvl, lc[e - n0], st);
     }
 }
 
@@ -2130,6 +2179,18 @@ struct Solver2D {
         after("k_alpha");
         launches += 1;
     }
+    // Boundary fill of stage `stage`'s input (1 or 2) and its LF speeds over the previous stage's
+    // update lists, in one launch; the speeds' accumulators are zeroed by k_lists.
+    void enq_bc_alpha(Field4 f, int stage)
+    {
+        const int ls = stage - 1;
+        const unsigned* C = st->cnt + 4 * ls;
+        const unsigned bcb = blocks_for(2L * kGhost * g.ny + 2L * kGhost * g.nx, 256);
+        launch(k_bc_alpha, bcb + face_blocks / 2, 256, g, f, lists[4 * ls], C, lists[4 * ls + 1], C + 1, ax[stage],
+               ay[stage], st, bcb);
+        after("k_bc_alpha");
+        launches += 1;
+    }
     // Stage `stage` (1 or 2) over the points of the previous stage's update lists (its mask).
     void enq_alpha_listed(Field4 f, int stage, double* axp = nullptr, double* ayp = nullptr)
     {
@@ -2165,22 +2226,16 @@ struct Solver2D {
         mark();
         const int ub = face_blocks / 2;
         if (stage == 0) {
-            launch(k_update_fin<1>, ub, 256, g, in, out, q, fx, fy, L[0], C + 0, st);
-            after("k_update_fin<1>");
-            launch(k_update_crs<1>, ub, 256, g, in, out, q, lvl[2], L[1], C + 1, st);
-            after("k_update_crs<1>");
+            launch(k_update<1>, ub, 256, g, in, out, q, fx, fy, lvl[2], L[0], C + 0, L[1], C + 1, st);
+            after("k_update<1>");
         } else if (stage == 1) {
-            launch(k_update_fin<2>, ub, 256, g, in, out, q, fx, fy, L[0], C + 0, st);
-            after("k_update_fin<2>");
-            launch(k_update_crs<2>, ub, 256, g, in, out, q, lvl[1], L[1], C + 1, st);
-            after("k_update_crs<2>");
+            launch(k_update<2>, ub, 256, g, in, out, q, fx, fy, lvl[1], L[0], C + 0, L[1], C + 1, st);
+            after("k_update<2>");
         } else {
-            launch(k_update_fin<3>, ub, 256, g, in, out, q, fx, fy, L[0], C + 0, st);
-            after("k_update_fin<3>");
-            launch(k_update_crs<3>, ub, 256, g, in, out, q, lvl[0], L[1], C + 1, st);
-            after("k_update_crs<3>");
+            launch(k_update<3>, ub, 256, g, in, out, q, fx, fy, lvl[0], L[0], C + 0, L[1], C + 1, st);
+            after("k_update<3>");
         }
-        launches += 2;
+        launches += 1;
         mark();
     }
 
@@ -2196,23 +2251,24 @@ struct Solver2D {
         mark();
         enq_bc(q, st, 0);
         enq_alpha(q, 3, 0, true);
-        launch(k_dt, 1, 1, g, st);
-        after("k_dt");
-        launches += 1;
         {
+            // the worklists, dt (after stage 1's speeds) and the zeroing of stage 2/3's speeds
             ListArgs la;
             for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
+            la.zx1 = ax[1];
+            la.zy1 = ay[1];
+            la.zx2 = ax[2];
+            la.zy2 = ay[2];
+            la.with_dt = 1;
             dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
             launch(k_lists, grid, 256, g, m, lvl[2], lvl[1], lvl[0], la, st);
             after("k_lists");
             launches += 1;
         }
         enq_faces_update(0, q, q2);
-        enq_bc(q2, st, 1);
-        enq_alpha_listed(q2, 1);
+        enq_bc_alpha(q2, 1);
         enq_faces_update(1, q2, q1);
-        enq_bc(q1, st, 2);
-        enq_alpha_listed(q1, 2);
+        enq_bc_alpha(q1, 2);
         enq_faces_update(2, q1, q1);
         launch(k_remove_residue, pb(words()), 256, g, q, m, 0, 1, st);
         after("k_remove_residue");
