@@ -507,13 +507,16 @@ __device__ void ph_interp_rows(const Grid2& g, Field4 q, const uint8_t* __restri
 }
 
 // ------------------------------------------------------------------------------- dense mask passes
-__device__ void ph_copy_bit_all(uint8_t* m, size_t n, int from, int to, Span sp)
+// Bits 1..3 (mask1..mask3) of the four bytes of a mask word.
+constexpr unsigned kMask123 = (kLaneBits << 1) | (kLaneBits << 2) | (kLaneBits << 3);
+// Copies bit `from` into bit `to` on every byte; `clear` (lane-replicated bits) is cleared too.
+__device__ void ph_copy_bit_all(uint8_t* m, size_t n, int from, int to, Span sp, unsigned clear = 0)
 {
     unsigned* mw = reinterpret_cast<unsigned*>(m);
     const unsigned nw = (unsigned)(n / 4);
     for (unsigned w = sp.t0; w < nw; w += sp.stride) {
         const unsigned v = mw[w];
-        const unsigned nv = (v & ~(kLaneBits << to)) | (((v >> from) & kLaneBits) << to);
+        const unsigned nv = ((v & ~(kLaneBits << to)) | (((v >> from) & kLaneBits) << to)) & ~clear;
         if (nv != v) mw[w] = nv;
     }
 }
@@ -673,6 +676,78 @@ __device__ void ph_apd(const Grid2& g, uint8_t* m, const int8_t* lvl, int bit, i
     }
 }
 
+// ComputeLevel of mask k-1 into lvl, mask_k = mask_{k-1} and AddPointForDifferentiation(mask_k,
+// level_{k-1}) in one pass, for bit k cleared beforehand on every byte: the copy and the pushes
+// both only set bit k (atomic ORs), nothing in the pass reads bit k, bit k-1 does not change,
+// and each point's level is computed by the thread that then reads it.  The same results as
+// ph_cl followed by ph_apd.
+__device__ void ph_cl_apd(const Grid2& g, uint8_t* m, int8_t* lvl, int k, size_t plane, Span sp)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    const int src = k - 1;
+    unsigned* mp = reinterpret_cast<unsigned*>(m);
+    unsigned* lp = reinterpret_cast<unsigned*>(lvl);
+    const unsigned nw = (unsigned)(plane / 4);
+    for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const MaskWord mw = mask_word(g, w);
+        const unsigned v = mp[w];
+        const unsigned G = grid_lanes(g, mw);
+        unsigned lv = 0;
+        if (G) {
+            const unsigned lv0 = lp[w];
+            lv = lv0;
+            const unsigned on = (v >> src) & kLaneBits;
+#pragma unroll
+            for (int L = 0; L < 4; ++L) {
+                if (!((G >> L) & 1u)) continue;
+                const unsigned sh = 8u * L;
+                if (!((on >> sh) & 1u)) {
+                    lv &= ~(0xffu << sh);
+                    continue;
+                }
+                const int i = mw.i0 + L, j = mw.j;
+                int dx = 1;
+                for (int lev = g.maxl; lev >= 0; --lev) {
+                    if (mask_or_ghost(g, m, i - dx, j, src) || mask_or_ghost(g, m, i + dx, j, src) ||
+                        mask_or_ghost(g, m, i, j - dx, src) || mask_or_ghost(g, m, i, j + dx, src)) {
+                        lv = (lv & ~(0xffu << sh)) | ((unsigned)(uint8_t)(int8_t)lev << sh);
+                        break;
+                    }
+                    dx *= 2;
+                }
+            }
+            if (lv != lv0) lp[w] = lv;
+        }
+        const unsigned cp = ((v >> src) & kLaneBits) << k;
+        if (cp) atomicOr(&mp[w], cp);
+        if (mw.j < 1 || mw.j > NY - 1) continue;
+        const unsigned I = lanes_in(mw.i0, 1, NX - 1);
+        unsigned hit = (v >> src) & lane_bits(I);
+        while (hit) {
+            const int L = (__ffs(hit) - 1) >> 3;
+            hit &= hit - 1;
+            const int i = mw.i0 + L, j = mw.j;
+            const int lev = (int)(int8_t)(uint8_t)(lv >> (8 * L));
+            if (lev == g.maxl) {
+                for (int c = -3; c <= 3; ++c) {
+                    push_bit(g, m, i + c, j, k);
+                    push_bit(g, m, i, j + c, k);
+                }
+                continue;
+            }
+            const int D = g.D(lev);
+            int lo = -2, hi = 2;
+            if (i - 2 * D < 0) lo = -1;
+            else if (i + 2 * D > NX) hi = 1;
+            for (int c = lo; c <= hi; ++c) push_bit(g, m, i + D * c, j, k);
+            lo = -2, hi = 2;
+            if (j - 2 * D < 0) lo = -1;
+            else if (j + 2 * D > NY) hi = 1;
+            for (int c = lo; c <= hi; ++c) push_bit(g, m, i, j + D * c, k);
+        }
+    }
+}
+
 // Work mask of InterpolateEuler: `to` minus `from` over the grid points (ghost bits untouched);
 // to < 0 stands for every grid point (InterpolateAllGridEuler).
 __device__ void ph_interp_init(const Grid2& g, uint8_t* m, int from, int to, Span sp)
@@ -768,11 +843,11 @@ __global__ void k_interp_rows(Grid2 g, Field4 q, const uint8_t* m, int lev, int 
     AWCM_SKIP_IF_DONE(st);
     ph_interp_rows<PH>(g, q, m, lev, from_bit, p0, grid_span());
 }
-__global__ void k_copy_bit_all(uint8_t* m, size_t n, int from, int to, const StepState* st)
+__global__ void k_copy_bit_all(uint8_t* m, size_t n, int from, int to, const StepState* st, unsigned clear)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_copy_bit_all(m, n, from, to, grid_span());
+    ph_copy_bit_all(m, n, from, to, grid_span(), clear);
 }
 __global__ void k_band_copy(Grid2 g, uint8_t* m, int bit, int copy_to, const StepState* st)
 {
@@ -797,6 +872,24 @@ __global__ void k_apd(Grid2 g, uint8_t* m, const int8_t* lvl, int bit, int src, 
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     ph_apd(g, m, lvl, bit, src, grid_span());
+}
+__global__ void k_cl_apd(Grid2 g, uint8_t* m, int8_t* lvl, int k, size_t plane, const StepState* st)
+{
+    pdl_begin();
+    AWCM_SKIP_IF_DONE(st);
+    ph_cl_apd(g, m, lvl, k, plane, grid_span());
+}
+// The coarsest level's first inverse-transform phase (CTAs [0, nb)) and the interpolation work mask
+// `to` minus `from` (the other CTAs) in one launch: the mask pass rewrites only the work bit.
+__global__ void k_iwt0_interp_init(Grid2 g, double* q, uint8_t* m, int lev, int to, int from, const StepState* st,
+                                   unsigned nb)
+{
+    pdl_begin();
+    AWCM_SKIP_IF_DONE(st);
+    if (blockIdx.x < nb)
+        ph_iwt<0>(g, q, m, lev, to, Span{blockIdx.x * blockDim.x + threadIdx.x, nb * blockDim.x});
+    else
+        ph_interp_init(g, m, from, to, Span{(blockIdx.x - nb) * blockDim.x + threadIdx.x, (gridDim.x - nb) * blockDim.x});
 }
 __global__ void k_interp_init(Grid2 g, uint8_t* m, int from, int to, const StepState* st)
 {
@@ -2054,12 +2147,20 @@ struct Solver2D {
         }
     }
 
-    void enq_iwt(int bit, const StepState* s)
+    // init_from >= 0: the first launch also builds the work mask of the interpolation that follows
+    // (ph_interp_init from init_from to bit), which the inverse transform does not read.
+    void enq_iwt(int bit, const StepState* s, int init_from = -1)
     {
         for (int lev = 0; lev < g.maxl; ++lev) {
             const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1), bc = band_of(g, lev, 3);
-            launch(k_iwt<0>, pb((long)bc.cx * bc.cy), 256, g, q.p[0], m, lev, bit, s);
-            after("k_iwt<0>");
+            if (lev == 0 && init_from >= 0) {
+                const unsigned nb = pb((long)bc.cx * bc.cy);
+                launch(k_iwt0_interp_init, nb + pb(words()), 256, g, q.p[0], m, lev, bit, init_from, s, nb);
+                after("k_iwt0_interp_init");
+            } else {
+                launch(k_iwt<0>, pb((long)bc.cx * bc.cy), 256, g, q.p[0], m, lev, bit, s);
+                after("k_iwt<0>");
+            }
             launch(k_iwt<1>, pb((long)b1.cx * b1.cy + (long)b2.cx * b2.cy), 256, g, q.p[0], m, lev, bit, s);
             after("k_iwt<1>");
             launch(k_iwt<2>, pb((long)b3.cx * b3.cy), 256, g, q.p[0], m, lev, bit, s);
@@ -2068,11 +2169,14 @@ struct Solver2D {
         }
     }
 
-    void enq_interp(int from, int to, const StepState* s, int p0 = 1)
+    // init_done: the work mask was built by the inverse transform's first launch.
+    void enq_interp(int from, int to, const StepState* s, int p0 = 1, bool init_done = false)
     {
-        launch(k_interp_init, pb(words()), 256, g, m, from, to, s);
-        after("k_interp_init");
-        launches += 1;
+        if (!init_done) {
+            launch(k_interp_init, pb(words()), 256, g, m, from, to, s);
+            after("k_interp_init");
+            launches += 1;
+        }
         enq_cr(kBitInterp, s);
         for (int lev = 0; lev < g.maxl; ++lev) {
             if (row_scan(lev)) {
@@ -2092,7 +2196,7 @@ struct Solver2D {
 
     void enq_aaz(int bit, const StepState* s)
     {
-        launch(k_copy_bit_all, pb(words()), 256, m, plane, bit, kBitCopy, s);
+        launch(k_copy_bit_all, pb(words()), 256, m, plane, bit, kBitCopy, s, 0u);
         after("k_copy_bit_all");
         launch(k_aaz, pb(words()), 256, g, m, bit, kBitCopy, s);
         after("k_aaz");
@@ -2134,7 +2238,9 @@ struct Solver2D {
             launches += 1;
             return;
         }
-        if (!scalar) launch(k_copy_bit_all, pb(words()), 256, m, plane, 0, kBitTemp, s);
+        // mask_temp = mask0; also clears mask1..3, which the merged ComputeLevel +
+        // AddPointForDifferentiation passes below rebuild by ORs
+        if (!scalar) launch(k_copy_bit_all, pb(words()), 256, m, plane, 0, kBitTemp, s, kMask123);
         after("k_copy_bit_all");
         launches += 1;
         enq_fwt(s);
@@ -2145,16 +2251,22 @@ struct Solver2D {
         launches += 2;
         enq_cr(0, s);
         for (int k = 1; k <= 3; ++k) {
-            launch(k_cl, pb(words()), 256, g, m, lvl[k - 1], k - 1, k, plane, s);
-            after("k_cl");
-            launch(k_apd, pb(words()), 256, g, m, lvl[k - 1], k, k - 1, s);
-            after("k_apd");
-            launches += 2;
+            if (!scalar) {
+                launch(k_cl_apd, pb(words()), 256, g, m, lvl[k - 1], k, plane, s);
+                after("k_cl_apd");
+                launches += 1;
+            } else {
+                launch(k_cl, pb(words()), 256, g, m, lvl[k - 1], k - 1, k, plane, s);
+                after("k_cl");
+                launch(k_apd, pb(words()), 256, g, m, lvl[k - 1], k, k - 1, s);
+                after("k_apd");
+                launches += 2;
+            }
             enq_cr(k, s);
         }
-        enq_iwt(3, s);
+        enq_iwt(3, s, scalar ? -1 : kBitTemp);
         // AWCM_2D::Prepare (the scalar form, Wavelet/AWCM_2D.h:52-79) ends with the inverse transform
-        if (!scalar) enq_interp(kBitTemp, 3, s);
+        if (!scalar) enq_interp(kBitTemp, 3, s, 1, true);
     }
 
     // Boundary fill of a stage input; with zero_stage >= 0 it also zeroes that stage's LF-speed
@@ -2600,7 +2712,7 @@ struct Solver2D {
             case 0: enq_aaz(b, nullptr); break;
             case 1: enq_cr(b, nullptr); break;
             case 2:
-                launch(k_copy_bit_all, pb(words()), 256, m, plane, b, kBitCopy, nullptr);
+                launch(k_copy_bit_all, pb(words()), 256, m, plane, b, kBitCopy, nullptr, 0u);
                 launch(k_apd, pb(words()), 256, g, m, lvl[level_id], b, kBitCopy, nullptr);
                 break;
             case 3: launch(k_cl, pb(words()), 256, g, m, lvl[level_id], b, -1, plane, nullptr); break;
