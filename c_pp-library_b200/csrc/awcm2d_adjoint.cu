@@ -488,21 +488,28 @@ __global__ void k_adj_rk(int stage, Grid2 g, size_t plane, const uint8_t* __rest
     const bool on = grid && ((m[a] >> bit) & 1u);
     const int lv = on ? lvl[a] : -1;
     const double s = (lv >= 0 && lv <= g.maxl) ? sc[lv] : 0.0;
+    // every plane is read before any is written (the round trips of the four components overlap)
+    double x[4], ln[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) x[k] = grid ? lam_next.p[k][a] : 0.0;
+    if (stage != 3 && on)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ln[k] = lam_n.p[k][a];
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const double x = grid ? lam_next.p[k][a] : 0.0;
         if (stage == 3) {
-            lam_n.p[k][a] = on ? x / 3.0 : x;
-            const double y = on ? 2.0 * x / 3.0 : 0.0;
+            lam_n.p[k][a] = on ? x[k] / 3.0 : x[k];
+            const double y = on ? 2.0 * x[k] / 3.0 : 0.0;
             lam_in.p[k][a] = y;
             nu.p[k][a] = s * y;
         } else if (stage == 2) {
-            if (on) lam_n.p[k][a] += 0.75 * x;
-            const double y = on ? 0.25 * x : 0.0;
+            if (on) lam_n.p[k][a] = ln[k] + 0.75 * x[k];
+            const double y = on ? 0.25 * x[k] : 0.0;
             lam_in.p[k][a] = y;
             nu.p[k][a] = s * y;
         } else {
-            if (on) lam_n.p[k][a] += x;
-            nu.p[k][a] = on ? s * x : 0.0;
+            if (on) lam_n.p[k][a] = ln[k] + x[k];
+            nu.p[k][a] = on ? s * x[k] : 0.0;
         }
     }
 }
