@@ -1327,7 +1327,7 @@ __global__ void k_finish(StepState* st)
 // finest-level point needs.  A CTA covers 256 consecutive columns of kListRows rows of the grid
 // extended by one row/column on the low side (faces -1/2); compaction is a warp ballot, a
 // per-block prefix over warps and one atomicAdd per list per block.
-constexpr int kListRows = 8;  // 16 or 32 rows per CTA measured slower (+2 %, +3 % step time)
+constexpr int kListRows = 4;  // rows per CTA: 4 measured fastest (8: +0.8 % step time, 2: +0.1 %, 16: +2 %)
 constexpr int kNumLists = 4 * kStages;
 
 struct ListArgs {
