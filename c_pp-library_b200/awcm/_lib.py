@@ -49,6 +49,7 @@ _SIGS = {
     "awcm2d_step_io_bytes": [c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
     "awcm2d_stream": [c_void_p, ctypes.POINTER(c_void_p)],
     "awcm2d_set_prepare_mode": [c_void_p, c_int],
+    "awcm2d_set_spin_limit": [c_void_p, ctypes.c_uint],
     "awcm2d_profile_step": [c_void_p, c_double, c_double, c_double, c_double, P_double],
     "awcm_measure_fp64_peak": [c_int, c_int, P_double],
     "awcm2d_profile_kernels": [c_void_p, c_double, c_double, c_double, c_double, c_int, ctypes.c_char_p, P_double, P_int],

@@ -15,7 +15,9 @@ import ctypes
 
 import numpy as np
 
-from ._lib import P_double, P_int, P_u8, c_void_p, call, ptr
+from ._lib import AWCM_OK, AwcmError, P_double, P_int, P_u8, c_void_p, call, load, ptr
+
+ERR_NONFINITE = 5
 
 AAZ, CR, APD, CL, RR, BAND = 0, 1, 2, 3, 4, 5
 BC_TRANSMISSIVE, BC_DOUBLE_MACH, BC_PERIODIC = 0, 1, 2
@@ -157,6 +159,10 @@ class AWCM2D:
     def set_prepare_mode(self, mode: int):
         """0: persistent cooperative prepare kernel (default); 1: one launch per pass."""
         call("awcm2d_set_prepare_mode", self.h, mode)
+
+    def set_spin_limit(self, polls: int):
+        """Test hook: polls before a grid-barrier wait of the persistent prepare gives up (0 = default)."""
+        call("awcm2d_set_spin_limit", self.h, int(polls))
 
     def launches_per_step(self):
         n = ctypes.c_int()
@@ -365,9 +371,17 @@ class AWCM1DBatch:
         call("awcm1d_batch_sync", self.h)
 
     def status(self, k):
+        """out[16] of instance k (awcm1d_batch_status); out[14] = 5 marks a non-finite state,
+        which is returned here rather than raised (check_finite raises it)."""
         out = np.zeros(16)
-        call("awcm1d_batch_status", self.h, k, ptr(out, ctypes.c_double))
+        rc = load().awcm1d_batch_status(self.h, k, ptr(out, ctypes.c_double))
+        if rc not in (AWCM_OK, ERR_NONFINITE):
+            raise AwcmError("awcm1d_batch_status", rc, load().awcm_last_error().decode(errors="replace"))
         return out
+
+    def check_finite(self, k):
+        """Raises AwcmError(ERR_NONFINITE) if instance k stopped on a NaN or infinite wave speed."""
+        call("awcm1d_batch_status", self.h, k, ptr(np.zeros(16), ctypes.c_double))
 
     def totals(self):
         out = np.zeros(3)
@@ -475,6 +489,7 @@ class AWCM1D:
         """One driver-loop pass; returns the checker's out[10] (dt, do_print, |mask0..3|, alphas, speed)."""
         self.b.set_run(tol, cfl, t, t_next)
         self.b.steps(1)
+        self.b.check_finite(0)
         s = self.b.status(0)
         out = np.zeros(10)
         out[0], out[1] = s[1], s[2]

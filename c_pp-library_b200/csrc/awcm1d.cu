@@ -360,7 +360,8 @@ __device__ void bc1(const Ctx& c, double* q)
     __syncthreads();
 }
 
-__device__ double lf_speed1(const Ctx& c, int b, int l, double* red)
+// nf: set when a speed is NaN or infinite (NaN/Inf state, negative pressure or density).
+__device__ double lf_speed1(const Ctx& c, int b, int l, double* red, bool& nf)
 {
     // main_1d_euler.cpp:86-95: max |u|+c over the finest-level points of mask b.
     double a = 0;
@@ -369,6 +370,7 @@ __device__ double lf_speed1(const Ctx& c, int b, int l, double* red)
         const double q0 = c.Q(0, i), q1 = c.Q(1, i), q2 = c.Q(2, i);
         const double u = q1 / q0;
         const double s = sound1(q0, q1, q2, c.I.gamma);
+        nf |= !isfinite(absd(u) + s);
         a = maxd(a, absd(u) + s);
     }
     return block_max(a, red);
@@ -461,11 +463,13 @@ __device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, u
 
     // CFL (main_1d_euler.cpp:67-81)
     double mv = 0;
+    bool nf = false;  // a NaN or infinite wave speed in the CFL or LF scans
     for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
         if (!c.bit(i, 3)) continue;
         const double q0 = c.Q(0, i), q1 = c.Q(1, i), q2 = c.Q(2, i);
         const double s = sound1(q0, q1, q2, I.gamma);
         const double u = q1 / q0;
+        nf |= !isfinite(absd(u) + s);
         mv = maxd(mv, absd(u) + s);
     }
     mv = block_max(mv, dred);
@@ -484,15 +488,16 @@ __device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, u
     }
 
     bc1(c, c.q);
-    const double a1 = lf_speed1(c, 3, 3, dred);
+    const double a1 = lf_speed1(c, 3, 3, dred, nf);
     copy_q(c, c.qc);
     stage1<SCHEME>(c, 2, 2, a1, dt, 1, list, ured);
     bc1(c, c.q);
-    const double a2 = lf_speed1(c, 2, 2, dred);
+    const double a2 = lf_speed1(c, 2, 2, dred, nf);
     stage1<SCHEME>(c, 1, 1, a2, dt, 2, list, ured);
     bc1(c, c.q);
-    const double a3 = lf_speed1(c, 1, 1, dred);
+    const double a3 = lf_speed1(c, 1, 1, dred, nf);
     stage1<SCHEME>(c, 0, 0, a3, dt, 3, list, ured);
+    const bool any_nf = __syncthreads_or(nf);
     // RemoveResidue (AWCM_MANAGER_1D.h:135-157)
     for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
         if (!c.bit(i, 0)) c.Q(0, i) = c.Q(1, i) = c.Q(2, i) = 0;
@@ -509,6 +514,12 @@ __device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, u
         I.steps += 1;
         I.t += dt;
         I.done = I.t >= I.t_end;
+        if (any_nf) {
+            // not a valid gas state: the instance stops and reports it (the reference carries
+            // the NaN on)
+            I.err = kErrNonFinite;
+            I.done = 1;
+        }
     }
     __syncthreads();
 }
@@ -653,7 +664,7 @@ __device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
 template <int SCHEME>
 __device__ void step_instance(Inst1& I, const Pool& P, uint32_t* list, double* dred, unsigned* ured)
 {
-    if (I.t >= I.t_end) {
+    if (I.t >= I.t_end || I.err) {
         if (threadIdx.x == 0) I.done = 1;
         return;
     }
@@ -901,6 +912,7 @@ struct Batch1D {
             I.t = t[k];
             I.t_end = t_end[k];
             I.dt_fixed = dt_fixed;
+            I.err = 0;
             I.done = I.t >= I.t_end;
         }
         AWCM_CUDA_TRY(upload_inst());
@@ -1222,6 +1234,15 @@ int awcm1d_batch_status(awcm1d_batch_t h, int k, double* out)
     out[13] = (double)I.upd;
     out[14] = I.err;
     out[15] = 0;
+    if (I.err == awcm::kErrNonFinite) {
+        char msg[200];
+        std::snprintf(msg, sizeof(msg),
+                      "instance %d: non-finite state: a CFL or Lax-Friedrichs wave speed was NaN or infinite in "
+                      "the step ending at t = %.17g (NaN/Inf values, negative pressure or density)",
+                      k, I.t);
+        awcm::set_last_error(msg, __FILE__, __LINE__);
+        return I.err;
+    }
     return awcm::kOk;
 }
 int awcm1d_batch_totals(awcm1d_batch_t h, double* out)

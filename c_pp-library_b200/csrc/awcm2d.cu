@@ -41,6 +41,8 @@ struct StepState {
     unsigned bar[2];               // grid barrier of the persistent prepare: arrivals, generation
     int bar_err;                   // set when a barrier wait ran out (or another CTA failed)
     int error;                     // first error of the run (reported by the host API)
+    int nonfinite;                 // set when a CFL or LF wave speed of the step is NaN or infinite
+    unsigned spin_limit;           // polls before a grid-barrier wait gives up (0 = kSpinLimit)
 };
 
 __device__ __forceinline__ int ctz_or(int v, int big) { return v == 0 ? big : __ffs(v) - 1; }
@@ -918,6 +920,7 @@ struct GridSync {
     unsigned* gen;
     int* err;
     unsigned nb;
+    unsigned limit;  // polls before a wait gives up
     __device__ bool sync() const
     {
         __syncthreads();
@@ -933,7 +936,7 @@ struct GridSync {
                 } else {
                     unsigned spins = 0;
                     while (G.load(cuda::memory_order_acquire) == my) {
-                        if (++spins > kSpinLimit || *ve) {
+                        if (++spins > limit || *ve) {
                             atomicCAS(err, 0, (int)kErrTimeout);
                             break;
                         }
@@ -970,7 +973,7 @@ __global__ void __launch_bounds__(kPrepThreads, 1) k_prepare(PrepArgs A)
     if (A.st->done) return;
     const Grid2& g = A.g;
     const Span sp = grid_span();
-    const GridSync gs{A.sync, A.sync + 1, A.err, gridDim.x};
+    const GridSync gs{A.sync, A.sync + 1, A.err, gridDim.x, A.st->spin_limit ? A.st->spin_limit : kSpinLimit};
     const double tol = A.st->tol;
 #define SYNC_OR_LEAVE \
     if (!gs.sync()) return
@@ -1131,7 +1134,8 @@ __global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, doub
 // lane) x 32 rows (four per warp); empty words cost one load.  Maxima are order-independent.
 constexpr int kAlphaRows = 4;
 __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t* __restrict__ m, int bit,
-                                               double* ax, double* ay, double* mv, const StepState* st)
+                                               double* ax, double* ay, double* mv, const StepState* st,
+                                               int* nonfinite)
 {
     pdl_begin();
     if (st && st->done) return;
@@ -1144,6 +1148,7 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
     const unsigned* mp = reinterpret_cast<const unsigned*>(m);
     double cm[4] = {0, 0, 0, 0};
     double vmax = 0;
+    bool nf = false;  // a NaN or infinite speed (NaN/Inf state, negative pressure or density)
     for (int r = 0; r < kAlphaRows; ++r) {
         const int j = (int)blockIdx.y * (8 * kAlphaRows) + warp * kAlphaRows + r;
         double sx_row = 0;
@@ -1158,6 +1163,7 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
                 const double c = sound2(q, g.gamma);
                 const double sx = absd(q[1] / q[0]) + c;
                 const double sy = absd(q[2] / q[0]) + c;
+                nf |= !(isfinite(sx) && isfinite(sy));
                 sx_row = maxd(sx_row, sx);
                 cm[L] = maxd(cm[L], sy);
                 vmax = maxd(vmax, sx + sy);
@@ -1166,6 +1172,7 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
         const double rowmax = warp_max(sx_row);
         if (lane == 0 && j < g.ny && rowmax > 0) atomic_max_nonneg(&ax[j], rowmax);
     }
+    if (nonfinite && __any_sync(0xffffffffu, nf) && lane == 0) atomicOr(nonfinite, 1);
 #pragma unroll
     for (int L = 0; L < 4; ++L) col[warp][4 * lane + L] = cm[L];
     vmax = warp_max(vmax);
@@ -1194,10 +1201,11 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
 __device__ void alpha_list_run(const Grid2& g, Field4 f, const uint32_t* __restrict__ la,
                                const unsigned* __restrict__ na, const uint32_t* __restrict__ lb,
                                const unsigned* __restrict__ nb, double* ax, double* ay, unsigned first,
-                               unsigned stride)
+                               unsigned stride, int* nonfinite)
 {
     const unsigned n0 = *na, n = n0 + *nb;
     const int lane = threadIdx.x & 31;
+    bool nf = false;
     for (unsigned base = first + (threadIdx.x & ~31u); base < n; base += stride) {
         const unsigned e = base + (unsigned)lane;
         const bool on = e < n;
@@ -1211,6 +1219,7 @@ __device__ void alpha_list_run(const Grid2& g, Field4 f, const uint32_t* __restr
             const double c = sound2(q, g.gamma);
             sx = absd(q[1] / q[0]) + c;
             const double sy = absd(q[2] / q[0]) + c;
+            nf |= !(isfinite(sx) && isfinite(sy));
             if (sy > 0) atomic_max_nonneg(&ay[i], sy);
         }
         const int jp = __shfl_up_sync(0xffffffffu, j, 1);
@@ -1225,17 +1234,18 @@ __device__ void alpha_list_run(const Grid2& g, Field4 f, const uint32_t* __restr
         const int jn = __shfl_down_sync(0xffffffffu, j, 1);
         if (on && (lane == 31 || jn != j) && v > 0) atomic_max_nonneg(&ax[j], v);
     }
+    if (nonfinite && __any_sync(0xffffffffu, nf) && lane == 0) atomicOr(nonfinite, 1);
 }
 
 __global__ void __launch_bounds__(256) k_alpha_list(Grid2 g, Field4 f, const uint32_t* __restrict__ la,
                                                     const unsigned* __restrict__ na,
                                                     const uint32_t* __restrict__ lb,
                                                     const unsigned* __restrict__ nb, double* ax, double* ay,
-                                                    const StepState* st)
+                                                    const StepState* st, int* nonfinite)
 {
     pdl_begin();
     if (st->done) return;
-    alpha_list_run(g, f, la, na, lb, nb, ax, ay, blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
+    alpha_list_run(g, f, la, na, lb, nb, ax, ay, blockIdx.x * blockDim.x, gridDim.x * blockDim.x, nonfinite);
 }
 
 // Boundary fill and LF speeds of stage 2 or 3 in one launch: the fill writes only ghost cells and
@@ -1245,7 +1255,7 @@ __global__ void __launch_bounds__(256) k_bc_alpha(Grid2 g, Field4 f, const uint3
                                                   const unsigned* __restrict__ na,
                                                   const uint32_t* __restrict__ lb,
                                                   const unsigned* __restrict__ nb, double* ax, double* ay,
-                                                  const StepState* st, unsigned bc_blocks)
+                                                  const StepState* st, unsigned bc_blocks, int* nonfinite)
 {
     pdl_begin();
     if (st->done) return;
@@ -1254,7 +1264,7 @@ __global__ void __launch_bounds__(256) k_bc_alpha(Grid2 g, Field4 f, const uint3
         return;
     }
     alpha_list_run(g, f, la, na, lb, nb, ax, ay, (blockIdx.x - bc_blocks) * blockDim.x,
-                   (gridDim.x - bc_blocks) * blockDim.x);
+                   (gridDim.x - bc_blocks) * blockDim.x, nonfinite);
 }
 
 // dt = cfl dx / max speed, clipped to the output time (main_2d_euler(quad).cpp:76-83), and the
@@ -1289,6 +1299,7 @@ __global__ void k_begin(StepState* st, int keep_lists)
     if (st->done) return;
     st->bar[0] = 0;
     st->bar_err = 0;
+    st->nonfinite = 0;
     st->mv = 0;
     if (keep_lists) return;
     for (int k = 0; k < 4 * kStages; ++k) st->cnt[k] = 0;
@@ -1319,6 +1330,11 @@ __global__ void k_finish(StepState* st)
     st->upd += st->mask_cnt[0];
     st->stage_pts += (unsigned long long)st->mask_cnt[2] + st->mask_cnt[1] + st->mask_cnt[0];
     st->full_zero = 0;
+    if (st->nonfinite) {
+        // a NaN or infinite wave speed: the state is not a valid gas state; stop and report
+        st->error = kErrNonFinite;
+        st->done = 1;
+    }
 }
 
 // ------------------------------------------------------------------------------------ worklists
@@ -2287,7 +2303,7 @@ struct Solver2D {
     {
         dim3 grid((unsigned)(g.pitch / 4 + 31) / 32, (unsigned)(g.ny + 8 * kAlphaRows - 1) / (8 * kAlphaRows));
         launch(k_alpha, grid, 256, g, f, m, bit, axp ? axp : ax[stage], ayp ? ayp : ay[stage],
-               with_cfl ? &st->mv : nullptr, st);
+               with_cfl ? &st->mv : nullptr, st, with_cfl ? &st->nonfinite : nullptr);
         after("k_alpha");
         launches += 1;
     }
@@ -2299,17 +2315,17 @@ struct Solver2D {
         const unsigned* C = st->cnt + 4 * ls;
         const unsigned bcb = blocks_for(2L * kGhost * g.ny + 2L * kGhost * g.nx, 256);
         launch(k_bc_alpha, bcb + face_blocks / 2, 256, g, f, lists[4 * ls], C, lists[4 * ls + 1], C + 1, ax[stage],
-               ay[stage], st, bcb);
+               ay[stage], st, bcb, &st->nonfinite);
         after("k_bc_alpha");
         launches += 1;
     }
     // Stage `stage` (1 or 2) over the points of the previous stage's update lists (its mask).
-    void enq_alpha_listed(Field4 f, int stage, double* axp = nullptr, double* ayp = nullptr)
+    void enq_alpha_listed(Field4 f, int stage, double* axp = nullptr, double* ayp = nullptr, int* nonfinite = nullptr)
     {
         const int ls = stage - 1;
         const unsigned* C = st->cnt + 4 * ls;
         launch(k_alpha_list, face_blocks / 2, 256, g, f, lists[4 * ls], C, lists[4 * ls + 1], C + 1,
-               axp ? axp : ax[stage], ayp ? ayp : ay[stage], st);
+               axp ? axp : ax[stage], ayp ? ayp : ay[stage], st, nonfinite);
         after("k_alpha_list");
         launches += 1;
     }
@@ -2479,8 +2495,38 @@ struct Solver2D {
         h.done = 0;
         h.error = 0;
         h.bar_err = 0;
+        h.nonfinite = 0;
         h.bar[0] = 0;
         AWCM_CUDA_TRY(cudaMemcpyAsync(st, &h, sizeof(StepState), cudaMemcpyHostToDevice, stream));
+        return kOk;
+    }
+
+    // Status of a run whose device-side error word is set, with its text.
+    static int report_error(const StepState& h)
+    {
+        if (h.error == kErrNonFinite) {
+            char msg[200];
+            std::snprintf(msg, sizeof(msg),
+                          "non-finite state: a CFL or Lax-Friedrichs wave speed was NaN or infinite in the "
+                          "step ending at t = %.17g (NaN/Inf values, negative pressure or density)",
+                          h.t);
+            set_last_error(msg, __FILE__, __LINE__);
+        } else {
+            set_last_error("grid barrier wait ran out in the prepare kernel", __FILE__, __LINE__);
+        }
+        return h.error;
+    }
+
+    // Test-only: polls before a grid-barrier wait of the persistent prepare kernel gives up
+    // (0 restores the default).
+    int set_spin_limit(unsigned polls)
+    {
+        StepState h;
+        int rc = read_state(&h);
+        if (rc) return rc;
+        h.spin_limit = polls;
+        AWCM_CUDA_TRY(cudaMemcpyAsync(st, &h, sizeof(StepState), cudaMemcpyHostToDevice, stream));
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
     }
 
@@ -2501,10 +2547,7 @@ struct Solver2D {
         StepState h;
         rc = read_state(&h);
         if (rc) return rc;
-        if (h.error) {
-            set_last_error("grid barrier wait ran out in the prepare kernel", __FILE__, __LINE__);
-            return h.error;
-        }
+        if (h.error) return report_error(h);
         if (out) {
             out[0] = h.dt;
             out[1] = h.do_print;
@@ -2528,10 +2571,7 @@ struct Solver2D {
         StepState h;
         rc = read_state(&h);
         if (rc) return rc;
-        if (h.error) {
-            set_last_error("grid barrier wait ran out in the prepare kernel", __FILE__, __LINE__);
-            return h.error;
-        }
+        if (h.error) return report_error(h);
         if (out) {
             out[0] = h.t;
             out[1] = h.steps - h0.steps;
@@ -3302,6 +3342,11 @@ int awcm2d_set_prepare_mode(awcm2d_t h, int mode)
     if (h->s.graph) cudaGraphExecDestroy(h->s.graph);
     h->s.graph = nullptr;
     return awcm::kOk;
+}
+int awcm2d_set_spin_limit(awcm2d_t h, unsigned polls)
+{
+    AWCM_H(h);
+    return h->s.set_spin_limit(polls);
 }
 int awcm2d_frozen_run(awcm2d_t h, double t0, double dt, int n_steps, int mode, double* out)
 {

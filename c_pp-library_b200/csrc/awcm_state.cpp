@@ -166,6 +166,11 @@ int awcm2d_load_state(awcm2d_t h, const char* path, double* t, long long* step)
         std::fclose(f);
         return fail(AWCM_ERR_STATE, "state file geometry differs from the instance");
     }
+    if (hd.gamma != geo->gamma) {
+        // energies and pressures of the stored state belong to another ratio of specific heats
+        std::fclose(f);
+        return fail(AWCM_ERR_STATE, "state file gamma differs from the instance");
+    }
     const size_t ng = (size_t)(nx + 6) * (ny + 6), ni = (size_t)nx * ny, plane_bytes = (ng + 7) / 8;
     const size_t expect = 5 * plane_bytes + 4 * ni + (size_t)hd.n_active * 4 * sizeof(double);
     if (hd.payload_bytes != expect || hd.n_active > ni) {

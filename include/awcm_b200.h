@@ -116,7 +116,11 @@ int awcm2d_apply_bc(awcm2d_t h, double t);
 /* One pass of the reference driver loop (Wavelet/main_2d_euler(quad).cpp:58-334): PrepareEuler,
  * CFL dt (clipped to t_next), three SSP-RK3 stages with WENO-Z/Roe fluxes on the finest level and
  * 4th-order central differences on coarser levels, PostProcessEuler.  dt_fixed > 0 replaces the
- * CFL step.  out[8]: dt, do_print, |mask0..mask3|, max wave speed, (unused).  Synchronous. */
+ * CFL step.  out[8]: dt, do_print, |mask0..mask3|, max wave speed, (unused).  Synchronous.
+ * A wave speed |u|+c or |v|+c that is NaN or infinite at a point of the CFL scan (mask3) or of a
+ * stage's Lax-Friedrichs scan (NaN/Inf in the state, negative pressure or density) ends the step
+ * with AWCM_ERR_NONFINITE (the reference has no such check and carries the NaN on); the next call
+ * starts clean, so a caller can restore a state and continue.  awcm2d_advance stops at that step. */
 int awcm2d_step(awcm2d_t h, double tol, double cfl, double t, double t_next, double dt_fixed, double* out);
 /* Advances n_steps steps from the device-held time without host round trips (one CUDA graph per
  * step), stopping early once t >= t_end.  out[4]: final t, steps taken, sum |mask0| over the steps,
@@ -138,6 +142,11 @@ int awcm2d_launches_per_step(awcm2d_t h, int* n);
 /* PrepareEuler execution: 1 = one kernel launch per pass (default), 0 = one persistent
  * cooperative kernel with bounded-spin grid barriers.  Both give identical results. */
 int awcm2d_set_prepare_mode(awcm2d_t h, int mode);
+/* Test and fault-injection hook (no counterpart in the reference): the number of polls after which
+ * a grid-barrier wait of the persistent PrepareEuler kernel (mode 0) gives up.  An expired wait
+ * makes every CTA leave at its next barrier and the step return AWCM_ERR_TIMEOUT with the device
+ * usable; the next step starts clean.  0 restores the default (2^22 polls, well over a second). */
+int awcm2d_set_spin_limit(awcm2d_t h, unsigned polls);
 /* CUDA stream the instance runs on (cudaStream_t), for event timing by the caller. */
 int awcm2d_stream(awcm2d_t h, void** stream);
 
@@ -248,7 +257,10 @@ int awcm1d_batch_set_run(awcm1d_batch_t h, const double* tol, const double* cfl,
 int awcm1d_batch_steps(awcm1d_batch_t h, int n_steps);
 int awcm1d_batch_sync(awcm1d_batch_t h);
 /* out[16]: t, dt, do_print, done, steps, |mask0..mask3|, max speed, alpha of stages 1..3,
- * sum over steps of |mask0|, error code, 0. */
+ * sum over steps of |mask0|, error code, 0.  An instance whose CFL or Lax-Friedrichs scan met a
+ * NaN or infinite wave speed (NaN/Inf state, negative pressure or density) stops stepping, and its
+ * status call fills `out` (out[14] = AWCM_ERR_NONFINITE) and returns AWCM_ERR_NONFINITE; set_run
+ * clears the flag.  The reference has no such check. */
 int awcm1d_batch_status(awcm1d_batch_t h, int k, double* out);
 /* out[3]: sum over instances and steps of |mask0|, total steps, finished instances. */
 int awcm1d_batch_totals(awcm1d_batch_t h, double* out);
@@ -274,7 +286,10 @@ int awcm1d_batch_stream(awcm1d_batch_t h, void** stream);
  *   state_dev (in/out) Nx+6 mask bytes (bits 0..3 = mask0..mask3, bit 4 = previous mask0;
  *             before the first step: 0x01 inside, 0xe1 on the ghost ring) followed by 4 planes of
  *             Nx+6 int8 levels (level0..level3; start at 0);
- *   out_dev   (out) 16 doubles in the layout of awcm1d_batch_status.
+ *   out_dev   (out) 16 doubles in the layout of awcm1d_batch_status, for this call only: out[4]
+ *             (steps) is 1 after a step and 0 when t >= t_end already, out[13] is this step's
+ *             |mask0| (not a running sum), out[14] is AWCM_ERR_NONFINITE when a wave speed of the
+ *             step was NaN or infinite, else 0.
  * Nx = (nx_coarse-1)*2^(num_levels-1)+1 must not exceed 8193; larger instances are rejected with
  * AWCM_ERR_ARG.  The work is enqueued on `stream` (0 = default stream) and the call returns
  * without waiting.  The first call on a device resolves the scratch array's device address (a

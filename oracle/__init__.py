@@ -26,7 +26,20 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "_build", "libawcm_oracle.so")
 REF_LIB_1D = os.path.join(HERE, "_ref", "libawcm_ref1d.so")
 REF_LIB_2D = os.path.join(HERE, "_ref", "libawcm_ref2d.so")
-REFERENCE_TREE = "/root/reference"
+
+
+def reference_tree() -> str:
+    """Location of the reference source tree: $AWCM_REFERENCE_TREE, else the default of the build
+    recipe (oracle/Makefile, variable REF).  The tree is read only to build oracle/_ref."""
+    env = os.environ.get("AWCM_REFERENCE_TREE")
+    if env:
+        return env
+    try:
+        r = subprocess.run(["make", "-s", "--no-print-directory", "-C", HERE, "print-ref"], capture_output=True,
+                           text=True, timeout=30)
+        return r.stdout.strip()
+    except Exception:
+        return ""
 
 # manager op codes shared by both checkers and by the product's C-ABI
 AAZ, CR, APD, CL, RR, BAND = 0, 1, 2, 3, 4, 5
@@ -38,11 +51,12 @@ _dp = ctypes.POINTER(ctypes.c_double)
 def build(with_reference: bool | None = None) -> None:
     """Compiles the restatement, and the reference harness when the reference tree exists."""
     targets = ["oracle"]
+    tree = reference_tree()
     if with_reference is None:
-        with_reference = os.path.isdir(REFERENCE_TREE)
+        with_reference = bool(tree) and os.path.isdir(tree)
     if with_reference:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE] + targets + ([f"REF={tree}"] if tree else []), check=True)
 
 
 def reference_available() -> bool:
@@ -314,3 +328,13 @@ class Oracle2D:
         out = np.zeros(2)
         n = self._run(self.h, tol, cfl, t_end, max_steps, _ptr(out, ctypes.c_double))
         return n, out[0], out[1]
+
+
+def run_tube(tube: dict, tol: float, cfl: float, t_end: float, scheme: int = 0, kind: str = "port"):
+    """One 1D Riemann tube (a dict with num_levels, nx_coarse, x_min, x_max, x_interface, left,
+    right) run from its initial state to t_end.  Returns (steps, t, sum |mask0|, q, masks, levels).
+    A module-level function so that a process pool can run tubes side by side."""
+    o = Oracle1D(tube["num_levels"], tube["nx_coarse"], tube["x_min"], tube["x_max"], scheme=scheme, kind=kind)
+    o.init_riemann(tube["x_interface"], tube["left"], tube["right"])
+    n, t, upd = o.run(tol, cfl, t_end)
+    return n, t, upd, o.get_q(), o.get_masks(), o.get_levels()

@@ -21,8 +21,12 @@ def _built():
     """Builds the checker library (and the product library when nvcc exists) once per session."""
     import oracle
 
-    if not os.path.exists(oracle.PORT_LIB) or (os.path.isdir(oracle.REFERENCE_TREE) and not oracle.reference_available()):
+    if not os.path.exists(oracle.PORT_LIB):
         oracle.build()
+    elif not oracle.reference_available():
+        tree = oracle.reference_tree()
+        if tree and os.path.isdir(tree):
+            oracle.build()
     yield
 
 

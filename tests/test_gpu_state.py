@@ -76,6 +76,7 @@ def test_damaged_and_mismatched_files_rejected(tmp_path, awcm_lib):
     s, t = gpu_stepped(awcm_lib, 2)
     p = tmp_path / "g.bin"
     s.save_state(p, t, 2)
+    q_before, m_before = s.get_q(), s.get_masks()
     raw = bytearray(p.read_bytes())
     raw[300] ^= 0x10
     bad = tmp_path / "bad.bin"
@@ -87,3 +88,19 @@ def test_damaged_and_mismatched_files_rejected(tmp_path, awcm_lib):
         other.load_state(p)
     with pytest.raises(awcm_lib.AwcmError):
         s.load_state(tmp_path / "missing.bin")
+    short = tmp_path / "short.bin"
+    short.write_bytes(p.read_bytes()[:-16])
+    with pytest.raises(awcm_lib.AwcmError, match="truncated payload"):
+        s.load_state(short)
+    short.write_bytes(p.read_bytes()[:100])
+    with pytest.raises(awcm_lib.AwcmError, match="truncated header"):
+        s.load_state(short)
+    # a state of another gas (gamma 1.3) is refused: its energies mean other pressures
+    r = read_state(p)
+    g13 = tmp_path / "g13.bin"
+    write_state(g13, r["geometry"][:-1] + (1.3,), r["q"], r["masks"], r["levels"], r["t"], r["step"])
+    with pytest.raises(awcm_lib.AwcmError, match="gamma") as ei:
+        s.load_state(g13)
+    assert ei.value.status == 6
+    # every rejection above left the instance as it was
+    assert np.array_equal(s.get_q(), q_before) and np.array_equal(s.get_masks(), m_before)
