@@ -6,11 +6,11 @@ include/awcm_b200.h); this package binds it with ctypes and mirrors the referenc
 from ._lib import AwcmError, LIB_PATH, exported_symbols, load
 from .solvers import (AAZ, APD, BAND, BC_DOUBLE_MACH, BC_PERIODIC, BC_TRANSMISSIVE, CL, CR, PROBLEM_DOUBLE_MACH,
                       PROBLEM_QUADRANTS, PROBLEM_VORTEX, RR, SCALAR_ADVECTION, WENO5, WENOZ, AWCM1D, AWCM1DBatch, AWCM1DScalar, AWCM2D,
-                      AWCM2DScalar,
+                      AWCM2DScalar, euler_flux, euler_spectral_radius,
                       measure_fp64_peak)
 
 __all__ = [
-    "AwcmError", "measure_fp64_peak", "LIB_PATH", "exported_symbols", "load", "AWCM1D", "AWCM1DBatch", "AWCM1DScalar", "AWCM2D", "AWCM2DScalar",
+    "AwcmError", "measure_fp64_peak", "euler_flux", "euler_spectral_radius", "LIB_PATH", "exported_symbols", "load", "AWCM1D", "AWCM1DBatch", "AWCM1DScalar", "AWCM2D", "AWCM2DScalar",
     "AAZ", "CR", "APD", "CL", "RR", "BAND", "BC_TRANSMISSIVE", "BC_DOUBLE_MACH", "BC_PERIODIC",
     "PROBLEM_QUADRANTS", "PROBLEM_DOUBLE_MACH", "PROBLEM_VORTEX", "WENOZ", "WENO5", "SCALAR_ADVECTION",
 ]

@@ -78,10 +78,18 @@ _SIGS = {
     "awcm1d_batch_status": [c_void_p, c_int, P_double],
     "awcm1d_batch_totals": [c_void_p, P_double],
     "awcm1d_batch_pass": [c_void_p, c_int, c_int, c_int, c_int],
+    "awcm1d_batch_prepare": [c_void_p, c_int, c_double],
+    "awcm1d_batch_fwt": [c_void_p, c_int, c_double],
+    "awcm1d_batch_iwt": [c_void_p, c_int, c_int],
+    "awcm1d_batch_interpolate": [c_void_p, c_int, c_int, c_int],
+    "awcm1d_batch_manager": [c_void_p, c_int, c_int, c_int, c_int],
+    "awcm1d_batch_apply_bc": [c_void_p, c_int],
     "awcm1d_batch_set_launch": [c_void_p, c_int, c_int],
     "awcm1d_batch_stream": [c_void_p, ctypes.POINTER(c_void_p)],
     "awcm1d_step_noalloc": [c_int, c_int, c_double, c_double, c_double, c_int, c_double, c_double, c_double, c_double,
                             c_void_p, c_void_p, c_void_p, c_void_p],
+    "euler1d_flux": [c_void_p, c_void_p, c_int, c_double, c_void_p],
+    "euler1d_spectral_radius": [c_void_p, c_void_p, c_int, c_double, c_void_p],
     "euler2d_flux": [c_void_p, c_void_p, c_int, c_int, c_double, c_void_p],
     "euler2d_spectral_radius": [c_void_p, c_void_p, c_int, c_int, c_double, c_void_p],
     "awcm_last_error": [],

@@ -27,6 +27,24 @@ WENOZ, WENO5 = 0, 1
 SCALAR_ADVECTION = 2
 
 
+def euler_flux(q_dev, f_dev, n: int, dim: int, direction: int = 0, gamma: float = 1.4, stream=None):
+    """EULER_EQUATION_1D::ComputeFu (dim 1) or EULER_EQUATION_2D::ComputeFu / ComputeGu (dim 2,
+    direction 0 / 1) on n device-resident states; q_dev, f_dev are device addresses (ints)."""
+    if dim == 1:
+        call("euler1d_flux", q_dev, f_dev, n, gamma, stream)
+    else:
+        call("euler2d_flux", q_dev, f_dev, n, direction, gamma, stream)
+
+
+def euler_spectral_radius(q_dev, s_dev, n: int, dim: int, direction: int = 0, gamma: float = 1.4, stream=None):
+    """EULER_EQUATION_1D::Spectral_Radius or EULER_EQUATION_2D::Spectral_RadiusX / Y on n
+    device-resident states."""
+    if dim == 1:
+        call("euler1d_spectral_radius", q_dev, s_dev, n, gamma, stream)
+    else:
+        call("euler2d_spectral_radius", q_dev, s_dev, n, direction, gamma, stream)
+
+
 def measure_fp64_peak(iters: int = 20000, repeats: int = 5) -> float:
     """Dense FP64 FMA throughput of the current device, TFLOP/s."""
     v = ctypes.c_double()
@@ -472,18 +490,28 @@ class AWCM1D:
         self.b.init_riemann(0, x_interface, left, right)
 
     def prepare(self, tol):
-        self.b.set_run(tol, 0.5, 0.0, 1.0)
-        self.b.pass_(0, 10, 0, 0)
+        """AWCM_1D::PrepareEuler(Q, tol)."""
+        call("awcm1d_batch_prepare", self.b.h, 0, tol)
 
     def fwt(self, tol):
-        self.b.set_run(tol, 0.5, 0.0, 1.0)
-        self.b.pass_(0, 11, 0, 0)
+        """WAVELET_1D::ForwardWaveletTransformEuler(Q, mra, mask0, tol)."""
+        call("awcm1d_batch_fwt", self.b.h, 0, tol)
 
     def iwt(self, mask_id=3):
-        self.b.pass_(0, 12, mask_id, 0)
+        """WAVELET_1D::InverseWaveletTransformEuler(Q, mra, mask)."""
+        call("awcm1d_batch_iwt", self.b.h, 0, mask_id)
+
+    def interpolate(self, from_id=4, to_id=3):
+        """WAVELET_1D::InterpolateEuler(Q, mra, mask_from, mask_to)."""
+        call("awcm1d_batch_interpolate", self.b.h, 0, from_id, to_id)
 
     def manager(self, op, mask_id, level_id=0):
-        self.b.pass_(0, op, mask_id, level_id)
+        """AWCM_MANAGER_1D pass `op` (AAZ, CR, APD, CL, RR, BAND) on mask `mask_id`."""
+        call("awcm1d_batch_manager", self.b.h, 0, op, mask_id, level_id)
+
+    def apply_bc(self):
+        """The instance's ghost fill (the transmissive BOUNDARY_MANAGER)."""
+        call("awcm1d_batch_apply_bc", self.b.h, 0)
 
     def step(self, tol, cfl, t, t_next):
         """One driver-loop pass; returns the checker's out[10] (dt, do_print, |mask0..3|, alphas, speed)."""

@@ -739,8 +739,30 @@ __global__ void k_pass1d(Inst1* insts, int inst, Pool P, int op, int bit, int le
             break;
         case 11: fwt1(c); break;
         case 12: iwt1(c, bit); break;
+        case 13: interp1(c, bit, level_id); break;  // InterpolateEuler(from = bit, to = level_id as a bit)
+        case 14: bc1(c, c.q); break;
         default: break;
     }
+}
+
+// EULER_EQUATION_1D batch entry points (EULER_EQUATION.h:16-26, 42-47): n states of 3 doubles.
+__global__ void k_euler1d_flux(const double* __restrict__ q, double* __restrict__ f, int n, double gamma)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double s[3] = {q[3 * t], q[3 * t + 1], q[3 * t + 2]};
+    double o[3];
+    flux1(s, gamma, o);
+    for (int k = 0; k < 3; ++k) f[3 * t + k] = o[k];
+}
+
+__global__ void k_euler1d_sr(const double* __restrict__ q, double* __restrict__ out, int n, double gamma)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double q0 = q[3 * t], q1 = q[3 * t + 1], q2 = q[3 * t + 2];
+    const double u = q1 / q0;
+    out[t] = absd(u) + sound1(q0, q1, q2, gamma);
 }
 
 }  // namespace
@@ -925,6 +947,15 @@ struct Batch1D {
         if (rc) return rc;
         for (int s = 0; s < n_steps; ++s) AWCM_CUDA_TRY(cudaGraphLaunch(graph, stream));
         AWCM_CUDA_TRY(cudaGetLastError());
+        return kOk;
+    }
+
+    // Threshold of instance k for a single-pass call (the step takes it from set_run).
+    int set_tol(int k, double tol)
+    {
+        AWCM_CUDA_TRY(download_inst());
+        host[k].tol = tol;
+        AWCM_CUDA_TRY(upload_inst());
         return kOk;
     }
 
@@ -1268,6 +1299,64 @@ int awcm1d_batch_pass(awcm1d_batch_t h, int k, int op, int mask_id, int level_id
     if (level_id < 0 || level_id > 3) return awcm::kErrArg;
     return h->b.pass(k, op, bit, level_id);
 }
+static int bit_of_mask(int mask_id) { return mask_id >= 0 && mask_id <= 3 ? mask_id : awcm::kBitTemp; }
+static bool mask_id_ok(int mask_id) { return mask_id >= 0 && mask_id <= 4; }
+
+int awcm1d_batch_prepare(awcm1d_batch_t h, int k, double tol)
+{
+    AWCM_B(h, k);
+    const int rc = h->b.set_tol(k, tol);
+    return rc ? rc : h->b.pass(k, 10, 0, 0);
+}
+int awcm1d_batch_fwt(awcm1d_batch_t h, int k, double tol)
+{
+    AWCM_B(h, k);
+    const int rc = h->b.set_tol(k, tol);
+    return rc ? rc : h->b.pass(k, 11, 0, 0);
+}
+int awcm1d_batch_iwt(awcm1d_batch_t h, int k, int mask_id)
+{
+    AWCM_B(h, k);
+    if (!mask_id_ok(mask_id)) return awcm::kErrArg;
+    return h->b.pass(k, 12, bit_of_mask(mask_id), 0);
+}
+int awcm1d_batch_interpolate(awcm1d_batch_t h, int k, int from_id, int to_id)
+{
+    AWCM_B(h, k);
+    if (!mask_id_ok(from_id) || !mask_id_ok(to_id)) return awcm::kErrArg;
+    return h->b.pass(k, 13, bit_of_mask(from_id), bit_of_mask(to_id));
+}
+int awcm1d_batch_manager(awcm1d_batch_t h, int k, int op, int mask_id, int level_id)
+{
+    AWCM_B(h, k);
+    if (op < AWCM_OP_ADD_ADJACENT_ZONE || op > AWCM_OP_BANDING || !mask_id_ok(mask_id) || level_id < 0 ||
+        level_id > 3)
+        return awcm::kErrArg;
+    return h->b.pass(k, op, bit_of_mask(mask_id), level_id);
+}
+int awcm1d_batch_apply_bc(awcm1d_batch_t h, int k)
+{
+    AWCM_B(h, k);
+    return h->b.pass(k, 14, 0, 0);
+}
+
+int euler1d_flux(const double* q_dev, double* f_dev, int n, double gamma, void* stream)
+{
+    if (n < 0 || (n && (!q_dev || !f_dev))) return awcm::kErrArg;
+    if (!n) return awcm::kOk;
+    awcm::k_euler1d_flux<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(q_dev, f_dev, n, gamma);
+    AWCM_CUDA_TRY(cudaGetLastError());
+    return awcm::kOk;
+}
+int euler1d_spectral_radius(const double* q_dev, double* s_dev, int n, double gamma, void* stream)
+{
+    if (n < 0 || (n && (!q_dev || !s_dev))) return awcm::kErrArg;
+    if (!n) return awcm::kOk;
+    awcm::k_euler1d_sr<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(q_dev, s_dev, n, gamma);
+    AWCM_CUDA_TRY(cudaGetLastError());
+    return awcm::kOk;
+}
+
 int awcm1d_batch_set_launch(awcm1d_batch_t h, int threads, int ctas_per_sm)
 {
     if (!h) return awcm::kErrArg;

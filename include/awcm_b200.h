@@ -267,6 +267,21 @@ int awcm1d_batch_totals(awcm1d_batch_t h, double* out);
 /* AWCM_MANAGER_1D pass (AWCM_OP_*) on instance k; also 10 = PrepareEuler (AWCM_1D.h:86-120),
  * 11 = ForwardWaveletTransformEuler (WAVELET_1D.h:282-335), 12 = InverseWaveletTransformEuler(mask). */
 int awcm1d_batch_pass(awcm1d_batch_t h, int k, int op, int mask_id, int level_id);
+/* Typed single passes on instance k (the AWCM_1D facade of Wavelet/AWCM_1D.h and the static passes
+ * it calls); mask ids 0..3 = mask0..mask3, 4 = mask_temp; synchronous.
+ *   AWCM_1D::PrepareEuler(Q, tol)                       Wavelet/AWCM_1D.h:86-120
+ *   WAVELET_1D::ForwardWaveletTransformEuler(Q, mra, mask0, tol)   Wavelet/WAVELET_1D.h:282-335
+ *   WAVELET_1D::InverseWaveletTransformEuler(Q, mra, mask)         Wavelet/WAVELET_1D.h:337-391
+ *   WAVELET_1D::InterpolateEuler(Q, mra, mask_from, mask_to)       Wavelet/WAVELET_1D.h:393-431
+ *   AWCM_MANAGER_1D::<op>(mask[, level]) for op = AWCM_OP_*        Wavelet/AWCM_MANAGER_1D.h:14-157,
+ *     AWCM_OP_BANDING = AWCM_1D::BadingBoundary                    Wavelet/AWCM_1D.h:73-80
+ *   BOUNDARY_MANAGER::SetBoundaryCondition() (transmissive)        Problems/1D/PROBLEM_SHOCKTUBE.h:86-107 */
+int awcm1d_batch_prepare(awcm1d_batch_t h, int k, double tol);
+int awcm1d_batch_fwt(awcm1d_batch_t h, int k, double tol);
+int awcm1d_batch_iwt(awcm1d_batch_t h, int k, int mask_id);
+int awcm1d_batch_interpolate(awcm1d_batch_t h, int k, int from_id, int to_id);
+int awcm1d_batch_manager(awcm1d_batch_t h, int k, int op, int mask_id, int level_id);
+int awcm1d_batch_apply_bc(awcm1d_batch_t h, int k);
 /* Launch shape of the step kernel: threads per CTA and CTAs per SM (0 = occupancy limit). */
 int awcm1d_batch_set_launch(awcm1d_batch_t h, int threads, int ctas_per_sm);
 int awcm1d_batch_stream(awcm1d_batch_t h, void** stream);
@@ -300,6 +315,10 @@ int awcm1d_step_noalloc(int num_levels, int nx_coarse, double x_min, double x_ma
                         double tol, double cfl, double t, double t_end, double* q_dev, uint8_t* state_dev,
                         double* out_dev, void* stream);
 
+/* EULER_EQUATION_1D on a batch of n conserved states in device memory (n x 3 doubles):
+ * ComputeFu (EULER_EQUATION.h:16-26) and Spectral_Radius |u| + c (:42-47). */
+int euler1d_flux(const double* q_dev, double* f_dev, int n, double gamma, void* stream);
+int euler1d_spectral_radius(const double* q_dev, double* s_dev, int n, double gamma, void* stream);
 /* EULER_EQUATION_2D on a batch of n conserved states in device memory (n x 4 doubles):
  * ComputeFu/ComputeGu (EULER_EQUATION.h:74-99) and Spectral_RadiusX/Y (:118-142). */
 int euler2d_flux(const double* q_dev, double* f_dev, int n, int dir, double gamma, void* stream);

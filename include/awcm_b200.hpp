@@ -2,7 +2,7 @@
 //
 // The reference (doseongju/C_pp-library) drives its path through header-only classes:
 // AWCM_1D/AWCM_2D (Wavelet/AWCM_1D.h, Wavelet/AWCM_2D.h), the static passes of AWCM_MANAGER_1D/2D
-// (Wavelet/AWCM_MANAGER_1D.h, Wavelet/AWCM_MANAGER_2D.h), EULER_EQUATION_2D (EULER_EQUATION.h)
+// (Wavelet/AWCM_MANAGER_1D.h, Wavelet/AWCM_MANAGER_2D.h), EULER_EQUATION_1D/2D (EULER_EQUATION.h)
 // and the BOUNDARY_MANAGER* classes of Problems/.  The classes below keep those names and method
 // names so a driver written against the reference changes its includes and its field hand-over,
 // not its loop: the state lives on the GPU, and the host field (the reference's FIELD_UNIFORM_*
@@ -188,17 +188,19 @@ struct AWCM_MANAGER_2D {
     }
 };
 
-// BOUNDARY_MANAGER_QUAD / _DMACH / _ISENVORTEX: the instance's boundary kind is fixed at creation.
-struct BOUNDARY_MANAGER_2D {
-    explicit BOUNDARY_MANAGER_2D(AWCM_2D& a) : a_(a) {}
+// BOUNDARY_MANAGER_QUAD / _DMACH / _ISENVORTEX / _SHOCK_VORTEX: the instance's boundary kind is
+// fixed at creation; SetBoundaryCondition fills the ghost ring of its conserved field.
+struct BOUNDARY_MANAGER_OF_INSTANCE_2D {
+    explicit BOUNDARY_MANAGER_OF_INSTANCE_2D(AWCM_2D& a) : a_(a) {}
     void SetBoundaryCondition(double t = 0) { check(awcm2d_apply_bc(a_.handle(), t), "SetBoundaryCondition"); }
 
 private:
     AWCM_2D& a_;
 };
-using BOUNDARY_MANAGER_QUAD = BOUNDARY_MANAGER_2D;
-using BOUNDARY_MANAGER_DMACH = BOUNDARY_MANAGER_2D;
-using BOUNDARY_MANAGER_ISENVORTEX = BOUNDARY_MANAGER_2D;
+using BOUNDARY_MANAGER_QUAD = BOUNDARY_MANAGER_OF_INSTANCE_2D;
+using BOUNDARY_MANAGER_DMACH = BOUNDARY_MANAGER_OF_INSTANCE_2D;
+using BOUNDARY_MANAGER_ISENVORTEX = BOUNDARY_MANAGER_OF_INSTANCE_2D;
+using BOUNDARY_MANAGER_SHOCK_VORTEX = BOUNDARY_MANAGER_OF_INSTANCE_2D;
 
 // EULER_EQUATION_2D (EULER_EQUATION.h:64-156) over batches of device-resident states (n x 4).
 struct EULER_EQUATION_2D {
@@ -223,7 +225,140 @@ struct EULER_EQUATION_2D {
 };
 
 // ------------------------------------------------------------------------------------------ 1D
-// AWCM_1D (Wavelet/AWCM_1D.h) as a batch of one instance, and the batch itself.
+// AWCM_1D (Wavelet/AWCM_1D.h:7-189) together with the field it serves: one instance on the GPU (a
+// batch of one).  The field hand-over uses the FIELD_UNIFORM_1D<VECTOR_3D<double>> storage with a
+// ghost ring of 3, (Nx+6) x 3 doubles.
+class AWCM_1D {
+public:
+    AWCM_1D(int num_levels, int nx_coarse, double x_min, double x_max, double gamma = 1.4, int scheme = 0)
+    {
+        check(awcm1d_batch_create(1, &num_levels, &nx_coarse, &x_min, &x_max, gamma, scheme, &h_),
+              "awcm1d_batch_create");
+        check(awcm1d_batch_nx(h_, 0, &nx_), "awcm1d_batch_nx");
+    }
+    ~AWCM_1D() { awcm1d_batch_destroy(h_); }
+    AWCM_1D(const AWCM_1D&) = delete;
+    AWCM_1D& operator=(const AWCM_1D&) = delete;
+
+    int Nx() const { return nx_; }
+    awcm1d_batch_t handle() const { return h_; }
+
+    void SetField(const double* q) { check(awcm1d_batch_set_q(h_, 0, q), "awcm1d_batch_set_q"); }
+    void GetField(double* q) const { check(awcm1d_batch_get_q(h_, 0, q), "awcm1d_batch_get_q"); }
+    std::vector<double> GetField() const
+    {
+        std::vector<double> q((size_t)(nx_ + 6) * 3);
+        GetField(q.data());
+        return q;
+    }
+    // SHOCKTUBE::Initialize (Problems/1D/PROBLEM_SHOCKTUBE.h:14-54): (rho, u, p) left and right.
+    void InitializeRiemann(double x_interface, const double* left3, const double* right3)
+    {
+        check(awcm1d_batch_init_riemann(h_, 0, x_interface, left3, right3), "awcm1d_batch_init_riemann");
+    }
+
+    // AWCM_1D::PrepareEuler / PostProcessEuler / BadingBoundary (Wavelet/AWCM_1D.h:73-125).
+    void PrepareEuler(double tol) { check(awcm1d_batch_prepare(h_, 0, tol), "PrepareEuler"); }
+    void PostProcessEuler() { check(awcm1d_batch_manager(h_, 0, AWCM_OP_REMOVE_RESIDUE, 0, 0), "PostProcessEuler"); }
+    void BadingBoundary(int mask_id) { check(awcm1d_batch_manager(h_, 0, AWCM_OP_BANDING, mask_id, 0), "BadingBoundary"); }
+    // The facade's WAVELET_1D member (Wavelet/WAVELET_1D.h:282-431) on the instance's field.
+    void ForwardWaveletTransformEuler(double tol) { check(awcm1d_batch_fwt(h_, 0, tol), "ForwardWaveletTransformEuler"); }
+    void InverseWaveletTransformEuler(int mask_id)
+    {
+        check(awcm1d_batch_iwt(h_, 0, mask_id), "InverseWaveletTransformEuler");
+    }
+    void InterpolateEuler(int from_id, int to_id)
+    {
+        check(awcm1d_batch_interpolate(h_, 0, from_id, to_id), "InterpolateEuler");
+    }
+
+    // One pass of the driver loop (Wavelet/main_1d_euler.cpp:61-260); returns dt, sets do_print.
+    double Step(double tol, double cfl, double t, double t_next, bool* do_print = nullptr)
+    {
+        check(awcm1d_batch_set_run(h_, &tol, &cfl, &t, &t_next, 0.0), "awcm1d_batch_set_run");
+        check(awcm1d_batch_steps(h_, 1), "awcm1d_batch_steps");
+        double s[16];
+        check(awcm1d_batch_status(h_, 0, s), "awcm1d_batch_status");
+        if (do_print) *do_print = s[2] != 0;
+        for (int k = 0; k < 4; ++k) last_mask_sizes_[k] = (long)s[5 + k];
+        return s[1];
+    }
+    long MaskSize(int k) const { return last_mask_sizes_[k]; }
+
+    // The public masks (mask_id 0..3 = mask0..mask3, 4 = mask_temp; Nx+6 bytes with ghosts) and
+    // levels (Nx ints) of the reference facade, read back on demand.
+    std::vector<uint8_t> Mask(int mask_id) const
+    {
+        const size_t n = (size_t)nx_ + 6;
+        std::vector<uint8_t> all(5 * n);
+        check(awcm1d_batch_get_masks(h_, 0, all.data()), "awcm1d_batch_get_masks");
+        const int plane = mask_id == 4 ? 0 : mask_id + 1;
+        return std::vector<uint8_t>(all.begin() + plane * n, all.begin() + (plane + 1) * n);
+    }
+    std::vector<int> Level(int level_id) const
+    {
+        const size_t n = (size_t)nx_;
+        std::vector<int> all(4 * n);
+        check(awcm1d_batch_get_levels(h_, 0, all.data()), "awcm1d_batch_get_levels");
+        return std::vector<int>(all.begin() + level_id * n, all.begin() + (level_id + 1) * n);
+    }
+
+private:
+    awcm1d_batch_t h_ = nullptr;
+    int nx_ = 0;
+    long last_mask_sizes_[4] = {0, 0, 0, 0};
+};
+
+// AWCM_MANAGER_1D (Wavelet/AWCM_MANAGER_1D.h:7-187): static passes on one of the facade's masks.
+struct AWCM_MANAGER_1D {
+    static void AddAdjacentZone(AWCM_1D& a, int mask_id)
+    {
+        check(awcm1d_batch_manager(a.handle(), 0, AWCM_OP_ADD_ADJACENT_ZONE, mask_id, 0), "AddAdjacentZone");
+    }
+    static void CheckReconstruction(AWCM_1D& a, int mask_id)
+    {
+        check(awcm1d_batch_manager(a.handle(), 0, AWCM_OP_CHECK_RECONSTRUCTION, mask_id, 0), "CheckReconstruction");
+    }
+    static void AddPointForDifferentiation(AWCM_1D& a, int mask_id, int level_id)
+    {
+        check(awcm1d_batch_manager(a.handle(), 0, AWCM_OP_ADD_POINT_FOR_DIFFERENTIATION, mask_id, level_id),
+              "AddPointForDifferentiation");
+    }
+    static void ComputeLevel(AWCM_1D& a, int level_id, int mask_id)
+    {
+        check(awcm1d_batch_manager(a.handle(), 0, AWCM_OP_COMPUTE_LEVEL, mask_id, level_id), "ComputeLevel");
+    }
+    static void RemoveResidue(AWCM_1D& a, int mask_id)
+    {
+        check(awcm1d_batch_manager(a.handle(), 0, AWCM_OP_REMOVE_RESIDUE, mask_id, 0), "RemoveResidue");
+    }
+};
+
+// BOUNDARY_MANAGER (Problems/1D/PROBLEM_SHOCKTUBE.h:57-107): transmissive ghost fill.
+struct BOUNDARY_MANAGER {
+    explicit BOUNDARY_MANAGER(AWCM_1D& a) : a_(a) {}
+    void SetBoundaryCondition() { check(awcm1d_batch_apply_bc(a_.handle(), 0), "SetBoundaryCondition"); }
+
+private:
+    AWCM_1D& a_;
+};
+
+// EULER_EQUATION_1D (EULER_EQUATION.h:6-62) over batches of device-resident states (n x 3).
+struct EULER_EQUATION_1D {
+    double gamma;
+    explicit EULER_EQUATION_1D(double g = 1.4) : gamma(g) {}
+    void ComputeFu(const double* q_dev, double* f_dev, int n, void* stream = nullptr) const
+    {
+        check(euler1d_flux(q_dev, f_dev, n, gamma, stream), "ComputeFu");
+    }
+    void Spectral_Radius(const double* q_dev, double* s_dev, int n, void* stream = nullptr) const
+    {
+        check(euler1d_spectral_radius(q_dev, s_dev, n, gamma, stream), "Spectral_Radius");
+    }
+};
+
+// A batch of independent AWCM_1D instances advanced together (no reference counterpart: the
+// reference runs one instance per process).
 // scheme AWCM_SCALAR_ADVECTION gives the scalar path of Wavelet/main_1d_advect.cpp (the field in
 // component 0 of SetField/GetField, dt = SetRun's dt_fixed).
 class AWCM_1D_BATCH {

@@ -111,6 +111,8 @@ class Oracle1D:
         self._step = b("step", None, [_vp, _c_double, _c_double, _c_double, _c_double, _dp])
         self._run = b("run", _c_int, [_vp, _c_double, _c_double, _c_double, _c_int, _dp])
         self._scalar_step = b("scalar_step", None, [_vp, _c_double, _c_double, _dp])
+        self._interpolate = b("interpolate", None, [_vp, _c_int, _c_int])
+        self._apply_bc = b("apply_bc", None, [_vp])
         self.h = self._create(num_levels, nx_coarse, x_min, x_max, gamma, scheme)
         self.nx = self._nx(self.h)
 
@@ -160,6 +162,14 @@ class Oracle1D:
 
     def manager(self, op, mask_id, level_id=0):
         self._manager(self.h, op, mask_id, level_id)
+
+    def interpolate(self, from_id=4, to_id=3):
+        """WAVELET_1D::InterpolateEuler(Q, mra, mask_from, mask_to)."""
+        self._interpolate(self.h, from_id, to_id)
+
+    def apply_bc(self):
+        """BOUNDARY_MANAGER::SetBoundaryCondition (transmissive)."""
+        self._apply_bc(self.h)
 
     def step(self, tol, cfl, t, t_next):
         out = np.zeros(10)
@@ -338,3 +348,45 @@ def run_tube(tube: dict, tol: float, cfl: float, t_end: float, scheme: int = 0, 
     o.init_riemann(tube["x_interface"], tube["left"], tube["right"])
     n, t, upd = o.run(tol, cfl, t_end)
     return n, t, upd, o.get_q(), o.get_masks(), o.get_levels()
+
+
+def euler_flux(q, dim: int, direction: int = 0, gamma: float = 1.4, kind: str = "port"):
+    """EULER_EQUATION_1D::ComputeFu (dim 1, q of shape (n, 3)) or EULER_EQUATION_2D::ComputeFu /
+    ComputeGu (dim 2, direction 0 / 1, q of shape (n, 4)) of every state, by the restatement or by
+    the reference's own class."""
+    nc = 3 if dim == 1 else 4
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, nc)
+    f = np.empty_like(q)
+    if kind == "port":
+        lib, name = _load(PORT_LIB), "or_euler%dd_flux" % dim
+    else:
+        lib, name = _load(REF_LIB_1D if dim == 1 else REF_LIB_2D), "ref_euler%dd_flux" % dim
+    fn = getattr(lib, name)
+    fn.restype = None
+    if dim == 1:
+        fn.argtypes = [_dp, _dp, _c_int, _c_double]
+        fn(_ptr(q, ctypes.c_double), _ptr(f, ctypes.c_double), q.shape[0], gamma)
+    else:
+        fn.argtypes = [_dp, _dp, _c_int, _c_int, _c_double]
+        fn(_ptr(q, ctypes.c_double), _ptr(f, ctypes.c_double), q.shape[0], direction, gamma)
+    return f
+
+
+def euler_spectral_radius(q, dim: int, direction: int = 0, gamma: float = 1.4, kind: str = "port"):
+    """EULER_EQUATION_1D::Spectral_Radius or EULER_EQUATION_2D::Spectral_RadiusX / Y of every state."""
+    nc = 3 if dim == 1 else 4
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, nc)
+    out = np.empty(q.shape[0])
+    if kind == "port":
+        lib, name = _load(PORT_LIB), "or_euler%dd_sr" % dim
+    else:
+        lib, name = _load(REF_LIB_1D if dim == 1 else REF_LIB_2D), "ref_euler%dd_sr" % dim
+    fn = getattr(lib, name)
+    fn.restype = None
+    if dim == 1:
+        fn.argtypes = [_dp, _dp, _c_int, _c_double]
+        fn(_ptr(q, ctypes.c_double), _ptr(out, ctypes.c_double), q.shape[0], gamma)
+    else:
+        fn.argtypes = [_dp, _dp, _c_int, _c_int, _c_double]
+        fn(_ptr(q, ctypes.c_double), _ptr(out, ctypes.c_double), q.shape[0], direction, gamma)
+    return out

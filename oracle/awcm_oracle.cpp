@@ -1449,6 +1449,40 @@ void or1d_manager(void* h, int op, int mask_id, int level_id)
     }
 }
 
+// WAVELET_1D::InterpolateEuler(Q, mra, from, to) (Wavelet/WAVELET_1D.h:393-431) and the
+// transmissive BOUNDARY_MANAGER::SetBoundaryCondition (Problems/1D/PROBLEM_SHOCKTUBE.h:86-107).
+void or1d_interpolate(void* h, int from_id, int to_id)
+{
+    interp1d(*static_cast<O1D*>(h), bit_of(from_id), bit_of(to_id));
+}
+void or1d_apply_bc(void* h) { bc1d(*static_cast<O1D*>(h)); }
+
+// EULER_EQUATION_1D::ComputeFu / Spectral_Radius (EULER_EQUATION.h:16-26, 42-47) and
+// EULER_EQUATION_2D::ComputeFu / ComputeGu / Spectral_RadiusX / Spectral_RadiusY (:74-99, :118-142)
+// over n states (3 or 4 doubles each).
+void or_euler1d_flux(const double* q, double* f, int n, double g)
+{
+    for (int t = 0; t < n; ++t) {
+        const V3 v = fu1(q + 3 * t, g);
+        for (int k = 0; k < 3; ++k) f[3 * t + k] = v.v[k];
+    }
+}
+void or_euler1d_sr(const double* q, double* out, int n, double g)
+{
+    for (int t = 0; t < n; ++t) out[t] = absd(q[3 * t + 1] / q[3 * t]) + c1(q + 3 * t, g);
+}
+void or_euler2d_flux(const double* q, double* f, int n, int dir, double g)
+{
+    for (int t = 0; t < n; ++t) {
+        const V4 v = dir == 0 ? fu2(q + 4 * t, g) : gu2(q + 4 * t, g);
+        for (int k = 0; k < 4; ++k) f[4 * t + k] = v.v[k];
+    }
+}
+void or_euler2d_sr(const double* q, double* out, int n, int dir, double g)
+{
+    for (int t = 0; t < n; ++t) out[t] = dir == 0 ? srx(q + 4 * t, g) : sry(q + 4 * t, g);
+}
+
 void or1d_step(void* h, double tol, double cfl, double t, double t_next, double* out)
 {
     step1d(*static_cast<O1D*>(h), tol, cfl, t, t_next, out);

@@ -369,6 +369,30 @@ void ref1d_scalar_step(void* h, double tol, double dt, double* out)
     for (int k = 0; k < 4; ++k) out[1 + k] = (double)cnt[k];
 }
 
+void ref1d_interpolate(void* h, int from_id, int to_id)
+{
+    Ref1D* s = static_cast<Ref1D*>(h);
+    s->awcm->wavelet.InterpolateEuler(s->Q, s->mra, mask_ref(s, from_id), mask_ref(s, to_id));
+}
+
+void ref1d_apply_bc(void* h) { static_cast<Ref1D*>(h)->bc->SetBoundaryCondition(); }
+
+// The reference's EULER_EQUATION_1D itself over n states of 3 doubles.
+void ref_euler1d_flux(const double* q, double* f, int n, double gamma)
+{
+    const EULER_EQUATION_1D eq(gamma);
+    for (int t = 0; t < n; ++t) {
+        VECTOR_3D<double> Q(q[3 * t], q[3 * t + 1], q[3 * t + 2]), fu;
+        eq.ComputeFu(Q, fu);
+        for (int k = 0; k < 3; ++k) f[3 * t + k] = fu[k];
+    }
+}
+void ref_euler1d_sr(const double* q, double* out, int n, double gamma)
+{
+    const EULER_EQUATION_1D eq(gamma);
+    for (int t = 0; t < n; ++t) out[t] = eq.Spectral_Radius(VECTOR_3D<double>(q[3 * t], q[3 * t + 1], q[3 * t + 2]));
+}
+
 // AWCM_MANAGER_1D passes on one of the facade's masks.
 // op 0 AddAdjacentZone, 1 CheckReconstruction, 2 AddPointForDifferentiation(level_id),
 // 3 ComputeLevel(level_id <- mask), 4 RemoveResidue(Q, mask), 5 BadingBoundary.

@@ -657,4 +657,25 @@ int ref2d_run(void* h, double tol, double cfl, double t_end, int max_steps, doub
 
 int ref2d_threads(void) { return omp_get_max_threads(); }
 
+// The reference's EULER_EQUATION_2D itself over n states of 4 doubles: ComputeFu / ComputeGu
+// (dir 0 / 1) and Spectral_RadiusX / Spectral_RadiusY.
+void ref_euler2d_flux(const double* q, double* f, int n, int dir, double gamma)
+{
+    const EULER_EQUATION_2D eq(gamma);
+    for (int t = 0; t < n; ++t) {
+        VECTOR_4D<double> Q(q[4 * t], q[4 * t + 1], q[4 * t + 2], q[4 * t + 3]), o;
+        if (dir == 0) eq.ComputeFu(Q, o);
+        else eq.ComputeGu(Q, o);
+        for (int k = 0; k < 4; ++k) f[4 * t + k] = o[k];
+    }
+}
+void ref_euler2d_sr(const double* q, double* out, int n, int dir, double gamma)
+{
+    const EULER_EQUATION_2D eq(gamma);
+    for (int t = 0; t < n; ++t) {
+        const VECTOR_4D<double> Q(q[4 * t], q[4 * t + 1], q[4 * t + 2], q[4 * t + 3]);
+        out[t] = dir == 0 ? eq.Spectral_RadiusX(Q) : eq.Spectral_RadiusY(Q);
+    }
+}
+
 }  // extern "C"

@@ -38,3 +38,41 @@ def test_driver_matches_oracle(tmp_path, awcm_lib):
     for v in ref.get_q().reshape(-1, 4)[:, 0]:  # same left-to-right sum as the driver
         acc += float(v)
     assert rho_sum == acc
+
+
+SOD_SRC = os.path.join(PKG, "examples", "sod_driver.cpp")
+
+
+def build_sod_driver(tmp_path):
+    exe = str(tmp_path / "sod_driver")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), SOD_SRC, "-o", exe,
+                    "-L", PKG, "-lawcm_b200", f"-Wl,-rpath,{PKG}"], check=True)
+    return exe
+
+
+def test_sod_driver_compiles(tmp_path, awcm_lib):
+    assert os.path.exists(build_sod_driver(tmp_path))
+
+
+@pytest.mark.gpu
+def test_sod_driver_matches_oracle(tmp_path, awcm_lib):
+    """The 1D mirror (AWCM_1D, AWCM_MANAGER_1D, the facade's wavelet calls) in a compiled driver:
+    PrepareEuler pass by pass equals the one-call form, and the Sod run to t = 0.2 equals the
+    oracle's (897 steps)."""
+    from oracle import Oracle1D
+
+    exe = build_sod_driver(tmp_path)
+    out = subprocess.run([exe, "7", "17", "0.2", "1e-4", "0.5", "passes"], capture_output=True, text=True,
+                         check=True).stdout.split("\n")
+    assert out[0] == "passes equal 1", out[0]
+    f = out[1].split()
+    steps, t, upd, rho_sum = int(f[1]), float(f[3]), float(f[7]), float(f[9])
+    n = 1025
+    ref = Oracle1D(7, 17, 0.5 / n, 1 - 0.5 / n, kind="port")
+    ref.init_riemann(0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+    n_r, t_r, u_r = ref.run(1e-4, 0.5, 0.2)
+    assert (steps, t, upd) == (n_r, t_r, u_r) == (897, 0.2, 151533.0)
+    acc = 0.0
+    for v in ref.get_q()[:, 0]:  # same left-to-right sum as the driver
+        acc += float(v)
+    assert rho_sum == acc

@@ -56,6 +56,29 @@ def test_manager_passes_in_sequence(awcm_lib):
     assert_same(gpu, ref, "iwt")
 
 
+def test_interpolate_and_boundary_fill(awcm_lib):
+    """The typed single passes WAVELET_1D::InterpolateEuler(mask_temp -> mask3) and the
+    transmissive ghost fill, on a stepped state with a perturbed field."""
+    ref, gpu = make(awcm_lib)
+    t = 0.0
+    for _ in range(40):
+        o_r = ref.step(1e-4, 0.5, t, 0.2)
+        gpu.step(1e-4, 0.5, t, 0.2)
+        t += o_r[0]
+    assert_same(gpu, ref, "40 steps")
+    q = ref.get_q() + np.random.default_rng(3).uniform(0, 1e-3, ref.get_q().shape)
+    for o in (ref, gpu):
+        o.set_q(q)
+        o.interpolate(4, 3)
+    assert_same(gpu, ref, "interpolate")
+    for o in (ref, gpu):
+        o.apply_bc()
+    assert_same(gpu, ref, "boundary fill")
+    for o in (ref, gpu):
+        o.iwt(3)
+    assert_same(gpu, ref, "inverse transform")
+
+
 @pytest.mark.parametrize("scheme", [0, 1])
 def test_steps(scheme, awcm_lib):
     ref, gpu = make(awcm_lib, scheme=scheme)
