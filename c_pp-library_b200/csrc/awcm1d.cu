@@ -58,55 +58,77 @@ __device__ __forceinline__ double block_max(double v, double* red)
     return r;
 }
 
-__device__ __forceinline__ unsigned block_sum(unsigned v, unsigned* red)
+// Sums of four per-thread counts over the block (one shared-memory round for all four).
+__device__ __forceinline__ void block_sum4(unsigned (&v)[4], unsigned* red)
 {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    unsigned r = 0;
     const int nw = (blockDim.x + 31) >> 5;
-    for (int k = 0; k < nw; ++k) r += red[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
     __syncthreads();
-    return r;
+    if (lane == 0)
+        for (int k = 0; k < 4; ++k) red[4 * warp + k] = v[k];
+    __syncthreads();
+    for (int k = 0; k < 4; ++k) {
+        unsigned r = 0;
+        for (int q = 0; q < nw; ++q) r += red[4 * q + k];
+        v[k] = r;
+    }
+    __syncthreads();
+}
+
+// Exclusive prefix of v over the threads of the block (thread order); *total = the block sum.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* red, unsigned* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    unsigned x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) red[warp] = x;
+    __syncthreads();
+    unsigned before = 0, all = 0;
+    for (int k = 0; k < nw; ++k) {
+        const unsigned r = red[k];
+        before += k < warp ? r : 0u;
+        all += r;
+    }
+    *total = all;
+    return before + x - v;
 }
 
 // Block-wide stream compaction of the indices lo..hi whose predicate holds into `list` (order
-// preserved).  Returns the count.  Warp ballots plus a serial prefix over warps per round.
+// preserved).  Returns the count.  Each thread owns a contiguous chunk of the range: it counts its
+// hits, one block-wide exclusive scan gives its output offset, and it writes its hits in order
+// (two evaluations of the predicate, three barriers in all, whatever the range).
 template <class Pred>
 __device__ int block_compact(int lo, int hi, Pred pred, uint32_t* list, unsigned* red)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nw = (blockDim.x + 31) >> 5;
-    __shared__ int base_s;
-    if (threadIdx.x == 0) base_s = 0;
+    const int n = hi - lo + 1;
+    const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int a0 = lo + (int)threadIdx.x * per;
+    const int a1 = min(a0 + per, hi + 1);
+    unsigned cnt = 0;
+    for (int i = a0; i < a1; ++i) cnt += pred(i) ? 1u : 0u;
+    unsigned total;
+    unsigned off = block_exclusive_scan(cnt, red, &total);
+    for (int i = a0; i < a1; ++i)
+        if (pred(i)) list[off++] = (uint32_t)i;
     __syncthreads();
-    for (int start = lo; start <= hi; start += blockDim.x) {
-        const int i = start + threadIdx.x;
-        const bool p = i <= hi && pred(i);
-        const unsigned bal = __ballot_sync(0xffffffffu, p);
-        if (lane == 0) red[warp] = __popc(bal);
-        __syncthreads();
-        int off = base_s;
-        for (int k = 0; k < warp; ++k) off += red[k];
-        if (p) list[off + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)i;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int tot = 0;
-            for (int k = 0; k < nw; ++k) tot += red[k];
-            base_s += tot;
-        }
-        __syncthreads();
-    }
-    const int n = base_s;
-    __syncthreads();
-    return n;
+    return (int)total;
 }
 
+// Views of one instance for a step or a pass.  Pointers are generic: in the step kernel the mask
+// bytes, the levels and the density plane point into the CTA's shared memory (staged in and out
+// around the step), elsewhere into the instance's global buffers.
 struct Ctx {
     const Inst1& I;
-    double* q;   // q[p*w + i + 3]
+    double* q;   // q[p*w + i + 3] (plane 0 is read through q0)
     double* qc;
     double* qt;
     double* fl;
@@ -114,7 +136,8 @@ struct Ctx {
     int8_t* lv;  // lv[l*w + i + 3]
     const Weights& W;
     int w, nx, N1, maxl;
-    __device__ double& Q(int p, int i) const { return q[p * w + i + kGhost]; }
+    double* q0;  // density plane: q0[i + 3]
+    __device__ double& Q(int p, int i) const { return (p == 0 ? q0 : q + p * w)[i + kGhost]; }
     __device__ double& QT(int p, int i) const { return qt[p * w + i + kGhost]; }
     __device__ double& QC(int p, int i) const { return qc[p * w + i + kGhost]; }
     __device__ uint8_t& M(int i) const { return m[i + kGhost]; }
@@ -349,13 +372,13 @@ __device__ void prepare1(const Ctx& c)
 }
 
 // --------------------------------------------------------------------------------- RK3 stages
-__device__ void bc1(const Ctx& c, double* q)
+__device__ void bc1(const Ctx& c)
 {
     // BOUNDARY_MANAGER::SetBoundaryCondition (Problems/1D/PROBLEM_SHOCKTUBE.h:86-107).
     if (threadIdx.x < 3 * kGhost) {
         const int p = threadIdx.x / kGhost, g = threadIdx.x % kGhost + 1;
-        q[p * c.w + kGhost - g] = q[p * c.w + kGhost];
-        q[p * c.w + kGhost + c.N1 + g] = q[p * c.w + kGhost + c.N1];
+        c.Q(p, -g) = c.Q(p, 0);
+        c.Q(p, c.N1 + g) = c.Q(p, c.N1);
     }
     __syncthreads();
 }
@@ -376,9 +399,9 @@ __device__ double lf_speed1(const Ctx& c, int b, int l, double* red, bool& nf)
     return block_max(a, red);
 }
 
-__device__ void copy_q(const Ctx& c, double* dst)
+__device__ void copy_q(const Ctx& c, double* __restrict__ dst)
 {
-    for (int t = threadIdx.x; t < 3 * c.w; t += blockDim.x) dst[t] = c.q[t];
+    for (int t = threadIdx.x; t < 3 * c.w; t += blockDim.x) dst[t] = t < c.w ? c.q0[t] : c.q[t];
     __syncthreads();
 }
 
@@ -480,21 +503,21 @@ __device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, u
         dt = I.t_end - I.t;
         do_print = 1;
     }
-    unsigned cnt[4];
-    for (int k = 0; k < 4; ++k) {
-        unsigned v = 0;
-        for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) v += c.bit(i, k);
-        cnt[k] = block_sum(v, ured);
+    unsigned cnt[4] = {0, 0, 0, 0};
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
+        const unsigned v = c.M(i);
+        for (int k = 0; k < 4; ++k) cnt[k] += (v >> k) & 1u;
     }
+    block_sum4(cnt, ured);
 
-    bc1(c, c.q);
+    bc1(c);
     const double a1 = lf_speed1(c, 3, 3, dred, nf);
     copy_q(c, c.qc);
     stage1<SCHEME>(c, 2, 2, a1, dt, 1, list, ured);
-    bc1(c, c.q);
+    bc1(c);
     const double a2 = lf_speed1(c, 2, 2, dred, nf);
     stage1<SCHEME>(c, 1, 1, a2, dt, 2, list, ured);
-    bc1(c, c.q);
+    bc1(c);
     const double a3 = lf_speed1(c, 1, 1, dred, nf);
     stage1<SCHEME>(c, 0, 0, a3, dt, 3, list, ured);
     const bool any_nf = __syncthreads_or(nf);
@@ -616,12 +639,12 @@ __device__ void step_ctx_scalar(Inst1& I, const Ctx& c, uint32_t* list, unsigned
 {
     prepare1_scalar(c);
     const double dt = I.dt_fixed;
-    unsigned cnt[4];
-    for (int k = 0; k < 4; ++k) {
-        unsigned v = 0;
-        for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) v += c.bit(i, k);
-        cnt[k] = block_sum(v, ured);
+    unsigned cnt[4] = {0, 0, 0, 0};
+    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
+        const unsigned v = c.M(i);
+        for (int k = 0; k < 4; ++k) cnt[k] += (v >> k) & 1u;
     }
+    block_sum4(cnt, ured);
     double* q = c.q;
     double* q2 = c.qc;
     double* q1 = c.qc + c.w;
@@ -652,36 +675,89 @@ __device__ void step_ctx_scalar(Inst1& I, const Ctx& c, uint32_t* list, unsigned
     __syncthreads();
 }
 
+// Byte offset of the level planes behind the mask bytes of an instance's state block.
+__host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Shared memory of the step kernel for an instance of w ghosted points: mask bytes, the four level
+// planes and the density plane staged for the step, and the worklist of the stages.
+__host__ __device__ __forceinline__ size_t step_smem_bytes(int w)
+{
+    return align16((size_t)w) + align16((size_t)4 * w) + sizeof(double) * (size_t)w + sizeof(uint32_t) * (size_t)(w + 32);
+}
+
+// Copy of n bytes by all threads of the block; 16-byte words where both ends allow it.
+__device__ __forceinline__ void block_copy_bytes(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, int n)
+{
+    int head = 0;
+    if ((((uintptr_t)dst | (uintptr_t)src) & 15) == 0) {
+        const int nv = n >> 4;
+        for (int t = threadIdx.x; t < nv; t += blockDim.x)
+            reinterpret_cast<int4*>(dst)[t] = reinterpret_cast<const int4*>(src)[t];
+        head = nv << 4;
+    }
+    for (int t = head + threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+}
+
+__device__ __forceinline__ void block_copy_doubles(double* __restrict__ dst, const double* __restrict__ src, int n)
+{
+    int head = 0;
+    if ((((uintptr_t)dst | (uintptr_t)src) & 15) == 0) {
+        const int nv = n >> 1;
+        for (int t = threadIdx.x; t < nv; t += blockDim.x)
+            reinterpret_cast<double2*>(dst)[t] = reinterpret_cast<const double2*>(src)[t];
+        head = nv << 1;
+    }
+    for (int t = head + threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+}
+
+// One RK3 step of an instance with its mask bytes, levels and density plane staged in the CTA's
+// shared memory: the ~100 level-sequential mask and transform phases of PrepareEuler and the
+// stage worklists then run on shared memory, with one global round trip in and one out per step.
+// q: the three conserved planes (global); qc, qt, fl: stage-start copy, stage input, face fluxes;
+// mg: w mask bytes, lg: four planes of w levels (global); smem: step_smem_bytes(w) bytes.
+__device__ void step_staged(Inst1& I, double* q, double* qc, double* qt, double* fl, uint8_t* mg, int8_t* lg,
+                            const Weights& W, uint8_t* smem, double* dred, unsigned* ured)
+{
+    const int w = I.nx + 2 * kGhost;
+    uint8_t* ms = smem;
+    int8_t* ls = reinterpret_cast<int8_t*>(smem + align16((size_t)w));
+    double* q0s = reinterpret_cast<double*>(smem + align16((size_t)w) + align16((size_t)4 * w));
+    uint32_t* list = reinterpret_cast<uint32_t*>(q0s + w);
+    // the scalar path reads and writes its field planes directly; only its masks are staged
+    const bool scalar = I.scheme == kScalarAdvection;
+    block_copy_bytes(ms, mg, w);
+    block_copy_bytes(reinterpret_cast<uint8_t*>(ls), reinterpret_cast<const uint8_t*>(lg), 4 * w);
+    if (!scalar) block_copy_doubles(q0s, q, w);
+    __syncthreads();
+    const Ctx c{I, q, qc, qt, fl, ms, ls, W, w, I.nx, I.nx - 1, I.maxl, scalar ? q : q0s};
+    if (scalar) step_ctx_scalar(I, c, list, ured);
+    else if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
+    else step_ctx<kWenoZ>(I, c, list, dred, ured);
+    block_copy_bytes(mg, ms, w);
+    block_copy_bytes(reinterpret_cast<uint8_t*>(lg), reinterpret_cast<const uint8_t*>(ls), 4 * w);
+    if (!scalar) block_copy_doubles(q, q0s, w);
+    __syncthreads();
+}
+
+// Global views of instance I in the pool.
 __device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
 {
     const int w = I.nx + 2 * kGhost;
     double* base = P.q + I.q_off;
     uint8_t* mb = P.m + I.m_off;
-    return Ctx{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + w), P.W, w, I.nx, I.nx - 1,
-               I.maxl};
-}
-
-template <int SCHEME>
-__device__ void step_instance(Inst1& I, const Pool& P, uint32_t* list, double* dred, unsigned* ured)
-{
-    if (I.t >= I.t_end || I.err) {
-        if (threadIdx.x == 0) I.done = 1;
-        return;
-    }
-    const int w = I.nx + 2 * kGhost;
-    double* base = P.q + I.q_off;
-    uint8_t* mb = P.m + I.m_off;
-    const Ctx c{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + w), P.W, w, I.nx, I.nx - 1,
-                I.maxl};
-    step_ctx<SCHEME>(I, c, list, dred, ured);
+    return Ctx{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + align16((size_t)w)), P.W,
+               w, I.nx, I.nx - 1, I.maxl, base};
 }
 
 // One RK3 step of every queued instance.  CTAs pull queue slots until the queue is exhausted.
-__global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, unsigned* queue, Pool P)
+// smem_bytes: the launch's dynamic shared memory; an instance whose staged step does not fit in
+// it runs on its global buffers (only its worklist in shared memory).
+__global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, unsigned* queue, Pool P,
+                         unsigned smem_bytes)
 {
-    extern __shared__ uint32_t list[];
+    extern __shared__ __align__(16) uint8_t smem[];
     __shared__ double dred[32];
-    __shared__ unsigned ured[32];
+    __shared__ unsigned ured[128];
     __shared__ int cur;
     for (;;) {
         if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
@@ -690,16 +766,20 @@ __global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, uns
         __syncthreads();
         if (k >= n) break;
         Inst1& I = insts[order[k]];
-        if (I.scheme == kScalarAdvection) {
-            if (I.t >= I.t_end) {
-                if (threadIdx.x == 0) I.done = 1;
-            } else {
-                step_ctx_scalar(I, make_ctx(I, P), list, ured);
-            }
-        } else if (I.scheme == kWeno5) {
-            step_instance<kWeno5>(I, P, list, dred, ured);
+        if (I.t >= I.t_end || I.err) {
+            if (threadIdx.x == 0) I.done = 1;
+        } else if (step_smem_bytes(I.nx + 2 * kGhost) <= smem_bytes) {
+            const int w = I.nx + 2 * kGhost;
+            double* base = P.q + I.q_off;
+            uint8_t* mb = P.m + I.m_off;
+            step_staged(I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + align16((size_t)w)),
+                        P.W, smem, dred, ured);
         } else {
-            step_instance<kWenoZ>(I, P, list, dred, ured);
+            uint32_t* list = reinterpret_cast<uint32_t*>(smem);
+            const Ctx c = make_ctx(I, P);
+            if (I.scheme == kScalarAdvection) step_ctx_scalar(I, c, list, ured);
+            else if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
+            else step_ctx<kWenoZ>(I, c, list, dred, ured);
         }
         __syncthreads();
     }
@@ -709,11 +789,7 @@ __global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, uns
 __global__ void k_pass1d(Inst1* insts, int inst, Pool P, int op, int bit, int level_id)
 {
     Inst1& I = insts[inst];
-    const int w = I.nx + 2 * kGhost;
-    double* base = P.q + I.q_off;
-    uint8_t* mb = P.m + I.m_off;
-    const Ctx c{I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + w), P.W, w, I.nx, I.nx - 1,
-                I.maxl};
+    const Ctx c = make_ctx(I, P);
     switch (op) {
         case 0:  // AddAdjacentZone
             copy_bit1(c, bit, kBitCopy, true);
@@ -740,7 +816,7 @@ __global__ void k_pass1d(Inst1* insts, int inst, Pool P, int op, int bit, int le
         case 11: fwt1(c); break;
         case 12: iwt1(c, bit); break;
         case 13: interp1(c, bit, level_id); break;  // InterpolateEuler(from = bit, to = level_id as a bit)
-        case 14: bc1(c, c.q); break;
+        case 14: bc1(c); break;
         default: break;
     }
 }
@@ -822,7 +898,7 @@ struct Batch1D {
             I.m_off = (long long)mo;
             qo += (size_t)12 * w;
             qo = (qo + 31) & ~(size_t)31;
-            mo += (size_t)5 * w;
+            mo += align16((size_t)w) + (size_t)4 * w;  // mask bytes, then the levels 16-byte aligned
             mo = (mo + 255) & ~(size_t)255;
         }
         q_doubles = qo;
@@ -858,9 +934,8 @@ struct Batch1D {
         P.W = make_weights();
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        set_launch(256, 0);
         (void)sms;
-        return kOk;
+        return set_launch(256, 0);
     }
 
     cudaError_t upload_inst()
@@ -874,7 +949,14 @@ struct Batch1D {
         return cudaMemcpy(host.data(), d_inst, sizeof(Inst1) * n, cudaMemcpyDeviceToHost);
     }
 
-    size_t smem_bytes() const { return sizeof(uint32_t) * (size_t)(max_w + 32); }
+    // Dynamic shared memory of the step kernel: the staged step of the largest instance when it
+    // fits the per-CTA limit, else the limit (larger instances run unstaged, with only their
+    // worklist, 4 (w + 32) bytes, in shared memory).
+    size_t smem_cap = 227 * 1024;
+    size_t smem_bytes() const
+    {
+        return std::max(std::min(step_smem_bytes(max_w), smem_cap), sizeof(uint32_t) * (size_t)(max_w + 32));
+    }
 
     // Launch shape: threads per CTA and CTAs per SM (0 = as many as fit).
     int set_launch(int threads, int ctas_per_sm)
@@ -886,8 +968,14 @@ struct Batch1D {
             return kErrArg;
         }
         block = threads;
-        int sms = 148, occ = 1;
+        int sms = 148, occ = 1, optin = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) == cudaSuccess && optin > 0)
+            smem_cap = (size_t)optin - 1024;  // leave room for the kernel's static shared arrays
+        if (sizeof(uint32_t) * (size_t)(max_w + 32) > smem_cap) {
+            set_last_error("instance too large for the step kernel's shared-memory worklist", __FILE__, __LINE__);
+            return kErrArg;
+        }
         cudaFuncSetAttribute(k_step1d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes());
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step1d, block, smem_bytes());
         if (occ < 1) occ = 1;
@@ -901,7 +989,7 @@ struct Batch1D {
     void enq_step()
     {
         cudaMemsetAsync(d_queue, 0, sizeof(unsigned), stream);
-        k_step1d<<<grid, block, smem_bytes(), stream>>>(d_inst, n, d_order, d_queue, P);
+        k_step1d<<<grid, block, smem_bytes(), stream>>>(d_inst, n, d_order, d_queue, P, (unsigned)smem_bytes());
     }
 
     int build_graph()
@@ -1023,7 +1111,8 @@ struct Batch1D {
         const int w = w_of(k), nx = host[k].nx;
         std::vector<int8_t> l(4 * (size_t)w);
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
-        AWCM_CUDA_TRY(cudaMemcpy(l.data(), d_m + host[k].m_off + w, 4 * (size_t)w, cudaMemcpyDeviceToHost));
+        AWCM_CUDA_TRY(cudaMemcpy(l.data(), d_m + host[k].m_off + align16((size_t)w), 4 * (size_t)w,
+                                 cudaMemcpyDeviceToHost));
         for (int r = 0; r < 4; ++r)
             for (int i = 0; i < nx; ++i) lv[r * nx + i] = l[r * w + i + kGhost];
         return kOk;
@@ -1035,7 +1124,8 @@ struct Batch1D {
         std::vector<int8_t> l(4 * (size_t)w, 0);
         for (int r = 0; r < 4; ++r)
             for (int i = 0; i < nx; ++i) l[r * w + i + kGhost] = (int8_t)lv[r * nx + i];
-        AWCM_CUDA_TRY(cudaMemcpy(d_m + host[k].m_off + w, l.data(), 4 * (size_t)w, cudaMemcpyHostToDevice));
+        AWCM_CUDA_TRY(cudaMemcpy(d_m + host[k].m_off + align16((size_t)w), l.data(), 4 * (size_t)w,
+                                 cudaMemcpyHostToDevice));
         return kOk;
     }
 
@@ -1079,9 +1169,9 @@ namespace {
 // scratch: the device address of g_noalloc_scratch (resolved on the host once per device).
 __global__ void k_step1d_noalloc(Inst1 param, double* q, uint8_t* state, double* scratch, double* out, Weights W)
 {
-    extern __shared__ uint32_t list[];
+    extern __shared__ __align__(16) uint8_t smem[];  // step_smem_bytes(w)
     __shared__ double dred[32];
-    __shared__ unsigned ured[32];
+    __shared__ unsigned ured[128];
     Inst1& I = *reinterpret_cast<Inst1*>(scratch);
     if (threadIdx.x == 0) I = param;  // the descriptor is rewritten by every call
     __syncthreads();
@@ -1090,9 +1180,7 @@ __global__ void k_step1d_noalloc(Inst1 param, double* q, uint8_t* state, double*
     double* qt = qc + 3 * w;
     double* fl = qt + 3 * w;
     if (I.t < I.t_end) {
-        const Ctx c{I, q, qc, qt, fl, state, (int8_t*)(state + w), W, w, I.nx, I.nx - 1, I.maxl};
-        if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
-        else step_ctx<kWenoZ>(I, c, list, dred, ured);
+        step_staged(I, q, qc, qt, fl, state, (int8_t*)(state + w), W, smem, dred, ured);
     } else if (threadIdx.x == 0) {
         I.done = 1;
     }
@@ -1409,7 +1497,8 @@ int awcm1d_step_noalloc(int num_levels, int nx_coarse, double x_min, double x_ma
     I.t = t;
     I.t_end = t_end;
     const int w = (int)nx + 2 * kGhost;
-    const size_t smem = sizeof(uint32_t) * (size_t)(w + 32);
+    const size_t smem = step_smem_bytes(w);  // 139 KB at the 8193-point limit
+    AWCM_CUDA_TRY(cudaFuncSetAttribute(k_step1d_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_step1d_noalloc<<<1, 256, smem, (cudaStream_t)stream>>>(I, q_dev, state_dev, scratch, out_dev, make_weights());
     AWCM_CUDA_TRY(cudaGetLastError());
     return kOk;
