@@ -21,6 +21,8 @@ ERR_NONFINITE = 5
 
 AAZ, CR, APD, CL, RR, BAND = 0, 1, 2, 3, 4, 5
 BC_TRANSMISSIVE, BC_DOUBLE_MACH, BC_PERIODIC = 0, 1, 2
+# BOUNDARY_CONDITION values of the generic managers (BOUNDARY_MANAGER_2D.h:7-13)
+SOLID_WALL, PERIODIC, EXTRAPOLATION_ZERO_ORDER, SPECIFIED, FLUID = -4, -3, -2, -1, 0
 PROBLEM_QUADRANTS, PROBLEM_DOUBLE_MACH, PROBLEM_VORTEX = 0, 1, 2
 WENOZ, WENO5 = 0, 1
 # 1D scalar AWCM (the path of Wavelet/main_1d_advect.cpp): a batch scheme like the two above.
@@ -131,6 +133,11 @@ class AWCM2D:
 
     def apply_bc(self, t=0.0):
         call("awcm2d_apply_bc", self.h, t)
+
+    def set_bc_field(self, bc):
+        """Attaches the enum-driven BOUNDARY_MANAGER_2D: bc is (Ny+6, Nx+6) BOUNDARY_CONDITION values."""
+        bc = np.ascontiguousarray(bc, dtype=np.int32).reshape(self.ny + 6, self.nx + 6)
+        call("awcm2d_set_bc_field", self.h, ptr(bc, ctypes.c_int))
 
     # stepping ---------------------------------------------------------------------------------
     def step(self, tol, cfl, t, t_next, dt_fixed=0.0):
@@ -510,8 +517,13 @@ class AWCM1D:
         call("awcm1d_batch_manager", self.b.h, 0, op, mask_id, level_id)
 
     def apply_bc(self):
-        """The instance's ghost fill (the transmissive BOUNDARY_MANAGER)."""
+        """The instance's ghost fill (transmissive BOUNDARY_MANAGER, or the attached generic one)."""
         call("awcm1d_batch_apply_bc", self.b.h, 0)
+
+    def set_bc_field(self, bc):
+        """Attaches the enum-driven BOUNDARY_MANAGER_1D: bc is Nx+6 BOUNDARY_CONDITION values."""
+        bc = np.ascontiguousarray(bc, dtype=np.int32).reshape(self.nx + 6)
+        call("awcm1d_batch_set_bc_field", self.b.h, 0, ptr(bc, ctypes.c_int))
 
     def step(self, tol, cfl, t, t_next):
         """One driver-loop pass; returns the checker's out[10] (dt, do_print, |mask0..3|, alphas, speed)."""

@@ -36,7 +36,14 @@ struct Inst1 {
     int do_print, done, steps, err;
     unsigned mask_cnt[4];
     unsigned long long upd;
+    // the enum-driven BOUNDARY_MANAGER_1D<T> when bc_generic: BOUNDARY_CONDITION of the ghost cells
+    // -1, -2, -3 (bcg[0..2]) and N1+1, N1+2, N1+3 (bcg[3..5])
+    int8_t bcg[6];
+    int8_t bc_generic, pad1;
 };
+
+// BOUNDARY_CONDITION values of the generic manager (BOUNDARY_MANAGER_1D.h:4-13).
+constexpr int kBcPeriodic1 = -3, kBcExtrapolation1 = -2;
 
 struct Pool {
     double* q;
@@ -374,11 +381,22 @@ __device__ void prepare1(const Ctx& c)
 // --------------------------------------------------------------------------------- RK3 stages
 __device__ void bc1(const Ctx& c)
 {
-    // BOUNDARY_MANAGER::SetBoundaryCondition (Problems/1D/PROBLEM_SHOCKTUBE.h:86-107).
     if (threadIdx.x < 3 * kGhost) {
         const int p = threadIdx.x / kGhost, g = threadIdx.x % kGhost + 1;
-        c.Q(p, -g) = c.Q(p, 0);
-        c.Q(p, c.N1 + g) = c.Q(p, c.N1);
+        if (!c.I.bc_generic) {
+            // BOUNDARY_MANAGER::SetBoundaryCondition (Problems/1D/PROBLEM_SHOCKTUBE.h:86-107).
+            c.Q(p, -g) = c.Q(p, 0);
+            c.Q(p, c.N1 + g) = c.Q(p, c.N1);
+        } else {
+            // BOUNDARY_MANAGER_1D<T>::SetBoundaryCondition (BOUNDARY_MANAGER_1D.h:47-75): zero-order
+            // extrapolation or the periodic image (ghost -g <- N1-(g-1), N1+g <- g-1) by the
+            // condition of each ghost cell; other conditions leave it.
+            const int kl = c.I.bcg[g - 1], kr = c.I.bcg[kGhost + g - 1];
+            if (kl == kBcExtrapolation1) c.Q(p, -g) = c.Q(p, 0);
+            else if (kl == kBcPeriodic1) c.Q(p, -g) = c.Q(p, c.N1 - (g - 1));
+            if (kr == kBcExtrapolation1) c.Q(p, c.N1 + g) = c.Q(p, c.N1);
+            else if (kr == kBcPeriodic1) c.Q(p, c.N1 + g) = c.Q(p, g - 1);
+        }
     }
     __syncthreads();
 }
@@ -1038,6 +1056,24 @@ struct Batch1D {
         return kOk;
     }
 
+    // Attaches the enum-driven BOUNDARY_MANAGER_1D to instance k: bc = Nx+6 BOUNDARY_CONDITION
+    // values in the FIELD_UNIFORM_1D layout (only the six ghost cells are read).
+    int set_bc_field(int k, const int* bc)
+    {
+        const int nx = host[k].nx;
+        const int idx[6] = {2, 1, 0, nx + 3, nx + 4, nx + 5};  // ghosts -1, -2, -3, N1+1, N1+2, N1+3
+        for (int q = 0; q < 6; ++q)
+            if (bc[idx[q]] < -4 || bc[idx[q]] > 0) {
+                set_last_error("BOUNDARY_CONDITION values are -4 (SOLID_WALL) .. 0 (FLUID)", __FILE__, __LINE__);
+                return kErrArg;
+            }
+        AWCM_CUDA_TRY(download_inst());
+        for (int q = 0; q < 6; ++q) host[k].bcg[q] = (int8_t)bc[idx[q]];
+        host[k].bc_generic = 1;
+        AWCM_CUDA_TRY(upload_inst());
+        return kOk;
+    }
+
     // Threshold of instance k for a single-pass call (the step takes it from set_run).
     int set_tol(int k, double tol)
     {
@@ -1421,6 +1457,12 @@ int awcm1d_batch_manager(awcm1d_batch_t h, int k, int op, int mask_id, int level
         level_id > 3)
         return awcm::kErrArg;
     return h->b.pass(k, op, bit_of_mask(mask_id), level_id);
+}
+int awcm1d_batch_set_bc_field(awcm1d_batch_t h, int k, const int* bc)
+{
+    AWCM_B(h, k);
+    if (!bc) return awcm::kErrArg;
+    return h->b.set_bc_field(k, bc);
 }
 int awcm1d_batch_apply_bc(awcm1d_batch_t h, int k)
 {

@@ -1038,6 +1038,62 @@ __device__ __forceinline__ double euler_E(double g, double rho, double u, double
 // BOUNDARY_MANAGER_ISENVORTEX (Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h:107-171) and
 // BOUNDARY_MANAGER_SHOCK_VORTEX (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:118-201:
 // transmissive left/right, bottom/top walls reflecting rho v).
+// BOUNDARY_CONDITION values of the generic manager (BOUNDARY_MANAGER_2D.h:7-13).
+constexpr int kBcPeriodic = -3, kBcExtrapolation = -2;
+
+// The enum-driven BOUNDARY_MANAGER_2D<TT>::SetBoundaryCondition(field) (BOUNDARY_MANAGER_2D.h:
+// 61-158): each ghost cell of the left/right strips (interior rows), the bottom/top strips
+// (interior columns) and the four corner blocks takes, by its own BOUNDARY_CONDITION, the zero-order
+// extrapolation of the nearest edge (corner) point or, on the strips, the periodic image
+// (ghost -1-c <- end-c, end+1+c <- start+c); any other kind leaves the cell as it is.  Every read is
+// of a grid point, every write of a ghost cell: the reference's sequence of five passes is
+// order-free, so one thread per ghost cell computes it.
+__device__ void bc_fill_generic(const Grid2& g, Field4 f, long tid)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    const long nside = (long)kGhost * g.ny, nbt = (long)kGhost * g.nx, ncorner = 4L * kGhost * kGhost;
+    int i, j, si, sj;
+    if (tid < 2 * nside) {
+        const bool right = tid >= nside;
+        const long r = right ? tid - nside : tid;
+        j = (int)(r / kGhost);
+        const int c = (int)(r % kGhost);
+        i = right ? NX + 1 + c : -1 - c;
+        const int k = g.bcf[g.at(i, j)];
+        if (k == kBcExtrapolation) si = right ? NX : 0;
+        else if (k == kBcPeriodic) si = right ? c : NX - c;
+        else return;
+        sj = j;
+    } else if (tid < 2 * nside + 2 * nbt) {
+        const long r0 = tid - 2 * nside;
+        const bool top = r0 >= nbt;
+        const long r = top ? r0 - nbt : r0;
+        i = (int)(r / kGhost);
+        const int c = (int)(r % kGhost);
+        j = top ? NY + 1 + c : -1 - c;
+        const int k = g.bcf[g.at(i, j)];
+        if (k == kBcExtrapolation) sj = top ? NY : 0;
+        else if (k == kBcPeriodic) sj = top ? c : NY - c;
+        else return;
+        si = i;
+    } else if (tid < 2 * nside + 2 * nbt + ncorner) {
+        const int r = (int)(tid - 2 * nside - 2 * nbt);
+        const int corner = r / (kGhost * kGhost), cell = r % (kGhost * kGhost);
+        const bool right = corner & 1, top = corner >> 1;
+        i = right ? NX + 1 + cell % kGhost : -1 - cell % kGhost;
+        j = top ? NY + 1 + cell / kGhost : -1 - cell / kGhost;
+        if (g.bcf[g.at(i, j)] != kBcExtrapolation) return;
+        si = right ? NX : 0;
+        sj = top ? NY : 0;
+    } else {
+        return;
+    }
+    const size_t a = g.at(i, j), s = g.at(si, sj);
+    double v[4];
+    for (int k = 0; k < 4; ++k) v[k] = f.p[k][s];
+    for (int k = 0; k < 4; ++k) f.p[k][a] = v[k];
+}
+
 __device__ void bc_fill(const Grid2& g, Field4 f, const StepState* st, double t_host, double* zx, double* zy,
                         long tid)
 {
@@ -1045,6 +1101,10 @@ __device__ void bc_fill(const Grid2& g, Field4 f, const StepState* st, double t_
     // zero the LF-speed accumulators of the stage this fill feeds (the grid covers nx and ny)
     if (zx && tid < g.ny) zx[tid] = 0.0;
     if (zy && tid < g.nx) zy[tid] = 0.0;
+    if (g.bc_kind == AWCM_BC_GENERIC) {
+        bc_fill_generic(g, f, tid);
+        return;
+    }
     const int NX = g.nx - 1, NY = g.ny - 1;
     const long nside = (long)kGhost * g.ny, nbt = (long)kGhost * g.nx;
     int i, j, si, sj;  // ghost point and source point
@@ -1854,6 +1914,7 @@ struct Solver2D {
     uint32_t* lists[kNumLists] = {};
     void* staging = nullptr;
     size_t staging_bytes = 0;
+    int8_t* bcf_dev = nullptr;  // BOUNDARY_CONDITION plane of the generic manager
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int launches = 0;
@@ -1933,6 +1994,8 @@ struct Solver2D {
         fr(st);
         for (auto& l : lists) fr(l);
         fr(staging);
+        fr(bcf_dev);
+        bcf_dev = nullptr;
         free_adj();
         fr(tape);
         tape = nullptr;
@@ -1946,7 +2009,7 @@ struct Solver2D {
     int create(int num_levels, int nxc, int nyc, double x_min, double x_max, double y_min, double y_max, int bc)
     {
         if (num_levels < 2 || num_levels > kMaxLevels - 1 || nxc < 5 || nyc < 5) return kErrArg;
-        if (bc < 0 || bc > 3) return kErrArg;
+        if (bc < 0 || bc > 3) return kErrArg;  // the generic manager is attached by set_bc_field
         geo = awcm2d_geometry{num_levels, nxc, nyc, bc, x_min, x_max, y_min, y_max, 1.4};
         const long nx = (long)(nxc - 1) * (1L << (num_levels - 1)) + 1;
         const long ny = (long)(nyc - 1) * (1L << (num_levels - 1)) + 1;
@@ -1966,6 +2029,7 @@ struct Solver2D {
         g.gamma = 1.4;
         g.wz_eps = 1e-40;
         g.wz_delta = 0.0;
+        g.bcf = nullptr;
         g.W = make_weights();
         plane = (size_t)g.pitch * g.rows;
         AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -2116,6 +2180,9 @@ struct Solver2D {
 
     // ---------------------------------------------------------------- enqueue helpers
     long grid_points() const { return (long)g.nx * g.ny; }
+    // Threads of a ghost fill: the four edge strips and the four corner blocks (the corners are
+    // filled by the generic manager only).
+    long bc_threads() const { return 2L * kGhost * g.ny + 2L * kGhost * g.nx + 4L * kGhost * kGhost; }
     long words() const { return (long)(plane / 4); }  // 32-bit words of a mask/level plane
 
     long band_count(int lev, int which) const
@@ -2289,7 +2356,7 @@ struct Solver2D {
     // accumulators for the k_alpha that follows.
     void enq_bc(Field4 f, const StepState* s, int zero_stage = -1, double* zx_in = nullptr, double* zy_in = nullptr)
     {
-        const long n = 2L * kGhost * g.ny + 2L * kGhost * g.nx;
+        const long n = bc_threads();
         double* zx = zx_in ? zx_in : (zero_stage >= 0 ? ax[zero_stage] : nullptr);
         double* zy = zy_in ? zy_in : (zero_stage >= 0 ? ay[zero_stage] : nullptr);
         launch(k_bc, blocks_for(n, 256), 256, g, f, s, 0.0, zx, zy);
@@ -2313,7 +2380,7 @@ struct Solver2D {
     {
         const int ls = stage - 1;
         const unsigned* C = st->cnt + 4 * ls;
-        const unsigned bcb = blocks_for(2L * kGhost * g.ny + 2L * kGhost * g.nx, 256);
+        const unsigned bcb = blocks_for(bc_threads(), 256);
         launch(k_bc_alpha, bcb + face_blocks / 2, 256, g, f, lists[4 * ls], C, lists[4 * ls + 1], C + 1, ax[stage],
                ay[stage], st, bcb, &st->nonfinite);
         after("k_bc_alpha");
@@ -2767,9 +2834,34 @@ struct Solver2D {
         return kOk;
     }
 
+    // Attaches the enum-driven manager: bc holds (Ny+6) x (Nx+6) BOUNDARY_CONDITION values in the
+    // FIELD_UNIFORM_2D layout; every later ghost fill of this instance applies it.
+    int set_bc_field(const int* bc)
+    {
+        const int w = g.nx + 6;
+        std::vector<int8_t> plane(this->plane, 0);
+        for (int j = -kGhost; j < g.ny + kGhost; ++j)
+            for (int i = -kGhost; i < g.nx + kGhost; ++i) {
+                const int v = bc[(size_t)(j + kGhost) * w + (i + kGhost)];
+                if (v < -4 || v > 0) {
+                    set_last_error("BOUNDARY_CONDITION values are -4 (SOLID_WALL) .. 0 (FLUID)", __FILE__, __LINE__);
+                    return kErrArg;
+                }
+                plane[g.at(i, j)] = (int8_t)v;
+            }
+        if (!bcf_dev) AWCM_CUDA_TRY(cudaMalloc(&bcf_dev, this->plane));
+        AWCM_CUDA_TRY(cudaMemcpy(bcf_dev, plane.data(), this->plane, cudaMemcpyHostToDevice));
+        g.bcf = bcf_dev;
+        g.bc_kind = AWCM_BC_GENERIC;
+        geo.bc_kind = AWCM_BC_GENERIC;
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        return kOk;
+    }
+
     int apply_bc(double t)
     {
-        const long n = 2L * kGhost * g.ny + 2L * kGhost * g.nx;
+        const long n = bc_threads();
         launch(k_bc, blocks_for(n, 256), 256, g, q, nullptr, t, nullptr, nullptr);
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -3259,6 +3351,13 @@ int awcm2d_manager(awcm2d_t h, int op, int mask_id, int level_id)
     AWCM_H(h);
     return h->s.manager(op, mask_id, level_id);
 }
+int awcm2d_set_bc_field(awcm2d_t h, const int* bc)
+{
+    AWCM_H(h);
+    AWCM_EULER_ONLY(h);
+    if (!bc) return awcm::kErrArg;
+    return h->s.set_bc_field(bc);
+}
 int awcm2d_apply_bc(awcm2d_t h, double t)
 {
     AWCM_H(h);
@@ -3359,6 +3458,11 @@ int awcm2d_adjoint(awcm2d_t h, double t0, double dt, int n_steps, int checkpoint
 {
     AWCM_H(h);
     AWCM_EULER_ONLY(h);
+    if (h->s.g.bc_kind == AWCM_BC_GENERIC) {
+        awcm::set_last_error("the adjoint's boundary transposes cover the fixed managers only, not the generic one",
+                             __FILE__, __LINE__);
+        return awcm::kErrArg;
+    }
     return h->s.adjoint(t0, dt, n_steps, checkpoint_every, mode, target, grad, out);
 }
 int awcm2d_set_wenoz(awcm2d_t h, double eps, double tau_delta)

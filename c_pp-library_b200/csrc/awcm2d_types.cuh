@@ -14,6 +14,7 @@ struct Grid2 {
     double x_min, y_min, dx, dy, gamma;
     double wz_eps;    // WENO-Z epsilon of the face reconstructions (1e-40 as in the reference)
     double wz_delta;  // > 0: tau = sqrt((b0-b2)^2 + wz_delta^2) instead of |b0 - b2| (0 as in the reference)
+    const int8_t* bcf;  // kind AWCM_BC_GENERIC: BOUNDARY_CONDITION of every ghosted point (plane layout)
     Weights W;
     __host__ __device__ __forceinline__ size_t at(int i, int j) const
     {

@@ -1,11 +1,13 @@
 // The reference's 1D driver loop (Wavelet/main_1d_euler.cpp:61-260) written against the C++
 // mirror classes: the AWCM_1D facade, its field hand-over and the step.  Usage:
-//   sod_driver <num_levels> <nx_coarse> <t_end> <tol> <cfl> [passes]
+//   sod_driver <num_levels> <nx_coarse> <t_end> <tol> <cfl> [passes|generic]
 // Sod tube on cell-centred nodes of [0,1], interface 0.5.  Prints steps, t, |mask0| of the last
 // step, the sum of |mask0| over the steps and a density checksum.  With "passes", the first
 // PrepareEuler is also done pass by pass through AWCM_MANAGER_1D and the facade's wavelet calls
 // (Wavelet/AWCM_1D.h:86-120, the mask copies through the host) on a second instance, and the
-// masks, levels and field are compared with the one-call PrepareEuler ("passes equal 1").
+// masks, levels and field are compared with the one-call PrepareEuler ("passes equal 1").  With
+// "generic", the ghost fills use the enum-driven BOUNDARY_MANAGER_1D<T> with zero-order
+// extrapolation at every ghost cell, which is the transmissive manager's fill.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -60,6 +62,7 @@ int main(int argc, char** argv)
     const double tol = argc > 4 ? std::atof(argv[4]) : 1e-4;
     const double cfl = argc > 5 ? std::atof(argv[5]) : 0.5;
     const bool passes = argc > 6 && std::strcmp(argv[6], "passes") == 0;
+    const bool generic = argc > 6 && std::strcmp(argv[6], "generic") == 0;
     try {
         const int nx = (nx_coarse - 1) * (1 << (num_levels - 1)) + 1;
         const double x0 = 0.5 / nx, x1 = 1 - 0.5 / nx;
@@ -67,6 +70,10 @@ int main(int argc, char** argv)
         AWCM_1D awcm(num_levels, nx_coarse, x0, x1);
         const double left[3] = {1.0, 0.0, 1.0}, right[3] = {0.125, 0.0, 0.1};
         awcm.InitializeRiemann(0.5, left, right);
+        if (generic) {
+            const std::vector<int> bc((size_t)nx + 6, awcm_b200::EXTRAPOLATION_ZERO_ORDER);
+            awcm_b200::BOUNDARY_MANAGER_1D<>(bc).SetBoundaryCondition(awcm);
+        }
         double t = 0, upd = 0;
         int steps = 0;
         while (true) {

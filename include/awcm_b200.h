@@ -54,6 +54,16 @@ extern "C" {
 #define AWCM_BC_PERIODIC 2     /* BOUNDARY_MANAGER_ISENVORTEX                          */
 #define AWCM_BC_SHOCK_VORTEX 3 /* BOUNDARY_MANAGER_SHOCK_VORTEX: transmissive left/right,
                                   reflecting bottom/top (PROBLEM_SHOCK_VORTEX_INTERACTION.h:78-201) */
+#define AWCM_BC_GENERIC 4      /* the enum-driven BOUNDARY_MANAGER_1D<T> / BOUNDARY_MANAGER_2D<TT>
+                                  (BOUNDARY_MANAGER_1D.h:17-76, BOUNDARY_MANAGER_2D.h:23-159), attached
+                                  with awcm1d_batch_set_bc_field / awcm2d_set_bc_field */
+
+/* BOUNDARY_CONDITION values of the generic managers (BOUNDARY_MANAGER_2D.h:7-13). */
+#define AWCM_SOLID_WALL (-4)
+#define AWCM_PERIODIC (-3)
+#define AWCM_EXTRAPOLATION_ZERO_ORDER (-2)
+#define AWCM_SPECIFIED (-1)
+#define AWCM_FLUID 0
 
 /* 2D problem initial states (Problems/2D/*::Initialize). */
 #define AWCM_PROBLEM_QUADRANTS 0   /* a, b = split point                      */
@@ -112,6 +122,15 @@ int awcm2d_interpolate_all(awcm2d_t h, int from_id);
 int awcm2d_manager(awcm2d_t h, int op, int mask_id, int level_id);
 /* BOUNDARY_MANAGER_{QUAD,DMACH,ISENVORTEX}::SetBoundaryCondition([t]) on the conserved field. */
 int awcm2d_apply_bc(awcm2d_t h, double t);
+/* Attaches the enum-driven BOUNDARY_MANAGER_2D<VECTOR_4D<double>> (BOUNDARY_MANAGER_2D.h:23-159) as
+ * the instance's boundary manager (kind AWCM_BC_GENERIC from then on): bc is its
+ * FIELD_UNIFORM_2D<BOUNDARY_CONDITION>, one AWCM_* condition per ghosted point ((Ny+6) x (Nx+6) ints,
+ * only the ghost ring is read).  Every ghost fill (awcm2d_apply_bc and the stage fills of the step)
+ * then does SetBoundaryCondition(field): zero-order extrapolation and periodic cells on the four
+ * strips, extrapolated corner blocks; SOLID_WALL, SPECIFIED and FLUID cells are left as they are,
+ * as in the reference, which marks the class "not used now" (:20).  The adjoint refuses such an
+ * instance; state files do not carry the condition field. */
+int awcm2d_set_bc_field(awcm2d_t h, const int* bc);
 
 /* One pass of the reference driver loop (Wavelet/main_2d_euler(quad).cpp:58-334): PrepareEuler,
  * CFL dt (clipped to t_next), three SSP-RK3 stages with WENO-Z/Roe fluxes on the finest level and
@@ -282,6 +301,12 @@ int awcm1d_batch_iwt(awcm1d_batch_t h, int k, int mask_id);
 int awcm1d_batch_interpolate(awcm1d_batch_t h, int k, int from_id, int to_id);
 int awcm1d_batch_manager(awcm1d_batch_t h, int k, int op, int mask_id, int level_id);
 int awcm1d_batch_apply_bc(awcm1d_batch_t h, int k);
+/* Attaches the enum-driven BOUNDARY_MANAGER_1D<VECTOR_3D<double>> (BOUNDARY_MANAGER_1D.h:17-76) to
+ * instance k in place of the transmissive BOUNDARY_MANAGER: bc is its FIELD_UNIFORM_1D<BOUNDARY_CONDITION>
+ * (Nx+6 AWCM_* conditions; the six ghost cells are read).  Every later ghost fill of the instance
+ * (awcm1d_batch_apply_bc and the stage fills of the step) applies SetBoundaryCondition(field):
+ * zero-order extrapolation or the periodic image per ghost cell, other conditions untouched. */
+int awcm1d_batch_set_bc_field(awcm1d_batch_t h, int k, const int* bc);
 /* Launch shape of the step kernel: threads per CTA and CTAs per SM (0 = occupancy limit). */
 int awcm1d_batch_set_launch(awcm1d_batch_t h, int threads, int ctas_per_sm);
 int awcm1d_batch_stream(awcm1d_batch_t h, void** stream);

@@ -202,6 +202,33 @@ using BOUNDARY_MANAGER_DMACH = BOUNDARY_MANAGER_OF_INSTANCE_2D;
 using BOUNDARY_MANAGER_ISENVORTEX = BOUNDARY_MANAGER_OF_INSTANCE_2D;
 using BOUNDARY_MANAGER_SHOCK_VORTEX = BOUNDARY_MANAGER_OF_INSTANCE_2D;
 
+// BOUNDARY_CONDITION of the generic managers (BOUNDARY_MANAGER_2D.h:7-13).
+enum BOUNDARY_CONDITION {
+    SOLID_WALL = AWCM_SOLID_WALL,
+    PERIODIC = AWCM_PERIODIC,
+    EXTRAPOLATION_ZERO_ORDER = AWCM_EXTRAPOLATION_ZERO_ORDER,
+    SPECIFIED = AWCM_SPECIFIED,
+    FLUID = AWCM_FLUID
+};
+
+// The enum-driven BOUNDARY_MANAGER_2D<TT> (BOUNDARY_MANAGER_2D.h:23-159): built over a condition
+// field ((Ny+6) x (Nx+6) values in the FIELD_UNIFORM_2D layout); SetBoundaryCondition(awcm)
+// attaches it to the instance (whose later stage fills then use it too) and fills the ghost ring
+// of the instance's conserved field.  TT is the reference's field element type, kept for the name.
+template <class TT = void>
+class BOUNDARY_MANAGER_2D {
+public:
+    explicit BOUNDARY_MANAGER_2D(const std::vector<int>& bc) : bc_(bc) {}
+    void SetBoundaryCondition(AWCM_2D& a) const
+    {
+        check(awcm2d_set_bc_field(a.handle(), bc_.data()), "awcm2d_set_bc_field");
+        check(awcm2d_apply_bc(a.handle(), 0.0), "SetBoundaryCondition");
+    }
+
+private:
+    std::vector<int> bc_;
+};
+
 // EULER_EQUATION_2D (EULER_EQUATION.h:64-156) over batches of device-resident states (n x 4).
 struct EULER_EQUATION_2D {
     double gamma;
@@ -341,6 +368,22 @@ struct BOUNDARY_MANAGER {
 
 private:
     AWCM_1D& a_;
+};
+
+// The enum-driven BOUNDARY_MANAGER_1D<T> (BOUNDARY_MANAGER_1D.h:17-76) over a condition field of
+// Nx+6 values; SetBoundaryCondition(awcm) attaches it to the instance and fills its ghost cells.
+template <class T = void>
+class BOUNDARY_MANAGER_1D {
+public:
+    explicit BOUNDARY_MANAGER_1D(const std::vector<int>& bc) : bc_(bc) {}
+    void SetBoundaryCondition(AWCM_1D& a) const
+    {
+        check(awcm1d_batch_set_bc_field(a.handle(), 0, bc_.data()), "awcm1d_batch_set_bc_field");
+        check(awcm1d_batch_apply_bc(a.handle(), 0), "SetBoundaryCondition");
+    }
+
+private:
+    std::vector<int> bc_;
 };
 
 // EULER_EQUATION_1D (EULER_EQUATION.h:6-62) over batches of device-resident states (n x 3).

@@ -113,6 +113,7 @@ class Oracle1D:
         self._scalar_step = b("scalar_step", None, [_vp, _c_double, _c_double, _dp])
         self._interpolate = b("interpolate", None, [_vp, _c_int, _c_int])
         self._apply_bc = b("apply_bc", None, [_vp])
+        self._set_bc_field = b("set_bc_field", None, [_vp, ctypes.POINTER(_c_int)])
         self.h = self._create(num_levels, nx_coarse, x_min, x_max, gamma, scheme)
         self.nx = self._nx(self.h)
 
@@ -168,8 +169,13 @@ class Oracle1D:
         self._interpolate(self.h, from_id, to_id)
 
     def apply_bc(self):
-        """BOUNDARY_MANAGER::SetBoundaryCondition (transmissive)."""
+        """The ghost fill: transmissive BOUNDARY_MANAGER, or the generic one once attached."""
         self._apply_bc(self.h)
+
+    def set_bc_field(self, bc):
+        """Attaches BOUNDARY_MANAGER_1D<T> with the BOUNDARY_CONDITION field bc (Nx+6 ints)."""
+        bc = np.ascontiguousarray(bc, dtype=np.int32).reshape(self.nx + 6)
+        self._set_bc_field(self.h, _ptr(bc, ctypes.c_int))
 
     def step(self, tol, cfl, t, t_next):
         out = np.zeros(10)
@@ -219,6 +225,7 @@ class Oracle2D:
         self._scalar_step = b("scalar_step", None, [_vp, _c_double, _c_double, _dp])
         self._manager = b("manager", None, [_vp, _c_int, _c_int, _c_int])
         self._apply_bc = b("apply_bc", None, [_vp, _c_double])
+        self._set_bc_field = b("set_bc_field", None, [_vp, ctypes.POINTER(_c_int)])
         self._step = b("step", None, [_vp] + [_c_double] * 5 + [_dp, _dp])
         self._set_freeze = b("set_freeze", None, [_vp, _c_int])
         if kind == "port":
@@ -311,6 +318,11 @@ class Oracle2D:
 
     def apply_bc(self, t=0.0):
         self._apply_bc(self.h, t)
+
+    def set_bc_field(self, bc):
+        """Attaches BOUNDARY_MANAGER_2D<TT> with the BOUNDARY_CONDITION field bc ((Ny+6, Nx+6) ints)."""
+        bc = np.ascontiguousarray(bc, dtype=np.int32).reshape(self.ny + 6, self.nx + 6)
+        self._set_bc_field(self.h, _ptr(bc, ctypes.c_int))
 
     def set_freeze(self, mode: int):
         """0 normal; 1 frozen mask (no PrepareEuler, no residue removal), LF speeds computed and

@@ -158,6 +158,9 @@ struct O1D {
     std::vector<double> q[3], qc[3], qt[3];
     std::vector<uint8_t> m;   // mask bits per ghosted point
     std::vector<int> lv[4];  // levels, interior points
+    // the enum-driven BOUNDARY_MANAGER_1D<T> (BOUNDARY_MANAGER_1D.h:17-76) when set: the condition
+    // of every ghosted point (FIELD_UNIFORM_1D<BOUNDARY_CONDITION> layout)
+    std::vector<int> bcf;
     int D(int lev) const { return 1 << (maxl - lev); }
     bool get(int i, int b) const { return (m[i + G] >> b) & 1; }
     void set(int i, int b)
@@ -362,8 +365,24 @@ void prepare1d(O1D& s, double tol)
 }
 
 // BOUNDARY_MANAGER::SetBoundaryCondition (Problems/1D/PROBLEM_SHOCKTUBE.h:86-107): copy the end points.
+// BOUNDARY_CONDITION values (BOUNDARY_MANAGER_2D.h:7-13).
+constexpr int kPeriodic = -3, kExtrapolation = -2;
+
 void bc1d(O1D& s)
 {
+    if (!s.bcf.empty()) {
+        // BOUNDARY_MANAGER_1D<T>::SetLeft/RightBoundaryCondition (BOUNDARY_MANAGER_1D.h:47-69)
+        const int N1 = s.nx - 1;
+        for (int p = 0; p < 3; ++p)
+            for (int c = 0; c < G; ++c) {
+                const int kl = s.bcf[G - 1 - c], kr = s.bcf[N1 + G + 1 + c];
+                if (kl == kExtrapolation) s.Q(p, -1 - c) = s.Q(p, 0);
+                if (kl == kPeriodic) s.Q(p, -1 - c) = s.Q(p, N1 - c);
+                if (kr == kExtrapolation) s.Q(p, N1 + 1 + c) = s.Q(p, N1);
+                if (kr == kPeriodic) s.Q(p, N1 + 1 + c) = s.Q(p, c);
+            }
+        return;
+    }
     for (int p = 0; p < 3; ++p)
         for (int g = 1; g <= G; ++g) {
             s.Q(p, -g) = s.Q(p, 0);
@@ -715,6 +734,9 @@ struct O2D {
     std::vector<uint8_t> m;
     std::vector<int> lv[4];
     bool scalar = false;  // scalar AWCM (main_2d_advect.cpp): q[0] carries the field
+    // the enum-driven BOUNDARY_MANAGER_2D<TT> (BOUNDARY_MANAGER_2D.h:23-159) when set: the condition
+    // of every ghosted point (FIELD_UNIFORM_2D<BOUNDARY_CONDITION> layout)
+    std::vector<int> bcf;
     int D(int lev) const { return 1 << (maxl - lev); }
     size_t at(int i, int j) const { return (size_t)(j + G) * w + (i + G); }
     bool get(int i, int j, int b) const { return (m[at(i, j)] >> b) & 1; }
@@ -1097,11 +1119,55 @@ double euler_E(double g, double rho, double u, double v, double p) { return p / 
 // BOUNDARY_MANAGER_DMACH(t) (Problems/2D/PROBLEM_DOUBLEMACH.h:106-245), periodic
 // BOUNDARY_MANAGER_ISENVORTEX (Problems/2D/PROBLEM_ISENTROPIC_VORTEX_ADVECTION.h:107-171).
 // Only edge ghosts are filled; corner ghosts are never read by the axis-aligned stencils.
+// BOUNDARY_MANAGER_2D<TT>::SetBoundaryCondition(field) (BOUNDARY_MANAGER_2D.h:61-158): left, right,
+// bottom, top strips (extrapolation or periodic image per ghost cell), then the corner blocks
+// (extrapolation only).
+void bc2d_generic(O2D& s, std::vector<double>* f)
+{
+    const int NX = s.nx - 1, NY = s.ny - 1;
+    auto F = [&](int p, int i, int j) -> double& { return f[p][s.at(i, j)]; };
+    auto K = [&](int i, int j) { return s.bcf[s.at(i, j)]; };
+    auto copy = [&](int i, int j, int si, int sj) {
+        for (int p = 0; p < 4; ++p) F(p, i, j) = F(p, si, sj);
+    };
+    for (int j = 0; j <= NY; ++j)
+        for (int c = 0; c < G; ++c) {
+            if (K(-1 - c, j) == kExtrapolation) copy(-1 - c, j, 0, j);
+            if (K(-1 - c, j) == kPeriodic) copy(-1 - c, j, NX - c, j);
+        }
+    for (int j = 0; j <= NY; ++j)
+        for (int c = 0; c < G; ++c) {
+            if (K(NX + 1 + c, j) == kExtrapolation) copy(NX + 1 + c, j, NX, j);
+            if (K(NX + 1 + c, j) == kPeriodic) copy(NX + 1 + c, j, c, j);
+        }
+    for (int i = 0; i <= NX; ++i)
+        for (int c = 0; c < G; ++c) {
+            if (K(i, -1 - c) == kExtrapolation) copy(i, -1 - c, i, 0);
+            if (K(i, -1 - c) == kPeriodic) copy(i, -1 - c, i, NY - c);
+        }
+    for (int i = 0; i <= NX; ++i)
+        for (int c = 0; c < G; ++c) {
+            if (K(i, NY + 1 + c) == kExtrapolation) copy(i, NY + 1 + c, i, NY);
+            if (K(i, NY + 1 + c) == kPeriodic) copy(i, NY + 1 + c, i, c);
+        }
+    for (int a = 0; a < G; ++a)
+        for (int b = 0; b < G; ++b) {
+            if (K(-1 - a, -1 - b) == kExtrapolation) copy(-1 - a, -1 - b, 0, 0);
+            if (K(-1 - a, NY + 1 + b) == kExtrapolation) copy(-1 - a, NY + 1 + b, 0, NY);
+            if (K(NX + 1 + a, -1 - b) == kExtrapolation) copy(NX + 1 + a, -1 - b, NX, 0);
+            if (K(NX + 1 + a, NY + 1 + b) == kExtrapolation) copy(NX + 1 + a, NY + 1 + b, NX, NY);
+        }
+}
+
 void bc2d(O2D& s, std::vector<double>* f, double t)
 {
     const int NX = s.nx - 1, NY = s.ny - 1;
     auto F = [&](int p, int i, int j) -> double& { return f[p][s.at(i, j)]; };
     const double g = 1.4;
+    if (!s.bcf.empty()) {
+        bc2d_generic(s, f);
+        return;
+    }
     if (s.bc_kind == BC_PERIODIC) {
         for (int j = 0; j <= NY; ++j)
             for (int c = 0; c < G; ++c)
@@ -1456,6 +1522,20 @@ void or1d_interpolate(void* h, int from_id, int to_id)
     interp1d(*static_cast<O1D*>(h), bit_of(from_id), bit_of(to_id));
 }
 void or1d_apply_bc(void* h) { bc1d(*static_cast<O1D*>(h)); }
+// bc: Nx+6 BOUNDARY_CONDITION values; attaches the generic manager.
+void or1d_set_bc_field(void* h, const int* bc)
+{
+    O1D& s = *static_cast<O1D*>(h);
+    s.bcf.assign(bc, bc + s.nx + 2 * G);
+}
+// bc: (Ny+6) x (Nx+6) BOUNDARY_CONDITION values; attaches the generic manager.
+void or2d_set_bc_field(void* h, const int* bc)
+{
+    O2D& s = *static_cast<O2D*>(h);
+    s.bcf.assign((size_t)(s.nx + 2 * G) * (s.ny + 2 * G), 0);
+    for (int j = -G; j < s.ny + G; ++j)
+        for (int i = -G; i < s.nx + G; ++i) s.bcf[s.at(i, j)] = bc[(size_t)(j + G) * (s.nx + 2 * G) + (i + G)];
+}
 
 // EULER_EQUATION_1D::ComputeFu / Spectral_Radius (EULER_EQUATION.h:16-26, 42-47) and
 // EULER_EQUATION_2D::ComputeFu / ComputeGu / Spectral_RadiusX / Spectral_RadiusY (:74-99, :118-142)

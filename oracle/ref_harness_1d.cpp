@@ -30,6 +30,7 @@ void FIELD_UNIFORM_1D<bool>::AssignAllValues(const bool& v)
 #include "ARRAY_1D.h"
 #include "Problems/1D/PROBLEM_SHOCKTUBE.h"
 #include "Wavelet/AWCM_1D.h"
+#include "BOUNDARY_MANAGER_1D.h"
 
 #include <cstdint>
 #include <cstring>
@@ -42,6 +43,10 @@ struct Ref1D {
     GRID_UNIFORM_1D grid;
     FIELD_UNIFORM_1D<VECTOR_3D<double>> Q, Q_temp, Q_copy;
     BOUNDARY_MANAGER* bc = nullptr;
+    // The enum-driven BOUNDARY_MANAGER_1D<VECTOR_3D<double>> (BOUNDARY_MANAGER_1D.h:17-76) and its
+    // condition field, used in place of bc once set (ref1d_set_bc_field).
+    FIELD_UNIFORM_1D<BOUNDARY_CONDITION> bcf;
+    BOUNDARY_MANAGER_1D<VECTOR_3D<double>>* generic = nullptr;
     WENO_EULER_SOLVER_1D* weno = nullptr;
     WENOZ_EULER_SOLVER_1D* wenoz = nullptr;
     FIELD_UNIFORM_1D<double> sq, sq_0, sq_1, sq_2;  // scheme 2: q and the stage fields q_0, q_1, q_2
@@ -50,6 +55,12 @@ struct Ref1D {
     int scheme = 0;
     int nx = 0;
 };
+
+void apply_bc(Ref1D* s)
+{
+    if (s->generic) s->generic->SetBoundaryCondition(s->Q);
+    else s->bc->SetBoundaryCondition();
+}
 
 FIELD_UNIFORM_1D<bool>& mask_ref(Ref1D* s, int id)
 {
@@ -225,6 +236,7 @@ void ref1d_destroy(void* h)
 {
     Ref1D* s = static_cast<Ref1D*>(h);
     delete s->bc;
+    delete s->generic;
     delete s->weno;
     delete s->wenoz;
     delete s->awcm;
@@ -375,7 +387,17 @@ void ref1d_interpolate(void* h, int from_id, int to_id)
     s->awcm->wavelet.InterpolateEuler(s->Q, s->mra, mask_ref(s, from_id), mask_ref(s, to_id));
 }
 
-void ref1d_apply_bc(void* h) { static_cast<Ref1D*>(h)->bc->SetBoundaryCondition(); }
+void ref1d_apply_bc(void* h) { apply_bc(static_cast<Ref1D*>(h)); }
+
+// bc: Nx+6 BOUNDARY_CONDITION values; the generic manager takes over the ghost fills.
+void ref1d_set_bc_field(void* h, const int* bc)
+{
+    Ref1D* s = static_cast<Ref1D*>(h);
+    s->bcf.Initialize(s->grid, 3);
+    for (int i = -3; i < s->nx + 3; ++i) s->bcf(i) = (BOUNDARY_CONDITION)bc[i + 3];
+    delete s->generic;
+    s->generic = new BOUNDARY_MANAGER_1D<VECTOR_3D<double>>(s->bcf);
+}
 
 // The reference's EULER_EQUATION_1D itself over n states of 3 doubles.
 void ref_euler1d_flux(const double* q, double* f, int n, double gamma)
@@ -447,18 +469,18 @@ void ref1d_step(void* h, double tol, double cfl, double t, double t_next, double
         cnt[3] += awcm.mask3(i);
     }
 
-    s->bc->SetBoundaryCondition();
+    apply_bc(s);
     double a1 = alpha1d(s, awcm.mask3, awcm.level3);
     s->Q_copy = Q;
     s->Q_temp = Q;
     stage1d(s, awcm.mask2, awcm.level2, a1, dt, 1);
 
-    s->bc->SetBoundaryCondition();
+    apply_bc(s);
     double a2 = alpha1d(s, awcm.mask2, awcm.level2);
     s->Q_temp = Q;
     stage1d(s, awcm.mask1, awcm.level1, a2, dt, 2);
 
-    s->bc->SetBoundaryCondition();
+    apply_bc(s);
     double a3 = alpha1d(s, awcm.mask1, awcm.level1);
     s->Q_temp = Q;
     stage1d(s, awcm.mask0, awcm.level0, a3, dt, 3);

@@ -14,6 +14,7 @@
 #include "WENO.h"
 #include "WENOZ.h"
 #include "EULER_EQUATION.h"
+#include "BOUNDARY_MANAGER_2D.h"
 
 #include <cstdint>
 #include <omp.h>
@@ -23,14 +24,17 @@ namespace {
 
 enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2, BC_SHOCK_VORTEX = 3 };
 
-// One boundary manager per field, of the kind the problem uses.
+// One boundary manager per field, of the kind the problem uses, or the enum-driven
+// BOUNDARY_MANAGER_2D<VECTOR_4D<double>> (BOUNDARY_MANAGER_2D.h:23-159) once a condition field is set.
 struct BC2D {
     int kind;
     BOUNDARY_MANAGER_QUAD* quad = nullptr;
     BOUNDARY_MANAGER_DMACH* dmach = nullptr;
     BOUNDARY_MANAGER_ISENVORTEX* periodic = nullptr;
     BOUNDARY_MANAGER_SHOCK_VORTEX* shock_vortex = nullptr;
-    BC2D(int k, FIELD_UNIFORM_2D<VECTOR_4D<double>>& Q) : kind(k)
+    BOUNDARY_MANAGER_2D<VECTOR_4D<double>>* generic = nullptr;
+    FIELD_UNIFORM_2D<VECTOR_4D<double>>* field;
+    BC2D(int k, FIELD_UNIFORM_2D<VECTOR_4D<double>>& Q) : kind(k), field(&Q)
     {
         if (k == BC_DMACH) dmach = new BOUNDARY_MANAGER_DMACH(Q);
         else if (k == BC_PERIODIC) periodic = new BOUNDARY_MANAGER_ISENVORTEX(Q);
@@ -43,10 +47,12 @@ struct BC2D {
         delete dmach;
         delete periodic;
         delete shock_vortex;
+        delete generic;
     }
     void apply(double t)
     {
-        if (dmach) dmach->SetBoundaryCondition(t);
+        if (generic) generic->SetBoundaryCondition(*field);
+        else if (dmach) dmach->SetBoundaryCondition(t);
         else if (periodic) periodic->SetBoundaryCondition();
         else if (shock_vortex) shock_vortex->SetBoundaryCondition();
         else quad->SetBoundaryCondition();
@@ -72,6 +78,8 @@ struct Ref2D {
     // periodic BOUNDARY_MANAGER of Problems/2D/PROBLEM_BOX_ADVECTION.h; created by ref2d_set_scalar.
     FIELD_UNIFORM_2D<double> S, S_0, S_1, S_2;
     BOUNDARY_MANAGER *bs = nullptr, *bs1 = nullptr, *bs2 = nullptr;
+    // The condition field of the enum-driven manager (ref2d_set_bc_field).
+    FIELD_UNIFORM_2D<BOUNDARY_CONDITION> bcf;
 };
 
 FIELD_UNIFORM_2D<bool>& mask_ref(Ref2D* s, int id)
@@ -528,6 +536,21 @@ void ref2d_manager(void* h, int op, int mask_id, int level_id)
             break;
         }
         default: break;
+    }
+}
+
+// bc: (Ny+6) x (Nx+6) BOUNDARY_CONDITION values; every field's manager becomes the reference's
+// BOUNDARY_MANAGER_2D<VECTOR_4D<double>> over that condition field.
+void ref2d_set_bc_field(void* h, const int* bc)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    s->bcf.Initialize(s->grid, 3);
+    const int w = s->nx + 6;
+    for (int j = -3; j < s->ny + 3; ++j)
+        for (int i = -3; i < s->nx + 3; ++i) s->bcf(i, j) = (BOUNDARY_CONDITION)bc[(size_t)(j + 3) * w + (i + 3)];
+    for (BC2D* b : {s->bc, s->bc0, s->bc1, s->bc2}) {
+        delete b->generic;
+        b->generic = new BOUNDARY_MANAGER_2D<VECTOR_4D<double>>(s->bcf);
     }
 }
 

@@ -76,3 +76,14 @@ def test_sod_driver_matches_oracle(tmp_path, awcm_lib):
     for v in ref.get_q()[:, 0]:  # same left-to-right sum as the driver
         acc += float(v)
     assert rho_sum == acc
+
+
+@pytest.mark.gpu
+def test_sod_driver_generic_manager(tmp_path, awcm_lib):
+    """The generic BOUNDARY_MANAGER_1D<T> mirror with extrapolation at every ghost cell gives the
+    transmissive run."""
+    exe = build_sod_driver(tmp_path)
+    a = subprocess.run([exe, "7", "17", "0.05", "1e-4", "0.5"], capture_output=True, text=True, check=True).stdout
+    b = subprocess.run([exe, "7", "17", "0.05", "1e-4", "0.5", "generic"], capture_output=True, text=True,
+                       check=True).stdout
+    assert a == b and a.startswith("steps ")

@@ -1,8 +1,8 @@
 """Parity where the benchmarks run: developed flow at full size, a whole run, the batched sizes.
 
-* Developed flow, full size: the GPU runs the 2049^2 four-quadrant problem 300 steps (the
+* Developed flow, full size: the GPU runs the 2049^2 four-quadrant problem 1500 steps (the
   shocks interacting, the active set several times its initial size) and the 4097x1025 double
-  Mach problem 150 steps, saves its state to the binary state file, and both the GPU and the
+  Mach problem 800 steps, saves its state to the binary state file, and both the GPU and the
   CPU oracle load that file and take three steps in lockstep: dt, mask sizes, masks, levels and
   fields bit for bit.
 * Whole run: the 513^2 four-quadrant problem from its initial state to t_end = 0.3 on both
@@ -34,8 +34,8 @@ def corner_free(q):
 
 DEVELOPED = {
     # name: (num_levels, nx_coarse, ny_coarse, domain, bc, problem, a, b, tol, cfl, t_end, steps)
-    "quadrants_2049_step300": (7, 33, 33, (0.0, 1.0, 0.0, 1.0), 0, 0, 0.5, 0.5, 1e-3, 0.4, 0.3, 300),
-    "double_mach_4097x1025_step150": (7, 65, 17, (0.0, 4.0, 0.0, 1.0), 1, 1, 1.4, 0.0, 1e-3, 0.5, 0.2, 150),
+    "quadrants_2049_step1500": (7, 33, 33, (0.0, 1.0, 0.0, 1.0), 0, 0, 0.5, 0.5, 1e-3, 0.4, 0.3, 1500),
+    "double_mach_4097x1025_step800": (7, 65, 17, (0.0, 4.0, 0.0, 1.0), 1, 1, 1.4, 0.0, 1e-3, 0.5, 0.2, 800),
 }
 
 

@@ -126,3 +126,70 @@ def test_1d_interpolate_and_boundary_fill():
     for o in (a, b):
         o.apply_bc()
     assert np.array_equal(a.get_q(), b.get_q())
+
+
+def random_conditions(shape, seed):
+    """A BOUNDARY_CONDITION field with every kind (SOLID_WALL..FLUID) drawn per cell."""
+    return np.random.default_rng(seed).integers(-4, 1, size=shape).astype(np.int32)
+
+
+def test_generic_manager_2d_fill():
+    """BOUNDARY_MANAGER_2D<TT>::SetBoundaryCondition on a random field with randomly mixed
+    conditions per ghost cell: restatement equal to the reference's class, corners included."""
+    geom = (4, 9, 9, 0.0, 1.0, 0.0, 1.0)
+    a = Oracle2D(*geom, kind="port")
+    b = Oracle2D(*geom, kind="reference")
+    q = np.random.default_rng(1).uniform(0.5, 2.0, (a.ny + 6, a.nx + 6, 4))
+    bc = random_conditions((a.ny + 6, a.nx + 6), 2)
+    for o in (a, b):
+        o.set_q(q)
+        o.set_bc_field(bc)
+        o.apply_bc()
+    assert np.array_equal(a.get_q(), b.get_q())
+
+
+def test_generic_manager_1d_fill_and_steps():
+    n = 257
+    geo = (5, 17, 0.5 / n, 1 - 0.5 / n)
+    a, b = Oracle1D(*geo, kind="port"), Oracle1D(*geo, kind="reference")
+    q = np.random.default_rng(3).uniform(0.5, 2.0, (n + 6, 3))
+    for seed in range(4):
+        bc = random_conditions(n + 6, 10 + seed)
+        for o in (a, b):
+            o.set_q(q)
+            o.set_bc_field(bc)
+            o.apply_bc()
+        assert np.array_equal(a.get_q(), b.get_q()), seed
+    # a run with periodic ends (left) and extrapolation (right)
+    bc = np.full(n + 6, -2, np.int32)
+    bc[:3] = -3
+    for o in (a, b):
+        o.init_riemann(0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+        o.set_bc_field(bc)
+    t = 0.0
+    for _ in range(20):
+        oa, ob = a.step(1e-4, 0.5, t, 0.2), b.step(1e-4, 0.5, t, 0.2)
+        assert np.array_equal(oa, ob)
+        t += oa[0]
+    assert np.array_equal(a.get_q(), b.get_q())
+
+
+def test_generic_manager_2d_steps():
+    """Steps with the generic manager (periodic in x, extrapolation in y, a SOLID_WALL corner
+    block left alone): restatement equal to the reference."""
+    geom = (4, 9, 9, 0.0, 10.0, 0.0, 10.0)
+    a = Oracle2D(*geom, bc_kind=2, kind="port")
+    b = Oracle2D(*geom, bc_kind=2, kind="reference")
+    bc = np.full((a.ny + 6, a.nx + 6), -2, np.int32)
+    bc[:, :3] = bc[:, -3:] = -3
+    bc[:3, :3] = -4
+    for o in (a, b):
+        o.init_problem(2, 5.0, 5.0)
+        o.set_bc_field(bc)
+    t = 0.0
+    for _ in range(4):
+        oa, ob = a.step(1e-3, 0.4, t, 10.0), b.step(1e-3, 0.4, t, 10.0)
+        assert np.array_equal(oa[:6], ob[:6])
+        t += oa[0]
+    assert np.array_equal(a.get_q(), b.get_q())
+    assert np.array_equal(a.get_masks(), b.get_masks())
