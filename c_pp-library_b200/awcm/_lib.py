@@ -86,6 +86,7 @@ _SIGS = {
     "awcm1d_batch_apply_bc": [c_void_p, c_int],
     "awcm1d_batch_set_bc_field": [c_void_p, c_int, P_int],
     "awcm2d_set_bc_field": [c_void_p, P_int],
+    "awcm2d_wt_set_bottom": [c_void_p, c_int, c_int],
     "awcm1d_batch_set_launch": [c_void_p, c_int, c_int],
     "awcm1d_batch_stream": [c_void_p, ctypes.POINTER(c_void_p)],
     "awcm1d_step_noalloc": [c_int, c_int, c_double, c_double, c_double, c_int, c_double, c_double, c_double, c_double,

@@ -20,10 +20,10 @@ from ._lib import AWCM_OK, AwcmError, P_double, P_int, P_u8, c_void_p, call, loa
 ERR_NONFINITE = 5
 
 AAZ, CR, APD, CL, RR, BAND = 0, 1, 2, 3, 4, 5
-BC_TRANSMISSIVE, BC_DOUBLE_MACH, BC_PERIODIC = 0, 1, 2
+BC_TRANSMISSIVE, BC_DOUBLE_MACH, BC_PERIODIC, BC_SHOCK_VORTEX, BC_GENERIC, BC_WIND_TUNNEL = 0, 1, 2, 3, 4, 5
 # BOUNDARY_CONDITION values of the generic managers (BOUNDARY_MANAGER_2D.h:7-13)
 SOLID_WALL, PERIODIC, EXTRAPOLATION_ZERO_ORDER, SPECIFIED, FLUID = -4, -3, -2, -1, 0
-PROBLEM_QUADRANTS, PROBLEM_DOUBLE_MACH, PROBLEM_VORTEX = 0, 1, 2
+PROBLEM_QUADRANTS, PROBLEM_DOUBLE_MACH, PROBLEM_VORTEX, PROBLEM_SHOCK_VORTEX, PROBLEM_WIND_TUNNEL = 0, 1, 2, 3, 4
 WENOZ, WENO5 = 0, 1
 # 1D scalar AWCM (the path of Wavelet/main_1d_advect.cpp): a batch scheme like the two above.
 SCALAR_ADVECTION = 2
@@ -133,6 +133,10 @@ class AWCM2D:
 
     def apply_bc(self, t=0.0):
         call("awcm2d_apply_bc", self.h, t)
+
+    def wt_set_bottom(self, x_direction: bool, y_direction: bool):
+        """BOUNDARY_MANAGER_WT::SetBottomBoundaryCondition(x_direction, y_direction)."""
+        call("awcm2d_wt_set_bottom", self.h, int(x_direction), int(y_direction))
 
     def set_bc_field(self, bc):
         """Attaches the enum-driven BOUNDARY_MANAGER_2D: bc is (Ny+6, Nx+6) BOUNDARY_CONDITION values."""

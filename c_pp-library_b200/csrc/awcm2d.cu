@@ -533,7 +533,13 @@ __device__ void ph_band_copy(const Grid2& g, uint8_t* m, int bit, int copy_to, S
         const MaskWord mw = mask_word(g, w);
         const unsigned G = grid_lanes(g, mw);
         if (!G) continue;
-        const unsigned inner = (mw.j >= 2 && mw.j <= g.ny - 3) ? lanes_in(mw.i0, 2, g.nx - 3) : 0u;
+        unsigned inner = (mw.j >= 2 && mw.j <= g.ny - 3) ? lanes_in(mw.i0, 2, g.nx - 3) : 0u;
+        if (g.bc_kind == AWCM_BC_WIND_TUNNEL) {
+            // BOUNDARY_MANAGER_WT::BandingMask (Problems/2D/PROBLEM_WINDTUNNEL.h:202-220): also the
+            // band around the step's top and front face
+            if (abs(mw.j - g.wt_j) <= 2) inner &= ~lanes_in(mw.i0, g.wt_i - 2, g.nx - 1);
+            if (mw.j <= g.wt_j + 2) inner &= ~lanes_in(mw.i0, g.wt_i - 2, g.wt_i + 2);
+        }
         const unsigned v = mp[w];
         unsigned nv = v | (lane_bits(G & ~inner) << bit);
         if (copy_to >= 0) {
@@ -1094,6 +1100,43 @@ __device__ void bc_fill_generic(const Grid2& g, Field4 f, long tid)
     for (int k = 0; k < 4; ++k) f.p[k][a] = v[k];
 }
 
+// BOUNDARY_MANAGER_WT::SetBoundaryCondition (Problems/2D/PROBLEM_WINDTUNNEL.h:94-199, "except bottom"):
+// Mach 3 inflow (rho 1.4, u 3, v 0, p 1) in the left ghost columns and zero-order extrapolation in
+// the right ones (interior rows), rho v reflected in the top ghost rows (interior columns).
+__device__ void bc_fill_wind_tunnel(const Grid2& g, Field4 f, long tid)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    const long nside = (long)kGhost * g.ny, nbt = (long)kGhost * g.nx;
+    if (tid < 2 * nside) {
+        const bool right = tid >= nside;
+        const long r = right ? tid - nside : tid;
+        const int j = (int)(r / kGhost), c = (int)(r % kGhost);
+        const size_t a = g.at(right ? NX + 1 + c : -1 - c, j);
+        if (!right) {
+            const double rho = 1.4, u = 3, v = 0, p = 1;
+            f.p[0][a] = rho;
+            f.p[1][a] = rho * u;
+            f.p[2][a] = rho * v;
+            f.p[3][a] = p / (1.4 - 1) + 0.5 * rho * (u * u + v * v);
+        } else {
+            const size_t s = g.at(NX, j);
+            double v[4];
+            for (int k = 0; k < 4; ++k) v[k] = f.p[k][s];
+            for (int k = 0; k < 4; ++k) f.p[k][a] = v[k];
+        }
+        return;
+    }
+    const long r0 = tid - 2 * nside;
+    if (r0 < nbt || r0 >= 2 * nbt) return;  // bottom: per sweep direction (k_wt_bottom_*)
+    const long r = r0 - nbt;
+    const int i = (int)(r / kGhost), c = (int)(r % kGhost);
+    const size_t a = g.at(i, NY + 1 + c), s = g.at(i, NY);
+    double v[4];
+    for (int k = 0; k < 4; ++k) v[k] = f.p[k][s];
+    v[2] = -v[2];
+    for (int k = 0; k < 4; ++k) f.p[k][a] = v[k];
+}
+
 __device__ void bc_fill(const Grid2& g, Field4 f, const StepState* st, double t_host, double* zx, double* zy,
                         long tid)
 {
@@ -1103,6 +1146,10 @@ __device__ void bc_fill(const Grid2& g, Field4 f, const StepState* st, double t_
     if (zy && tid < g.nx) zy[tid] = 0.0;
     if (g.bc_kind == AWCM_BC_GENERIC) {
         bc_fill_generic(g, f, tid);
+        return;
+    }
+    if (g.bc_kind == AWCM_BC_WIND_TUNNEL) {
+        bc_fill_wind_tunnel(g, f, tid);
         return;
     }
     const int NX = g.nx - 1, NY = g.ny - 1;
@@ -1185,6 +1232,45 @@ __global__ void k_bc(Grid2 g, Field4 f, const StepState* st, double t_host, doub
     pdl_begin();
     if (st && st->done) return;
     bc_fill(g, f, st, t_host, zx, zy, gtid());
+}
+
+// BOUNDARY_MANAGER_WT::SetBottomBoundaryCondition(true, false) (PROBLEM_WINDTUNNEL.h:129-141) on f
+// and, when f2.p[0] is set, on f2 too: the three columns i_bdry .. i_bdry+2 of rows -3 .. j_bdry
+// take column i_bdry-1 with rho u reflected.  One thread per written cell (and field).
+__global__ void k_wt_bottom_x(Grid2 g, Field4 f, Field4 f2, const StepState* st)
+{
+    pdl_begin();
+    if (st && st->done) return;
+    const unsigned t = gtid(), rows = (unsigned)(g.wt_j + kGhost + 1), per = 3u * rows;
+    if (t >= (f2.p[0] ? 2u : 1u) * per) return;
+    const Field4 F = t < per ? f : f2;
+    const unsigned r = t % per;
+    const int j = (int)(r / 3u) - kGhost, c = (int)(r % 3u);
+    const size_t a = g.at(g.wt_i + c, j), s = g.at(g.wt_i - 1, j);
+    double v[4];
+    for (int k = 0; k < 4; ++k) v[k] = F.p[k][s];
+    v[1] = -v[1];
+    for (int k = 0; k < 4; ++k) F.p[k][a] = v[k];
+}
+
+// SetBottomBoundaryCondition(false, true) (PROBLEM_WINDTUNNEL.h:143-167), its two loops in order:
+// part 0, the bottom ghost rows of columns -3 .. Nx+1 from row 0; part 1, the rows j_bdry-2 ..
+// j_bdry of columns i_bdry .. Nx+2 from row j_bdry+1; rho v reflected.
+__global__ void k_wt_bottom_y(Grid2 g, Field4 f, int part, const StepState* st)
+{
+    pdl_begin();
+    if (st && st->done) return;
+    const unsigned t = gtid();
+    const int i0 = part == 0 ? -kGhost : g.wt_i;
+    const int i1 = part == 0 ? g.nx - 1 + kGhost - 1 : g.nx - 1 + kGhost;  // inclusive
+    if (t >= 3u * (unsigned)(i1 - i0 + 1)) return;
+    const int i = i0 + (int)(t / 3u), c = (int)(t % 3u);
+    const size_t a = part == 0 ? g.at(i, -1 - c) : g.at(i, g.wt_j - c);
+    const size_t s = part == 0 ? g.at(i, 0) : g.at(i, g.wt_j + 1);
+    double v[4];
+    for (int k = 0; k < 4; ++k) v[k] = f.p[k][s];
+    v[2] = -v[2];
+    for (int k = 0; k < 4; ++k) f.p[k][a] = v[k];
 }
 
 // ------------------------------------------------------------------------- CFL and LF reductions
@@ -1616,8 +1702,9 @@ __device__ __forceinline__ void update_fin_point(const Grid2& g, Field4 in, Fiel
 // Coarse-level points: 4th-order central differences of F and G at spacing d = 2^(maxl-lev), with
 // the reference's one-sided forms next to the boundary (AWCM_2D::Differentiate*, Wavelet/AWCM_2D.h:154-187,
 // branch selection main_2d_euler(quad).cpp:132-160).
+// inx: the field of the x-direction fluxes (the wind tunnel's x-sweep copy of the stage input, else in).
 template <int KIND>
-__device__ __forceinline__ void update_crs_point(const Grid2& g, Field4 in, Field4 out, Field4 qn,
+__device__ __forceinline__ void update_crs_point(const Grid2& g, Field4 in, Field4 inx, Field4 out, Field4 qn,
                                                  const int8_t* __restrict__ lvl, size_t a, const StepState* st)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
@@ -1635,7 +1722,7 @@ __device__ __forceinline__ void update_crs_point(const Grid2& g, Field4 in, Fiel
     {
         double fl[4], fr[4], fo[4], q[4];
         auto load = [&](long off, double* o) {
-            for (int k = 0; k < 4; ++k) q[k] = in.p[k][(long)a + off];
+            for (int k = 0; k < 4; ++k) q[k] = inx.p[k][(long)a + off];
             flux2<0>(q, g.gamma, o);
         };
         load(-d, fl);
@@ -1681,10 +1768,11 @@ __device__ __forceinline__ void update_crs_point(const Grid2& g, Field4 in, Fiel
 // The finest-level and the coarse points of a stage in one launch: the two sets are disjoint and
 // neither reads what the other writes (the stage output, or qn at the point itself).
 template <int KIND>
-__global__ void __launch_bounds__(256) k_update(Grid2 g, Field4 in, Field4 out, Field4 qn, Field4 fx, Field4 fy,
-                                                const int8_t* __restrict__ lvl, const uint32_t* __restrict__ lf,
-                                                const unsigned* __restrict__ nf, const uint32_t* __restrict__ lc,
-                                                const unsigned* __restrict__ nc, const StepState* st)
+__global__ void __launch_bounds__(256) k_update(Grid2 g, Field4 in, Field4 inx, Field4 out, Field4 qn, Field4 fx,
+                                                Field4 fy, const int8_t* __restrict__ lvl,
+                                                const uint32_t* __restrict__ lf, const unsigned* __restrict__ nf,
+                                                const uint32_t* __restrict__ lc, const unsigned* __restrict__ nc,
+                                                const StepState* st)
 {
     pdl_begin();
     if (st->done) return;
@@ -1693,7 +1781,7 @@ __global__ void __launch_bounds__(256) k_update(Grid2 g, Field4 in, Field4 out, 
     const long stride = (long)gridDim.x * blockDim.x;
     for (long e = gtid(); e < n; e += stride) {
         if (e < n0) update_fin_point<KIND>(g, in, out, qn, fx, fy, lf[e], sc);
-        else update_crs_point<KIND>(g, in, out, qn, lvl, lc[e - n0], st);
+        else update_crs_point<KIND>(g, in, inx, out, qn, lvl, lc[e - n0], st);
     }
 }
 
@@ -1906,6 +1994,7 @@ struct Solver2D {
     Grid2 g{};
     size_t plane = 0;
     Field4 q{}, q2{}, q1{}, fx{}, fy{};
+    Field4 qx{};  // wind tunnel: the x-sweep copy of the stage input
     uint8_t* m = nullptr;
     int8_t* lvl[4] = {nullptr, nullptr, nullptr, nullptr};
     double* ax[kStages] = {};
@@ -1984,6 +2073,7 @@ struct Solver2D {
             fr(q1.p[k]);
             fr(fx.p[k]);
             fr(fy.p[k]);
+            fr(qx.p[k]);
             fr(lvl[k]);
         }
         fr(m);
@@ -2009,7 +2099,8 @@ struct Solver2D {
     int create(int num_levels, int nxc, int nyc, double x_min, double x_max, double y_min, double y_max, int bc)
     {
         if (num_levels < 2 || num_levels > kMaxLevels - 1 || nxc < 5 || nyc < 5) return kErrArg;
-        if (bc < 0 || bc > 3) return kErrArg;  // the generic manager is attached by set_bc_field
+        // the generic manager (kind 4) is attached by set_bc_field
+        if (bc < 0 || bc > 5 || bc == AWCM_BC_GENERIC) return kErrArg;
         geo = awcm2d_geometry{num_levels, nxc, nyc, bc, x_min, x_max, y_min, y_max, 1.4};
         const long nx = (long)(nxc - 1) * (1L << (num_levels - 1)) + 1;
         const long ny = (long)(nyc - 1) * (1L << (num_levels - 1)) + 1;
@@ -2030,6 +2121,13 @@ struct Solver2D {
         g.wz_eps = 1e-40;
         g.wz_delta = 0.0;
         g.bcf = nullptr;
+        // BOUNDARY_MANAGER_WT's corner of the step, int(0.6/dx) and int(0.2/dy) (PROBLEM_WINDTUNNEL.h:75-76)
+        g.wt_i = int(0.6 / g.dx);
+        g.wt_j = int(0.2 / g.dy);
+        if (bc == AWCM_BC_WIND_TUNNEL && (g.wt_i < 1 || g.wt_i + 2 > g.nx - 1 + kGhost || g.wt_j + 1 > g.ny - 1)) {
+            set_last_error("wind tunnel: the step corner (0.6, 0.2) must lie inside the grid", __FILE__, __LINE__);
+            return kErrArg;
+        }
         g.W = make_weights();
         plane = (size_t)g.pitch * g.rows;
         AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -2040,6 +2138,10 @@ struct Solver2D {
             AWCM_CUDA_TRY(cudaMalloc(&fx.p[k], plane * sizeof(double)));
             AWCM_CUDA_TRY(cudaMalloc(&fy.p[k], plane * sizeof(double)));
             AWCM_CUDA_TRY(cudaMalloc(&lvl[k], plane));
+            if (bc == AWCM_BC_WIND_TUNNEL) {
+                AWCM_CUDA_TRY(cudaMalloc(&qx.p[k], plane * sizeof(double)));
+                AWCM_CUDA_TRY(cudaMemsetAsync(qx.p[k], 0, plane * sizeof(double), stream));
+            }
             AWCM_CUDA_TRY(cudaMemsetAsync(q.p[k], 0, plane * sizeof(double), stream));
             AWCM_CUDA_TRY(cudaMemsetAsync(q2.p[k], 0, plane * sizeof(double), stream));
             AWCM_CUDA_TRY(cudaMemsetAsync(q1.p[k], 0, plane * sizeof(double), stream));
@@ -2397,6 +2499,26 @@ struct Solver2D {
         launches += 1;
     }
 
+    // The field the x-direction fluxes of a stage read: the wind tunnel's x-sweep copy, else the input.
+    Field4 xin(Field4 in) const { return g.bc_kind == AWCM_BC_WIND_TUNNEL ? qx : in; }
+
+    // The wind tunnel's stage input after its standard fill: the x-sweep copy qx with the
+    // x-direction bottom fill, and the input itself with the x- and then the y-direction one
+    // (BOUNDARY_MANAGER_WT::SetBottomBoundaryCondition, Problems/2D/PROBLEM_WINDTUNNEL.h:124-168).
+    void enq_wt_input(Field4 f)
+    {
+        launch(k_copy4, pb((long)plane), 256, qx, f, plane);
+        after("k_copy4");
+        launch(k_wt_bottom_x, blocks_for(2L * 3 * (g.wt_j + kGhost + 1), 256), 256, g, f, qx, (const StepState*)st);
+        after("k_wt_bottom_x");
+        const long ny0 = 3L * (g.nx + 2 * kGhost - 1), ny1 = 3L * (g.nx - 1 + kGhost - g.wt_i + 1);
+        launch(k_wt_bottom_y, blocks_for(ny0, 256), 256, g, f, 0, (const StepState*)st);
+        after("k_wt_bottom_y");
+        launch(k_wt_bottom_y, blocks_for(ny1, 256), 256, g, f, 1, (const StepState*)st);
+        after("k_wt_bottom_y");
+        launches += 4;
+    }
+
     // Face fluxes and point updates of one stage; the LF speeds come from ax[stage] / ay[stage],
     // or from (axp, ayp) when given.
     void enq_faces_update(int stage, Field4 in, Field4 out, const double* axp = nullptr, const double* ayp = nullptr)
@@ -2409,12 +2531,12 @@ struct Solver2D {
         const double* sy = ayp ? ayp : ay[stage];
         mark();
         if (g.wz_eps == 1e-40 && g.wz_delta == 0.0) {
-            launch(k_face<0, false>, 2 * face_blocks, 128, g, in, fx, L[2], C + 2, sx, st);
+            launch(k_face<0, false>, 2 * face_blocks, 128, g, xin(in), fx, L[2], C + 2, sx, st);
             after("k_face<0>");
             launch(k_face<1, false>, 2 * face_blocks, 128, g, in, fy, L[3], C + 3, sy, st);
             after("k_face<1>");
         } else {
-            launch(k_face<0, true>, 2 * face_blocks, 128, g, in, fx, L[2], C + 2, sx, st);
+            launch(k_face<0, true>, 2 * face_blocks, 128, g, xin(in), fx, L[2], C + 2, sx, st);
             after("k_face<0>");
             launch(k_face<1, true>, 2 * face_blocks, 128, g, in, fy, L[3], C + 3, sy, st);
             after("k_face<1>");
@@ -2423,13 +2545,13 @@ struct Solver2D {
         mark();
         const int ub = face_blocks / 2;
         if (stage == 0) {
-            launch(k_update<1>, ub, 256, g, in, out, q, fx, fy, lvl[2], L[0], C + 0, L[1], C + 1, st);
+            launch(k_update<1>, ub, 256, g, in, xin(in), out, q, fx, fy, lvl[2], L[0], C + 0, L[1], C + 1, st);
             after("k_update<1>");
         } else if (stage == 1) {
-            launch(k_update<2>, ub, 256, g, in, out, q, fx, fy, lvl[1], L[0], C + 0, L[1], C + 1, st);
+            launch(k_update<2>, ub, 256, g, in, xin(in), out, q, fx, fy, lvl[1], L[0], C + 0, L[1], C + 1, st);
             after("k_update<2>");
         } else {
-            launch(k_update<3>, ub, 256, g, in, out, q, fx, fy, lvl[0], L[0], C + 0, L[1], C + 1, st);
+            launch(k_update<3>, ub, 256, g, in, xin(in), out, q, fx, fy, lvl[0], L[0], C + 0, L[1], C + 1, st);
             after("k_update<3>");
         }
         launches += 1;
@@ -2446,7 +2568,9 @@ struct Solver2D {
         launches += 1;
         enq_prepare(st);
         mark();
+        const bool wt = g.bc_kind == AWCM_BC_WIND_TUNNEL;
         enq_bc(q, st, 0);
+        if (wt) enq_wt_input(q);
         enq_alpha(q, 3, 0, true);
         {
             // the worklists, dt (after stage 1's speeds) and the zeroing of stage 2/3's speeds
@@ -2463,10 +2587,18 @@ struct Solver2D {
             launches += 1;
         }
         enq_faces_update(0, q, q2);
-        enq_bc_alpha(q2, 1);
-        enq_faces_update(1, q2, q1);
-        enq_bc_alpha(q1, 2);
-        enq_faces_update(2, q1, q1);
+        for (int stage = 1; stage <= 2; ++stage) {
+            Field4 in = stage == 1 ? q2 : q1;
+            if (!wt) {
+                enq_bc_alpha(in, stage);
+            } else {
+                // the wind tunnel's bottom fills write interior (solid) cells the speeds read
+                enq_bc(in, st);
+                enq_wt_input(in);
+                enq_alpha_listed(in, stage, nullptr, nullptr, &st->nonfinite);
+            }
+            enq_faces_update(stage, in, q1);
+        }
         launch(k_remove_residue, pb(words()), 256, g, q, m, 0, 1, st);
         after("k_remove_residue");
         launch(k_finish, 1, 1, st);
@@ -2834,6 +2966,27 @@ struct Solver2D {
         return kOk;
     }
 
+    // BOUNDARY_MANAGER_WT::SetBottomBoundaryCondition(x_direction, y_direction) on the conserved field.
+    int wt_bottom(int x_direction, int y_direction)
+    {
+        if (g.bc_kind != AWCM_BC_WIND_TUNNEL || (x_direction != 0) == (y_direction != 0)) {
+            set_last_error("SetBottomBoundaryCondition: a wind-tunnel instance and exactly one direction", __FILE__,
+                           __LINE__);
+            return kErrArg;
+        }
+        if (x_direction) {
+            launch(k_wt_bottom_x, blocks_for(3L * (g.wt_j + kGhost + 1), 256), 256, g, q, Field4{},
+                   (const StepState*)nullptr);
+        } else {
+            launch(k_wt_bottom_y, blocks_for(3L * (g.nx + 2 * kGhost - 1), 256), 256, g, q, 0, (const StepState*)nullptr);
+            launch(k_wt_bottom_y, blocks_for(3L * (g.nx - 1 + kGhost - g.wt_i + 1), 256), 256, g, q, 1,
+                   (const StepState*)nullptr);
+        }
+        AWCM_CUDA_TRY(cudaGetLastError());
+        AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+
     // Attaches the enum-driven manager: bc holds (Ny+6) x (Nx+6) BOUNDARY_CONDITION values in the
     // FIELD_UNIFORM_2D layout; every later ghost fill of this instance applies it.
     int set_bc_field(const int* bc)
@@ -3184,6 +3337,10 @@ struct Solver2D {
                     rhov *= rho;
                     p = std::pow(rho, gam);
                     Q[0] = rho, Q[1] = rhou, Q[2] = rhov, Q[3] = E(rho, rhou / rho, rhov / rho, p);
+                } else if (kind == AWCM_PROBLEM_WIND_TUNNEL) {
+                    // WINDTUNNEL::Initialize (Problems/2D/PROBLEM_WINDTUNNEL.h:14-47): Mach 3 uniform flow
+                    rho = 1.4, u = 3, v = 0, p = 1;
+                    Q[0] = rho, Q[1] = rho * u, Q[2] = rho * v, Q[3] = E(rho, u, v, p);
                 } else if (kind == AWCM_PROBLEM_SHOCK_VORTEX) {
                     // SHOCK_VORTEX::Initialize (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:32-66):
                     // post-shock state for x <= 0, vortex of Mach 0.5 centred at (a, b) ahead of it.
@@ -3351,6 +3508,12 @@ int awcm2d_manager(awcm2d_t h, int op, int mask_id, int level_id)
     AWCM_H(h);
     return h->s.manager(op, mask_id, level_id);
 }
+int awcm2d_wt_set_bottom(awcm2d_t h, int x_direction, int y_direction)
+{
+    AWCM_H(h);
+    AWCM_EULER_ONLY(h);
+    return h->s.wt_bottom(x_direction, y_direction);
+}
 int awcm2d_set_bc_field(awcm2d_t h, const int* bc)
 {
     AWCM_H(h);
@@ -3451,6 +3614,10 @@ int awcm2d_frozen_run(awcm2d_t h, double t0, double dt, int n_steps, int mode, d
 {
     AWCM_H(h);
     AWCM_EULER_ONLY(h);
+    if (h->s.g.bc_kind == AWCM_BC_WIND_TUNNEL) {
+        awcm::set_last_error("the frozen-mask run has no per-direction wind-tunnel fills", __FILE__, __LINE__);
+        return awcm::kErrArg;
+    }
     return h->s.frozen_run(t0, dt, n_steps, mode, out);
 }
 int awcm2d_adjoint(awcm2d_t h, double t0, double dt, int n_steps, int checkpoint_every, int mode,
@@ -3458,8 +3625,9 @@ int awcm2d_adjoint(awcm2d_t h, double t0, double dt, int n_steps, int checkpoint
 {
     AWCM_H(h);
     AWCM_EULER_ONLY(h);
-    if (h->s.g.bc_kind == AWCM_BC_GENERIC) {
-        awcm::set_last_error("the adjoint's boundary transposes cover the fixed managers only, not the generic one",
+    if (h->s.g.bc_kind == AWCM_BC_GENERIC || h->s.g.bc_kind == AWCM_BC_WIND_TUNNEL) {
+        awcm::set_last_error("the adjoint's boundary transposes cover the fixed edge managers only, not the generic "
+                             "or the wind-tunnel one",
                              __FILE__, __LINE__);
         return awcm::kErrArg;
     }

@@ -15,6 +15,7 @@ struct Grid2 {
     double wz_eps;    // WENO-Z epsilon of the face reconstructions (1e-40 as in the reference)
     double wz_delta;  // > 0: tau = sqrt((b0-b2)^2 + wz_delta^2) instead of |b0 - b2| (0 as in the reference)
     const int8_t* bcf;  // kind AWCM_BC_GENERIC: BOUNDARY_CONDITION of every ghosted point (plane layout)
+    int wt_i, wt_j;     // kind AWCM_BC_WIND_TUNNEL: the step corner int(0.6/dx), int(0.2/dy)
     Weights W;
     __host__ __device__ __forceinline__ size_t at(int i, int j) const
     {

@@ -57,6 +57,10 @@ extern "C" {
 #define AWCM_BC_GENERIC 4      /* the enum-driven BOUNDARY_MANAGER_1D<T> / BOUNDARY_MANAGER_2D<TT>
                                   (BOUNDARY_MANAGER_1D.h:17-76, BOUNDARY_MANAGER_2D.h:23-159), attached
                                   with awcm1d_batch_set_bc_field / awcm2d_set_bc_field */
+#define AWCM_BC_WIND_TUNNEL 5  /* BOUNDARY_MANAGER_WT (Problems/2D/PROBLEM_WINDTUNNEL.h:52-222): Mach 3
+                                  inflow left, extrapolation right, reflecting top, and the
+                                  forward-facing step at (int(0.6/dx), int(0.2/dy)) filled per sweep
+                                  direction; its BandingMask replaces the edge banding */
 
 /* BOUNDARY_CONDITION values of the generic managers (BOUNDARY_MANAGER_2D.h:7-13). */
 #define AWCM_SOLID_WALL (-4)
@@ -70,6 +74,7 @@ extern "C" {
 #define AWCM_PROBLEM_DOUBLE_MACH 1 /* a = pre-shock density                   */
 #define AWCM_PROBLEM_VORTEX 2      /* a, b = vortex centre                    */
 #define AWCM_PROBLEM_SHOCK_VORTEX 3 /* SHOCK_VORTEX: Mach 1.2 shock at x = 0, vortex at (a, b) */
+#define AWCM_PROBLEM_WIND_TUNNEL 4  /* WINDTUNNEL: uniform Mach 3 flow (rho 1.4, u 3, v 0, p 1) */
 
 /* Last error message of the calling thread ("" if none). */
 const char* awcm_last_error(void);
@@ -131,6 +136,18 @@ int awcm2d_apply_bc(awcm2d_t h, double t);
  * as in the reference, which marks the class "not used now" (:20).  The adjoint refuses such an
  * instance; state files do not carry the condition field. */
 int awcm2d_set_bc_field(awcm2d_t h, const int* bc);
+/* BOUNDARY_MANAGER_WT::SetBottomBoundaryCondition(x_direction, y_direction)
+ * (Problems/2D/PROBLEM_WINDTUNNEL.h:124-168) on the conserved field of a wind-tunnel instance
+ * (exactly one direction).  x: the columns i_bdry .. i_bdry+2 of rows -3 .. j_bdry mirror column
+ * i_bdry-1 with rho u reflected (the step's front face); y: the bottom ghost rows mirror row 0 and
+ * the rows j_bdry-2 .. j_bdry right of i_bdry mirror row j_bdry+1, rho v reflected (the floor and
+ * the step's top).  The reference has no AWCM driver for the wind tunnel (its AWCM_2D::PrepareEuler
+ * leaves the manager commented out, Wavelet/AWCM_2D.h:121); the step of a wind-tunnel instance
+ * applies, per stage, SetBoundaryCondition, then the x-direction fill to a copy that the x fluxes
+ * read, then the x- and y-direction fills to the stage input that the y fluxes, the LF speeds and
+ * the updates read; PrepareEuler bands with the manager's BandingMask.  The frozen-mask run and
+ * the adjoint refuse a wind-tunnel instance. */
+int awcm2d_wt_set_bottom(awcm2d_t h, int x_direction, int y_direction);
 
 /* One pass of the reference driver loop (Wavelet/main_2d_euler(quad).cpp:58-334): PrepareEuler,
  * CFL dt (clipped to t_next), three SSP-RK3 stages with WENO-Z/Roe fluxes on the finest level and

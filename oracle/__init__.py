@@ -226,6 +226,7 @@ class Oracle2D:
         self._manager = b("manager", None, [_vp, _c_int, _c_int, _c_int])
         self._apply_bc = b("apply_bc", None, [_vp, _c_double])
         self._set_bc_field = b("set_bc_field", None, [_vp, ctypes.POINTER(_c_int)])
+        self._wt_call = b("wt_call", None, [_vp, _c_int, _c_int])
         self._step = b("step", None, [_vp] + [_c_double] * 5 + [_dp, _dp])
         self._set_freeze = b("set_freeze", None, [_vp, _c_int])
         if kind == "port":
@@ -318,6 +319,11 @@ class Oracle2D:
 
     def apply_bc(self, t=0.0):
         self._apply_bc(self.h, t)
+
+    def wt_call(self, which: int, mask_id: int = 0):
+        """BOUNDARY_MANAGER_WT on the conserved field: 0 SetBottomBoundaryCondition(true, false),
+        1 SetBottomBoundaryCondition(false, true), 2 BandingMask(mask mask_id)."""
+        self._wt_call(self.h, which, mask_id)
 
     def set_bc_field(self, bc):
         """Attaches BOUNDARY_MANAGER_2D<TT> with the BOUNDARY_CONDITION field bc ((Ny+6, Nx+6) ints)."""

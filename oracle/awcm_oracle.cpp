@@ -720,7 +720,7 @@ V4 face_flux_2d(const double* const* s, double alpha, double g, int dir, double 
 
 // =============================================================================================
 // 2D AWCM state.
-enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2, BC_SHOCK_VORTEX = 3 };
+enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2, BC_SHOCK_VORTEX = 3, BC_WIND_TUNNEL = 5 };
 
 struct O2D {
     int L = 0, maxl = 0, nx = 0, ny = 0, w = 0;
@@ -737,6 +737,10 @@ struct O2D {
     // the enum-driven BOUNDARY_MANAGER_2D<TT> (BOUNDARY_MANAGER_2D.h:23-159) when set: the condition
     // of every ghosted point (FIELD_UNIFORM_2D<BOUNDARY_CONDITION> layout)
     std::vector<int> bcf;
+    // wind tunnel (BOUNDARY_MANAGER_WT, Problems/2D/PROBLEM_WINDTUNNEL.h:52-222): the step's corner
+    // i_bdry = int(0.6/dx), j_bdry = int(0.2/dy) (:75-76) and the x-sweep copy of a stage input
+    int wt_i = 0, wt_j = 0;
+    std::vector<double> qx[4];
     int D(int lev) const { return 1 << (maxl - lev); }
     size_t at(int i, int j) const { return (size_t)(j + G) * w + (i + G); }
     bool get(int i, int j, int b) const { return (m[at(i, j)] >> b) & 1; }
@@ -1024,6 +1028,14 @@ void band2d(O2D& s, int b)
     for (int j = 0; j < s.ny; ++j)
         for (int i = 0; i < s.nx; ++i)
             if (!(2 <= i && i <= s.nx - 3 && j >= 2 && j <= s.ny - 3)) s.set(i, j, b);
+    if (s.bc_kind != BC_WIND_TUNNEL) return;
+    // BOUNDARY_MANAGER_WT::BandingMask (PROBLEM_WINDTUNNEL.h:202-220): also the band around the
+    // step's top (|j - j_bdry| <= 2, i >= i_bdry - 2) and front (|i - i_bdry| <= 2, j <= j_bdry + 2).
+    for (int j = 0; j < s.ny; ++j)
+        for (int i = 0; i < s.nx; ++i) {
+            if (std::abs(j - s.wt_j) <= 2 && i >= s.wt_i - 2) s.set(i, j, b);
+            if (std::abs(i - s.wt_i) <= 2 && j <= s.wt_j + 2) s.set(i, j, b);
+        }
 }
 
 // WAVELET_2D::InterpolateEuler (Wavelet/WAVELET_2D.h:784-907): components 1..3 at new points.
@@ -1168,6 +1180,22 @@ void bc2d(O2D& s, std::vector<double>* f, double t)
         bc2d_generic(s, f);
         return;
     }
+    if (s.bc_kind == BC_WIND_TUNNEL) {
+        // BOUNDARY_MANAGER_WT::SetBoundaryCondition (PROBLEM_WINDTUNNEL.h:94-199): Mach 3 inflow on the
+        // left, zero-order extrapolation on the right (interior rows), reflected v on the top
+        // (interior columns); the bottom is filled per sweep direction (wt_fill_x / wt_fill_y).
+        const double in[4] = {1.4, 1.4 * 3, 1.4 * 0, euler_E(1.4, 1.4, 3, 0, 1)};
+        for (int j = 0; j <= NY; ++j)
+            for (int c = 0; c < G; ++c)
+                for (int p = 0; p < 4; ++p) F(p, -1 - c, j) = in[p];
+        for (int j = 0; j <= NY; ++j)
+            for (int c = 0; c < G; ++c)
+                for (int p = 0; p < 4; ++p) F(p, NX + 1 + c, j) = F(p, NX, j);
+        for (int i = 0; i <= NX; ++i)
+            for (int c = 0; c < G; ++c)
+                for (int p = 0; p < 4; ++p) F(p, i, NY + 1 + c) = p == 2 ? -F(p, i, NY) : F(p, i, NY);
+        return;
+    }
     if (s.bc_kind == BC_PERIODIC) {
         for (int j = 0; j <= NY; ++j)
             for (int c = 0; c < G; ++c)
@@ -1238,6 +1266,38 @@ void bc2d(O2D& s, std::vector<double>* f, double t)
     }
 }
 
+// BOUNDARY_MANAGER_WT::SetBottomBoundaryCondition (PROBLEM_WINDTUNNEL.h:124-168).  x direction: the
+// three columns i_bdry.. i_bdry+2 up to row j_bdry (ghost rows included) mirror column i_bdry-1 with
+// rho u reflected; y direction: the bottom ghost rows mirror row 0 (columns -3 .. Nx+1) and the rows
+// j_bdry-2 .. j_bdry right of i_bdry mirror row j_bdry+1, rho v reflected.
+void wt_fill_x(O2D& s, std::vector<double>* f)
+{
+    auto F = [&](int p, int i, int j) -> double& { return f[p][s.at(i, j)]; };
+    for (int j = -G; j <= s.wt_j; ++j)
+        for (int c = 0; c < 3; ++c)
+            for (int p = 0; p < 4; ++p) F(p, s.wt_i + c, j) = p == 1 ? -F(p, s.wt_i - 1, j) : F(p, s.wt_i - 1, j);
+}
+void wt_fill_y(O2D& s, std::vector<double>* f)
+{
+    auto F = [&](int p, int i, int j) -> double& { return f[p][s.at(i, j)]; };
+    const int NX = s.nx - 1;
+    for (int i = -G; i < NX + G; ++i)
+        for (int c = 0; c < 3; ++c)
+            for (int p = 0; p < 4; ++p) F(p, i, -1 - c) = p == 2 ? -F(p, i, 0) : F(p, i, 0);
+    for (int i = s.wt_i; i <= NX + G; ++i)
+        for (int c = 0; c < 3; ++c)
+            for (int p = 0; p < 4; ++p) F(p, i, s.wt_j - c) = p == 2 ? -F(p, i, s.wt_j + 1) : F(p, i, s.wt_j + 1);
+}
+// The wind tunnel's stage input: the x-sweep copy gets the x-direction bottom fill; the field
+// itself the x- and then the y-direction fill.
+void wt_stage_input(O2D& s, std::vector<double>* f)
+{
+    for (int p = 0; p < 4; ++p) s.qx[p] = f[p];
+    wt_fill_x(s, s.qx);
+    wt_fill_x(s, f);
+    wt_fill_y(s, f);
+}
+
 void alpha2d(O2D& s, std::vector<double>* f, int b, std::vector<double>& ax, std::vector<double>& ay)
 {
     ax.assign(s.ny, 0.0);
@@ -1261,9 +1321,11 @@ void alpha2d(O2D& s, std::vector<double>* f, int b, std::vector<double>& ax, std
 }
 
 // One RK3 stage (main_2d_euler(quad).cpp:108-163, 188-243, 267-322) over mask bit b, level set l.
+// inx: the field the x-direction fluxes read (the wind tunnel's x-sweep copy), else in.
 void stage2d(O2D& s, std::vector<double>* in, std::vector<double>* out, int b, int l, const std::vector<double>& ax,
-             const std::vector<double>& ay, double dt, int kind)
+             const std::vector<double>& ay, double dt, int kind, std::vector<double>* inx = nullptr)
 {
+    if (!inx) inx = in;
     const int NX = s.nx - 1, NY = s.ny - 1;
     const double g = s.gamma;
     const double d1 = 2.0 / 3.0, d2 = -1.0 / 12.0;
@@ -1278,11 +1340,15 @@ void stage2d(O2D& s, std::vector<double>* in, std::vector<double>* out, int b, i
                 const size_t a = s.at(ii, jj);
                 for (int p = 0; p < 4; ++p) o[p] = in[p][a];
             };
+            auto stx = [&](int ii, int jj, double* o) {
+                const size_t a = s.at(ii, jj);
+                for (int p = 0; p < 4; ++p) o[p] = inx[p][a];
+            };
             if (lev == s.maxl) {
                 double bx[7][4], by[7][4];
                 const double *px[7], *py[7];
                 for (int o = 0; o < 7; ++o) {
-                    st(i - 3 + o, j, bx[o]);
+                    stx(i - 3 + o, j, bx[o]);
                     st(i, j - 3 + o, by[o]);
                     px[o] = bx[o];
                     py[o] = by[o];
@@ -1299,7 +1365,7 @@ void stage2d(O2D& s, std::vector<double>* in, std::vector<double>* out, int b, i
                 for (int o = 0; o < 5; ++o) {
                     const int ii = i + (o - 2) * d;
                     if ((o == 0 && i <= d) || (o == 4 && i >= NX - d && !(i <= d))) continue;
-                    st(ii, j, b5[o]);
+                    stx(ii, j, b5[o]);
                     f[o] = fu2(b5[o], g);
                 }
                 for (int p = 0; p < 4; ++p) {
@@ -1371,15 +1437,20 @@ void step2d(O2D& s, double tol, double cfl, double t, double t_next, double dt_f
             }
         }
     };
+    const bool wt = s.bc_kind == BC_WIND_TUNNEL && s.bcf.empty();
+    std::vector<double>* qx = wt ? s.qx : nullptr;
     bc2d(s, s.q, t);
+    if (wt) wt_stage_input(s, s.q);
     load_alpha(0, s.q, 3);
-    stage2d(s, s.q, s.q2, 2, 2, ax, ay, dt, 1);
+    stage2d(s, s.q, s.q2, 2, 2, ax, ay, dt, 1, qx);
     bc2d(s, s.q2, t);
+    if (wt) wt_stage_input(s, s.q2);
     load_alpha(1, s.q2, 2);
-    stage2d(s, s.q2, s.q1, 1, 1, ax, ay, dt, 2);
+    stage2d(s, s.q2, s.q1, 1, 1, ax, ay, dt, 2, qx);
     bc2d(s, s.q1, t);
+    if (wt) wt_stage_input(s, s.q1);
     load_alpha(2, s.q1, 1);
-    stage2d(s, s.q1, s.q0, 0, 0, ax, ay, dt, 3);
+    stage2d(s, s.q1, s.q0, 0, 0, ax, ay, dt, 3, qx);
 #pragma omp parallel for schedule(static)
     for (int j = 0; j < s.ny; ++j)
         for (int i = 0; i < s.nx; ++i) {
@@ -1604,6 +1675,8 @@ void* or2d_create(int num_levels, int nx_coarse, int ny_coarse, double x_min, do
     s->dx = (x_max - x_min) / (s->nx - 1);
     s->dy = (y_max - y_min) / (s->ny - 1);
     s->bc_kind = bc_kind;
+    s->wt_i = int(0.6 / s->dx);
+    s->wt_j = int(0.2 / s->dy);
     for (int p = 0; p < 4; ++p) {
         s->q[p].assign(s->plane, 0.0);
         s->q2[p].assign(s->plane, 0.0);
@@ -1673,6 +1746,11 @@ void or2d_init_problem(void* h, int kind, double a, double b)
                 rhov *= rho;
                 p = std::pow(rho, g);
                 Q[0] = rho, Q[1] = rhou, Q[2] = rhov, Q[3] = euler_E(g, rho, rhou / rho, rhov / rho, p);
+            }
+            if (kind == 4) {
+                // WINDTUNNEL::Initialize (Problems/2D/PROBLEM_WINDTUNNEL.h:14-47): Mach 3 uniform flow
+                rho = 1.4, u = 3, v = 0, p = 1;
+                Q[0] = rho, Q[1] = rho * u, Q[2] = rho * v, Q[3] = euler_E(g, rho, u, v, p);
             }
             if (kind == 3) {
                 // SHOCK_VORTEX::Initialize (Problems/2D/PROBLEM_SHOCK_VORTEX_INTERACTION.h:32-66)
@@ -1850,6 +1928,16 @@ void or2d_manager(void* h, int op, int mask_id, int level_id)
         case 5: band2d(s, b); break;
         default: break;
     }
+}
+
+// The wind tunnel manager's own calls (see ref2d_wt_call): 0 = bottom fill for the x direction,
+// 1 = for the y direction, 2 = BandingMask(mask_id).
+void or2d_wt_call(void* h, int which, int mask_id)
+{
+    O2D& s = *static_cast<O2D*>(h);
+    if (which == 0) wt_fill_x(s, s.q);
+    else if (which == 1) wt_fill_y(s, s.q);
+    else band2d(s, bit_of(mask_id));
 }
 
 void or2d_apply_bc(void* h, double t)

@@ -22,7 +22,7 @@
 
 namespace {
 
-enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2, BC_SHOCK_VORTEX = 3 };
+enum { BC_QUAD = 0, BC_DMACH = 1, BC_PERIODIC = 2, BC_SHOCK_VORTEX = 3, BC_WIND_TUNNEL = 5 };
 
 // One boundary manager per field, of the kind the problem uses, or the enum-driven
 // BOUNDARY_MANAGER_2D<VECTOR_4D<double>> (BOUNDARY_MANAGER_2D.h:23-159) once a condition field is set.
@@ -33,10 +33,12 @@ struct BC2D {
     BOUNDARY_MANAGER_ISENVORTEX* periodic = nullptr;
     BOUNDARY_MANAGER_SHOCK_VORTEX* shock_vortex = nullptr;
     BOUNDARY_MANAGER_2D<VECTOR_4D<double>>* generic = nullptr;
+    BOUNDARY_MANAGER_WT* wt = nullptr;
     FIELD_UNIFORM_2D<VECTOR_4D<double>>* field;
     BC2D(int k, FIELD_UNIFORM_2D<VECTOR_4D<double>>& Q) : kind(k), field(&Q)
     {
-        if (k == BC_DMACH) dmach = new BOUNDARY_MANAGER_DMACH(Q);
+        if (k == BC_WIND_TUNNEL) wt = new BOUNDARY_MANAGER_WT(Q);
+        else if (k == BC_DMACH) dmach = new BOUNDARY_MANAGER_DMACH(Q);
         else if (k == BC_PERIODIC) periodic = new BOUNDARY_MANAGER_ISENVORTEX(Q);
         else if (k == BC_SHOCK_VORTEX) shock_vortex = new BOUNDARY_MANAGER_SHOCK_VORTEX(Q);
         else quad = new BOUNDARY_MANAGER_QUAD(Q);
@@ -48,10 +50,14 @@ struct BC2D {
         delete periodic;
         delete shock_vortex;
         delete generic;
+        delete wt;
     }
+    // The wind tunnel's SetBoundaryCondition fills left, right and top ("Except bottom boundary!!",
+    // PROBLEM_WINDTUNNEL.h:193-199); its bottom fills are per sweep direction (stage_input_wt).
     void apply(double t)
     {
         if (generic) generic->SetBoundaryCondition(*field);
+        else if (wt) wt->SetBoundaryCondition();
         else if (dmach) dmach->SetBoundaryCondition(t);
         else if (periodic) periodic->SetBoundaryCondition();
         else if (shock_vortex) shock_vortex->SetBoundaryCondition();
@@ -80,7 +86,52 @@ struct Ref2D {
     BOUNDARY_MANAGER *bs = nullptr, *bs1 = nullptr, *bs2 = nullptr;
     // The condition field of the enum-driven manager (ref2d_set_bc_field).
     FIELD_UNIFORM_2D<BOUNDARY_CONDITION> bcf;
+    // Wind tunnel: the x-sweep copy of a stage input (its bottom filled for the x direction).
+    FIELD_UNIFORM_2D<VECTOR_4D<double>> Qx;
 };
+
+// The stage input of the wind tunnel (BOUNDARY_MANAGER_WT, Problems/2D/PROBLEM_WINDTUNNEL.h:52-222):
+// after SetBoundaryCondition (left, right, top), the x-direction fluxes read a copy with
+// SetBottomBoundaryCondition(true, false) applied (the step's front face), while the field itself
+// takes the x- and then the y-direction bottom fill (bottom wall, step top) and feeds the
+// y-direction fluxes, the LF speeds and the point updates.
+void stage_input_wt(Ref2D* s, FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qs)
+{
+    for (int j = Qs.j_start_g; j <= Qs.j_end_g; ++j)
+        for (int i = Qs.i_start_g; i <= Qs.i_end_g; ++i) s->Qx(i, j) = Qs(i, j);
+    BOUNDARY_MANAGER_WT(s->Qx).SetBottomBoundaryCondition(true, false);
+    BOUNDARY_MANAGER_WT bm(Qs);
+    bm.SetBottomBoundaryCondition(true, false);
+    bm.SetBottomBoundaryCondition(false, true);
+}
+
+// AWCM_2D::PrepareEuler (Wavelet/AWCM_2D.h:114-147) with the wind tunnel's BandingMask in place
+// of the shock-vortex one: the alternative the reference leaves commented out at AWCM_2D.h:121.
+void prepare_euler_wt(Ref2D* s, double tol)
+{
+    AWCM_2D& a = *s->awcm;
+    FIELD_UNIFORM_2D<VECTOR_4D<double>>& q = s->Q;
+    a.mask_temp = a.mask0;
+    a.wavelet.ForwardWaveletTransformationEuler(q, a.mra_grid, a.mask0, tol);
+    BOUNDARY_MANAGER_WT boundary_manager(q);
+    boundary_manager.BandingMask(a.mask0);
+    AWCM_MANAGER_2D::AddAdjacentZone(a.mask0, a.mra_grid);
+    AWCM_MANAGER_2D::CheckReconstruction(a.mask0, a.mra_grid);
+    a.mask1 = a.mask0;
+    AWCM_MANAGER_2D::ComputeLevel(a.level0, a.mask0, a.mra_grid);
+    AWCM_MANAGER_2D::AddPointForDifferentiation(a.mask1, a.mra_grid, a.level0);
+    AWCM_MANAGER_2D::CheckReconstruction(a.mask1, a.mra_grid);
+    a.mask2 = a.mask1;
+    AWCM_MANAGER_2D::ComputeLevel(a.level1, a.mask1, a.mra_grid);
+    AWCM_MANAGER_2D::AddPointForDifferentiation(a.mask2, a.mra_grid, a.level1);
+    AWCM_MANAGER_2D::CheckReconstruction(a.mask2, a.mra_grid);
+    a.mask3 = a.mask2;
+    AWCM_MANAGER_2D::ComputeLevel(a.level2, a.mask2, a.mra_grid);
+    AWCM_MANAGER_2D::AddPointForDifferentiation(a.mask3, a.mra_grid, a.level2);
+    AWCM_MANAGER_2D::CheckReconstruction(a.mask3, a.mra_grid);
+    a.wavelet.InverseWaveletTransformationEuler(q, a.mra_grid, a.mask3);
+    a.wavelet.InterpolateEuler(q, a.mra_grid, a.mask_temp, a.mask3);
+}
 
 FIELD_UNIFORM_2D<bool>& mask_ref(Ref2D* s, int id)
 {
@@ -131,10 +182,13 @@ void alpha2d(Ref2D* s, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qs, const FIEL
 // One RK3 stage body (main_2d_euler(quad).cpp:108-163, :188-243, :267-322).
 // out = Qin - dt/dx (dF + dG)                      (kind 1, 3)
 // out = 0.75 Qn + 0.25 (Qin - dt/dx (dF + dG))     (kind 2)
+// Qx: the field the x-direction fluxes read (the wind tunnel's x-sweep copy), else Qin.
 void stage2d(Ref2D* s, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qin, FIELD_UNIFORM_2D<VECTOR_4D<double>>& out,
              const FIELD_UNIFORM_2D<bool>& mask, const FIELD_UNIFORM_2D<int>& level,
-             const std::vector<double>& alpha_x, const std::vector<double>& alpha_y, double dt, int kind)
+             const std::vector<double>& alpha_x, const std::vector<double>& alpha_y, double dt, int kind,
+             const FIELD_UNIFORM_2D<VECTOR_4D<double>>* Qx_ = nullptr)
 {
+    const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qx = Qx_ ? *Qx_ : Qin;
     const int max_lev = s->mra.num_levels - 1;
     const GRID_UNIFORM_2D& grid = s->grid;
     const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qn = s->Q;
@@ -156,10 +210,10 @@ void stage2d(Ref2D* s, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qin, FIELD_UNI
             const double dx = grid.dx * d;
             if (lev == max_lev) {
                 VECTOR_4D<double> a, b;
-                wenoz_solver.ComputeFluxX(Qin(i - 3, j), Qin(i - 2, j), Qin(i - 1, j), Qin(i, j), Qin(i + 1, j),
-                                          Qin(i + 2, j), alpha_x[j], a);
-                wenoz_solver.ComputeFluxX(Qin(i - 2, j), Qin(i - 1, j), Qin(i, j), Qin(i + 1, j), Qin(i + 2, j),
-                                          Qin(i + 3, j), alpha_x[j], b);
+                wenoz_solver.ComputeFluxX(Qx(i - 3, j), Qx(i - 2, j), Qx(i - 1, j), Qx(i, j), Qx(i + 1, j),
+                                          Qx(i + 2, j), alpha_x[j], a);
+                wenoz_solver.ComputeFluxX(Qx(i - 2, j), Qx(i - 1, j), Qx(i, j), Qx(i + 1, j), Qx(i + 2, j),
+                                          Qx(i + 3, j), alpha_x[j], b);
                 dF = b - a;
                 wenoz_solver.ComputeFluxY(Qin(i, j - 3), Qin(i, j - 2), Qin(i, j - 1), Qin(i, j), Qin(i, j + 1),
                                           Qin(i, j + 2), alpha_y[i], a);
@@ -169,10 +223,10 @@ void stage2d(Ref2D* s, const FIELD_UNIFORM_2D<VECTOR_4D<double>>& Qin, FIELD_UNI
             } else {
                 // The reference evaluates F (G) at all five points; the ones its branch does not use
                 // (i-2d when i <= d, i+2d when i >= i_end-d) can lie outside the field, so they are skipped.
-                if (i > d) euler_eqn.ComputeFu(Qin(i - 2 * d, j), F_ll);
-                euler_eqn.ComputeFu(Qin(i - d, j), F_l), euler_eqn.ComputeFu(Qin(i, j), F_c);
-                euler_eqn.ComputeFu(Qin(i + d, j), F_r);
-                if (i <= d || i < grid.i_end - d) euler_eqn.ComputeFu(Qin(i + 2 * d, j), F_rr);
+                if (i > d) euler_eqn.ComputeFu(Qx(i - 2 * d, j), F_ll);
+                euler_eqn.ComputeFu(Qx(i - d, j), F_l), euler_eqn.ComputeFu(Qx(i, j), F_c);
+                euler_eqn.ComputeFu(Qx(i + d, j), F_r);
+                if (i <= d || i < grid.i_end - d) euler_eqn.ComputeFu(Qx(i + 2 * d, j), F_rr);
                 if (i <= d)
                     awcm.DifferentiateAtLeftBoundary(F_l, F_c, F_r, F_rr, dF);
                 else if (i >= grid.i_end - d)
@@ -219,6 +273,7 @@ void* ref2d_create(int num_levels, int nx_coarse, int ny_coarse, double x_min, d
     s->Q_0.Initialize(s->grid, 3);
     s->Q_1.Initialize(s->grid, 3);
     s->Q_2.Initialize(s->grid, 3);
+    s->Qx.Initialize(s->grid, 3);
     s->bc = new BC2D(bc_kind, s->Q);
     s->bc0 = new BC2D(bc_kind, s->Q_0);
     s->bc1 = new BC2D(bc_kind, s->Q_1);
@@ -297,6 +352,13 @@ void ref2d_init_problem(void* h, int kind, double a, double b)
         } else if (kind == 1) {
             if (y > sqrt(3.0) * (x - 1.0 / 6.0)) { rho = 8; u = 8.25 * sqrt(3.0) * 0.5; v = -8.25 * 0.5; p = 116.5; }
             else { rho = a; u = 0; v = 0; p = 1; }
+            Q(i, j)[0] = rho;
+            Q(i, j)[1] = rho * u;
+            Q(i, j)[2] = rho * v;
+            Q(i, j)[3] = EOS.E(rho, u, v, p);
+        } else if (kind == 4) {
+            // WINDTUNNEL::Initialize (Problems/2D/PROBLEM_WINDTUNNEL.h:14-47): Mach 3 uniform flow
+            rho = 1.4; u = 3; v = 0; p = 1;
             Q(i, j)[0] = rho;
             Q(i, j)[1] = rho * u;
             Q(i, j)[2] = rho * v;
@@ -554,6 +616,17 @@ void ref2d_set_bc_field(void* h, const int* bc)
     }
 }
 
+// The wind tunnel manager's own calls on the conserved field (PROBLEM_WINDTUNNEL.h:124-216):
+// which 0 = SetBottomBoundaryCondition(true, false), 1 = (false, true), 2 = BandingMask(mask_id).
+void ref2d_wt_call(void* h, int which, int mask_id)
+{
+    Ref2D* s = static_cast<Ref2D*>(h);
+    BOUNDARY_MANAGER_WT bm(s->Q);
+    if (which == 0) bm.SetBottomBoundaryCondition(true, false);
+    else if (which == 1) bm.SetBottomBoundaryCondition(false, true);
+    else bm.BandingMask(mask_ref(s, mask_id));
+}
+
 void ref2d_apply_bc(void* h, double t)
 {
     Ref2D* s = static_cast<Ref2D*>(h);
@@ -577,7 +650,11 @@ void ref2d_step(void* h, double tol, double cfl, double t, double t_next, double
     const int nth = omp_get_max_threads();
     OMP_MANAGER omp_manager(nth);
 
-    if (!s->freeze_mask) awcm.PrepareEuler(Q, tol);
+    const bool wt = s->bc_kind == BC_WIND_TUNNEL;
+    if (!s->freeze_mask) {
+        if (wt) prepare_euler_wt(s, tol);
+        else awcm.PrepareEuler(Q, tol);
+    }
 
     double max_velocity = 0;
 #pragma omp parallel
@@ -618,17 +695,21 @@ void ref2d_step(void* h, double tol, double cfl, double t, double t_next, double
         }
     };
 
+    const FIELD_UNIFORM_2D<VECTOR_4D<double>>* qx = wt ? &s->Qx : nullptr;
     s->bc->apply(t);
+    if (wt) stage_input_wt(s, Q);
     load_alpha(0, Q, awcm.mask3);
-    stage2d(s, Q, s->Q_2, awcm.mask2, awcm.level2, ax, ay, dt, 1);
+    stage2d(s, Q, s->Q_2, awcm.mask2, awcm.level2, ax, ay, dt, 1, qx);
 
     s->bc2->apply(t);
+    if (wt) stage_input_wt(s, s->Q_2);
     load_alpha(1, s->Q_2, awcm.mask2);
-    stage2d(s, s->Q_2, s->Q_1, awcm.mask1, awcm.level1, ax, ay, dt, 2);
+    stage2d(s, s->Q_2, s->Q_1, awcm.mask1, awcm.level1, ax, ay, dt, 2, qx);
 
     s->bc1->apply(t);
+    if (wt) stage_input_wt(s, s->Q_1);
     load_alpha(2, s->Q_1, awcm.mask1);
-    stage2d(s, s->Q_1, s->Q_0, awcm.mask0, awcm.level0, ax, ay, dt, 3);
+    stage2d(s, s->Q_1, s->Q_0, awcm.mask0, awcm.level0, ax, ay, dt, 3, qx);
 
 #pragma omp parallel for
     ITERATION_GRID_2D(grid, 0)

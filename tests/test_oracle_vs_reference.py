@@ -193,3 +193,44 @@ def test_generic_manager_2d_steps():
         t += oa[0]
     assert np.array_equal(a.get_q(), b.get_q())
     assert np.array_equal(a.get_masks(), b.get_masks())
+
+
+WT = (5, 13, 5, 0.0, 3.0, 0.0, 1.0)  # the wind tunnel's [0,3] x [0,1] on 193 x 65 nodes
+
+
+def test_wind_tunnel_manager_calls():
+    """BOUNDARY_MANAGER_WT: SetBoundaryCondition, the two bottom fills and BandingMask of the
+    restatement equal the reference class's on a random field."""
+    a = Oracle2D(*WT, bc_kind=5, kind="port")
+    b = Oracle2D(*WT, bc_kind=5, kind="reference")
+    q = np.random.default_rng(4).uniform(0.5, 2.0, (a.ny + 6, a.nx + 6, 4))
+    for call in ("bc", 0, 1):
+        for o in (a, b):
+            o.set_q(q)
+            if call == "bc":
+                o.apply_bc()
+            else:
+                o.wt_call(call)
+        assert np.array_equal(a.get_q(), b.get_q()), call
+    m = np.zeros((5, a.ny + 6, a.nx + 6), np.uint8)
+    for o in (a, b):
+        o.set_masks(m)
+        o.wt_call(2, 0)
+    assert np.array_equal(a.get_masks(), b.get_masks())
+    assert a.get_masks()[1].sum() > 0
+
+
+def test_wind_tunnel_steps():
+    """Mach 3 flow over the forward-facing step: 15 steps, restatement equal to the reference."""
+    a = Oracle2D(*WT, bc_kind=5, kind="port")
+    b = Oracle2D(*WT, bc_kind=5, kind="reference")
+    for o in (a, b):
+        o.init_problem(4, 0.0, 0.0)
+    assert np.array_equal(a.get_q(), b.get_q())
+    t = 0.0
+    for k in range(15):
+        oa, ob = a.step(1e-3, 0.4, t, 4.0), b.step(1e-3, 0.4, t, 4.0)
+        assert np.array_equal(oa[:7], ob[:7]), (k, oa, ob)
+        t += oa[0]
+    assert np.array_equal(a.get_masks(), b.get_masks())
+    assert np.array_equal(corner_free(a.get_q()), corner_free(b.get_q()))
