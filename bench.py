@@ -37,6 +37,22 @@ WORKLOAD = {
     "num_levels": 7, "nx_coarse": 33, "ny_coarse": 33, "domain": [0.0, 1.0, 0.0, 1.0],
     "split": [0.5, 0.5], "tol": 1e-3, "cfl": 0.4, "t_end": 0.3,
 }
+# The two other AWCM Euler configurations of the benchmark set, reported beside the headline.
+DOUBLE_MACH = {
+    "workload": "2D Mach-10 double-Mach reflection, 4097x1025 finest (65x17 coarse, 7 levels) on [0,4]x[0,1], "
+                "eps 1e-3, CFL 0.5, WENO-Z+Roe, SSP-RK3, reflecting wall for x > 1/6 and exact moving-shock top, "
+                "t_end 0.2",
+    "num_levels": 7, "nx_coarse": 65, "ny_coarse": 17, "domain": [0.0, 4.0, 0.0, 1.0], "bc": 1, "problem": 1,
+    "a": 1.4, "b": 0.0, "tol": 1e-3, "cfl": 0.5, "t_end": 0.2,
+}
+SOD = {
+    "workload": "1D Sod shock tube, 1025 cell-centred nodes on [0,1] (Jmin 4, Jmax 10), interface 0.5, eps 1e-4, "
+                "CFL 0.5, WENO-Z+Roe, SSP-RK3, transmissive, t_end 0.2 (one instance, whole run)",
+    "num_levels": 7, "nx_coarse": 17, "n": 1025, "tol": 1e-4, "cfl": 0.5, "t_end": 0.2,
+}
+# Step of the headline run whose state is the late timing window (developed flow: the four
+# waves interacting, the active set several times its initial size).
+LATE_STEP = 2000
 METRIC = "active-pt RK3 updates/s"
 UNIT = "updates/s"
 # Algorithmic FP64 operations of one 2D WENO-Z/Roe face flux in the reference
@@ -56,6 +72,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched shock-tube comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
+    ap.add_argument("--no-full-run", action="store_true", help="skip the whole-run and late-window figures")
+    ap.add_argument("--no-configs", action="store_true", help="skip the double-Mach and 1D Sod lines")
     ap.add_argument("--capture", type=int, default=-1,
                     help="profiling mode: K graph-replayed steps, then one eagerly launched step; prints its phases")
     return ap.parse_args()
@@ -126,25 +144,34 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------- CPU arms
-def reference_solver():
-    """The reference's own 2D code (oracle/_ref), all host threads, on the benchmark workload."""
+def reference_solver(w=WORKLOAD, state_file=None):
+    """The reference's own 2D code (oracle/_ref), all host threads, on workload `w`: from its
+    initial state, or from a state file written by the GPU run."""
     import oracle
 
-    w = WORKLOAD
     if not oracle.reference_available():
         return None, "reference build (oracle/_ref) not present"
-    s = oracle.Oracle2D(w["num_levels"], w["nx_coarse"], w["ny_coarse"], *w["domain"], bc_kind=0, kind="reference")
-    s.init_problem(0, *w["split"])
+    s = oracle.Oracle2D(w["num_levels"], w["nx_coarse"], w["ny_coarse"], *w["domain"], bc_kind=w.get("bc", 0),
+                        kind="reference")
+    if state_file is None:
+        s.init_problem(w.get("problem", 0), *(w["split"] if "split" in w else (w["a"], w["b"])))
+    else:
+        from oracle.state_format import read_state
+
+        r = read_state(state_file)
+        s.set_q(r["q"])
+        s.set_masks(r["masks"])
+        s.set_levels(r["levels"])
     return s, None
 
 
-def time_reference(steps_max: int, seconds: float, warmup: int = 0):
-    """Steps of the reference solver from the initial state; returns (updates/s, steps, wall, threads)."""
-    s, why = reference_solver()
+def time_reference(steps_max: int, seconds: float, warmup: int = 0, w=WORKLOAD, state_file=None, t0_run=0.0):
+    """Steps warmup+1 .. warmup+steps_max of the reference solver (at most `seconds` of timed
+    work); returns (updates/s, steps, wall, threads)."""
+    s, why = reference_solver(w, state_file)
     if s is None:
         return None, why
-    w = WORKLOAD
-    t = 0.0
+    t = t0_run
     for _ in range(warmup):
         t += s.step(w["tol"], w["cfl"], t, w["t_end"])[0]
     upd, n = 0.0, 0
@@ -165,14 +192,16 @@ def run_reference_arm(args):
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-    k = max(1, min(args.steps, 20))
-    w = max(0, min(args.warmup, 2))
+    # the GPU arm's window: warm-up steps 1..W untimed, steps W+1..W+K timed (W >= 3 there too)
+    k = max(1, min(args.steps, 400))
+    w = max(3, args.warmup)
     r, why = time_reference(k, 1e9, warmup=w)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+        "window": {"first_step": w + 1, "last_step": w + r["steps"]},
         "steps": r["steps"], "warmup": w, "ms_per_step": 1e3 * r["wall_s"] / r["steps"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (deterministic initial state)",
         "config": {k2: v for k2, v in WORKLOAD.items()},
@@ -234,12 +263,48 @@ def run_batched(rank: int, world: int):
     torch.cuda.synchronize()
     ms, upd = reduce_run(e0.elapsed_time(e1), tot[0] - u0, device="cuda")
     value = upd / (ms / 1e3)
-    # plain form: instances one per launch (a sample across the size mix), same kernel and graph
-    sample = [tubes[k] for k in range(0, len(tubes), max(1, len(tubes) // 6))][:6]
-    p_ms, p_upd = 0.0, 0.0
+    # Plain form: one instance per launch.  (a) concurrent: each instance of a sample across the
+    # size mix is its own batch of one (its own stream and graph), and every step launches each
+    # unfinished instance separately, round robin over the streams, so the GPU runs as many
+    # single-instance launches side by side as the host can issue; (b) serial: the same instances
+    # one after the other on one stream.  Wall clock with the device synchronised on both sides.
+    per_class = 8
+    sample = []
+    for J in sorted({t["jmax"] for t in tubes}):
+        sample += [t for t in tubes if t["jmax"] == J][:per_class]
+    plains = []
     for t in sample:
         p = workloads.make_batch(awcm, [t])
-        p.set_launch(256, 0)
+        p.set_launch(best[0], 0)
+        p.set_run(tol, cfl, 0.0, t_end)
+        p.steps(2)
+        plains.append(p)
+    for p in plains:
+        p.sync()
+    u0 = sum(p.totals()[0] for p in plains)
+    live = list(plains)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rounds = 0
+    while live and time.perf_counter() - t0 < 4.0:
+        for p in live:
+            p.steps(1)
+        rounds += 1
+        if rounds % 64 == 0:
+            live = [p for p in live if p.totals()[2] < 1]
+    torch.cuda.synchronize()
+    wall_c = time.perf_counter() - t0
+    upd_c = sum(p.totals()[0] for p in plains) - u0
+    for p in plains:
+        p.close()
+    conc_ms, conc_upd = reduce_run(wall_c * 1e3, upd_c, device="cuda")
+    plain_conc = conc_upd / (conc_ms / 1e3)
+    # (b) serial, one instance at a time on one stream, a sample of six across the mix
+    serial = [sample[k] for k in range(0, len(sample), max(1, len(sample) // 6))][:6]
+    p_ms, p_upd = 0.0, 0.0
+    for t in serial:
+        p = workloads.make_batch(awcm, [t])
+        p.set_launch(best[0], 0)
         p.set_run(tol, cfl, 0.0, t_end)
         p.steps(3)
         p.sync()
@@ -248,7 +313,7 @@ def run_batched(rank: int, world: int):
         torch.cuda.synchronize()
         e0.record(pst)
         t0 = time.perf_counter()
-        while p.totals()[2] < 1 and time.perf_counter() - t0 < 4.0:
+        while p.totals()[2] < 1 and time.perf_counter() - t0 < 2.0:
             p.steps(100)
         e1.record(pst)
         torch.cuda.synchronize()
@@ -256,15 +321,20 @@ def run_batched(rank: int, world: int):
         p_upd += p.totals()[0] - pu0
         p.close()
     p_ms, p_upd = reduce_run(p_ms, p_upd, device="cuda")
-    plain = p_upd / (p_ms / 1e3)
+    plain_serial = p_upd / (p_ms / 1e3)
     return {
         "workload": b_cfg["workload"], "metric": METRIC, "value": value, "unit": UNIT,
         "steady_value": steady, "launches": launches, "instances": len(tubes_all), "ms": ms,
         "launch_shape": {"threads": best[0], "ctas_per_sm": best[1]},
         "autotune": {f"{k[0]}x{k[1]}": v for k, v in rates.items()},
-        "plain": {"value": plain, "unit": UNIT, "sample": f"{len(sample)} instances across the size mix, "
-                  "each alone in its own launch per step, up to 4 s each"},
-        "batched_over_plain": value / plain,
+        "plain": {"value": plain_conc, "unit": UNIT,
+                  "sample": f"{len(sample)} instances ({per_class} per Jmax), each its own batch of one with its own "
+                            "stream and graph; each step launches every unfinished instance separately, round robin "
+                            "over the streams (one instance per launch, launches side by side); 4 s of wall clock"},
+        "plain_serial": {"value": plain_serial, "unit": UNIT,
+                         "sample": f"{len(serial)} of those instances one after another on one stream, up to 2 s each"},
+        "batched_over_plain": value / plain_conc,
+        "steady_over_plain": steady / plain_conc,
     }
 
 
@@ -338,6 +408,148 @@ def run_adjoint(rank: int, world: int):
                 "including the recomputation of each checkpoint segment's stage inputs (device time, "
                 "median of 3)",
     }
+
+
+# --------------------------------------------------------------------- whole runs and late window
+def make_2d(awcm, w):
+    s = awcm.AWCM2D(w["num_levels"], w["nx_coarse"], w["ny_coarse"], *w["domain"], bc_kind=w.get("bc", 0))
+    s.init_problem(w.get("problem", 0), *(w["split"] if "split" in w else (w["a"], w["b"])))
+    return s
+
+
+def timed_advance(torch, s, w, t, n):
+    """n graph-replayed steps from t; device ms from CUDA events on the solver's stream."""
+    st = torch.cuda.ExternalStream(s.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    t, k, upd, _ = s.advance(w["tol"], w["cfl"], t, w["t_end"], n)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return t, k, upd, e0.elapsed_time(e1)
+
+
+def whole_run(awcm, torch, w, save_at=None, path=None):
+    """Workload w from its initial state to t_end in chunks of graph-replayed steps; device time
+    summed over the chunks.  With save_at the state after exactly that many steps is written to
+    `path` between two chunks (outside the timed chunks)."""
+    warm = make_2d(awcm, w)
+    warm.advance(w["tol"], w["cfl"], 0.0, w["t_end"], 2)  # graph and module load outside the timing
+    warm.close()
+    s = make_2d(awcm, w)
+    t, steps, upd, ms, t_saved = 0.0, 0, 0.0, 0.0, None
+    while t < w["t_end"]:
+        n = 256 if not save_at or steps >= save_at else min(256, save_at - steps)
+        t, k, u, dms = timed_advance(torch, s, w, t, n)
+        steps, upd, ms = steps + k, upd + u, ms + dms
+        if save_at and steps == save_at and t_saved is None:
+            s.save_state(path, t, steps)
+            t_saved = t
+        if k < n:
+            break
+    s.close()
+    return {"value": upd / (ms / 1e3), "unit": UNIT, "steps": steps, "t_end": t, "device_ms": ms,
+            "active_points": upd, "ms_per_step": ms / max(1, steps)}, t_saved
+
+
+def run_full_and_late(awcm, torch, args, cpu_ok):
+    """The headline workload's whole run to t_end, and a late window: the GPU and the reference's
+    own code each time the steps after the same mid-run state (written by the whole run)."""
+    w = WORKLOAD
+    fd, path = tempfile.mkstemp(suffix=".awcmstate")
+    os.close(fd)
+    try:
+        full, t_late = whole_run(awcm, torch, w, save_at=LATE_STEP, path=path)
+        full["note"] = ("whole run of the headline workload from its initial state to t_end, graph-replayed "
+                        "steps in chunks of 256, device time (CUDA events) summed over the chunks")
+        late = None
+        if t_late is not None:
+            s = make_2d(awcm, w)
+            s.advance(w["tol"], w["cfl"], 0.0, w["t_end"], 1)  # graph built before the state is loaded
+            s.load_state(path)
+            _, k, upd, ms = timed_advance(torch, s, w, t_late, args.steps)
+            m = s.get_masks()
+            late = {"first_step": LATE_STEP + 1, "last_step": LATE_STEP + k, "t_start": t_late,
+                    "gpu": {"value": upd / (ms / 1e3), "unit": UNIT, "steps": k, "ms_per_step": ms / max(1, k),
+                            "active_points_per_step": upd / max(1, k)},
+                    "mask3_points": int(m[4, 3:-3, 3:-3].sum())}
+            s.close()
+            if cpu_ok:
+                r, why = time_reference(args.steps, args.cpu_seconds, w=w, state_file=path, t0_run=t_late)
+                if r is not None:
+                    late["reference"] = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                                         "steps": r["steps"], "ms_per_step": 1e3 * r["wall_s"] / r["steps"],
+                                         "sample": f"steps {LATE_STEP + 1}..{LATE_STEP + r['steps']} from the GPU "
+                                                   f"run's state file at step {LATE_STEP} (OpenMP)"}
+                    late["gpu_over_reference"] = late["gpu"]["value"] / r["value"]
+                else:
+                    late["reference"] = {"value": None, "sample": why}
+        return {"full_run": full, "late_window": late}
+    finally:
+        try:
+            os.unlink(path)
+        except OSError:
+            pass
+
+
+def run_configs(awcm, torch, args, warmup, cpu_ok):
+    """The double-Mach (4097x1025) and 1D Sod configurations beside the headline: GPU and the
+    reference's own code on the same steps."""
+    out = {}
+    # double Mach: the headline's window (W warm-up steps, K timed) and the whole run to t_end
+    w = DOUBLE_MACH
+    s = make_2d(awcm, w)
+    t, _, _, _ = s.advance(w["tol"], w["cfl"], 0.0, w["t_end"], warmup)
+    _, k, upd, ms = timed_advance(torch, s, w, t, args.steps)
+    s.close()
+    full, _ = whole_run(awcm, torch, w)
+    dm = {"workload": w["workload"], "metric": METRIC,
+          "window": {"first_step": warmup + 1, "last_step": warmup + k},
+          "value": upd / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / max(1, k), "full_run": full}
+    if cpu_ok:
+        r, why = time_reference(args.steps, args.cpu_seconds, warmup=warmup, w=w)
+        if r is not None:
+            dm["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                                  "sample": f"steps {warmup + 1}..{warmup + r['steps']} from the initial state "
+                                            f"(OpenMP), the GPU's window"}
+            dm["gpu_over_reference"] = dm["value"] / r["value"]
+    out["double_mach_4097x1025"] = dm
+    # 1D Sod: one instance, whole run to t_end (897 steps)
+    c = SOD
+    n = c["n"]
+    geo = (c["num_levels"], c["nx_coarse"], 0.5 / n, 1 - 0.5 / n)
+    warm = awcm.AWCM1D(*geo)
+    warm.init_riemann(0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+    warm.run(c["tol"], c["cfl"], c["t_end"])
+    warm.b.close()
+    g = awcm.AWCM1D(*geo)
+    g.init_riemann(0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+    st = torch.cuda.ExternalStream(g.b.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    steps, t, upd = g.run(c["tol"], c["cfl"], c["t_end"], chunk=1024)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    sod = {"workload": c["workload"], "metric": METRIC, "value": upd / (ms / 1e3), "unit": UNIT, "steps": steps,
+           "device_ms": ms, "active_points": upd,
+           "note": "one instance on one CTA (the batch kernel with a batch of one), one graph replay per step"}
+    g.b.close()
+    if cpu_ok:
+        import oracle
+
+        if oracle.reference_available():
+            o = oracle.Oracle1D(*geo, kind="reference")
+            o.init_riemann(0.5, (1.0, 0.0, 1.0), (0.125, 0.0, 0.1))
+            t0 = time.perf_counter()
+            n_r, _, u_r = o.run(c["tol"], c["cfl"], c["t_end"])
+            wall = time.perf_counter() - t0
+            sod["cpu_baseline"] = {"value": u_r / wall, "unit": UNIT, "cores": 1, "kind": "reference",
+                                   "steps": n_r, "sample": "the whole run, the reference's serial 1D code"}
+            sod["gpu_over_reference"] = sod["value"] / (u_r / wall)
+    out["sod_1d_1025"] = sod
+    return out
 
 
 # ------------------------------------------------------------------------------------- GPU arm
@@ -458,15 +670,21 @@ def run_b200(args):
                              "step, D2H of the field"}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r, why = time_reference(200, args.cpu_seconds, warmup=0)
+    cpu_ok = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if cpu_ok:
+        # the same step window as the timed GPU steps: W untimed warm-up steps, then steps W+1 ..
+        r, why = time_reference(args.steps, args.cpu_seconds, warmup=warmup)
         if r is not None:
             cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
-                   "sample": f"first {r['steps']} RK3 steps of the same 2049^2 workload from its initial state "
-                             f"({r['wall_s']:.1f} s, reference code compiled from the reference tree, OpenMP)"}
+                   "window": {"first_step": warmup + 1, "last_step": warmup + r["steps"]},
+                   "sample": f"steps {warmup + 1}..{warmup + r['steps']} of the same 2049^2 workload from its "
+                             f"initial state, the GPU's timed window ({r['wall_s']:.1f} s, reference code "
+                             f"compiled from the reference tree, OpenMP)"}
         else:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
 
+    full = None if args.no_full_run else run_full_and_late(awcm, torch, args, cpu_ok)
+    configs = None if args.no_configs else run_configs(awcm, torch, args, warmup, cpu_ok)
     batched = None if args.no_batched else run_batched(rank, world)
     gradient = None if args.no_adjoint else run_adjoint(rank, world)
 
@@ -491,6 +709,10 @@ def run_b200(args):
         "e2e": e2e,
         "e2e_field_roundtrip": e2e_field,
         "cpu_baseline": cpu,
+        "window": {"first_step": warmup + 1, "last_step": warmup + n_steps},
+        "full_run": full["full_run"] if full else None,
+        "late_window": full["late_window"] if full else None,
+        "configs": configs,
         "batched_1d": batched,
         "adjoint": gradient,
         "gpu_launches": launches * n_steps,
