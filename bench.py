@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--no-configs", action="store_true", help="skip the double-Mach and 1D Sod lines")
     ap.add_argument("--capture", type=int, default=-1,
                     help="profiling mode: K graph-replayed steps, then one eagerly launched step; prints its phases")
+    ap.add_argument("--capture-batch", type=int, default=-1,
+                    help="profiling mode: the 512-tube batch, K graph-replayed RK3 steps (launches 1..K of k_step1d)")
     return ap.parse_args()
 
 
@@ -736,10 +738,27 @@ def run_capture(k: int):
     print(json.dumps(s.profile_step(w["tol"], w["cfl"], t, w["t_end"])))
 
 
+def run_capture_batch(k: int):
+    """Small, self-ending run for ncu: the seeded 512-tube batch at 384 threads per CTA, k RK3 steps
+    (each one k_step1d launch), then its totals."""
+    import awcm
+    from awcm import workloads
+
+    b = workloads.make_batch(awcm, workloads.shock_tubes(BATCHED["instances"]))
+    b.set_launch(384, 0)
+    b.set_run(BATCHED["tol"], BATCHED["cfl"], 0.0, BATCHED["t_end"])
+    b.steps(k)
+    b.sync()
+    print(json.dumps({"steps": k, "totals": b.totals().tolist()}))
+
+
 def main():
     args = parse()
     if args.capture >= 0:
         run_capture(args.capture)
+        return
+    if args.capture_batch >= 0:
+        run_capture_batch(args.capture_batch)
         return
     if args.impl == "reference":
         run_reference_arm(args)

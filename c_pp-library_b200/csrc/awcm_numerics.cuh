@@ -47,29 +47,32 @@ __device__ __forceinline__ double recon_left(double ll, double l, double c, doub
     const double b0 = kC13_12 * sqr(c - 2 * r + rr) + 0.25 * sqr(3 * c - 4 * r + rr);
     const double b1 = kC13_12 * sqr(l - 2 * c + r) + 0.25 * sqr(l - r);
     const double b2 = kC13_12 * sqr(ll - 2 * l + c) + 0.25 * sqr(ll - 4 * l + 3 * c);
-    double a0, a1, a2;
+    double w0, w1, w2;
     if (SCHEME == kWeno5) {
         const double eps = 1e-6;
-        a0 = 0.1 / sqr(eps + b0);
-        a1 = 0.6 / sqr(eps + b1);
-        a2 = 0.3 / sqr(eps + b2);
+        const double a0 = 0.1 / sqr(eps + b0);
+        const double a1 = 0.6 / sqr(eps + b1);
+        const double a2 = 0.3 / sqr(eps + b2);
+        const double s = a0 + a1 + a2;
+        w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
     } else {
         const double eps = wz_eps;
         const double tau = wz_delta > 0 ? sqrt(sqr(b0 - b2) + sqr(wz_delta)) : absd(b0 - b2);
         const double d0 = b0 + eps, d1 = b1 + eps, d2 = b2 + eps;
         if (tau == 0 && d0 > 0 && d1 > 0 && d2 > 0) {
-            // tau / d_k is a signed zero and 1 + (+-0) = 1, so a_k = d_k exactly: the three
-            // divisions are skipped (a zero quotient sends IEEE division down its slow path,
-            // and piecewise-constant stencils make tau = 0 common).
-            a0 = 0.1, a1 = 0.6, a2 = 0.3;
+            // tau / d_k is a signed zero and 1 + (+-0) = 1, so alpha_k = d_k exactly; their sum
+            // 0.1 + 0.6 + 0.3 rounds to exactly 1.0 in IEEE double, so the normalised weights are
+            // the d_k themselves.  All six divisions are skipped (a zero quotient sends IEEE
+            // division down its slow path, and piecewise-constant stencils make tau = 0 common).
+            w0 = 0.1, w1 = 0.6, w2 = 0.3;
         } else {
-            a0 = 0.1 * (1 + tau / d0);
-            a1 = 0.6 * (1 + tau / d1);
-            a2 = 0.3 * (1 + tau / d2);
+            const double a0 = 0.1 * (1 + tau / d0);
+            const double a1 = 0.6 * (1 + tau / d1);
+            const double a2 = 0.3 * (1 + tau / d2);
+            const double s = a0 + a1 + a2;
+            w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
         }
     }
-    const double s = a0 + a1 + a2;
-    const double w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
     double left = w0 * (kC11_6 * c + kCm7_6 * r + kC1_3 * rr);
     left += w1 * (kC1_3 * l + kC5_6 * c + kCm1_6 * r);
     left += w2 * (kCm1_6 * ll + kC5_6 * l + kC1_3 * c);
