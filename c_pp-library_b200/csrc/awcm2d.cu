@@ -1316,7 +1316,7 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
             }
         }
         const double rowmax = warp_max(sx_row);
-        if (lane == 0 && j < g.ny && rowmax > 0) atomic_max_nonneg(&ax[j], rowmax);
+        if (ax && lane == 0 && j < g.ny && rowmax > 0) atomic_max_nonneg(&ax[j], rowmax);
     }
     if (nonfinite && __any_sync(0xffffffffu, nf) && lane == 0) atomicOr(nonfinite, 1);
 #pragma unroll
@@ -1328,7 +1328,7 @@ __global__ void __launch_bounds__(256) k_alpha(Grid2 g, Field4 f, const uint8_t*
         double c = col[0][threadIdx.x];
         for (int y = 1; y < 8; ++y) c = maxd(c, col[y][threadIdx.x]);
         const int i = 4 * ((int)blockIdx.x * 32) - kGhost + (int)threadIdx.x;
-        if (i >= 0 && i < g.nx && c > 0) atomic_max_nonneg(&ay[i], c);
+        if (ay && i >= 0 && i < g.nx && c > 0) atomic_max_nonneg(&ay[i], c);
         if (mv && threadIdx.x == 0) {
             double v = cfl[0];
             for (int y = 1; y < 8; ++y) v = maxd(v, cfl[y]);
@@ -1628,10 +1628,13 @@ __global__ void __launch_bounds__(256) k_lists(Grid2 g, const uint8_t* __restric
 template <int DIR, bool CUSTOM>
 __global__ void __launch_bounds__(128, AWCM_FACE_MIN_CTAS)
     k_face(Grid2 g, Field4 f, Field4 out, const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
-           const double* __restrict__ alpha, const StepState* st)
+           const double* __restrict__ alpha, const StepState* st, StepState* dt_st)
 {
     pdl_begin();
     if (st->done) return;
+    // dt_st: this launch also computes the step's dt (from the CFL speed of the scan before it);
+    // the faces do not read it, the point updates after them do
+    if (dt_st && blockIdx.x == 0 && threadIdx.x == 0) compute_dt(g, dt_st);
     const unsigned n = *count;
     const long stride = (long)gridDim.x * blockDim.x;
     for (long e = gtid(); e < n; e += stride) {
@@ -2005,6 +2008,26 @@ struct Solver2D {
     size_t staging_bytes = 0;
     int8_t* bcf_dev = nullptr;  // BOUNDARY_CONDITION plane of the generic manager
     cudaStream_t stream = nullptr;
+    // Second branch of the step graph: PrepareEuler's interpolation of the momenta and energy runs
+    // beside the density's inverse transform, and the x faces beside the y faces.  `cur` is the
+    // stream the launch helper enqueues on (null = `stream`).
+    cudaStream_t side = nullptr, side2 = nullptr;
+    cudaStream_t cur = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
+    // a finely profiled step keeps one stream: its per-kernel events time the launches in order
+    bool fork_ok() const { return side && !fine; }
+    void fork(cudaStream_t to)
+    {
+        cudaEventRecord(ev_fork, stream);
+        cudaStreamWaitEvent(to, ev_fork, 0);
+        cur = to;
+    }
+    void join(cudaStream_t from, cudaEvent_t ev)
+    {
+        cur = nullptr;
+        cudaEventRecord(ev, from);
+        cudaStreamWaitEvent(stream, ev, 0);
+    }
     cudaGraphExec_t graph = nullptr;
     int launches = 0;
     int device = 0;
@@ -2035,7 +2058,7 @@ struct Solver2D {
         if (!fine) return;
         cudaEvent_t e;
         cudaEventCreate(&e);
-        cudaEventRecord(e, stream);
+        cudaEventRecord(e, cur ? cur : stream);
         fine->emplace_back(name, e);
     }
 
@@ -2049,7 +2072,7 @@ struct Solver2D {
         cfg.gridDim = grid;
         cfg.blockDim = block;
         cfg.dynamicSmemBytes = 0;
-        cfg.stream = stream;
+        cfg.stream = cur ? cur : stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
         attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -2092,6 +2115,13 @@ struct Solver2D {
         tape_steps = 0;
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
+        if (side) cudaStreamDestroy(side);
+        if (side2) cudaStreamDestroy(side2);
+        side = side2 = nullptr;
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (ev_join2) cudaEventDestroy(ev_join2);
+        ev_fork = ev_join = ev_join2 = nullptr;
     }
 
     awcm2d_geometry geo{};
@@ -2131,6 +2161,11 @@ struct Solver2D {
         g.W = make_weights();
         plane = (size_t)g.pitch * g.rows;
         AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        AWCM_CUDA_TRY(cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking));
+        AWCM_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        AWCM_CUDA_TRY(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        AWCM_CUDA_TRY(cudaEventCreateWithFlags(&ev_join2, cudaEventDisableTiming));
         for (int k = 0; k < 4; ++k) {
             AWCM_CUDA_TRY(cudaMalloc(&q.p[k], plane * sizeof(double)));
             AWCM_CUDA_TRY(cudaMalloc(&q2.p[k], plane * sizeof(double)));
@@ -2396,7 +2431,26 @@ struct Solver2D {
     // Scalar AWCM instance (Wavelet/main_2d_advect.cpp): plane 0 of q, q2, q1 carries the field.
     bool scalar = false;
 
-    void enq_prepare(const StepState* s)
+    // Worklists of the step's three stages and the mask counts; with_dt also computes dt (from the
+    // CFL speed, so after the stage-1 scan).
+    void enq_lists(int with_dt)
+    {
+        ListArgs la;
+        for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
+        la.zx1 = ax[1];
+        la.zy1 = ay[1];
+        la.zx2 = ax[2];
+        la.zy2 = ay[2];
+        la.with_dt = with_dt;
+        dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
+        launch(k_lists, grid, 256, g, m, lvl[2], lvl[1], lvl[0], la, st);
+        after("k_lists");
+        launches += 1;
+    }
+
+    // lists: the step's worklists are built too (without dt), as soon as the masks and levels are
+    // final.
+    void enq_prepare(const StepState* s, bool lists = false)
     {
         if (prep_mode == 0 && s == st && prep_blocks > 0) {
             PrepArgs A;
@@ -2421,6 +2475,7 @@ struct Solver2D {
             cudaLaunchKernelEx(&cfg, k_prepare, A);
             after("k_prepare");
             launches += 1;
+            if (lists) enq_lists(0);
             return;
         }
         // mask_temp = mask0; also clears mask1..3, which the merged ComputeLevel +
@@ -2449,9 +2504,33 @@ struct Solver2D {
             }
             enq_cr(k, s);
         }
-        enq_iwt(3, s, scalar ? -1 : kBitTemp);
         // AWCM_2D::Prepare (the scalar form, Wavelet/AWCM_2D.h:52-79) ends with the inverse transform
-        if (!scalar) enq_interp(kBitTemp, 3, s, 1, true);
+        if (scalar) {
+            enq_iwt(3, s);
+            if (lists) enq_lists(0);
+        } else if (!fork_ok()) {
+            enq_iwt(3, s, kBitTemp);
+            enq_interp(kBitTemp, 3, s, 1, true);
+            if (lists) enq_lists(0);
+        } else {
+            // The inverse transform writes the density only and reads mask3; the interpolation
+            // reads and writes components 1..3 and the interpolation work bit; the worklist build
+            // reads the mask bits 0..3 and the level planes and writes the lists: disjoint, so the
+            // three run as parallel branches of the graph.
+            cudaEventRecord(ev_fork, stream);
+            cudaStreamWaitEvent(side, ev_fork, 0);
+            if (lists) cudaStreamWaitEvent(side2, ev_fork, 0);
+            cur = side;
+            enq_interp(kBitTemp, 3, s, 1, false);
+            if (lists) {
+                cur = side2;
+                enq_lists(0);
+            }
+            cur = nullptr;
+            enq_iwt(3, s);
+            join(side, ev_join);
+            if (lists) join(side2, ev_join2);
+        }
     }
 
     // Boundary fill of a stage input; with zero_stage >= 0 it also zeroes that stage's LF-speed
@@ -2521,8 +2600,10 @@ struct Solver2D {
 
     // Face fluxes and point updates of one stage; the LF speeds come from ax[stage] / ay[stage],
     // or from (axp, ayp) when given.
-    void enq_faces_update(int stage, Field4 in, Field4 out, const double* axp = nullptr, const double* ayp = nullptr)
+    void enq_faces_update(int stage, Field4 in, Field4 out, const double* axp = nullptr, const double* ayp = nullptr,
+                          bool with_dt = false)
     {
+        StepState* dts = with_dt ? st : nullptr;
         uint32_t* const* L = lists + 4 * stage;
         const unsigned* C = st->cnt + 4 * stage;
         const double* sx = axp ? axp : ax[stage];
@@ -2530,17 +2611,21 @@ struct Solver2D {
         // per SM measured 1.3 % and 7 % slower faces
         const double* sy = ayp ? ayp : ay[stage];
         mark();
-        if (g.wz_eps == 1e-40 && g.wz_delta == 0.0) {
-            launch(k_face<0, false>, 2 * face_blocks, 128, g, xin(in), fx, L[2], C + 2, sx, st);
-            after("k_face<0>");
-            launch(k_face<1, false>, 2 * face_blocks, 128, g, in, fy, L[3], C + 3, sy, st);
-            after("k_face<1>");
-        } else {
-            launch(k_face<0, true>, 2 * face_blocks, 128, g, xin(in), fx, L[2], C + 2, sx, st);
-            after("k_face<0>");
-            launch(k_face<1, true>, 2 * face_blocks, 128, g, in, fy, L[3], C + 3, sy, st);
-            after("k_face<1>");
-        }
+        // the x faces (fx) and the y faces (fy) read the same stage input: parallel branches
+        const bool par = fork_ok();
+        if (par) fork(side);
+        if (g.wz_eps == 1e-40 && g.wz_delta == 0.0)
+            launch(k_face<0, false>, 2 * face_blocks, 128, g, xin(in), fx, L[2], C + 2, sx, st, (StepState*)nullptr);
+        else
+            launch(k_face<0, true>, 2 * face_blocks, 128, g, xin(in), fx, L[2], C + 2, sx, st, (StepState*)nullptr);
+        after("k_face<0>");
+        cur = nullptr;
+        if (g.wz_eps == 1e-40 && g.wz_delta == 0.0)
+            launch(k_face<1, false>, 2 * face_blocks, 128, g, in, fy, L[3], C + 3, sy, st, dts);
+        else
+            launch(k_face<1, true>, 2 * face_blocks, 128, g, in, fy, L[3], C + 3, sy, st, dts);
+        after("k_face<1>");
+        if (par) join(side, ev_join);
         launches += 2;
         mark();
         const int ub = face_blocks / 2;
@@ -2566,27 +2651,18 @@ struct Solver2D {
         launch(k_begin, 1, 1, st, 0);
         after("k_begin");
         launches += 1;
-        enq_prepare(st);
+        // the worklists (and the zeroing of stage 2/3's speed accumulators) are built beside the
+        // last PrepareEuler passes; dt is computed by the first stage's y-face launch
+        enq_prepare(st, true);
         mark();
         const bool wt = g.bc_kind == AWCM_BC_WIND_TUNNEL;
         enq_bc(q, st, 0);
+        // The wind tunnel's bottom fills write solid cells of mask3 that PrepareEuler leaves in
+        // non-physical states, so the CFL scan (with the LF speeds) reads the filled stage input;
+        // the other managers write ghost cells only, outside the scan.
         if (wt) enq_wt_input(q);
         enq_alpha(q, 3, 0, true);
-        {
-            // the worklists, dt (after stage 1's speeds) and the zeroing of stage 2/3's speeds
-            ListArgs la;
-            for (int L = 0; L < kNumLists; ++L) la.list[L] = lists[L];
-            la.zx1 = ax[1];
-            la.zy1 = ay[1];
-            la.zx2 = ax[2];
-            la.zy2 = ay[2];
-            la.with_dt = 1;
-            dim3 grid((g.nx + 1 + 255) / 256, (g.ny + 1 + kListRows - 1) / kListRows);
-            launch(k_lists, grid, 256, g, m, lvl[2], lvl[1], lvl[0], la, st);
-            after("k_lists");
-            launches += 1;
-        }
-        enq_faces_update(0, q, q2);
+        enq_faces_update(0, q, q2, nullptr, nullptr, true);
         for (int stage = 1; stage <= 2; ++stage) {
             Field4 in = stage == 1 ? q2 : q1;
             if (!wt) {
@@ -2781,7 +2857,8 @@ struct Solver2D {
     }
 
     // One step with the same kernels launched eagerly and CUDA events at the phase boundaries.
-    // out[0] prepare ms, [1] CFL/LF speeds/dt/worklists ms, [2..4] face kernels ms per stage,
+    // out[0] prepare ms (with the worklist build beside its last passes), [1] boundary fill and
+    // CFL/LF speeds ms, [2..4] face kernels ms per stage,
     // [5..7] point-update kernels ms per stage, [8] boundary fills + LF speeds of stages 2-3 ms,
     // [9] residue removal ms, [10] total ms, [11..13] faces per stage, [14..16] stage points,
     // [17] |mask0|, [18] dt.

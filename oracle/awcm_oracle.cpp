@@ -1397,6 +1397,15 @@ void stage2d(O2D& s, std::vector<double>* in, std::vector<double>* out, int b, i
 void step2d(O2D& s, double tol, double cfl, double t, double t_next, double dt_fixed, double* alpha_io, double* out)
 {
     if (!s.freeze) prepare2d(s, tol);
+    const bool wt = s.bc_kind == BC_WIND_TUNNEL && s.bcf.empty();
+    std::vector<double>* qx = wt ? s.qx : nullptr;
+    // Wind tunnel: the bottom fills write solid cells of mask3 (left non-physical by PrepareEuler),
+    // so its first stage input is filled before the CFL scan; the other managers write ghost cells
+    // only and keep the driver's order (main_2d_euler(quad).cpp:61-85).
+    if (wt) {
+        bc2d(s, s.q, t);
+        wt_stage_input(s, s.q);
+    }
     double mv = 0;
     {
         std::vector<double> part(omp_get_max_threads(), 0.0);
@@ -1437,10 +1446,7 @@ void step2d(O2D& s, double tol, double cfl, double t, double t_next, double dt_f
             }
         }
     };
-    const bool wt = s.bc_kind == BC_WIND_TUNNEL && s.bcf.empty();
-    std::vector<double>* qx = wt ? s.qx : nullptr;
-    bc2d(s, s.q, t);
-    if (wt) wt_stage_input(s, s.q);
+    if (!wt) bc2d(s, s.q, t);
     load_alpha(0, s.q, 3);
     stage2d(s, s.q, s.q2, 2, 2, ax, ay, dt, 1, qx);
     bc2d(s, s.q2, t);

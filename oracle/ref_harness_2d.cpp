@@ -656,6 +656,15 @@ void ref2d_step(void* h, double tol, double cfl, double t, double t_next, double
         else awcm.PrepareEuler(Q, tol);
     }
 
+    // The wind tunnel's bottom fills write interior (solid) cells of mask3, which PrepareEuler leaves
+    // in non-physical states (negative pressure behind the step face): for it the first stage input
+    // is filled before the CFL scan, so that the scan reads the states the stage reads.  The other
+    // managers write ghost cells only, outside the scan, and keep the driver's order (scan, then
+    // SetBoundaryCondition: main_2d_euler(quad).cpp:61-85).
+    if (wt) {
+        s->bc->apply(t);
+        stage_input_wt(s, Q);
+    }
     double max_velocity = 0;
 #pragma omp parallel
     {
@@ -696,8 +705,7 @@ void ref2d_step(void* h, double tol, double cfl, double t, double t_next, double
     };
 
     const FIELD_UNIFORM_2D<VECTOR_4D<double>>* qx = wt ? &s->Qx : nullptr;
-    s->bc->apply(t);
-    if (wt) stage_input_wt(s, Q);
+    if (!wt) s->bc->apply(t);
     load_alpha(0, Q, awcm.mask3);
     stage2d(s, Q, s->Q_2, awcm.mask2, awcm.level2, ax, ay, dt, 1, qx);
 
