@@ -9,8 +9,10 @@
 // CUDA graph (queue reset + step kernel) and replayed.
 //
 // Per-instance layout in the pool (w = Nx + 6, ghost ring 3): doubles q[3][w] (conserved),
-// qc[3][w] (stage-start copy), qt[3][w] (stage input copy), fl[3][w] (face fluxes, face i+1/2 at
-// point i); bytes mask[w] (bits 0..3 mask0..3, 4 previous mask0, 5/6 work bits), level[4][w].
+// qc[3][w] (stage-start copy), qt[3][w] (coarse-point flux derivatives of a stage), fl[3][w] (face
+// fluxes, face i+1/2 at point i), then w + 32 doubles holding the stage worklists of an instance
+// too large to stage in shared memory (2 (w + 32) indices); bytes mask[w] (bits 0..3 mask0..3,
+// 4 previous mask0, 5/6 work bits), then 16-byte aligned level[4][w].
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -109,6 +111,31 @@ __device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* r
     return before + x - v;
 }
 
+// The same over 64-bit values (three packed 21-bit counts); red holds one 64-bit word per warp.
+__device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned long long v, unsigned long long* red,
+                                                                     unsigned long long* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) red[warp] = x;
+    __syncthreads();
+    unsigned long long before = 0, all = 0;
+    for (int k = 0; k < nw; ++k) {
+        const unsigned long long r = red[k];
+        before += k < warp ? r : 0ull;
+        all += r;
+    }
+    *total = all;
+    return before + x - v;
+}
+
 // Block-wide stream compaction of the indices lo..hi whose predicate holds into `list` (order
 // preserved).  Returns the count.  Each thread owns a contiguous chunk of the range: it counts its
 // hits, one block-wide exclusive scan gives its output offset, and it writes its hits in order
@@ -158,6 +185,22 @@ struct Ctx {
         if (i < -kGhost || i >= nx + kGhost) return;
         const uintptr_t a = reinterpret_cast<uintptr_t>(m + i + kGhost);
         atomicOr(reinterpret_cast<unsigned*>(a & ~(uintptr_t)3), 1u << (8 * (unsigned)(a & 3) + b));
+    }
+    // The same push on the n <= 8 consecutive points i0 .. i0+n-1: one atomicOr per 32-bit word.
+    __device__ void set_run(int i0, int n, int b) const
+    {
+        const int lo = i0 < -kGhost ? -kGhost : i0, hi = min(i0 + n - 1, nx + kGhost - 1);
+        if (lo > hi) return;
+        uintptr_t a = reinterpret_cast<uintptr_t>(m + lo + kGhost);
+        const uintptr_t e = reinterpret_cast<uintptr_t>(m + hi + kGhost);
+        while (a <= e) {
+            const uintptr_t wb = a & ~(uintptr_t)3;
+            const uintptr_t we = wb + 3 < e ? wb + 3 : e;
+            unsigned bits = 0;
+            for (uintptr_t x = a; x <= we; ++x) bits |= 1u << (8 * (unsigned)(x & 3) + b);
+            atomicOr(reinterpret_cast<unsigned*>(wb), bits);
+            a = we + 1;
+        }
     }
     __device__ int D(int lev) const { return 1 << (maxl - lev); }
     __device__ double w_(int cnt, int k) const { return W.w[cnt][k + 1]; }
@@ -269,7 +312,7 @@ __device__ void apd1(const Ctx& c, int b, int l)
         const int D = c.D(lev);
         const int is = i - 2 * D, ie = i + 2 * D;
         if (lev == c.maxl) {
-            for (int cnt = -3; cnt < 4; ++cnt) c.set(i + cnt, b);
+            c.set_run(i - 3, 7, b);
         } else if (is <= 0) {
             for (int cnt = 0; cnt < 6; ++cnt) c.set(cnt * D, b);
         } else if (ie >= c.N1) {
@@ -288,16 +331,25 @@ __device__ __forceinline__ bool mask_or_ghost1(const Ctx& c, int i, int b)
 }
 
 // AWCM_MANAGER_1D::ComputeLevel (Wavelet/AWCM_MANAGER_1D.h:109-133), with the optional copy
-// mask_{k+1} = mask_k of the own point.
+// mask_{k+1} = mask_k of the own point.  One 32-bit mask word (four points) per iteration: the copy
+// is one word operation and the level search runs for the mask's points only.  The search reads
+// bit b of other bytes, which no thread changes here (the copy writes bit copy_to).
 __device__ void cl1(const Ctx& c, int l, int b, int copy_to)
 {
-    for (int i = (int)threadIdx.x - kGhost; i <= c.N1 + kGhost; i += blockDim.x) {
-        const unsigned v = c.M(i);
-        const bool on = (v >> b) & 1u;
-        if (i < 0 || i > c.N1) {
-            // ghost byte: only the copy (the reference copies whole fields)
-        } else if (i >= 1 && i <= c.N1 - 1) {
-            if (!on) {
+    unsigned* mw = reinterpret_cast<unsigned*>(c.m);
+    const int nw = (c.w + 3) >> 2;
+    for (int wi = threadIdx.x; wi < nw; wi += blockDim.x) {
+        const unsigned v = mw[wi];
+        unsigned lanes = 0;  // the bytes of the word that are points of the line (ghosts included)
+#pragma unroll
+        for (int L = 0; L < 4; ++L) {
+            const int i = 4 * wi + L - kGhost;
+            if (i > c.N1 + kGhost) continue;
+            lanes |= 1u << (8 * L);
+            if (i < 0 || i > c.N1) continue;  // ghost byte: only the copy (the reference copies whole fields)
+            if (i == 0 || i == c.N1) {
+                c.L(l, i) = (int8_t)c.maxl;
+            } else if (!((v >> (8 * L + b)) & 1u)) {
                 c.L(l, i) = 0;
             } else {
                 int dx = 1;
@@ -309,20 +361,30 @@ __device__ void cl1(const Ctx& c, int l, int b, int copy_to)
                     dx *= 2;
                 }
             }
-        } else {
-            c.L(l, i) = (int8_t)c.maxl;
         }
-        if (copy_to >= 0) c.M(i) = (uint8_t)((v & ~(1u << copy_to)) | ((on ? 1u : 0u) << copy_to));
+        if (copy_to >= 0) {
+            const unsigned nv = (v & ~(lanes << copy_to)) | (((v >> b) & lanes) << copy_to);
+            if (nv != v) mw[wi] = nv;
+        }
     }
     __syncthreads();
 }
 
+// Copies bit `from` into bit `to` on the points [0, N1] (ghosts: [-3, N1+3]), a word at a time.
 __device__ void copy_bit1(const Ctx& c, int from, int to, bool ghosts)
 {
-    const int lo = ghosts ? -kGhost : 0, hi = ghosts ? c.N1 + kGhost : c.N1;
-    for (int i = lo + (int)threadIdx.x; i <= hi; i += blockDim.x) {
-        const unsigned v = c.M(i);
-        c.M(i) = (uint8_t)((v & ~(1u << to)) | (((v >> from) & 1u) << to));
+    const int x0 = ghosts ? 0 : kGhost, x1 = ghosts ? c.N1 + 2 * kGhost : c.N1 + kGhost;  // byte range
+    unsigned* mw = reinterpret_cast<unsigned*>(c.m);
+    for (int wi = (x0 >> 2) + (int)threadIdx.x; wi <= (x1 >> 2); wi += blockDim.x) {
+        unsigned lanes = 0;
+#pragma unroll
+        for (int L = 0; L < 4; ++L) {
+            const int x = 4 * wi + L;
+            if (x >= x0 && x <= x1) lanes |= 1u << (8 * L);
+        }
+        const unsigned v = mw[wi];
+        const unsigned nv = (v & ~(lanes << to)) | (((v >> from) & lanes) << to);
+        if (nv != v) mw[wi] = nv;
     }
     __syncthreads();
 }
@@ -330,10 +392,19 @@ __device__ void copy_bit1(const Ctx& c, int from, int to, bool ghosts)
 // WAVELET_1D::InterpolateEuler(q, mra, from, to) (Wavelet/WAVELET_1D.h:393-431).
 __device__ void interp1(const Ctx& c, int from, int to)
 {
-    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
-        const unsigned v = c.M(i);
-        const unsigned on = ((v >> to) & 1u) & ~((v >> from) & 1u);
-        c.M(i) = (uint8_t)((v & ~(1u << kBitInterp)) | (on << kBitInterp));
+    // work bit = to and not from, on the points [0, N1], a word at a time
+    unsigned* mw = reinterpret_cast<unsigned*>(c.m);
+    for (int wi = (kGhost >> 2) + (int)threadIdx.x; wi <= ((c.N1 + kGhost) >> 2); wi += blockDim.x) {
+        unsigned lanes = 0;
+#pragma unroll
+        for (int L = 0; L < 4; ++L) {
+            const int x = 4 * wi + L;
+            if (x >= kGhost && x <= c.N1 + kGhost) lanes |= 1u << (8 * L);
+        }
+        const unsigned v = mw[wi];
+        const unsigned on = (v >> to) & ~(v >> from) & lanes;
+        const unsigned nv = (v & ~(lanes << kBitInterp)) | (on << kBitInterp);
+        if (nv != v) mw[wi] = nv;
     }
     __syncthreads();
     cr1(c, kBitInterp);
@@ -417,19 +488,14 @@ __device__ double lf_speed1(const Ctx& c, int b, int l, double* red, bool& nf)
     return block_max(a, red);
 }
 
-__device__ void copy_q(const Ctx& c, double* __restrict__ dst)
-{
-    for (int t = threadIdx.x; t < 3 * c.w; t += blockDim.x) dst[t] = t < c.w ? c.q0[t] : c.q[t];
-    __syncthreads();
-}
-
 // Coarse-level flux derivative (AWCM_1D::DifferentiateEuler*, Wavelet/AWCM_1D.h:142-189) with the
 // driver's branch selection (main_1d_euler.cpp:111-133); right-boundary forms mirror the left ones.
+// Reads the stage input Q, which no point update has touched yet when it runs.
 __device__ void coarse_dF1(const Ctx& c, int i, int d, double* dF)
 {
     const double g = 1.4;  // EULER_EQUATION_1D euler_eqn(1.4) in the reference helpers
     auto F = [&](int ii, double* f) {
-        const double s[3] = {c.QT(0, ii), c.QT(1, ii), c.QT(2, ii)};
+        const double s[3] = {c.Q(0, ii), c.Q(1, ii), c.Q(2, ii)};
         flux1(s, g, f);
     };
     const int iend = c.N1;
@@ -452,38 +518,198 @@ __device__ void coarse_dF1(const Ctx& c, int i, int d, double* dF)
     }
 }
 
-// One stage over mask bit b / level set l (main_1d_euler.cpp:97-245).  Faces are computed once
-// (face i+1/2 is shared by points i and i+1; the reference evaluates it for both, identically).
-template <int SCHEME>
-__device__ void stage1(const Ctx& c, int b, int l, double alpha, double dt, int kind, uint32_t* list, unsigned* ured)
+// Lists of one stage, from one pass over the points: faces f in [-1, N1] (face f+1/2 is needed when a
+// finest-level point of the stage's mask lies on either side) into fl_list[0, nf), finest-level
+// points into pl[0, nfin), coarse points (valid level, derivative stencil inside the ghosted line)
+// into pl[cap - ncrs, cap).  copy_qc: also the stage-start copy QC of every mask1 point (the only
+// points whose QC stages 2 and 3 read; mask0 is inside mask1).  Each thread owns a contiguous
+// chunk of positions and keeps its hits as bit sets (chunks of up to 64 positions; longer chunks
+// evaluate again), one block scan of the three packed counts places them; order is preserved.
+struct StageLists {
+    int nf, nfin, ncrs;
+};
+// Stage class of a point whose mask bit is set: 1 finest level, 2 coarse point with its derivative
+// stencil inside the ghosted line, 0 neither (main_1d_euler.cpp:111-133).
+__device__ __forceinline__ int stage_class(const Ctx& c, int l, int i)
 {
-    copy_q(c, c.qt);
-    auto fin = [&](int i) { return i >= 0 && i <= c.N1 && c.bit(i, b) && c.L(l, i) == c.maxl; };
-    const int nf = block_compact(-1, c.N1, [&](int f) { return fin(f) || fin(f + 1); }, list, ured);
-    for (int e = threadIdx.x; e < nf; e += blockDim.x) {
-        const int f = (int)list[e];
-        double s[6][3];
+    const int lev = c.L(l, i);
+    if (lev == c.maxl) return 1;
+    if (lev < 0 || lev > c.maxl) return 0;
+    const int d = c.D(lev);
+    return (i - 2 * d < -kGhost || i + 2 * d > c.N1 + kGhost) ? 0 : 2;
+}
+__device__ __forceinline__ bool fin_byte(const Ctx& c, int b, int l, int x)
+{
+    return x >= kGhost && x <= c.N1 + kGhost && ((c.m[x] >> b) & 1u) && c.L(l, x - kGhost) == c.maxl;
+}
+
+// Word-level form of stage_lists for instances whose per-thread share is at most 16 mask words:
+// each thread reads its run of 32-bit mask words (four points each), looks up levels for the
+// stage's points only, and keeps its hits as bit sets over the run.
+__device__ StageLists stage_lists_words(const Ctx& c, int b, int l, bool copy_qc, uint32_t* fl_list, uint32_t* pl,
+                                        int cap, unsigned long long* red, int w0, int w1)
+{
+    const int xlo = kGhost - 1, xhi = c.N1 + kGhost;  // faces x in [xlo, xhi], points x in [kGhost, xhi]
+    const unsigned* mw = reinterpret_cast<const unsigned*>(c.m);
+    const int base = 4 * w0;
+    unsigned long long mf = 0, mp = 0, mc = 0;
+    bool fprev = w0 < w1 && fin_byte(c, b, l, base - 1);
+    for (int wi = w0; wi < w1; ++wi) {
+        const unsigned v = mw[wi];
 #pragma unroll
-        for (int p = 0; p < 6; ++p)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) s[p][k] = c.QT(k, f - 2 + p);
-        double o[3];
-        face_flux_1d<SCHEME>(s, alpha, c.I.gamma, o);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) c.fl[k * c.w + f + kGhost] = o[k];
+        for (int L = 0; L < 4; ++L) {
+            const int x = 4 * wi + L;
+            int k = 0;
+            if (x >= kGhost && x <= xhi) {
+                if ((v >> (8 * L + b)) & 1u) k = stage_class(c, l, x - kGhost);
+                if (copy_qc && ((v >> (8 * L + 1)) & 1u))
+                    for (int q = 0; q < 3; ++q) c.QC(q, x - kGhost) = c.Q(q, x - kGhost);
+            }
+            const unsigned long long bit = 1ull << (x - base);
+            if (k == 1) mp |= bit;
+            else if (k == 2) mc |= bit;
+            // face x - 1 needs a finest-level point at x - 1 or x
+            if (x - 1 >= base && x - 1 >= xlo && (fprev || k == 1)) mf |= bit >> 1;
+            fprev = k == 1;
+        }
+    }
+    if (w0 < w1) {
+        const int xl = 4 * w1 - 1;
+        if (xl >= xlo && xl <= xhi && (fprev || fin_byte(c, b, l, xl + 1))) mf |= 1ull << (xl - base);
+    }
+    constexpr unsigned long long M21 = (1ull << 21) - 1;
+    unsigned long long tot;
+    const unsigned long long off = block_exclusive_scan64(
+        (unsigned long long)__popcll(mf) | ((unsigned long long)__popcll(mp) << 21) | ((unsigned long long)__popcll(mc) << 42),
+        red, &tot);
+    StageLists o{(int)(tot & M21), (int)((tot >> 21) & M21), (int)((tot >> 42) & M21)};
+    unsigned of = (unsigned)(off & M21), op = (unsigned)((off >> 21) & M21), oc = (unsigned)((off >> 42) & M21);
+    uint32_t* crs = pl + cap - o.ncrs;
+    for (; mf; mf &= mf - 1) fl_list[of++] = (uint32_t)(base + __ffsll(mf) - 1 - kGhost);
+    for (; mp; mp &= mp - 1) pl[op++] = (uint32_t)(base + __ffsll(mp) - 1 - kGhost);
+    for (; mc; mc &= mc - 1) crs[oc++] = (uint32_t)(base + __ffsll(mc) - 1 - kGhost);
+    __syncthreads();
+    return o;
+}
+
+__device__ StageLists stage_lists(const Ctx& c, int b, int l, bool copy_qc, uint32_t* fl_list, uint32_t* pl, int cap,
+                                  unsigned long long* red)
+{
+    {
+        const int wlo = (kGhost - 1) >> 2, whi = (c.N1 + kGhost) >> 2;
+        const int pw = (whi - wlo + (int)blockDim.x) / (int)blockDim.x;
+        if (pw <= 16) {
+            const int w0 = wlo + (int)threadIdx.x * pw;
+            return stage_lists_words(c, b, l, copy_qc, fl_list, pl, cap, red, w0, min(w0 + pw, whi + 1));
+        }
+    }
+    const int lo = -1, hi = c.N1;
+    const int n = hi - lo + 1;
+    const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int a0 = lo + (int)threadIdx.x * per;
+    const int a1 = min(a0 + per, hi + 1);
+    // 0: not a stage point, 1: finest-level point, 2: coarse point (main_1d_euler.cpp:111-133)
+    auto cls = [&](int i) -> int {
+        if (i < 0 || i > c.N1 || !c.bit(i, b)) return 0;
+        const int lev = c.L(l, i);
+        if (lev == c.maxl) return 1;
+        if (lev < 0 || lev > c.maxl) return 0;
+        const int d = c.D(lev);
+        return (i - 2 * d < -kGhost || i + 2 * d > c.N1 + kGhost) ? 0 : 2;
+    };
+    const bool bits = per <= 64;
+    unsigned long long mf = 0, mp = 0, mc = 0;
+    unsigned cf = 0, cp = 0, cc = 0;
+    int k_i = a0 < a1 ? cls(a0) : 0;
+    for (int i = a0; i < a1; ++i) {
+        const int k_n = cls(i + 1);
+        const unsigned long long bit = 1ull << ((i - a0) & 63);
+        if (k_i == 1 || k_n == 1) {
+            ++cf;
+            if (bits) mf |= bit;
+        }
+        if (k_i == 1) {
+            ++cp;
+            if (bits) mp |= bit;
+        } else if (k_i == 2) {
+            ++cc;
+            if (bits) mc |= bit;
+        }
+        if (copy_qc && i >= 0 && c.bit(i, 1))
+            for (int k = 0; k < 3; ++k) c.QC(k, i) = c.Q(k, i);
+        k_i = k_n;
+    }
+    constexpr unsigned long long M21 = (1ull << 21) - 1;
+    unsigned long long tot;
+    const unsigned long long off =
+        block_exclusive_scan64((unsigned long long)cf | ((unsigned long long)cp << 21) | ((unsigned long long)cc << 42),
+                               red, &tot);
+    StageLists o{(int)(tot & M21), (int)((tot >> 21) & M21), (int)((tot >> 42) & M21)};
+    unsigned of = (unsigned)(off & M21), op = (unsigned)((off >> 21) & M21), oc = (unsigned)((off >> 42) & M21);
+    uint32_t* crs = pl + cap - o.ncrs;
+    if (bits) {
+        for (; mf; mf &= mf - 1) fl_list[of++] = (uint32_t)(a0 + __ffsll(mf) - 1);
+        for (; mp; mp &= mp - 1) pl[op++] = (uint32_t)(a0 + __ffsll(mp) - 1);
+        for (; mc; mc &= mc - 1) crs[oc++] = (uint32_t)(a0 + __ffsll(mc) - 1);
+    } else {
+        k_i = a0 < a1 ? cls(a0) : 0;
+        for (int i = a0; i < a1; ++i) {
+            const int k_n = cls(i + 1);
+            if (k_i == 1 || k_n == 1) fl_list[of++] = (uint32_t)i;
+            if (k_i == 1) pl[op++] = (uint32_t)i;
+            else if (k_i == 2) crs[oc++] = (uint32_t)i;
+            k_i = k_n;
+        }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x) {
-        if (!c.bit(i, b)) continue;
-        const int lev = c.L(l, i);
-        if (lev < 0 || lev > c.maxl) continue;
-        const int d = c.D(lev);
-        if (lev != c.maxl && (i - 2 * d < -kGhost || i + 2 * d > c.N1 + kGhost)) continue;
+    return o;
+}
+
+// One stage over mask bit b / level set l (main_1d_euler.cpp:97-245).  Faces are computed once
+// (face i+1/2 is shared by points i and i+1; the reference evaluates it for both, identically).
+// The faces and the coarse derivatives read the stage input Q and run in one phase (the coarse
+// derivatives are parked in qt); the point updates follow in a second phase, so Q is never read
+// after a point of this stage has been written and no copy of the stage input is needed.
+template <int SCHEME>
+__device__ void stage1(const Ctx& c, int b, int l, double alpha, double dt, int kind, uint32_t* list,
+                       unsigned long long* red)
+{
+    const int cap = c.w + 32;
+    uint32_t* pl = list + cap;
+    const StageLists L = stage_lists(c, b, l, kind == 1, list, pl, cap, red);
+    const uint32_t* crs = pl + cap - L.ncrs;
+    for (int e = threadIdx.x; e < L.nf + L.ncrs; e += blockDim.x) {
+        if (e < L.nf) {
+            const int f = (int)list[e];
+            double s[6][3];
+#pragma unroll
+            for (int p = 0; p < 6; ++p)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) s[p][k] = c.Q(k, f - 2 + p);
+            double o[3];
+            face_flux_1d<SCHEME>(s, alpha, c.I.gamma, o);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) c.fl[k * c.w + f + kGhost] = o[k];
+        } else {
+            const int i = (int)crs[e - L.nf];
+            double dF[3];
+            coarse_dF1(c, i, c.D(c.L(l, i)), dF);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) c.QT(k, i) = dF[k];
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < L.nfin + L.ncrs; e += blockDim.x) {
+        int i, d;
         double dF[3];
-        if (lev == c.maxl) {
+        if (e < L.nfin) {
+            i = (int)pl[e];
+            d = 1;
             for (int k = 0; k < 3; ++k) dF[k] = c.fl[k * c.w + i + kGhost] - c.fl[k * c.w + i - 1 + kGhost];
         } else {
-            coarse_dF1(c, i, d, dF);
+            i = (int)crs[e - L.nfin];
+            d = c.D(c.L(l, i));
+            for (int k = 0; k < 3; ++k) dF[k] = c.QT(k, i);
         }
         const double sc = dt / (c.I.dx * d);
         for (int k = 0; k < 3; ++k) {
@@ -500,6 +726,7 @@ __device__ void stage1(const Ctx& c, int b, int l, double alpha, double dt, int 
 template <int SCHEME>
 __device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, unsigned* ured)
 {
+    unsigned long long* red64 = reinterpret_cast<unsigned long long*>(ured);
     prepare1(c);
 
     // CFL (main_1d_euler.cpp:67-81)
@@ -530,14 +757,14 @@ __device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, u
 
     bc1(c);
     const double a1 = lf_speed1(c, 3, 3, dred, nf);
-    copy_q(c, c.qc);
-    stage1<SCHEME>(c, 2, 2, a1, dt, 1, list, ured);
+    // the stage-start copy QC is taken inside stage 1's list pass
+    stage1<SCHEME>(c, 2, 2, a1, dt, 1, list, red64);
     bc1(c);
     const double a2 = lf_speed1(c, 2, 2, dred, nf);
-    stage1<SCHEME>(c, 1, 1, a2, dt, 2, list, ured);
+    stage1<SCHEME>(c, 1, 1, a2, dt, 2, list, red64);
     bc1(c);
     const double a3 = lf_speed1(c, 1, 1, dred, nf);
-    stage1<SCHEME>(c, 0, 0, a3, dt, 3, list, ured);
+    stage1<SCHEME>(c, 0, 0, a3, dt, 3, list, red64);
     const bool any_nf = __syncthreads_or(nf);
     // RemoveResidue (AWCM_MANAGER_1D.h:135-157)
     for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
@@ -696,11 +923,14 @@ __device__ void step_ctx_scalar(Inst1& I, const Ctx& c, uint32_t* list, unsigned
 // Byte offset of the level planes behind the mask bytes of an instance's state block.
 __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
+// The stage worklists of an instance of w ghosted points: faces, then finest and coarse points.
+__host__ __device__ __forceinline__ size_t list_bytes(int w) { return sizeof(uint32_t) * 2 * (size_t)(w + 32); }
+
 // Shared memory of the step kernel for an instance of w ghosted points: mask bytes, the four level
-// planes and the density plane staged for the step, and the worklist of the stages.
+// planes and the density plane staged for the step, and the worklists of the stages.
 __host__ __device__ __forceinline__ size_t step_smem_bytes(int w)
 {
-    return align16((size_t)w) + align16((size_t)4 * w) + sizeof(double) * (size_t)w + sizeof(uint32_t) * (size_t)(w + 32);
+    return align16((size_t)w) + align16((size_t)4 * w) + sizeof(double) * (size_t)w + list_bytes(w);
 }
 
 // Copy of n bytes by all threads of the block; 16-byte words where both ends allow it.
@@ -728,33 +958,44 @@ __device__ __forceinline__ void block_copy_doubles(double* __restrict__ dst, con
     for (int t = head + threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
 }
 
-// One RK3 step of an instance with its mask bytes, levels and density plane staged in the CTA's
-// shared memory: the ~100 level-sequential mask and transform phases of PrepareEuler and the
-// stage worklists then run on shared memory, with one global round trip in and one out per step.
-// q: the three conserved planes (global); qc, qt, fl: stage-start copy, stage input, face fluxes;
-// mg: w mask bytes, lg: four planes of w levels (global); smem: step_smem_bytes(w) bytes.
-__device__ void step_staged(Inst1& I, double* q, double* qc, double* qt, double* fl, uint8_t* mg, int8_t* lg,
-                            const Weights& W, uint8_t* smem, double* dred, unsigned* ured)
+// One RK3 step of an instance.  staged: its mask bytes, levels and density plane are copied into
+// the CTA's shared memory (smem: step_smem_bytes(w) bytes) and the ~100 level-sequential mask and
+// transform phases of PrepareEuler and the stage worklists run there, with one global round trip
+// in and one out per step; otherwise the step runs on the global buffers with its worklists at
+// glist.  q: the three conserved planes (global); qc, qt, fl: stage-start copy, coarse
+// derivatives, face fluxes; mg: w mask bytes, lg: four planes of w levels (global).  One call
+// site for both forms keeps the step kernel's code to one copy of each scheme.
+__device__ void step_inst(Inst1& I, double* q, double* qc, double* qt, double* fl, uint8_t* mg, int8_t* lg,
+                          const Weights& W, uint8_t* smem, bool staged, uint32_t* glist, double* dred, unsigned* ured)
 {
     const int w = I.nx + 2 * kGhost;
-    uint8_t* ms = smem;
-    int8_t* ls = reinterpret_cast<int8_t*>(smem + align16((size_t)w));
-    double* q0s = reinterpret_cast<double*>(smem + align16((size_t)w) + align16((size_t)4 * w));
-    uint32_t* list = reinterpret_cast<uint32_t*>(q0s + w);
     // the scalar path reads and writes its field planes directly; only its masks are staged
     const bool scalar = I.scheme == kScalarAdvection;
-    block_copy_bytes(ms, mg, w);
-    block_copy_bytes(reinterpret_cast<uint8_t*>(ls), reinterpret_cast<const uint8_t*>(lg), 4 * w);
-    if (!scalar) block_copy_doubles(q0s, q, w);
-    __syncthreads();
-    const Ctx c{I, q, qc, qt, fl, ms, ls, W, w, I.nx, I.nx - 1, I.maxl, scalar ? q : q0s};
+    uint8_t* ms = mg;
+    int8_t* ls = lg;
+    double* q0 = q;
+    uint32_t* list = glist;
+    if (staged) {
+        ms = smem;
+        ls = reinterpret_cast<int8_t*>(smem + align16((size_t)w));
+        double* q0s = reinterpret_cast<double*>(smem + align16((size_t)w) + align16((size_t)4 * w));
+        list = reinterpret_cast<uint32_t*>(q0s + w);
+        if (!scalar) q0 = q0s;
+        block_copy_bytes(ms, mg, w);
+        block_copy_bytes(reinterpret_cast<uint8_t*>(ls), reinterpret_cast<const uint8_t*>(lg), 4 * w);
+        if (!scalar) block_copy_doubles(q0s, q, w);
+        __syncthreads();
+    }
+    const Ctx c{I, q, qc, qt, fl, ms, ls, W, w, I.nx, I.nx - 1, I.maxl, q0};
     if (scalar) step_ctx_scalar(I, c, list, ured);
     else if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
     else step_ctx<kWenoZ>(I, c, list, dred, ured);
-    block_copy_bytes(mg, ms, w);
-    block_copy_bytes(reinterpret_cast<uint8_t*>(lg), reinterpret_cast<const uint8_t*>(ls), 4 * w);
-    if (!scalar) block_copy_doubles(q, q0s, w);
-    __syncthreads();
+    if (staged) {
+        block_copy_bytes(mg, ms, w);
+        block_copy_bytes(reinterpret_cast<uint8_t*>(lg), reinterpret_cast<const uint8_t*>(ls), 4 * w);
+        if (!scalar) block_copy_doubles(q, q0, w);
+        __syncthreads();
+    }
 }
 
 // Global views of instance I in the pool.
@@ -769,13 +1010,13 @@ __device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
 
 // One RK3 step of every queued instance.  CTAs pull queue slots until the queue is exhausted.
 // smem_bytes: the launch's dynamic shared memory; an instance whose staged step does not fit in
-// it runs on its global buffers (only its worklist in shared memory).
+// it runs on its global buffers (its worklists in the pool too).
 __global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, unsigned* queue, Pool P,
                          unsigned smem_bytes)
 {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ double dred[32];
-    __shared__ unsigned ured[128];
+    __shared__ __align__(8) unsigned ured[128];
     __shared__ int cur;
     for (;;) {
         if (threadIdx.x == 0) cur = (int)atomicAdd(queue, 1u);
@@ -786,18 +1027,13 @@ __global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, uns
         Inst1& I = insts[order[k]];
         if (I.t >= I.t_end || I.err) {
             if (threadIdx.x == 0) I.done = 1;
-        } else if (step_smem_bytes(I.nx + 2 * kGhost) <= smem_bytes) {
+        } else {
             const int w = I.nx + 2 * kGhost;
             double* base = P.q + I.q_off;
             uint8_t* mb = P.m + I.m_off;
-            step_staged(I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + align16((size_t)w)),
-                        P.W, smem, dred, ured);
-        } else {
-            uint32_t* list = reinterpret_cast<uint32_t*>(smem);
-            const Ctx c = make_ctx(I, P);
-            if (I.scheme == kScalarAdvection) step_ctx_scalar(I, c, list, ured);
-            else if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
-            else step_ctx<kWenoZ>(I, c, list, dred, ured);
+            step_inst(I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + align16((size_t)w)), P.W,
+                      smem, step_smem_bytes(w) <= smem_bytes, reinterpret_cast<uint32_t*>(base + 12 * (size_t)w), dred,
+                      ured);
         }
         __syncthreads();
     }
@@ -914,7 +1150,7 @@ struct Batch1D {
             max_w = std::max(max_w, w);
             I.q_off = (long long)qo;
             I.m_off = (long long)mo;
-            qo += (size_t)12 * w;
+            qo += (size_t)12 * w + (size_t)(w + 32);
             qo = (qo + 31) & ~(size_t)31;
             mo += align16((size_t)w) + (size_t)4 * w;  // mask bytes, then the levels 16-byte aligned
             mo = (mo + 255) & ~(size_t)255;
@@ -973,7 +1209,7 @@ struct Batch1D {
     size_t smem_cap = 227 * 1024;
     size_t smem_bytes() const
     {
-        return std::max(std::min(step_smem_bytes(max_w), smem_cap), sizeof(uint32_t) * (size_t)(max_w + 32));
+        return std::min(step_smem_bytes(max_w), smem_cap);
     }
 
     // Launch shape: threads per CTA and CTAs per SM (0 = as many as fit).
@@ -990,10 +1226,6 @@ struct Batch1D {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) == cudaSuccess && optin > 0)
             smem_cap = (size_t)optin - 1024;  // leave room for the kernel's static shared arrays
-        if (sizeof(uint32_t) * (size_t)(max_w + 32) > smem_cap) {
-            set_last_error("instance too large for the step kernel's shared-memory worklist", __FILE__, __LINE__);
-            return kErrArg;
-        }
         cudaFuncSetAttribute(k_step1d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes());
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step1d, block, smem_bytes());
         if (occ < 1) occ = 1;
@@ -1207,7 +1439,7 @@ __global__ void k_step1d_noalloc(Inst1 param, double* q, uint8_t* state, double*
 {
     extern __shared__ __align__(16) uint8_t smem[];  // step_smem_bytes(w)
     __shared__ double dred[32];
-    __shared__ unsigned ured[128];
+    __shared__ __align__(8) unsigned ured[128];
     Inst1& I = *reinterpret_cast<Inst1*>(scratch);
     if (threadIdx.x == 0) I = param;  // the descriptor is rewritten by every call
     __syncthreads();
@@ -1216,7 +1448,7 @@ __global__ void k_step1d_noalloc(Inst1 param, double* q, uint8_t* state, double*
     double* qt = qc + 3 * w;
     double* fl = qt + 3 * w;
     if (I.t < I.t_end) {
-        step_staged(I, q, qc, qt, fl, state, (int8_t*)(state + w), W, smem, dred, ured);
+        step_inst(I, q, qc, qt, fl, state, (int8_t*)(state + w), W, smem, true, nullptr, dred, ured);
     } else if (threadIdx.x == 0) {
         I.done = 1;
     }
@@ -1539,7 +1771,7 @@ int awcm1d_step_noalloc(int num_levels, int nx_coarse, double x_min, double x_ma
     I.t = t;
     I.t_end = t_end;
     const int w = (int)nx + 2 * kGhost;
-    const size_t smem = step_smem_bytes(w);  // 139 KB at the 8193-point limit
+    const size_t smem = step_smem_bytes(w);  // 172 KB at the 8193-point limit
     AWCM_CUDA_TRY(cudaFuncSetAttribute(k_step1d_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_step1d_noalloc<<<1, 256, smem, (cudaStream_t)stream>>>(I, q_dev, state_dev, scratch, out_dev, make_weights());
     AWCM_CUDA_TRY(cudaGetLastError());
