@@ -78,6 +78,9 @@ def parse():
                     help="profiling mode: K graph-replayed steps, then one eagerly launched step; prints its phases")
     ap.add_argument("--capture-batch", type=int, default=-1,
                     help="profiling mode: the 512-tube batch, K graph-replayed RK3 steps (launches 1..K of k_step1d)")
+    ap.add_argument("--capture-skip", type=int, default=0,
+                    help="with --capture-batch: S steps before the K (k_step1d launches S+1..S+K; at S = 24000 only "
+                         "the four slowest Jmax-13 tubes are still running)")
     return ap.parse_args()
 
 
@@ -738,18 +741,23 @@ def run_capture(k: int):
     print(json.dumps(s.profile_step(w["tol"], w["cfl"], t, w["t_end"])))
 
 
-def run_capture_batch(k: int):
-    """Small, self-ending run for ncu: the seeded 512-tube batch at 384 threads per CTA, k RK3 steps
-    (each one k_step1d launch), then its totals."""
+def run_capture_batch(k: int, skip: int = 0):
+    """Small, self-ending run for ncu: the seeded 512-tube batch at 384 threads per CTA, `skip` RK3
+    steps, then k more (each step one k_step1d launch), then its totals and the running instances."""
     import awcm
     from awcm import workloads
 
     b = workloads.make_batch(awcm, workloads.shock_tubes(BATCHED["instances"]))
     b.set_launch(384, 0)
     b.set_run(BATCHED["tol"], BATCHED["cfl"], 0.0, BATCHED["t_end"])
+    if skip:
+        b.steps(skip)
+        b.sync()
+    live = [i for i in range(b.n) if b.status(i)[3] == 0]
     b.steps(k)
     b.sync()
-    print(json.dumps({"steps": k, "totals": b.totals().tolist()}))
+    print(json.dumps({"skip": skip, "steps": k, "running_before": len(live), "running": live[:16],
+                      "totals": b.totals().tolist()}))
 
 
 def main():
@@ -758,7 +766,7 @@ def main():
         run_capture(args.capture)
         return
     if args.capture_batch >= 0:
-        run_capture_batch(args.capture_batch)
+        run_capture_batch(args.capture_batch, args.capture_skip)
         return
     if args.impl == "reference":
         run_reference_arm(args)
