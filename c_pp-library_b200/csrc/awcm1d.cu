@@ -926,12 +926,34 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 // The stage worklists of an instance of w ghosted points: faces, then finest and coarse points.
 __host__ __device__ __forceinline__ size_t list_bytes(int w) { return sizeof(uint32_t) * 2 * (size_t)(w + 32); }
 
-// Shared memory of the step kernel for an instance of w ghosted points: mask bytes, the four level
-// planes and the density plane staged for the step, and the worklists of the stages.
-__host__ __device__ __forceinline__ size_t step_smem_bytes(int w)
+// What a step keeps in the CTA's shared memory (the rest stays in the instance's global buffers):
+// kStageAll: mask bytes, the four level planes, the three conserved planes and the worklists;
+// kStagePlanes: mask bytes and the three conserved planes (levels and worklists global, for an
+// instance too large for kStageAll: a Jmax-13 tube needs 205 KB this way against 303 KB);
+// kStageDensity: mask bytes, levels, the density plane and the worklists (the scalar path stages
+// no plane); kStageNone: nothing.
+enum StageLayout : int { kStageNone = 0, kStageDensity = 1, kStagePlanes = 2, kStageAll = 3 };
+__host__ __device__ __forceinline__ size_t stage_bytes(int layout, int w)
 {
-    return align16((size_t)w) + align16((size_t)4 * w) + sizeof(double) * (size_t)w + list_bytes(w);
+    const size_t m = align16((size_t)w), l = align16((size_t)4 * w), d = sizeof(double) * (size_t)w;
+    switch (layout) {
+        case kStageAll: return m + l + 3 * d + list_bytes(w);
+        case kStagePlanes: return m + 3 * d;
+        case kStageDensity: return m + l + d + list_bytes(w);
+        default: return 0;
+    }
 }
+// The fullest layout that fits `avail` bytes; pool_lists: the instance has worklist space in the
+// pool (the batch; the allocation-free step has none).
+__host__ __device__ __forceinline__ int pick_layout(int w, size_t avail, bool scalar, bool pool_lists)
+{
+    if (!scalar && stage_bytes(kStageAll, w) <= avail) return kStageAll;
+    if (!scalar && pool_lists && stage_bytes(kStagePlanes, w) <= avail) return kStagePlanes;
+    if (stage_bytes(kStageDensity, w) <= avail) return kStageDensity;
+    return kStageNone;
+}
+// Shared memory of the allocation-free step (kStageDensity).
+__host__ __device__ __forceinline__ size_t step_smem_bytes(int w) { return stage_bytes(kStageDensity, w); }
 
 // Copy of n bytes by all threads of the block; 16-byte words where both ends allow it.
 __device__ __forceinline__ void block_copy_bytes(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, int n)
@@ -958,42 +980,59 @@ __device__ __forceinline__ void block_copy_doubles(double* __restrict__ dst, con
     for (int t = head + threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
 }
 
-// One RK3 step of an instance.  staged: its mask bytes, levels and density plane are copied into
-// the CTA's shared memory (smem: step_smem_bytes(w) bytes) and the ~100 level-sequential mask and
-// transform phases of PrepareEuler and the stage worklists run there, with one global round trip
-// in and one out per step; otherwise the step runs on the global buffers with its worklists at
-// glist.  q: the three conserved planes (global); qc, qt, fl: stage-start copy, coarse
-// derivatives, face fluxes; mg: w mask bytes, lg: four planes of w levels (global).  One call
-// site for both forms keeps the step kernel's code to one copy of each scheme.
+// One RK3 step of an instance, with the part of its state that `layout` names staged in the CTA's
+// shared memory (smem: stage_bytes(layout, w) bytes): the ~100 level-sequential mask and transform
+// phases of PrepareEuler and the stages then run on shared memory, with one global round trip in
+// and one out per step.  q: the three conserved planes (global); qc, qt, fl: stage-start copy,
+// coarse derivatives, face fluxes; mg: w mask bytes, lg: four planes of w levels (global); glist:
+// worklist space in the pool (layouts that keep the worklists global).  One call site for every
+// layout keeps the step kernel's code to one copy of each scheme.
 __device__ void step_inst(Inst1& I, double* q, double* qc, double* qt, double* fl, uint8_t* mg, int8_t* lg,
-                          const Weights& W, uint8_t* smem, bool staged, uint32_t* glist, double* dred, unsigned* ured)
+                          const Weights& W, uint8_t* smem, int layout, uint32_t* glist, double* dred, unsigned* ured)
 {
     const int w = I.nx + 2 * kGhost;
     // the scalar path reads and writes its field planes directly; only its masks are staged
     const bool scalar = I.scheme == kScalarAdvection;
+    const bool st_lv = layout == kStageDensity || layout == kStageAll;
+    const bool st_q0 = layout == kStageDensity && !scalar;
+    const bool st_q = layout == kStagePlanes || layout == kStageAll;
     uint8_t* ms = mg;
     int8_t* ls = lg;
-    double* q0 = q;
+    double* qp = q;   // plane p at qp + p w
+    double* q0 = q;   // plane 0
     uint32_t* list = glist;
-    if (staged) {
-        ms = smem;
-        ls = reinterpret_cast<int8_t*>(smem + align16((size_t)w));
-        double* q0s = reinterpret_cast<double*>(smem + align16((size_t)w) + align16((size_t)4 * w));
-        list = reinterpret_cast<uint32_t*>(q0s + w);
-        if (!scalar) q0 = q0s;
+    if (layout != kStageNone) {
+        uint8_t* p = smem;
+        ms = p;
+        p += align16((size_t)w);
+        if (st_lv) {
+            ls = reinterpret_cast<int8_t*>(p);
+            p += align16((size_t)4 * w);
+        }
+        if (layout == kStageDensity) {
+            if (st_q0) q0 = reinterpret_cast<double*>(p);
+            p += sizeof(double) * (size_t)w;
+        }
+        if (st_q) {
+            qp = q0 = reinterpret_cast<double*>(p);
+            p += 3 * sizeof(double) * (size_t)w;
+        }
+        if (st_lv) list = reinterpret_cast<uint32_t*>(p);
         block_copy_bytes(ms, mg, w);
-        block_copy_bytes(reinterpret_cast<uint8_t*>(ls), reinterpret_cast<const uint8_t*>(lg), 4 * w);
-        if (!scalar) block_copy_doubles(q0s, q, w);
+        if (st_lv) block_copy_bytes(reinterpret_cast<uint8_t*>(ls), reinterpret_cast<const uint8_t*>(lg), 4 * w);
+        if (st_q0) block_copy_doubles(q0, q, w);
+        if (st_q) block_copy_doubles(qp, q, 3 * w);
         __syncthreads();
     }
-    const Ctx c{I, q, qc, qt, fl, ms, ls, W, w, I.nx, I.nx - 1, I.maxl, q0};
+    const Ctx c{I, qp, qc, qt, fl, ms, ls, W, w, I.nx, I.nx - 1, I.maxl, q0};
     if (scalar) step_ctx_scalar(I, c, list, ured);
     else if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
     else step_ctx<kWenoZ>(I, c, list, dred, ured);
-    if (staged) {
+    if (layout != kStageNone) {
         block_copy_bytes(mg, ms, w);
-        block_copy_bytes(reinterpret_cast<uint8_t*>(lg), reinterpret_cast<const uint8_t*>(ls), 4 * w);
-        if (!scalar) block_copy_doubles(q, q0, w);
+        if (st_lv) block_copy_bytes(reinterpret_cast<uint8_t*>(lg), reinterpret_cast<const uint8_t*>(ls), 4 * w);
+        if (st_q0) block_copy_doubles(q, q0, w);
+        if (st_q) block_copy_doubles(q, qp, 3 * w);
         __syncthreads();
     }
 }
@@ -1032,8 +1071,8 @@ __global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, uns
             double* base = P.q + I.q_off;
             uint8_t* mb = P.m + I.m_off;
             step_inst(I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + align16((size_t)w)), P.W,
-                      smem, step_smem_bytes(w) <= smem_bytes, reinterpret_cast<uint32_t*>(base + 12 * (size_t)w), dred,
-                      ured);
+                      smem, pick_layout(w, smem_bytes, I.scheme == kScalarAdvection, true),
+                      reinterpret_cast<uint32_t*>(base + 12 * (size_t)w), dred, ured);
         }
         __syncthreads();
     }
@@ -1203,13 +1242,16 @@ struct Batch1D {
         return cudaMemcpy(host.data(), d_inst, sizeof(Inst1) * n, cudaMemcpyDeviceToHost);
     }
 
-    // Dynamic shared memory of the step kernel: the staged step of the largest instance when it
-    // fits the per-CTA limit, else the limit (larger instances run unstaged, with only their
-    // worklist, 4 (w + 32) bytes, in shared memory).
+    // Dynamic shared memory of the step kernel: the fullest staging layout of the largest instance
+    // that fits the per-CTA limit, else the limit (the largest instances then run on their global
+    // buffers, the smaller ones still staged).  Smaller instances take the fullest layout that fits.
     size_t smem_cap = 227 * 1024;
     size_t smem_bytes() const
     {
-        return std::min(step_smem_bytes(max_w), smem_cap);
+        const size_t e = stage_bytes(pick_layout(max_w, smem_cap, false, true), max_w);
+        const size_t sc = stage_bytes(pick_layout(max_w, smem_cap, true, true), max_w);
+        const size_t b = std::max(e, sc);
+        return b ? b : smem_cap;
     }
 
     // Launch shape: threads per CTA and CTAs per SM (0 = as many as fit).
@@ -1448,7 +1490,7 @@ __global__ void k_step1d_noalloc(Inst1 param, double* q, uint8_t* state, double*
     double* qt = qc + 3 * w;
     double* fl = qt + 3 * w;
     if (I.t < I.t_end) {
-        step_inst(I, q, qc, qt, fl, state, (int8_t*)(state + w), W, smem, true, nullptr, dred, ured);
+        step_inst(I, q, qc, qt, fl, state, (int8_t*)(state + w), W, smem, kStageDensity, nullptr, dred, ured);
     } else if (threadIdx.x == 0) {
         I.done = 1;
     }
