@@ -742,13 +742,13 @@ def run_capture(k: int):
 
 
 def run_capture_batch(k: int, skip: int = 0):
-    """Small, self-ending run for ncu: the seeded 512-tube batch at 384 threads per CTA, `skip` RK3
+    """Small, self-ending run for ncu: the seeded 512-tube batch at 768 threads per CTA, `skip` RK3
     steps, then k more (each step one k_step1d launch), then its totals and the running instances."""
     import awcm
     from awcm import workloads
 
     b = workloads.make_batch(awcm, workloads.shock_tubes(BATCHED["instances"]))
-    b.set_launch(384, 0)
+    b.set_launch(768, 0)
     b.set_run(BATCHED["tol"], BATCHED["cfl"], 0.0, BATCHED["t_end"])
     if skip:
         b.steps(skip)

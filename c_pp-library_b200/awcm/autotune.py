@@ -1,14 +1,14 @@
 """Launch-shape autotuner of the batched 1D step kernel.
 
-The step kernel runs one instance per CTA; its register footprint (~154 per thread) makes the CTA
-size trade occupancy (CTAs resident per SM, i.e. instances in flight) against per-instance
+The step kernel runs one instance per CTA, with up to 768 threads (85 registers a thread); the CTA
+size trades occupancy (CTAs resident per SM, i.e. instances in flight) against per-instance
 parallelism.  The tuner times a few RK3 steps of the actual batch for each candidate shape on a
 throw-away copy of the batch and keeps the fastest (active-point updates per second)."""
 from __future__ import annotations
 
 import time
 
-CANDIDATES = [(128, 0), (256, 0), (384, 0), (512, 0), (128, 2), (256, 2)]
+CANDIDATES = [(128, 0), (256, 0), (384, 0), (512, 0), (640, 0), (768, 0), (128, 2), (256, 2)]
 
 
 def tune(make_copy, t_end: float, tol: float = 1e-4, cfl: float = 0.5, steps: int = 40, candidates=CANDIDATES):

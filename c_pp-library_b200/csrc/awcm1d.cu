@@ -1050,7 +1050,11 @@ __device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
 // One RK3 step of every queued instance.  CTAs pull queue slots until the queue is exhausted.
 // smem_bytes: the launch's dynamic shared memory; an instance whose staged step does not fit in
 // it runs on its global buffers (its worklists in the pool too).
-__global__ void k_step1d(Inst1* insts, int n, const int* __restrict__ order, unsigned* queue, Pool P,
+// Up to 768 threads per CTA (85 registers a thread, some of the face computation spilled to L1):
+// a CTA advances one instance through ~150 block-barrier phases per step, latency-bound, so more
+// warps per instance pay for the spills (Jmax-13 tail step 0.312 -> 0.255 ms against 384 threads
+// and 162 registers; the batched whole run 3.48e7 -> 4.20e7 updates/s).
+__global__ void __launch_bounds__(768, 1) k_step1d(Inst1* insts, int n, const int* __restrict__ order, unsigned* queue, Pool P,
                          unsigned smem_bytes)
 {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -1228,7 +1232,7 @@ struct Batch1D {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         (void)sms;
-        return set_launch(256, 0);
+        return set_launch(768, 0);
     }
 
     cudaError_t upload_inst()
