@@ -393,7 +393,11 @@ __device__ void ph_cr_rows(const Grid2& g, uint8_t* __restrict__ m, int lev, int
     const int D = g.D(lev), h = D >> 1;
     const unsigned n = rowscan_n(g, lev, 2);
     const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    const unsigned row0 = (unsigned)kGhost * ((unsigned)g.pitch / 4u);
     for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        // on the finest detail level (h = 1) every row is scanned and word t is word t of the
+        // plane's grid rows: test it before decoding its row and column
+        if (h == 1 && !((mp[row0 + t] >> bit) & kLaneBits)) continue;
         int j, i0;
         unsigned wdx;
         const unsigned lanes = rowscan_word(g, lev, 2, t, j, i0, wdx);
@@ -491,7 +495,10 @@ __device__ void ph_interp_rows(const Grid2& g, Field4 q, const uint8_t* __restri
     const int rows = PH == 0 ? 2 : 1;
     const unsigned n = rowscan_n(g, lev, rows);
     const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    const unsigned row0 = (unsigned)kGhost * ((unsigned)g.pitch / 4u);
     for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        // every row of the finest detail level (h = 1, PH 0): word t of the grid rows
+        if (PH == 0 && h == 1 && !((mp[row0 + t] >> kBitInterp) & kLaneBits)) continue;
         int j, i0;
         unsigned wdx;
         const unsigned lanes = rowscan_word(g, lev, rows, t, j, i0, wdx);
@@ -560,10 +567,12 @@ __device__ void ph_aaz(const Grid2& g, uint8_t* m, int bit, int src, Span sp)
     const unsigned* mp = reinterpret_cast<const unsigned*>(m);
     const unsigned nw = plane_words(g);
     for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const unsigned v = mp[w];
+        if (!((v >> src) & kLaneBits)) continue;  // no detail of `src` in this word
         const MaskWord mw = mask_word(g, w);
         const unsigned G = grid_lanes(g, mw);
         if (!G) continue;
-        unsigned hit = (mp[w] >> src) & lane_bits(G);
+        unsigned hit = (v >> src) & lane_bits(G);
         while (hit) {
             const int L = (__ffs(hit) - 1) >> 3;
             hit &= hit - 1;
@@ -697,8 +706,10 @@ __device__ void ph_cl_apd(const Grid2& g, uint8_t* m, int8_t* lvl, int k, size_t
     unsigned* lp = reinterpret_cast<unsigned*>(lvl);
     const unsigned nw = (unsigned)(plane / 4);
     for (unsigned w = sp.t0; w < nw; w += sp.stride) {
-        const MaskWord mw = mask_word(g, w);
         const unsigned v = mp[w];
+        // most words hold no point of mask k-1 and no non-zero level: nothing to write or push
+        if (!((v >> src) & kLaneBits) && !lp[w]) continue;
+        const MaskWord mw = mask_word(g, w);
         const unsigned G = grid_lanes(g, mw);
         unsigned lv = 0;
         if (G) {
@@ -763,11 +774,13 @@ __device__ void ph_interp_init(const Grid2& g, uint8_t* m, int from, int to, Spa
     unsigned* mp = reinterpret_cast<unsigned*>(m);
     const unsigned nw = plane_words(g);
     for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const unsigned v = mp[w];
+        // no point of `to` and no work bit to clear: the word stays as it is
+        if (to >= 0 && !(((v >> to) | (v >> kBitInterp)) & kLaneBits)) continue;
         const MaskWord mw = mask_word(g, w);
         const unsigned G = grid_lanes(g, mw);
         if (!G) continue;
         const unsigned gb = lane_bits(G);
-        const unsigned v = mp[w];
         const unsigned on = (to >= 0 ? (v >> to) : ~0u) & ~(v >> from) & gb;
         const unsigned nv = (v & ~(gb << kBitInterp)) | (on << kBitInterp);
         if (nv != v) mp[w] = nv;
@@ -781,11 +794,12 @@ __device__ void ph_remove_residue(const Grid2& g, Field4 q, const uint8_t* m, in
     const unsigned* mp = reinterpret_cast<const unsigned*>(m);
     const unsigned nw = plane_words(g);
     for (unsigned w = sp.t0; w < nw; w += sp.stride) {
+        const unsigned v = mp[w];
+        if (!full && !(((v >> 3) | (v >> kBitTemp)) & kLaneBits)) continue;  // nothing non-zero here
         const MaskWord mw = mask_word(g, w);
         if (mw.j < 1 || mw.j > g.ny - 2) continue;
         const unsigned I = lanes_in(mw.i0, 1, g.nx - 2);
         if (!I) continue;
-        const unsigned v = mp[w];
         unsigned hit = ~(v >> bit) & lane_bits(I);
         if (!full) hit &= (v >> 3) | (v >> kBitTemp);
         hit &= kLaneBits;
