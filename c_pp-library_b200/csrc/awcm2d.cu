@@ -172,8 +172,10 @@ __device__ __forceinline__ unsigned band_n(const Grid2& g, int lev, int which)
 // values; phase A computes all three detail sub-bands at once with the d1/d2 results staged in
 // the scratch plane `tb`, and phase B applies the c update (reading d1/d2 from `tb`) and moves the
 // staged details into q.  Same operations on the same operands: identical results.
+// idle: kBitTemp holds the mask0 of the start of the pass (PrepareEuler copies it there first);
+// the d1/d2 points outside it are then left in q instead of going through the staging plane.
 __device__ void ph_fwt_a(const Grid2& g, double* __restrict__ q, double* __restrict__ tb, uint8_t* __restrict__ m,
-                         int lev, double tol, Span sp)
+                         int lev, double tol, bool idle, Span sp)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
     const int which[3] = {2, 0, 1};
@@ -199,6 +201,7 @@ __device__ void ph_fwt_a(const Grid2& g, double* __restrict__ q, double* __restr
             if (absd(v) < tol) m[a] &= (uint8_t)~1u;
             continue;
         }
+        if (idle && !on) continue;  // q[a] stays; ph_fwt_b reads it from q
         double v = q[a];
         if (on) {
             int s0, k;
@@ -217,7 +220,7 @@ __device__ void ph_fwt_a(const Grid2& g, double* __restrict__ q, double* __restr
 }
 
 __device__ void ph_fwt_b(const Grid2& g, double* __restrict__ q, const double* __restrict__ tb,
-                         const uint8_t* __restrict__ m, int lev, Span sp)
+                         const uint8_t* __restrict__ m, int lev, bool idle, Span sp)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
     const int which[3] = {3, 0, 1};
@@ -228,16 +231,19 @@ __device__ void ph_fwt_b(const Grid2& g, double* __restrict__ q, const double* _
         union_point(g, lev, which, t, i, j, w);
         const size_t a = g.at(i, j);
         if (w != 3) {
-            q[a] = tb[a];
+            if (!idle || ((m[a] >> kBitTemp) & 1u)) q[a] = tb[a];
             continue;
         }
         if (!(m[a] & 1u)) continue;
         int is, k1, js, k2;
         update_stencil(i, D, NX, is, k1);
         update_stencil(j, D, NY, js, k2);
+        // a d1/d2 value: the staged detail of a point of the pass's mask0, else q itself (it is
+        // not written in this pass)
+        auto d12 = [&](size_t b) { return (!idle || ((m[b] >> kBitTemp) & 1u)) ? tb[b] : q[b]; };
         double v = q[a];
-        for (int c = 0; c < 4; ++c) v += tb[g.at(is + c * D, j)] * g.w(c, k1);
-        for (int c = 0; c < 4; ++c) v += tb[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c = 0; c < 4; ++c) v += d12(g.at(is + c * D, j)) * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v += d12(g.at(i, js + c * D)) * g.w(c, k2);
         for (int c2 = 0; c2 < 4; ++c2)
             for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
         q[a] = v;
@@ -819,17 +825,17 @@ __device__ void ph_remove_residue(const Grid2& g, Field4 q, const uint8_t* m, in
 #define AWCM_SKIP_IF_DONE(st) \
     if ((st) && (st)->done) return
 
-__global__ void k_fwt_a(Grid2 g, double* q, double* tb, uint8_t* m, int lev, const StepState* st)
+__global__ void k_fwt_a(Grid2 g, double* q, double* tb, uint8_t* m, int lev, int idle, const StepState* st)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_fwt_a(g, q, tb, m, lev, st->tol, grid_span());
+    ph_fwt_a(g, q, tb, m, lev, st->tol, idle != 0, grid_span());
 }
-__global__ void k_fwt_b(Grid2 g, double* q, const double* tb, const uint8_t* m, int lev, const StepState* st)
+__global__ void k_fwt_b(Grid2 g, double* q, const double* tb, const uint8_t* m, int lev, int idle, const StepState* st)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_fwt_b(g, q, tb, m, lev, grid_span());
+    ph_fwt_b(g, q, tb, m, lev, idle != 0, grid_span());
 }
 template <int PH>
 __global__ void k_iwt(Grid2 g, double* q, const uint8_t* m, int lev, int bit, const StepState* st)
@@ -1000,9 +1006,9 @@ __global__ void __launch_bounds__(kPrepThreads, 1) k_prepare(PrepArgs A)
     ph_copy_bit_all(A.m, A.plane, 0, kBitTemp, sp);
     SYNC_OR_LEAVE;
     for (int lev = g.maxl - 1; lev >= 0; --lev) {
-        ph_fwt_a(g, A.q.p[0], A.tb, A.m, lev, tol, sp);
+        ph_fwt_a(g, A.q.p[0], A.tb, A.m, lev, tol, true, sp);
         SYNC_OR_LEAVE;
-        ph_fwt_b(g, A.q.p[0], A.tb, A.m, lev, sp);
+        ph_fwt_b(g, A.q.p[0], A.tb, A.m, lev, true, sp);
         SYNC_OR_LEAVE;
     }
     ph_band_copy(g, A.m, 0, kBitCopy, sp);
@@ -2369,13 +2375,16 @@ struct Solver2D {
 
     // The forward transform's scratch plane is the first x-face flux plane (faces are not live
     // during PrepareEuler).
-    void enq_fwt(const StepState* s)
+    // idle: kBitTemp holds mask0 (PrepareEuler's first pass copied it), so the points outside it
+    // skip the staging plane.
+    void enq_fwt(const StepState* s, bool idle = false)
     {
+        const int id = idle ? 1 : 0;
         for (int lev = g.maxl - 1; lev >= 0; --lev) {
-            launch(k_fwt_a, pb(details(lev)), 256, g, q.p[0], fx.p[0], m, lev, s);
+            launch(k_fwt_a, pb(details(lev)), 256, g, q.p[0], fx.p[0], m, lev, id, s);
             after("k_fwt_a");
             const long nb = band_count(lev, 3) + band_count(lev, 0) + band_count(lev, 1);
-            launch(k_fwt_b, pb(nb), 256, g, q.p[0], fx.p[0], m, lev, s);
+            launch(k_fwt_b, pb(nb), 256, g, q.p[0], fx.p[0], m, lev, id, s);
             after("k_fwt_b");
             launches += 2;
         }
@@ -2497,7 +2506,7 @@ struct Solver2D {
         if (!scalar) launch(k_copy_bit_all, pb(words()), 256, m, plane, 0, kBitTemp, s, kMask123);
         after("k_copy_bit_all");
         launches += 1;
-        enq_fwt(s);
+        enq_fwt(s, !scalar);
         launch(k_band_copy, pb(words()), 256, g, m, 0, kBitCopy, s);
         after("k_band_copy");
         launch(k_aaz, pb(words()), 256, g, m, 0, kBitCopy, s);
