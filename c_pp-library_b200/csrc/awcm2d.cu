@@ -252,8 +252,11 @@ __device__ void ph_fwt_b(const Grid2& g, double* __restrict__ q, const double* _
 
 // Inverse transform, one phase of one level (InverseWaveletTransformationEuler, WAVELET_2D.h:626-782):
 // PH 0 = c, PH 1 = d2 and d1, PH 2 = d3; points outside the mask get density 0.
+// zero_all false: the density outside mask_temp (the step's starting mask0) is zero already (the
+// previous step's residue removal), so only the points of mask_temp outside `bit` are zeroed.
 template <int PH>
-__device__ void ph_iwt(const Grid2& g, double* __restrict__ q, const uint8_t* __restrict__ m, int lev, int bit, Span sp)
+__device__ void ph_iwt(const Grid2& g, double* __restrict__ q, const uint8_t* __restrict__ m, int lev, int bit,
+                       bool zero_all, Span sp)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
     const int D = g.D(lev);
@@ -275,7 +278,7 @@ __device__ void ph_iwt(const Grid2& g, double* __restrict__ q, const uint8_t* __
         }
         const size_t a = g.at(i, j);
         if (!((m[a] >> bit) & 1u)) {
-            q[a] = 0;
+            if (zero_all || ((m[a] >> kBitTemp) & 1u)) q[a] = 0;
             continue;
         }
         if (w == 3) {
@@ -838,11 +841,11 @@ __global__ void k_fwt_b(Grid2 g, double* q, const double* tb, const uint8_t* m, 
     ph_fwt_b(g, q, tb, m, lev, idle != 0, grid_span());
 }
 template <int PH>
-__global__ void k_iwt(Grid2 g, double* q, const uint8_t* m, int lev, int bit, const StepState* st)
+__global__ void k_iwt(Grid2 g, double* q, const uint8_t* m, int lev, int bit, int sparse, const StepState* st)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_iwt<PH>(g, q, m, lev, bit, grid_span());
+    ph_iwt<PH>(g, q, m, lev, bit, !sparse || !st || st->full_zero, grid_span());
 }
 __global__ void k_cr(Grid2 g, uint8_t* m, int lev, int bit, const StepState* st)
 {
@@ -909,13 +912,14 @@ __global__ void k_cl_apd(Grid2 g, uint8_t* m, int8_t* lvl, int k, size_t plane, 
 }
 // The coarsest level's first inverse-transform phase (CTAs [0, nb)) and the interpolation work mask
 // `to` minus `from` (the other CTAs) in one launch: the mask pass rewrites only the work bit.
-__global__ void k_iwt0_interp_init(Grid2 g, double* q, uint8_t* m, int lev, int to, int from, const StepState* st,
-                                   unsigned nb)
+__global__ void k_iwt0_interp_init(Grid2 g, double* q, uint8_t* m, int lev, int to, int from, int sparse,
+                                   const StepState* st, unsigned nb)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
     if (blockIdx.x < nb)
-        ph_iwt<0>(g, q, m, lev, to, Span{blockIdx.x * blockDim.x + threadIdx.x, nb * blockDim.x});
+        ph_iwt<0>(g, q, m, lev, to, !sparse || !st || st->full_zero,
+                  Span{blockIdx.x * blockDim.x + threadIdx.x, nb * blockDim.x});
     else
         ph_interp_init(g, m, from, to, Span{(blockIdx.x - nb) * blockDim.x + threadIdx.x, (gridDim.x - nb) * blockDim.x});
 }
@@ -1030,11 +1034,11 @@ __global__ void __launch_bounds__(kPrepThreads, 1) k_prepare(PrepArgs A)
         }
     }
     for (int lev = 0; lev < g.maxl; ++lev) {
-        ph_iwt<0>(g, A.q.p[0], A.m, lev, 3, sp);
+        ph_iwt<0>(g, A.q.p[0], A.m, lev, 3, A.st->full_zero != 0, sp);
         SYNC_OR_LEAVE;
-        ph_iwt<1>(g, A.q.p[0], A.m, lev, 3, sp);
+        ph_iwt<1>(g, A.q.p[0], A.m, lev, 3, A.st->full_zero != 0, sp);
         SYNC_OR_LEAVE;
-        ph_iwt<2>(g, A.q.p[0], A.m, lev, 3, sp);
+        ph_iwt<2>(g, A.q.p[0], A.m, lev, 3, A.st->full_zero != 0, sp);
         SYNC_OR_LEAVE;
     }
     ph_interp_init(g, A.m, kBitTemp, 3, sp);
@@ -2329,8 +2333,9 @@ struct Solver2D {
 
     void mark_full_zero()
     {
-        // After an external write the sparse residue removal's invariant (values only inside
-        // mask3 or the previous mask0) is not known to hold: the next step zeroes densely.
+        // After an external write (or a frozen run) the invariant of the sparse residue removal and
+        // of the sparse inverse-transform zeroing (values only inside mask3 or the previous mask0)
+        // is not known to hold: the next step zeroes densely.
         const int one = 1;
         cudaMemcpyAsync(&st->full_zero, &one, sizeof(int), cudaMemcpyHostToDevice, stream);
     }
@@ -2392,21 +2397,23 @@ struct Solver2D {
 
     // init_from >= 0: the first launch also builds the work mask of the interpolation that follows
     // (ph_interp_init from init_from to bit), which the inverse transform does not read.
-    void enq_iwt(int bit, const StepState* s, int init_from = -1)
+    // sparse: in PrepareEuler (mask_temp = the starting mask0), see ph_iwt.
+    void enq_iwt(int bit, const StepState* s, int init_from = -1, bool sparse = false)
     {
+        const int sp = sparse ? 1 : 0;
         for (int lev = 0; lev < g.maxl; ++lev) {
             const Band b3 = band_of(g, lev, 2), b1 = band_of(g, lev, 0), b2 = band_of(g, lev, 1), bc = band_of(g, lev, 3);
             if (lev == 0 && init_from >= 0) {
                 const unsigned nb = pb((long)bc.cx * bc.cy);
-                launch(k_iwt0_interp_init, nb + pb(words()), 256, g, q.p[0], m, lev, bit, init_from, s, nb);
+                launch(k_iwt0_interp_init, nb + pb(words()), 256, g, q.p[0], m, lev, bit, init_from, sp, s, nb);
                 after("k_iwt0_interp_init");
             } else {
-                launch(k_iwt<0>, pb((long)bc.cx * bc.cy), 256, g, q.p[0], m, lev, bit, s);
+                launch(k_iwt<0>, pb((long)bc.cx * bc.cy), 256, g, q.p[0], m, lev, bit, sp, s);
                 after("k_iwt<0>");
             }
-            launch(k_iwt<1>, pb((long)b1.cx * b1.cy + (long)b2.cx * b2.cy), 256, g, q.p[0], m, lev, bit, s);
+            launch(k_iwt<1>, pb((long)b1.cx * b1.cy + (long)b2.cx * b2.cy), 256, g, q.p[0], m, lev, bit, sp, s);
             after("k_iwt<1>");
-            launch(k_iwt<2>, pb((long)b3.cx * b3.cy), 256, g, q.p[0], m, lev, bit, s);
+            launch(k_iwt<2>, pb((long)b3.cx * b3.cy), 256, g, q.p[0], m, lev, bit, sp, s);
             after("k_iwt<2>");
             launches += 3;
         }
@@ -2532,7 +2539,7 @@ struct Solver2D {
             enq_iwt(3, s);
             if (lists) enq_lists(0);
         } else if (!fork_ok()) {
-            enq_iwt(3, s, kBitTemp);
+            enq_iwt(3, s, kBitTemp, true);
             enq_interp(kBitTemp, 3, s, 1, true);
             if (lists) enq_lists(0);
         } else {
@@ -2550,7 +2557,7 @@ struct Solver2D {
                 enq_lists(0);
             }
             cur = nullptr;
-            enq_iwt(3, s);
+            enq_iwt(3, s, -1, true);
             join(side, ev_join);
             if (lists) join(side2, ev_join2);
         }
@@ -2970,6 +2977,7 @@ struct Solver2D {
         if (rc) return rc;
         launch(k_begin, 1, 1, st, 0);
         enq_fwt(st);
+        mark_full_zero();  // standalone passes: the next step zeroes densely
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
@@ -2980,6 +2988,7 @@ struct Solver2D {
     int iwt(int mask_id)
     {
         enq_iwt(bit_of(mask_id), nullptr);
+        mark_full_zero();
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
@@ -2988,6 +2997,7 @@ struct Solver2D {
     int interpolate(int from_id, int to_id)
     {
         enq_interp(bit_of(from_id), bit_of(to_id), nullptr);
+        mark_full_zero();
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
@@ -3049,6 +3059,7 @@ struct Solver2D {
     {
         const int b = bit_of(mask_id);
         if (level_id < 0 || level_id > 3) return kErrArg;
+        mark_full_zero();
         switch (op) {
             case 0: enq_aaz(b, nullptr); break;
             case 1: enq_cr(b, nullptr); break;
@@ -3082,6 +3093,7 @@ struct Solver2D {
             launch(k_wt_bottom_y, blocks_for(3L * (g.nx - 1 + kGhost - g.wt_i + 1), 256), 256, g, q, 1,
                    (const StepState*)nullptr);
         }
+        mark_full_zero();  // writes interior (solid) cells
         AWCM_CUDA_TRY(cudaGetLastError());
         AWCM_CUDA_TRY(cudaStreamSynchronize(stream));
         return kOk;
@@ -3274,6 +3286,8 @@ struct Solver2D {
         cudaEventDestroy(e1);
         StepState h;
         if ((rc = read_state(&h))) return rc;
+        // frozen steps leave values outside mask0 (no residue removal)
+        mark_full_zero();
         if (out) {
             out[0] = h.t;
             out[1] = ms;
@@ -3398,6 +3412,7 @@ struct Solver2D {
             out[4] = (double)((keep_all ? 0 : n_seg) + 3 * every + 5) * 4 * plane * sizeof(double) +
                      (double)n * tape_stride() * sizeof(double);
         }
+        mark_full_zero();  // the frozen forward leaves values outside mask0
         return kOk;
     }
 
