@@ -186,7 +186,7 @@ class AWCM2D:
         return [(raw[32 * k:32 * k + 32].split(b"\0")[0].decode(), float(ms[k])) for k in range(n.value)]
 
     def set_prepare_mode(self, mode: int):
-        """0: persistent cooperative prepare kernel (default); 1: one launch per pass."""
+        """0: persistent cooperative prepare kernel; 1: one launch per pass (the default)."""
         call("awcm2d_set_prepare_mode", self.h, mode)
 
     def set_spin_limit(self, polls: int):

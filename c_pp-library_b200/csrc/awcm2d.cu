@@ -123,6 +123,31 @@ __device__ __forceinline__ bool union_point(const Grid2& g, int lev, const int (
 // test the word's bits of interest at once and skip empty words, which is most of them.
 constexpr unsigned kLaneBits = 0x01010101u;  // bit 0 of each of the four bytes
 
+// Pushes onto points that lie on the ghosted plane by construction (no bounds test).
+__device__ __forceinline__ void push_bit_in(const Grid2& g, uint8_t* m, int i, int j, int bit)
+{
+    const size_t a = g.at(i, j);
+    atomicOr(reinterpret_cast<unsigned*>(m + (a & ~(size_t)3)), 1u << (8 * (unsigned)(a & 3) + bit));
+}
+// `bit` onto the n points i0, i0 + s, .., i0 + (n-1) s of row j (s = 1 or 2, span at most 8 bytes,
+// all on the ghosted plane): one atomicOr per 32-bit word they touch, its lane mask built by shifts.
+__device__ __forceinline__ void push_run(const Grid2& g, uint8_t* m, int i0, int n, int s, int j, int bit)
+{
+    const size_t a0 = g.at(i0, j), a1 = a0 + (size_t)((n - 1) * s);
+    unsigned* w = reinterpret_cast<unsigned*>(m + (a0 & ~(size_t)3));
+    const unsigned lanes = (s == 1 ? kLaneBits : ((a0 & 1) ? 0x01000100u : 0x00010001u)) << bit;
+    const unsigned head = lanes & (0xFFFFFFFFu << (8u * (unsigned)(a0 & 3)));         // bytes >= a0's
+    const unsigned tail = lanes & (0xFFFFFFFFu >> (8u * (3u - (unsigned)(a1 & 3))));  // bytes <= a1's
+    const int nw = (int)((a1 >> 2) - (a0 >> 2));
+    if (nw == 0) {
+        atomicOr(w, head & tail);
+        return;
+    }
+    atomicOr(w, head);
+    if (nw == 2) atomicOr(w + 1, lanes);
+    atomicOr(w + nw, tail);
+}
+
 struct MaskWord {
     unsigned w;  // word index; bytes 4w .. 4w+3 of the plane
     int i0, j;   // grid coordinates of byte 0 (ghosts negative / beyond the grid)
@@ -324,23 +349,31 @@ __device__ void ph_iwt(const Grid2& g, double* __restrict__ q, const uint8_t* __
 // d3 -> d1 -> d2 so that d1/d2 points switched on by a d3 point also mark their stencils; those
 // stencils ((is..is+3D, n) for a d1 point (i, n), (m, js..js+3D) for a d2 point (m, j)) lie inside
 // the d3 point's own 4x4 block of marks, so all three sub-bands can run concurrently.
+// The stencil points lie in [0, NX] x [0, NY] (predict_stencil clamps them), so the pushes need no
+// bounds test; at spacing D = 2 the four points of a row span 7 bytes and go in 2-3 word ORs.
 __device__ __forceinline__ void cr_push(const Grid2& g, uint8_t* m, int i, int j, int D, int w, int bit)
 {
     const int NX = g.nx - 1, NY = g.ny - 1;
     int is, js, k;
+    auto row4 = [&](int jr) {
+        if (D == 2) {
+            push_run(g, m, is, 4, 2, jr, bit);
+        } else {
+            for (int c = 0; c < 4; ++c) push_bit_in(g, m, is + c * D, jr, bit);
+        }
+    };
     if (w == 2) {
         predict_stencil(i, D, NX, is, k);
         predict_stencil(j, D, NY, js, k);
-        for (int c = 0; c < 4; ++c) push_bit(g, m, is + c * D, j, bit);
-        for (int c = 0; c < 4; ++c) push_bit(g, m, i, js + c * D, bit);
-        for (int c2 = 0; c2 < 4; ++c2)
-            for (int c1 = 0; c1 < 4; ++c1) push_bit(g, m, is + c1 * D, js + c2 * D, bit);
+        row4(j);
+        for (int c = 0; c < 4; ++c) push_bit_in(g, m, i, js + c * D, bit);
+        for (int c2 = 0; c2 < 4; ++c2) row4(js + c2 * D);
     } else if (w == 0) {
         predict_stencil(i, D, NX, is, k);
-        for (int c = 0; c < 4; ++c) push_bit(g, m, is + c * D, j, bit);
+        row4(j);
     } else {
         predict_stencil(j, D, NY, js, k);
-        for (int c = 0; c < 4; ++c) push_bit(g, m, i, js + c * D, bit);
+        for (int c = 0; c < 4; ++c) push_bit_in(g, m, i, js + c * D, bit);
     }
 }
 
@@ -757,10 +790,10 @@ __device__ void ph_cl_apd(const Grid2& g, uint8_t* m, int8_t* lvl, int k, size_t
             const int i = mw.i0 + L, j = mw.j;
             const int lev = (int)(int8_t)(uint8_t)(lv >> (8 * L));
             if (lev == g.maxl) {
-                for (int c = -3; c <= 3; ++c) {
-                    push_bit(g, m, i + c, j, k);
-                    push_bit(g, m, i, j + c, k);
-                }
+                // i, j in [1, N-1]: the cross i-3..i+3, j-3..j+3 lies on the ghosted plane
+                push_run(g, m, i - 3, 7, 1, j, k);
+                for (int c = -3; c <= 3; ++c)
+                    if (c) push_bit_in(g, m, i, j + c, k);
                 continue;
             }
             const int D = g.D(lev);
