@@ -199,10 +199,49 @@ __device__ __forceinline__ unsigned band_n(const Grid2& g, int lev, int which)
 // staged details into q.  Same operations on the same operands: identical results.
 // idle: kBitTemp holds the mask0 of the start of the pass (PrepareEuler copies it there first);
 // the d1/d2 points outside it are then left in q instead of going through the staging plane.
+// Forward predict of one detail point of a level (w: 2 = d3 into q, 0/1 = d1/d2 into the staging
+// plane tb); on: the point is in mask0 (its detail is computed and thresholded).
+__device__ __forceinline__ void fwt_a_point(const Grid2& g, double* __restrict__ q, double* __restrict__ tb,
+                                            uint8_t* __restrict__ m, int i, int j, size_t a, int D, int w, double tol,
+                                            bool on)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    if (w == 2) {
+        if (!on) return;
+        int is, k1, js, k2;
+        predict_stencil(i, D, NX, is, k1);
+        predict_stencil(j, D, NY, js, k2);
+        double v = q[a];
+        for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+        v *= 0.25;
+        q[a] = v;
+        if (absd(v) < tol) m[a] &= (uint8_t)~1u;
+        return;
+    }
+    double v = q[a];
+    if (on) {
+        int s0, k;
+        if (w == 0) {
+            predict_stencil(i, D, NX, s0, k);
+            for (int c = 0; c < 4; ++c) v -= q[g.at(s0 + c * D, j)] * g.w(c, k);
+        } else {
+            predict_stencil(j, D, NY, s0, k);
+            for (int c = 0; c < 4; ++c) v -= q[g.at(i, s0 + c * D)] * g.w(c, k);
+        }
+        v *= 0.5;
+        if (absd(v) < tol) m[a] &= (uint8_t)~1u;
+    }
+    tb[a] = v;
+}
+
+// idle: kBitTemp holds the mask0 of the start of the pass (PrepareEuler copies it there first);
+// the d1/d2 points outside it are then left in q instead of going through the staging plane.
 __device__ void ph_fwt_a(const Grid2& g, double* __restrict__ q, double* __restrict__ tb, uint8_t* __restrict__ m,
                          int lev, double tol, bool idle, Span sp)
 {
-    const int NX = g.nx - 1, NY = g.ny - 1;
     const int which[3] = {2, 0, 1};
     const unsigned n = band_n(g, lev, 0) + band_n(g, lev, 1) + band_n(g, lev, 2);
     const int D = g.D(lev);
@@ -211,43 +250,32 @@ __device__ void ph_fwt_a(const Grid2& g, double* __restrict__ q, double* __restr
         union_point(g, lev, which, t, i, j, w);
         const size_t a = g.at(i, j);
         const bool on = m[a] & 1u;
-        if (w == 2) {
-            if (!on) continue;
-            int is, k1, js, k2;
-            predict_stencil(i, D, NX, is, k1);
-            predict_stencil(j, D, NY, js, k2);
-            double v = q[a];
-            for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
-            for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
-            for (int c2 = 0; c2 < 4; ++c2)
-                for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-            v *= 0.25;
-            q[a] = v;
-            if (absd(v) < tol) m[a] &= (uint8_t)~1u;
-            continue;
-        }
-        if (idle && !on) continue;  // q[a] stays; ph_fwt_b reads it from q
-        double v = q[a];
-        if (on) {
-            int s0, k;
-            if (w == 0) {
-                predict_stencil(i, D, NX, s0, k);
-                for (int c = 0; c < 4; ++c) v -= q[g.at(s0 + c * D, j)] * g.w(c, k);
-            } else {
-                predict_stencil(j, D, NY, s0, k);
-                for (int c = 0; c < 4; ++c) v -= q[g.at(i, s0 + c * D)] * g.w(c, k);
-            }
-            v *= 0.5;
-            if (absd(v) < tol) m[a] &= (uint8_t)~1u;
-        }
-        tb[a] = v;
+        if (idle && !on) continue;  // d1/d2: q[a] stays, ph_fwt_b reads it from q; d3: nothing to do
+        fwt_a_point(g, q, tb, m, i, j, a, D, w, tol, on);
     }
+}
+
+// Forward update of one c point of mask0 (the d1/d2 neighbours: the staged detail of a point of the
+// pass's mask0, else q itself, which this pass does not write; without idle all come from tb).
+__device__ __forceinline__ void fwt_b_point(const Grid2& g, double* __restrict__ q, const double* __restrict__ tb,
+                                            const uint8_t* __restrict__ m, int i, int j, size_t a, int D, bool idle)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    int is, k1, js, k2;
+    update_stencil(i, D, NX, is, k1);
+    update_stencil(j, D, NY, js, k2);
+    auto d12 = [&](size_t b) { return (!idle || ((m[b] >> kBitTemp) & 1u)) ? tb[b] : q[b]; };
+    double v = q[a];
+    for (int c = 0; c < 4; ++c) v += d12(g.at(is + c * D, j)) * g.w(c, k1);
+    for (int c = 0; c < 4; ++c) v += d12(g.at(i, js + c * D)) * g.w(c, k2);
+    for (int c2 = 0; c2 < 4; ++c2)
+        for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+    q[a] = v;
 }
 
 __device__ void ph_fwt_b(const Grid2& g, double* __restrict__ q, const double* __restrict__ tb,
                          const uint8_t* __restrict__ m, int lev, bool idle, Span sp)
 {
-    const int NX = g.nx - 1, NY = g.ny - 1;
     const int which[3] = {3, 0, 1};
     const unsigned n = band_n(g, lev, 3) + band_n(g, lev, 0) + band_n(g, lev, 1);
     const int D = g.D(lev);
@@ -260,18 +288,7 @@ __device__ void ph_fwt_b(const Grid2& g, double* __restrict__ q, const double* _
             continue;
         }
         if (!(m[a] & 1u)) continue;
-        int is, k1, js, k2;
-        update_stencil(i, D, NX, is, k1);
-        update_stencil(j, D, NY, js, k2);
-        // a d1/d2 value: the staged detail of a point of the pass's mask0, else q itself (it is
-        // not written in this pass)
-        auto d12 = [&](size_t b) { return (!idle || ((m[b] >> kBitTemp) & 1u)) ? tb[b] : q[b]; };
-        double v = q[a];
-        for (int c = 0; c < 4; ++c) v += d12(g.at(is + c * D, j)) * g.w(c, k1);
-        for (int c = 0; c < 4; ++c) v += d12(g.at(i, js + c * D)) * g.w(c, k2);
-        for (int c2 = 0; c2 < 4; ++c2)
-            for (int c1 = 0; c1 < 4; ++c1) v += q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-        q[a] = v;
+        fwt_b_point(g, q, tb, m, i, j, a, D, idle);
     }
 }
 
@@ -279,11 +296,52 @@ __device__ void ph_fwt_b(const Grid2& g, double* __restrict__ q, const double* _
 // PH 0 = c, PH 1 = d2 and d1, PH 2 = d3; points outside the mask get density 0.
 // zero_all false: the density outside mask_temp (the step's starting mask0) is zero already (the
 // previous step's residue removal), so only the points of mask_temp outside `bit` are zeroed.
+// Inverse transform of one point of the mask (w: 3 = c update, 1 = d2, 0 = d1, 2 = d3 predict).
+__device__ __forceinline__ void iwt_point(const Grid2& g, double* __restrict__ q, int i, int j, size_t a, int D, int w)
+{
+    const int NX = g.nx - 1, NY = g.ny - 1;
+    if (w == 3) {
+        int is, k1, js, k2;
+        update_stencil(i, D, NX, is, k1);
+        update_stencil(j, D, NY, js, k2);
+        double v = q[a];
+        for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+        q[a] = v;
+    } else if (w == 1) {
+        int s0, k;
+        predict_stencil(j, D, NY, s0, k);
+        double v = q[a];
+        v *= 2.0;
+        for (int c = 0; c < 4; ++c) v += q[g.at(i, s0 + c * D)] * g.w(c, k);
+        q[a] = v;
+    } else if (w == 0) {
+        int s0, k;
+        predict_stencil(i, D, NX, s0, k);
+        double v = q[a];
+        v *= 2.0;
+        for (int c = 0; c < 4; ++c) v += q[g.at(s0 + c * D, j)] * g.w(c, k);
+        q[a] = v;
+    } else {
+        int is, k1, js, k2;
+        predict_stencil(i, D, NX, is, k1);
+        predict_stencil(j, D, NY, js, k2);
+        double v = q[a];
+        v *= 4.0;
+        for (int c = 0; c < 4; ++c) v += q[g.at(is + c * D, j)] * g.w(c, k1);
+        for (int c = 0; c < 4; ++c) v += q[g.at(i, js + c * D)] * g.w(c, k2);
+        for (int c2 = 0; c2 < 4; ++c2)
+            for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
+        q[a] = v;
+    }
+}
+
 template <int PH>
 __device__ void ph_iwt(const Grid2& g, double* __restrict__ q, const uint8_t* __restrict__ m, int lev, int bit,
                        bool zero_all, Span sp)
 {
-    const int NX = g.nx - 1, NY = g.ny - 1;
     const int D = g.D(lev);
     unsigned n;
     if (PH == 0) n = band_n(g, lev, 3);
@@ -306,43 +364,74 @@ __device__ void ph_iwt(const Grid2& g, double* __restrict__ q, const uint8_t* __
             if (zero_all || ((m[a] >> kBitTemp) & 1u)) q[a] = 0;
             continue;
         }
-        if (w == 3) {
-            int is, k1, js, k2;
-            update_stencil(i, D, NX, is, k1);
-            update_stencil(j, D, NY, js, k2);
-            double v = q[a];
-            for (int c = 0; c < 4; ++c) v -= q[g.at(is + c * D, j)] * g.w(c, k1);
-            for (int c = 0; c < 4; ++c) v -= q[g.at(i, js + c * D)] * g.w(c, k2);
-            for (int c2 = 0; c2 < 4; ++c2)
-                for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-            q[a] = v;
-        } else if (w == 1) {
-            int s0, k;
-            predict_stencil(j, D, NY, s0, k);
-            double v = q[a];
-            v *= 2.0;
-            for (int c = 0; c < 4; ++c) v += q[g.at(i, s0 + c * D)] * g.w(c, k);
-            q[a] = v;
-        } else if (w == 0) {
-            int s0, k;
-            predict_stencil(i, D, NX, s0, k);
-            double v = q[a];
-            v *= 2.0;
-            for (int c = 0; c < 4; ++c) v += q[g.at(s0 + c * D, j)] * g.w(c, k);
-            q[a] = v;
-        } else {
-            int is, k1, js, k2;
-            predict_stencil(i, D, NX, is, k1);
-            predict_stencil(j, D, NY, js, k2);
-            double v = q[a];
-            v *= 4.0;
-            for (int c = 0; c < 4; ++c) v += q[g.at(is + c * D, j)] * g.w(c, k1);
-            for (int c = 0; c < 4; ++c) v += q[g.at(i, js + c * D)] * g.w(c, k2);
-            for (int c2 = 0; c2 < 4; ++c2)
-                for (int c1 = 0; c1 < 4; ++c1) v -= q[g.at(is + c1 * D, js + c2 * D)] * g.w(c1, k1) * g.w(c2, k2);
-            q[a] = v;
+        iwt_point(g, q, i, j, a, D, w);
+    }
+}
+
+// The finest level (point spacing 1) of the step's transforms as a row scan: word t of the grid rows
+// is tested for the two mask bits that can make one of its points need work before its row and
+// column are decoded (most words have neither), and the set lanes are classified by parity:
+// 2 = d3 (odd, odd), 0 = d1 (odd, even; not the top or bottom row), 1 = d2 (even, odd; not the left
+// or right column), 3 = c (even, even; not on the boundary), -1 = none -- the extents of band_of.
+__device__ __forceinline__ int fine_band(const Grid2& g, int i, int j)
+{
+    const bool io = i & 1, jo = j & 1;
+    if (io && jo) return 2;
+    if (io) return (j == 0 || j == g.ny - 1) ? -1 : 0;
+    if (jo) return (i == 0 || i == g.nx - 1) ? -1 : 1;
+    return (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1) ? -1 : 3;
+}
+// f(i, j, a, byte) for the grid points of the scanned words whose byte has bit b1 or b2.
+template <class F>
+__device__ __forceinline__ void fine_rows(const Grid2& g, const uint8_t* m, int b1, int b2, Span sp, F&& f)
+{
+    const unsigned wpr = (unsigned)g.pitch / 4u, row0 = (unsigned)kGhost * wpr;
+    const unsigned n = (unsigned)g.ny * wpr;
+    const unsigned* mp = reinterpret_cast<const unsigned*>(m);
+    for (unsigned t = sp.t0; t < n; t += sp.stride) {
+        const unsigned v = mp[row0 + t];
+        unsigned hit = ((v >> b1) | (v >> b2)) & kLaneBits;
+        if (!hit) continue;
+        const unsigned r = t / wpr, wi = t - r * wpr;
+        const int j = (int)r, i0 = 4 * (int)wi - kGhost;
+        hit &= lane_bits(lanes_in(i0, 0, g.nx - 1));
+        while (hit) {
+            const int L = (__ffs(hit) - 1) >> 3;
+            hit &= hit - 1;
+            f(i0 + L, j, 4u * (row0 + t) + (unsigned)L, (v >> (8 * L)) & 0xffu);
         }
     }
+}
+// Row-scan forms of the finest level (idle mode / sparse zeroing, see ph_fwt_a and ph_iwt).
+__device__ void ph_fwt_a_fine(const Grid2& g, double* __restrict__ q, double* __restrict__ tb,
+                              uint8_t* __restrict__ m, double tol, Span sp)
+{
+    fine_rows(g, m, 0, 0, sp, [&](int i, int j, size_t a, unsigned) {
+        const int w = fine_band(g, i, j);
+        if (w >= 0 && w != 3) fwt_a_point(g, q, tb, m, i, j, a, 2, w, tol, true);
+    });
+}
+__device__ void ph_fwt_b_fine(const Grid2& g, double* __restrict__ q, const double* __restrict__ tb,
+                              const uint8_t* __restrict__ m, Span sp)
+{
+    fine_rows(g, m, 0, kBitTemp, sp, [&](int i, int j, size_t a, unsigned byte) {
+        const int w = fine_band(g, i, j);
+        if (w == 3) {
+            if (byte & 1u) fwt_b_point(g, q, tb, m, i, j, a, 2, true);
+        } else if (w == 0 || w == 1) {
+            if ((byte >> kBitTemp) & 1u) q[a] = tb[a];
+        }
+    });
+}
+template <int PH>
+__device__ void ph_iwt_fine(const Grid2& g, double* __restrict__ q, const uint8_t* __restrict__ m, int bit, Span sp)
+{
+    fine_rows(g, m, bit, kBitTemp, sp, [&](int i, int j, size_t a, unsigned byte) {
+        const int w = fine_band(g, i, j);
+        if (PH == 0 ? w != 3 : PH == 1 ? (w != 0 && w != 1) : w != 2) return;
+        if ((byte >> bit) & 1u) iwt_point(g, q, i, j, a, 2, w);
+        else q[a] = 0;  // in mask_temp, not in the mask
+    });
 }
 
 // CheckReconstruction of one level (AWCM_MANAGER_2D.h:63-158) in one phase.  The reference runs
@@ -865,20 +954,24 @@ __global__ void k_fwt_a(Grid2 g, double* q, double* tb, uint8_t* m, int lev, int
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_fwt_a(g, q, tb, m, lev, st->tol, idle != 0, grid_span());
+    if (idle && lev == g.maxl - 1) ph_fwt_a_fine(g, q, tb, m, st->tol, grid_span());
+    else ph_fwt_a(g, q, tb, m, lev, st->tol, idle != 0, grid_span());
 }
 __global__ void k_fwt_b(Grid2 g, double* q, const double* tb, const uint8_t* m, int lev, int idle, const StepState* st)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_fwt_b(g, q, tb, m, lev, idle != 0, grid_span());
+    if (idle && lev == g.maxl - 1) ph_fwt_b_fine(g, q, tb, m, grid_span());
+    else ph_fwt_b(g, q, tb, m, lev, idle != 0, grid_span());
 }
 template <int PH>
 __global__ void k_iwt(Grid2 g, double* q, const uint8_t* m, int lev, int bit, int sparse, const StepState* st)
 {
     pdl_begin();
     AWCM_SKIP_IF_DONE(st);
-    ph_iwt<PH>(g, q, m, lev, bit, !sparse || !st || st->full_zero, grid_span());
+    const bool zero_all = !sparse || !st || st->full_zero;
+    if (!zero_all && lev == g.maxl - 1) ph_iwt_fine<PH>(g, q, m, bit, grid_span());
+    else ph_iwt<PH>(g, q, m, lev, bit, zero_all, grid_span());
 }
 __global__ void k_cr(Grid2 g, uint8_t* m, int lev, int bit, const StepState* st)
 {
