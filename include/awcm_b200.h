@@ -324,8 +324,9 @@ int awcm1d_batch_apply_bc(awcm1d_batch_t h, int k);
  * (awcm1d_batch_apply_bc and the stage fills of the step) applies SetBoundaryCondition(field):
  * zero-order extrapolation or the periodic image per ghost cell, other conditions untouched. */
 int awcm1d_batch_set_bc_field(awcm1d_batch_t h, int k, const int* bc);
-/* Launch shape of the step kernel: threads per CTA (a multiple of 32, 64..768; the default is 768)
- * and CTAs per SM (0 = occupancy limit).  More threads than the kernel's launch bound is AWCM_ERR_ARG. */
+/* Launch shape of the step kernel: threads per CTA (a multiple of 32, 64..768; the default is 512
+ * when no instance has more than 1100 points, else 768) and CTAs per SM (0 = occupancy limit).
+ * More threads than the kernel's launch bound is AWCM_ERR_ARG.  Results do not depend on it. */
 int awcm1d_batch_set_launch(awcm1d_batch_t h, int threads, int ctas_per_sm);
 int awcm1d_batch_stream(awcm1d_batch_t h, void** stream);
 

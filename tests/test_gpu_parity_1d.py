@@ -130,3 +130,15 @@ def test_batch_uneven_matches_single(awcm_lib):
         assert s[3] == 1 and int(s[4]) == n and s[0] == t and s[13] == upd, (k, s[:5], n, t)
         assert np.array_equal(b.get_q(k), o.get_q()), f"instance {k}"
         assert np.array_equal(b.get_masks(k), o.get_masks()), f"instance {k} masks"
+
+
+@pytest.mark.parametrize("threads,ctas", [(64, 0), (128, 2), (256, 0), (512, 0), (768, 0)])
+def test_launch_shapes_agree(threads, ctas, awcm_lib):
+    """Every launch shape the autotuner may pick gives the oracle's run, bit for bit (the step's
+    reductions are order-free and its worklists keep the point order)."""
+    ref, gpu = make(awcm_lib)
+    gpu.b.set_launch(threads, ctas)
+    n_r, t_r, u_r = ref.run(1e-4, 0.5, 0.05)
+    n_g, t_g, u_g = gpu.run(1e-4, 0.5, 0.05)
+    assert (n_g, t_g, u_g) == (n_r, t_r, u_r)
+    assert_same(gpu, ref, f"{threads}x{ctas}")
