@@ -1,6 +1,6 @@
 """Launch-shape autotuner of the batched 1D step kernel.
 
-The step kernel runs one instance per CTA, with up to 768 threads (85 registers a thread); the CTA
+The step kernel runs one instance per CTA, with up to 768 threads (80 registers a thread); the CTA
 size trades occupancy (CTAs resident per SM, i.e. instances in flight) against per-instance
 parallelism.  The tuner times a few RK3 steps of the actual batch for each candidate shape on a
 throw-away copy of the batch and keeps the fastest (active-point updates per second)."""

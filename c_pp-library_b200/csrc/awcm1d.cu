@@ -1050,7 +1050,7 @@ __device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
 // One RK3 step of every queued instance.  CTAs pull queue slots until the queue is exhausted.
 // smem_bytes: the launch's dynamic shared memory; an instance whose staged step does not fit in
 // it runs on its global buffers (its worklists in the pool too).
-// Up to 768 threads per CTA (85 registers a thread, some of the face computation spilled to L1):
+// Up to 768 threads per CTA (80 registers a thread, some of the face computation spilled to L1):
 // a CTA advances one instance through ~150 block-barrier phases per step, latency-bound, so more
 // warps per instance pay for the spills (Jmax-13 tail step 0.312 -> 0.255 ms against 384 threads
 // and 162 registers; the batched whole run 3.48e7 -> 4.20e7 updates/s).
