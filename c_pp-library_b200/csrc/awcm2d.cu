@@ -2819,8 +2819,21 @@ struct Solver2D {
         if (wt) enq_wt_input(q);
         enq_alpha(q, 3, 0, true);
         enq_faces_update(0, q, q2, nullptr, nullptr, true);
+        // RemoveResidue zeroes q off mask0.  After the second stage's update (the last reader of q
+        // off mask0: its combination reads q on mask1) nothing else touches those points: the third
+        // stage reads q1 and reads and writes q on mask0 only.  So it runs as a graph branch beside
+        // the third stage.
+        const bool rr_par = fork_ok() && side2;
         for (int stage = 1; stage <= 2; ++stage) {
             Field4 in = stage == 1 ? q2 : q1;
+            if (stage == 2 && rr_par) {
+                cudaEventRecord(ev_fork, stream);
+                cudaStreamWaitEvent(side2, ev_fork, 0);
+                cur = side2;
+                launch(k_remove_residue, pb(words()), 256, g, q, m, 0, 1, st);
+                after("k_remove_residue");
+                cur = nullptr;
+            }
             if (!wt) {
                 enq_bc_alpha(in, stage);
             } else {
@@ -2831,8 +2844,12 @@ struct Solver2D {
             }
             enq_faces_update(stage, in, q1);
         }
-        launch(k_remove_residue, pb(words()), 256, g, q, m, 0, 1, st);
-        after("k_remove_residue");
+        if (rr_par) {
+            join(side2, ev_join2);
+        } else {
+            launch(k_remove_residue, pb(words()), 256, g, q, m, 0, 1, st);
+            after("k_remove_residue");
+        }
         launch(k_finish, 1, 1, st);
         after("k_finish");
         launches += 2;
