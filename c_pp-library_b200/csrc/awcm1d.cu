@@ -186,6 +186,13 @@ struct Ctx {
         const uintptr_t a = reinterpret_cast<uintptr_t>(m + i + kGhost);
         atomicOr(reinterpret_cast<unsigned*>(a & ~(uintptr_t)3), 1u << (8 * (unsigned)(a & 3) + b));
     }
+    // The push of the bits `bits` (one byte's worth) of point i in one atomicOr.
+    __device__ void set_bits(int i, unsigned bits) const
+    {
+        if (i < -kGhost || i >= nx + kGhost) return;
+        const uintptr_t a = reinterpret_cast<uintptr_t>(m + i + kGhost);
+        atomicOr(reinterpret_cast<unsigned*>(a & ~(uintptr_t)3), bits << (8 * (unsigned)(a & 3)));
+    }
     // The same push on the n <= 8 consecutive points i0 .. i0+n-1: one atomicOr per 32-bit word.
     __device__ void set_run(int i0, int n, int b) const
     {
@@ -289,15 +296,38 @@ __device__ void cr1(const Ctx& c, int b)
 }
 
 // AWCM_MANAGER_1D::AddAdjacentZone (Wavelet/AWCM_MANAGER_1D.h:14-43): detail points whose `src`
-// bit is set mark their finer neighbours in `b`.  i = odd * 2^t is a detail of level maxl-1-t.
-__device__ void aaz1(const Ctx& c, int b, int src)
+// bit is set mark their finer neighbours in `b` (and in `b2` too when it is given, in the same
+// atomic).  i = odd * 2^t is a detail of level maxl-1-t.
+__device__ void aaz1(const Ctx& c, int b, int src, int b2 = -1)
 {
+    const unsigned bits = (1u << b) | (b2 >= 0 ? 1u << b2 : 0u);
     for (int i = 1 + threadIdx.x; i <= c.N1 - 1; i += blockDim.x) {
         const int t = __ffs(i) - 1;
         if (t >= c.maxl || !c.bit(i, src)) continue;
         const int off = t == 0 ? 1 : (1 << (t - 1));
-        c.set(i - off, b);
-        c.set(i + off, b);
+        c.set_bits(i - off, bits);
+        c.set_bits(i + off, bits);
+    }
+    __syncthreads();
+}
+
+// BadingBoundary (AWCM_1D.h:73-80: mask0 set on the three points at each end, i < 3 and
+// i > N1 - 3), then mask0 copied into the copy bit on the points [0, N1], one word at a time.
+__device__ void band_copy1(const Ctx& c)
+{
+    unsigned* mw = reinterpret_cast<unsigned*>(c.m);
+    for (int wi = (kGhost >> 2) + (int)threadIdx.x; wi <= ((c.N1 + kGhost) >> 2); wi += blockDim.x) {
+        unsigned pts = 0, band = 0;  // bit 0 of the bytes of points [0, N1] / of the banded ones
+#pragma unroll
+        for (int L = 0; L < 4; ++L) {
+            const int i = 4 * wi + L - kGhost;
+            if (i < 0 || i > c.N1) continue;
+            pts |= 1u << (8 * L);
+            if (!(3 <= i && i <= c.N1 - 3)) band |= 1u << (8 * L);
+        }
+        const unsigned v0 = mw[wi], v = v0 | band;
+        const unsigned nv = (v & ~(pts << kBitCopy)) | ((v & pts) << kBitCopy);
+        if (nv != v0) mw[wi] = nv;
     }
     __syncthreads();
 }
@@ -333,8 +363,9 @@ __device__ __forceinline__ bool mask_or_ghost1(const Ctx& c, int i, int b)
 // AWCM_MANAGER_1D::ComputeLevel (Wavelet/AWCM_MANAGER_1D.h:109-133), with the optional copy
 // mask_{k+1} = mask_k of the own point.  One 32-bit mask word (four points) per iteration: the copy
 // is one word operation and the level search runs for the mask's points only.  The search reads
-// bit b of other bytes, which no thread changes here (the copy writes bit copy_to).
-__device__ void cl1(const Ctx& c, int l, int b, int copy_to)
+// bit b of other bytes, which no thread changes here (the copy writes bit copy_to, and bit
+// copy_to2 too when it is given).
+__device__ void cl1(const Ctx& c, int l, int b, int copy_to, int copy_to2 = -1)
 {
     unsigned* mw = reinterpret_cast<unsigned*>(c.m);
     const int nw = (c.w + 3) >> 2;
@@ -363,7 +394,8 @@ __device__ void cl1(const Ctx& c, int l, int b, int copy_to)
             }
         }
         if (copy_to >= 0) {
-            const unsigned nv = (v & ~(lanes << copy_to)) | (((v >> b) & lanes) << copy_to);
+            unsigned nv = (v & ~(lanes << copy_to)) | (((v >> b) & lanes) << copy_to);
+            if (copy_to2 >= 0) nv = (nv & ~(lanes << copy_to2)) | (((v >> b) & lanes) << copy_to2);
             if (nv != v) mw[wi] = nv;
         }
     }
@@ -430,17 +462,15 @@ __device__ void prepare1(const Ctx& c)
 {
     copy_bit1(c, 0, kBitTemp, true);
     fwt1(c);
-    // BadingBoundary (AWCM_1D.h:73-80): three points at each end.
-    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
-        if (!(3 <= i && i <= c.N1 - 3)) c.set(i, 0);
-    __syncthreads();
-    copy_bit1(c, 0, kBitCopy, false);
+    band_copy1(c);
     aaz1(c, 0, kBitCopy);
     cr1(c, 0);
     for (int k = 1; k <= 3; ++k) {
-        cl1(c, k - 1, k - 1, k);      // level_{k-1} of mask_{k-1}; mask_k = mask_{k-1}
-        aaz1(c, k, k - 1);            // AddAdjacentZone(mask_k) reads its copy (== mask_{k-1})
-        copy_bit1(c, k, kBitCopy, false);
+        // level_{k-1} of mask_{k-1}; mask_k = mask_{k-1}, and the copy bit too
+        cl1(c, k - 1, k - 1, k, kBitCopy);
+        // AddAdjacentZone(mask_k) reads bit k-1 (== mask_k before it) and marks bit k and the copy
+        // bit, so the copy bit is mask_k after it: the input of AddPointForDifferentiation
+        aaz1(c, k, k - 1, kBitCopy);
         apd1(c, k, k - 1);            // AddPointForDifferentiation(mask_k, level_{k-1})
         cr1(c, k);
     }
@@ -804,16 +834,12 @@ __device__ void step_ctx(Inst1& I, const Ctx& c, uint32_t* list, double* dred, u
 __device__ void prepare1_scalar(const Ctx& c)
 {
     fwt1(c);
-    for (int i = threadIdx.x; i <= c.N1; i += blockDim.x)
-        if (!(3 <= i && i <= c.N1 - 3)) c.set(i, 0);
-    __syncthreads();
-    copy_bit1(c, 0, kBitCopy, false);
+    band_copy1(c);
     aaz1(c, 0, kBitCopy);
     cr1(c, 0);
     for (int k = 1; k <= 3; ++k) {
-        cl1(c, k - 1, k - 1, k);  // level_{k-1} of mask_{k-1}; mask_k = mask_{k-1}
-        copy_bit1(c, k, kBitCopy, false);
-        apd1(c, k, k - 1);        // AddPointForDifferentiation(mask_k, level_{k-1})
+        cl1(c, k - 1, k - 1, k, kBitCopy);  // level_{k-1} of mask_{k-1}; mask_k = the copy bit = mask_{k-1}
+        apd1(c, k, k - 1);                  // AddPointForDifferentiation(mask_k, level_{k-1})
         cr1(c, k);
     }
     cl1(c, 3, 3, -1);
