@@ -227,9 +227,11 @@ BATCHED = {
 
 
 def run_batched(rank: int, world: int):
-    """Batched form (one persistent launch, one CUDA graph per RK3 step, autotuned launch shape)
-    against the plain form (one instance per launch) on the same seeded tubes.  Instances are
-    sharded over ranks; timing is max over ranks."""
+    """Batched form against the plain form (one instance per launch) on the same seeded tubes.  The
+    batched whole run is one persistent launch (each CTA runs tubes to their end, largest first);
+    its step-synchronous form (one CUDA graph replay per RK3 step of the batch) gives the steady
+    rate and a second whole-run figure.  Autotuned launch shape.  Instances are sharded over ranks;
+    timing is max over ranks."""
     import torch
 
     import awcm
@@ -242,32 +244,51 @@ def run_batched(rank: int, world: int):
     tubes = [tubes_all[k] for k in mine]
     tol, cfl, t_end = b_cfg["tol"], b_cfg["cfl"], b_cfg["t_end"]
     best, rates = autotune.tune(lambda: workloads.make_batch(awcm, tubes), t_end, tol, cfl)
-    b = workloads.make_batch(awcm, tubes)
-    b.set_launch(*best)
-    b.set_run(tol, cfl, 0.0, t_end)
-    b.steps(3)
-    b.sync()
-    u0 = b.totals()[0]
-    st = torch.cuda.ExternalStream(b.stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches = 3
+
+    def fresh():
+        bb = workloads.make_batch(awcm, tubes)
+        bb.set_launch(*best)
+        bb.set_run(tol, cfl, 0.0, t_end)
+        bb.steps(3)
+        bb.sync()
+        return bb, bb.totals()[0], torch.cuda.ExternalStream(bb.stream)
+
+    # Whole run: after 3 warm-up steps, one launch runs every tube to t_end (each CTA takes tubes
+    # largest first and runs each one's steps back to back).
+    b, u0, st = fresh()
+    torch.cuda.synchronize()
+    e0.record(st)
+    b.run_all()
+    e1.record(st)
+    torch.cuda.synchronize()
+    tot = b.totals()
+    ms, upd = reduce_run(e0.elapsed_time(e1), tot[0] - u0, device="cuda")
+    value = upd / (ms / 1e3)
+    all_done = int(tot[2]) == b.n
+    b.close()
+    launches = 3 + 1
+    # The same run as one graph replay per step of the whole batch (every tube one step a launch):
+    # its first 250 steps are the steady rate, its whole run the step-synchronous figure.
+    b, u0, st = fresh()
     torch.cuda.synchronize()
     e0.record(st)
     steady = None
+    sw_launches = 3
     while True:
         b.steps(250)
-        launches += 250
+        sw_launches += 250
         tot = b.totals()
         if steady is None:
             e1.record(st)
             torch.cuda.synchronize()
             steady = ((tot[0] - u0) / (e0.elapsed_time(e1) / 1e3))
-        if tot[2] == b.n or launches > 200000:
+        if tot[2] == b.n or sw_launches > 200000:
             break
     e1.record(st)
     torch.cuda.synchronize()
-    ms, upd = reduce_run(e0.elapsed_time(e1), tot[0] - u0, device="cuda")
-    value = upd / (ms / 1e3)
+    sw_ms, sw_upd = reduce_run(e0.elapsed_time(e1), tot[0] - u0, device="cuda")
+    b.close()
     # Plain form: one instance per launch.  (a) concurrent: each instance of a sample across the
     # size mix is its own batch of one (its own stream and graph), and every step launches each
     # unfinished instance separately, round robin over the streams, so the GPU runs as many
@@ -330,6 +351,9 @@ def run_batched(rank: int, world: int):
     return {
         "workload": b_cfg["workload"], "metric": METRIC, "value": value, "unit": UNIT,
         "steady_value": steady, "launches": launches, "instances": len(tubes_all), "ms": ms,
+        "all_done": all_done,
+        "stepwise": {"value": sw_upd / (sw_ms / 1e3), "ms": sw_ms, "launches": sw_launches,
+                     "note": "the whole run as one launch per RK3 step of the batch (CUDA graph replays)"},
         "launch_shape": {"threads": best[0], "ctas_per_sm": best[1]},
         "autotune": {f"{k[0]}x{k[1]}": v for k, v in rates.items()},
         "plain": {"value": plain_conc, "unit": UNIT,

@@ -74,6 +74,7 @@ _SIGS = {
     "awcm1d_batch_init_riemann": [c_void_p, c_int, c_double, P_double, P_double],
     "awcm1d_batch_set_run": [c_void_p, P_double, P_double, P_double, P_double, c_double],
     "awcm1d_batch_steps": [c_void_p, c_int],
+    "awcm1d_batch_run": [c_void_p, c_int],
     "awcm1d_batch_sync": [c_void_p],
     "awcm1d_batch_status": [c_void_p, c_int, P_double],
     "awcm1d_batch_totals": [c_void_p, P_double],

@@ -396,6 +396,11 @@ class AWCM1DBatch:
     def steps(self, n_steps: int):
         call("awcm1d_batch_steps", self.h, n_steps)
 
+    def run_all(self, max_steps: int = (1 << 31) - 1):
+        """Every unfinished instance to its end time (at most max_steps steps each) in one launch,
+        each instance's steps back to back on one CTA (asynchronous, like steps)."""
+        call("awcm1d_batch_run", self.h, max_steps)
+
     def sync(self):
         call("awcm1d_batch_sync", self.h)
 

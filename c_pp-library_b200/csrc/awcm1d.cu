@@ -1013,8 +1013,11 @@ __device__ __forceinline__ void block_copy_doubles(double* __restrict__ dst, con
 // coarse derivatives, face fluxes; mg: w mask bytes, lg: four planes of w levels (global); glist:
 // worklist space in the pool (layouts that keep the worklists global).  One call site for every
 // layout keeps the step kernel's code to one copy of each scheme.
+// Up to nsteps RK3 steps of instance I (the caller has checked that it is not done), staged into
+// shared memory once around them; the steps stop when the instance is done.
 __device__ void step_inst(Inst1& I, double* q, double* qc, double* qt, double* fl, uint8_t* mg, int8_t* lg,
-                          const Weights& W, uint8_t* smem, int layout, uint32_t* glist, double* dred, unsigned* ured)
+                          const Weights& W, uint8_t* smem, int layout, uint32_t* glist, double* dred, unsigned* ured,
+                          int nsteps = 1)
 {
     const int w = I.nx + 2 * kGhost;
     // the scalar path reads and writes its field planes directly; only its masks are staged
@@ -1051,9 +1054,13 @@ __device__ void step_inst(Inst1& I, double* q, double* qc, double* qt, double* f
         __syncthreads();
     }
     const Ctx c{I, qp, qc, qt, fl, ms, ls, W, w, I.nx, I.nx - 1, I.maxl, q0};
-    if (scalar) step_ctx_scalar(I, c, list, ured);
-    else if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
-    else step_ctx<kWenoZ>(I, c, list, dred, ured);
+    for (int s = 0; s < nsteps; ++s) {
+        // the step's end (thread 0, then a block barrier) sets done at t_end or on an error
+        if (s > 0 && *reinterpret_cast<volatile int*>(&I.done)) break;
+        if (scalar) step_ctx_scalar(I, c, list, ured);
+        else if (I.scheme == kWeno5) step_ctx<kWeno5>(I, c, list, dred, ured);
+        else step_ctx<kWenoZ>(I, c, list, dred, ured);
+    }
     if (layout != kStageNone) {
         block_copy_bytes(mg, ms, w);
         if (st_lv) block_copy_bytes(reinterpret_cast<uint8_t*>(lg), reinterpret_cast<const uint8_t*>(ls), 4 * w);
@@ -1073,7 +1080,10 @@ __device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
                w, I.nx, I.nx - 1, I.maxl, base};
 }
 
-// One RK3 step of every queued instance.  CTAs pull queue slots until the queue is exhausted.
+// nsteps RK3 steps of every queued instance (fewer for an instance that reaches t_end).  CTAs pull
+// queue slots until the queue is exhausted, and run each instance's steps back to back before
+// taking the next: nsteps = 1 is one step of the whole batch (the per-step graph); a large
+// nsteps runs every instance to its end in one launch, each CTA independently of the others.
 // smem_bytes: the launch's dynamic shared memory; an instance whose staged step does not fit in
 // it runs on its global buffers (its worklists in the pool too).
 // Up to 768 threads per CTA (80 registers a thread, some of the face computation spilled to L1):
@@ -1081,7 +1091,7 @@ __device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
 // warps per instance pay for the spills (Jmax-13 tail step 0.312 -> 0.255 ms against 384 threads
 // and 162 registers; the batched whole run 3.48e7 -> 4.20e7 updates/s).
 __global__ void __launch_bounds__(768, 1) k_step1d(Inst1* insts, int n, const int* __restrict__ order, unsigned* queue, Pool P,
-                         unsigned smem_bytes)
+                         unsigned smem_bytes, int nsteps)
 {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ double dred[32];
@@ -1102,7 +1112,7 @@ __global__ void __launch_bounds__(768, 1) k_step1d(Inst1* insts, int n, const in
             uint8_t* mb = P.m + I.m_off;
             step_inst(I, base, base + 3 * w, base + 6 * w, base + 9 * w, mb, (int8_t*)(mb + align16((size_t)w)), P.W,
                       smem, pick_layout(w, smem_bytes, I.scheme == kScalarAdvection, true),
-                      reinterpret_cast<uint32_t*>(base + 12 * (size_t)w), dred, ured);
+                      reinterpret_cast<uint32_t*>(base + 12 * (size_t)w), dred, ured, nsteps);
         }
         __syncthreads();
     }
@@ -1309,10 +1319,10 @@ struct Batch1D {
         return kOk;
     }
 
-    void enq_step()
+    void enq_step(int nsteps = 1)
     {
         cudaMemsetAsync(d_queue, 0, sizeof(unsigned), stream);
-        k_step1d<<<grid, block, smem_bytes(), stream>>>(d_inst, n, d_order, d_queue, P, (unsigned)smem_bytes());
+        k_step1d<<<grid, block, smem_bytes(), stream>>>(d_inst, n, d_order, d_queue, P, (unsigned)smem_bytes(), nsteps);
     }
 
     int build_graph()
@@ -1357,6 +1367,14 @@ struct Batch1D {
         int rc = build_graph();
         if (rc) return rc;
         for (int s = 0; s < n_steps; ++s) AWCM_CUDA_TRY(cudaGraphLaunch(graph, stream));
+        AWCM_CUDA_TRY(cudaGetLastError());
+        return kOk;
+    }
+
+    // Every unfinished instance to its end time, at most max_steps steps each, in one launch.
+    int run(int max_steps)
+    {
+        enq_step(max_steps);
         AWCM_CUDA_TRY(cudaGetLastError());
         return kOk;
     }
@@ -1667,6 +1685,12 @@ int awcm1d_batch_steps(awcm1d_batch_t h, int n_steps)
     if (!h || n_steps < 0) return awcm::kErrArg;
     cudaSetDevice(h->b.device);
     return h->b.steps(n_steps);
+}
+int awcm1d_batch_run(awcm1d_batch_t h, int max_steps)
+{
+    if (!h || max_steps < 1) return awcm::kErrArg;
+    cudaSetDevice(h->b.device);
+    return h->b.run(max_steps);
 }
 int awcm1d_batch_sync(awcm1d_batch_t h)
 {

@@ -430,6 +430,8 @@ public:
         check(awcm1d_batch_set_run(h_, tol.data(), cfl.data(), t.data(), t_end.data(), dt_fixed), "set_run");
     }
     void Steps(int n) { check(awcm1d_batch_steps(h_, n), "awcm1d_batch_steps"); }
+    // Every instance to its end time in one launch (at most max_steps steps each).
+    void RunToEnd(int max_steps = 0x7fffffff) { check(awcm1d_batch_run(h_, max_steps), "awcm1d_batch_run"); }
     void Sync() { check(awcm1d_batch_sync(h_), "awcm1d_batch_sync"); }
     std::vector<double> Status(int k) const
     {

@@ -142,3 +142,45 @@ def test_launch_shapes_agree(threads, ctas, awcm_lib):
     n_g, t_g, u_g = gpu.run(1e-4, 0.5, 0.05)
     assert (n_g, t_g, u_g) == (n_r, t_r, u_r)
     assert_same(gpu, ref, f"{threads}x{ctas}")
+
+
+def _uneven_batch(awcm_lib, seed=7):
+    rng = np.random.default_rng(seed)
+    tubes = []
+    for L in [5, 7, 6, 8, 5, 9]:
+        nx = 16 * 2 ** (L - 1) + 1
+        dxf = 1.0 / nx
+        tubes.append((L, 0.5 * dxf, 1 - 0.5 * dxf, rng.uniform(0.3, 0.7),
+                       (10 ** rng.uniform(-1, 1), rng.uniform(-1, 1), 10 ** rng.uniform(-1, 1)),
+                       (10 ** rng.uniform(-1, 1), rng.uniform(-1, 1), 10 ** rng.uniform(-1, 1))))
+    b = awcm_lib.AWCM1DBatch([t[0] for t in tubes], 17, [t[1] for t in tubes], [t[2] for t in tubes])
+    refs = []
+    for k, (L, x0, x1, xi, l, r) in enumerate(tubes):
+        b.init_riemann(k, xi, l, r)
+        o = Oracle1D(L, 17, x0, x1, kind="port")
+        o.init_riemann(xi, l, r)
+        refs.append(o)
+    return b, refs
+
+
+@pytest.mark.parametrize("max_steps", [None, 7])
+def test_batch_run_to_end(max_steps, awcm_lib):
+    """awcm1d_batch_run: every instance run to t_end (or max_steps steps) in one launch, each on its
+    CTA back to back, equals the oracle run instance by instance."""
+    b, refs = _uneven_batch(awcm_lib)
+    t_end = 0.01
+    b.set_run(1e-4, 0.5, 0.0, t_end)
+    if max_steps is None:
+        b.run_all()
+    else:
+        b.run_all(max_steps)
+    b.sync()
+    for k, o in enumerate(refs):
+        n, t, upd = o.run(1e-4, 0.5, t_end, (1 << 30) if max_steps is None else max_steps)
+        s = b.status(k)
+        assert int(s[4]) == n and s[0] == t and s[13] == upd, (k, s[:5], n, t)
+        if max_steps is None:
+            assert s[3] == 1, (k, s[:5])
+        assert np.array_equal(b.get_q(k), o.get_q()), f"instance {k}"
+        assert np.array_equal(b.get_masks(k), o.get_masks()), f"instance {k} masks"
+        assert np.array_equal(b.get_levels(k), o.get_levels()), f"instance {k} levels"
