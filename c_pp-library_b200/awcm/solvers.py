@@ -547,15 +547,10 @@ class AWCM1D:
         out[9] = s[9]
         return out
 
-    def run(self, tol, cfl, t_end, max_steps=1 << 30, chunk=256):
+    def run(self, tol, cfl, t_end, max_steps=1 << 30):
+        """The driver loop from t = 0 to t_end (at most max_steps steps) as one launch, the instance
+        staged into shared memory once; returns (steps, t, sum over the steps of |mask0|)."""
         self.b.set_run(tol, cfl, 0.0, t_end)
-        steps = 0
-        while steps < max_steps:
-            n = min(chunk, max_steps - steps)
-            self.b.steps(n)
-            s = self.b.status(0)
-            steps = int(s[4])
-            if s[3]:
-                break
+        self.b.run_all(min(max_steps, (1 << 31) - 1))
         s = self.b.status(0)
         return int(s[4]), s[0], s[13]
