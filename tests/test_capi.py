@@ -49,3 +49,15 @@ def test_fails_loudly_without_device(awcm_lib):
         pytest.skip("a GPU is present")
     with pytest.raises(awcm_lib.AwcmError):
         awcm_lib.AWCM2D(4, 9, 9, 0.0, 1.0, 0.0, 1.0)
+
+
+@pytest.mark.parametrize("name,args", [
+    ("awcm1d_batch_run", (None, 1)),
+    ("awcm1d_batch_steps", (None, 1)),
+    ("awcm1d_batch_sync", (None,)),
+    ("awcm1d_batch_set_launch", (None, 256, 0)),
+])
+def test_null_handle_is_an_argument_error(name, args, awcm_lib):
+    """The batch entry points reject a null handle with AWCM_ERR_ARG before touching the device."""
+    lib = awcm_lib.load()
+    assert getattr(lib, name)(*args) == 1
