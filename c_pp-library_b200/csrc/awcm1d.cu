@@ -1089,7 +1089,7 @@ __device__ __forceinline__ Ctx make_ctx(Inst1& I, const Pool& P)
 // Up to 768 threads per CTA (80 registers a thread, some of the face computation spilled to L1):
 // a CTA advances one instance through ~150 block-barrier phases per step, latency-bound, so more
 // warps per instance pay for the spills (Jmax-13 tail step 0.312 -> 0.255 ms against 384 threads
-// and 162 registers; the batched whole run 3.48e7 -> 4.20e7 updates/s).
+// and 162 registers; the step-synchronous batched whole run 3.48e7 -> 4.20e7 updates/s).
 __global__ void __launch_bounds__(768, 1) k_step1d(Inst1* insts, int n, const int* __restrict__ order, unsigned* queue, Pool P,
                          unsigned smem_bytes, int nsteps)
 {
