@@ -294,7 +294,8 @@ int awcm1d_batch_steps(awcm1d_batch_t h, int n_steps);
 /* Enqueues the run of every unfinished instance to its end time (set_run), at most max_steps >= 1
  * steps each, as one launch: each CTA takes instances from the largest-first queue and runs each
  * one's steps back to back before the next, so the instances do not wait for one another at every
- * step.  No counterpart in the reference (its driver loop is one instance). */
+ * step.  The launch lasts as long as the longest instance's run: max_steps bounds it.  No
+ * counterpart in the reference (its driver loop is one instance). */
 int awcm1d_batch_run(awcm1d_batch_t h, int max_steps);
 int awcm1d_batch_sync(awcm1d_batch_t h);
 /* out[16]: t, dt, do_print, done, steps, |mask0..mask3|, max speed, alpha of stages 1..3,
